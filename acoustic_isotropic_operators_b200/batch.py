@@ -1,0 +1,164 @@
+"""Batched operator context over the C ABI (numpy in, numpy out).
+
+``Context`` wraps one ``aio_context``: one grid / velocity / device. Each call
+runs a whole list of shots; the engine groups them into waves that fit the
+device-memory budget and advances every shot of a wave with one fused stepper
+launch per fine time step.
+
+Shots are ``Shot`` objects holding regular-grid device positions (linear
+indices ``ix*nz+iz``), fine-time source traces and coarse-time data, exactly
+the arrays the reference's per-shot operators hand to their GPU functions.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _capi as A
+
+
+@dataclass
+class Shot:
+    src_pos: np.ndarray                 # int32 [nSrcReg]
+    rec_pos: np.ndarray                 # int32 [nRecReg]
+    src_sig: Optional[np.ndarray] = None  # float32 [nSrcReg, ntw]
+    data: Optional[np.ndarray] = None     # float32 [nRecReg, nts]
+    wemva_data: Optional[np.ndarray] = None  # float32 [nRecReg, nts]
+    src_out: Optional[np.ndarray] = None  # float32 [nSrcReg, ntw] (nonlinear adjoint output)
+    _keep: list = field(default_factory=list, repr=False)
+
+    def __post_init__(self):
+        self.src_pos = np.ascontiguousarray(self.src_pos, dtype=np.int32)
+        self.rec_pos = np.ascontiguousarray(self.rec_pos, dtype=np.int32)
+        for name in ("src_sig", "data", "wemva_data", "src_out"):
+            v = getattr(self, name)
+            if v is not None:
+                setattr(self, name, np.ascontiguousarray(v, dtype=np.float32))
+
+
+_WFLD = {"fp32": A.AIO_WFLD_FP32, "bf16": A.AIO_WFLD_BF16, "fp16": A.AIO_WFLD_FP16}
+
+
+class Context:
+    """One operator instance on one GPU (grid, time axis, velocity fields)."""
+
+    def __init__(self, nz, nx, nts, dts, sub, dz, dx, minPad, vel2Dtw2, reflectivity_scale=None, *, nExt=1,
+                 alphaCos=0.99, leg1=1, leg2=1, sloth=0, wavefield="fp32", image_fp64=False, device=0,
+                 mem_budget_bytes=0):
+        self.nz, self.nx, self.nts, self.sub, self.nExt = nz, nx, nts, sub, nExt
+        self.ntw = (nts - 1) * sub + 1
+        p = A.AioParams(nz, nx, nts, sub, minPad, nExt, dz, dx, dts, alphaCos, leg1, leg2, sloth,
+                        _WFLD[wavefield], int(bool(image_fp64)), device, int(mem_budget_bytes))
+        v2 = np.ascontiguousarray(vel2Dtw2, dtype=np.float32).reshape(-1)
+        rs = None if reflectivity_scale is None else np.ascontiguousarray(reflectivity_scale,
+                                                                          dtype=np.float32).reshape(-1)
+        assert v2.size == nz * nx
+        h = C.c_void_p()
+        A.check(A.lib().aio_context_create(C.byref(p), A.fptr(v2), A.fptr(rs), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            A.lib().aio_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def last_launches(self) -> int:
+        return int(A.lib().aio_context_last_launches(self._h))
+
+    def capacity(self, family: int) -> int:
+        return int(A.lib().aio_context_wave_capacity(self._h, family))
+
+    # ------------------------------------------------------------------ helpers
+    def _shots(self, shots: Sequence[Shot], *, data_out: bool, need_sig=True, src_out=False):
+        arr = (A.AioShot * len(shots))()
+        for i, s in enumerate(shots):
+            if data_out and (s.data is None or s.data.shape != (len(s.rec_pos), self.nts)):
+                s.data = np.zeros((len(s.rec_pos), self.nts), np.float32)
+            if src_out and (s.src_out is None or s.src_out.shape != (len(s.src_pos), self.ntw)):
+                s.src_out = np.zeros((len(s.src_pos), self.ntw), np.float32)
+            if need_sig:
+                assert s.src_sig is not None and s.src_sig.shape == (len(s.src_pos), self.ntw)
+            arr[i] = A.AioShot(A.iptr(s.src_pos), len(s.src_pos), A.iptr(s.rec_pos), len(s.rec_pos),
+                               A.fptr(s.src_sig), A.fptr(s.data), A.fptr(s.wemva_data), A.fptr(s.src_out))
+        return arr
+
+    def _model(self, m, slices):
+        m = np.ascontiguousarray(m, dtype=np.float32)
+        assert m.size == slices * self.nz * self.nx
+        return m
+
+    # ---------------------------------------------------------------- operators
+    def nonlinear_forward(self, shots: List[Shot]) -> List[np.ndarray]:
+        arr = self._shots(shots, data_out=True)
+        A.check(A.lib().aio_nonlinear_forward(self._h, len(shots), arr, A.AIO_MEM_HOST))
+        return [s.data for s in shots]
+
+    def nonlinear_adjoint(self, shots: List[Shot]) -> List[np.ndarray]:
+        arr = self._shots(shots, data_out=False, need_sig=False, src_out=True)
+        A.check(A.lib().aio_nonlinear_adjoint(self._h, len(shots), arr, A.AIO_MEM_HOST))
+        return [s.src_out for s in shots]
+
+    def born_forward(self, model, shots: List[Shot]) -> List[np.ndarray]:
+        m = self._model(model, 1)
+        arr = self._shots(shots, data_out=True)
+        A.check(A.lib().aio_born_forward(self._h, A.fptr(m), len(shots), arr, A.AIO_MEM_HOST))
+        return [s.data for s in shots]
+
+    def born_adjoint(self, shots: List[Shot], model=None, add=False) -> np.ndarray:
+        out = np.zeros((self.nx, self.nz), np.float32) if model is None else model
+        arr = self._shots(shots, data_out=False)
+        A.check(A.lib().aio_born_adjoint(self._h, A.fptr(out), int(add), len(shots), arr, A.AIO_MEM_HOST))
+        return out
+
+    def born_ext_forward(self, model, shots: List[Shot]) -> List[np.ndarray]:
+        m = self._model(model, self.nExt)
+        arr = self._shots(shots, data_out=True)
+        A.check(A.lib().aio_born_ext_forward(self._h, A.fptr(m), len(shots), arr, A.AIO_MEM_HOST))
+        return [s.data for s in shots]
+
+    def born_ext_adjoint(self, shots: List[Shot], model=None, add=False) -> np.ndarray:
+        out = np.zeros((self.nExt, self.nx, self.nz), np.float32) if model is None else model
+        arr = self._shots(shots, data_out=False)
+        A.check(A.lib().aio_born_ext_adjoint(self._h, A.fptr(out), int(add), len(shots), arr, A.AIO_MEM_HOST))
+        return out
+
+    def tomo_forward(self, model, ext_reflectivity, shots: List[Shot]) -> List[np.ndarray]:
+        m = self._model(model, 1)
+        e = self._model(ext_reflectivity, self.nExt)
+        arr = self._shots(shots, data_out=True)
+        A.check(A.lib().aio_tomo_ext_forward(self._h, A.fptr(m), A.fptr(e), len(shots), arr, A.AIO_MEM_HOST))
+        return [s.data for s in shots]
+
+    def tomo_adjoint(self, ext_reflectivity, shots: List[Shot], model=None, add=False) -> np.ndarray:
+        out = np.zeros((self.nx, self.nz), np.float32) if model is None else model
+        e = self._model(ext_reflectivity, self.nExt)
+        arr = self._shots(shots, data_out=False)
+        A.check(A.lib().aio_tomo_ext_adjoint(self._h, A.fptr(out), int(add), A.fptr(e), len(shots), arr,
+                                             A.AIO_MEM_HOST))
+        return out
+
+    def wemva_forward(self, model, shots: List[Shot], image=None, add=False) -> np.ndarray:
+        m = self._model(model, 1)
+        out = np.zeros((self.nExt, self.nx, self.nz), np.float32) if image is None else image
+        arr = self._shots(shots, data_out=False)
+        A.check(A.lib().aio_wemva_ext_forward(self._h, A.fptr(m), A.fptr(out), int(add), len(shots), arr,
+                                              A.AIO_MEM_HOST))
+        return out
+
+    def wemva_adjoint(self, image, shots: List[Shot], model=None, add=False) -> np.ndarray:
+        im = self._model(image, self.nExt)
+        out = np.zeros((self.nx, self.nz), np.float32) if model is None else model
+        arr = self._shots(shots, data_out=False)
+        A.check(A.lib().aio_wemva_ext_adjoint(self._h, A.fptr(out), int(add), A.fptr(im), len(shots), arr,
+                                              A.AIO_MEM_HOST))
+        return out

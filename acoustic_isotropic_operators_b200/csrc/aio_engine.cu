@@ -1,0 +1,1384 @@
+// B200 engine for the 2-D acoustic isotropic operators: operator contexts,
+// batched pass drivers and the C ABI declared in include/aio_b200.h.
+//
+// A context owns the velocity-derived fields of one operator instance and
+// reusable per-wave buffers. An operator call splits its shots into waves that
+// fit the device-memory budget; inside a wave every shot advances together,
+// one fused stepper launch per fine step (gridDim.z = shot), one element-wise
+// launch per coarse step for imaging. The pass sequences follow the reference
+// drivers (F/src/*ShotsGpuFunctions.cu), cited at each pass.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "aio_b200.h"
+#include "aio_kernels.cuh"
+
+namespace aio {
+
+static thread_local std::string g_err;
+
+struct Error {
+    int code;
+    std::string msg;
+};
+
+#define AIO_CK(x)                                                                                   \
+    do {                                                                                            \
+        cudaError_t e_ = (x);                                                                       \
+        if (e_ != cudaSuccess)                                                                      \
+            throw Error{AIO_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_) + " (line " + \
+                                          std::to_string(__LINE__) + ")"};                          \
+    } while (0)
+
+static void require(bool ok, const std::string& msg) {
+    if (!ok) throw Error{AIO_ERR_ARGUMENT, msg};
+}
+
+template <class F>
+static int guard(F&& f) {
+    try {
+        f();
+        return AIO_OK;
+    } catch (const Error& e) {
+        g_err = e.msg;
+        return e.code;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return AIO_ERR_ARGUMENT;
+    }
+}
+
+struct DevMem {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void ensure(size_t b) {
+        if (b <= bytes) return;
+        release();
+        if (b == 0) return;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            bytes = 0;
+            throw Error{AIO_ERR_MEMORY, "cudaMalloc of " + std::to_string(b) + " bytes failed"};
+        }
+        bytes = b;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    ~DevMem() { release(); }
+    template <class T>
+    T* as() const { return (T*)p; }
+};
+
+// Host copies of the scheme constants, computed with the reference's own
+// expressions and FP32 rounding (F/src/nonlinearShotsGpuFunctions.cu:123-170,
+// F/src/tomoExtShotsGpuFunctions.cu:138-139).
+struct HostConsts {
+    Coefs c;
+    float h[2 * (SUB_MAX + 1)];
+    float taper[PAD_MAX];
+    float cSide, cCenter;
+};
+
+static HostConsts make_consts(const aio_params& P) {
+    HostConsts k;
+    static const double C[6] = {-2.927222222, 1.666666667, -0.238095238, 0.039682539, -0.004960317, 0.000317460};
+    for (int i = 0; i < 6; i++) {
+        k.c.zc[i] = (float)(C[i] / (double)(P.dz * P.dz));
+        k.c.xc[i] = (float)(C[i] / (double)(P.dx * P.dx));
+    }
+    const int ntw = (P.nts - 1) * P.sub + 1, H = P.sub + 1;
+    std::fill(k.h, k.h + 2 * (SUB_MAX + 1), 0.f);
+    const float r = std::sqrt((float)ntw / (float)P.nts);
+    const double sc = 1.0 / (double)r;
+    for (int i = 0; i < H; i++) {
+        k.h[i] = (float)(1.0 - 1.0 * i / P.sub);
+        k.h[i + H] = (float)(1.0 - (double)k.h[i]);
+        k.h[i] = (float)((double)k.h[i] * sc);
+        k.h[i + H] = (float)((double)k.h[i + H] * sc);
+    }
+    std::fill(k.taper, k.taper + PAD_MAX, 1.f);
+    for (int i = 0; i < P.minPad; i++) {
+        const float a = (float)(M_PI / (1.0 * P.minPad) * 1.0 * (P.minPad - i));
+        const float cs = std::cos(a);
+        k.taper[i] = (float)((double)P.alphaCos + (1.0 - (double)P.alphaCos) * (double)cs);
+    }
+    k.cSide = (float)(1.0 / (double)(P.dts * P.dts));
+    k.cCenter = (float)(-2.0 / (double)(P.dts * P.dts));
+    return k;
+}
+
+// Sparse device lists of one wave: per shot a CSR over stepper tiles.
+struct WaveLists {
+    std::vector<int> words;             // concatenated [start (nT+1, padded even)] [entries int2]
+    std::vector<long long> srcOff, recOff;  // word offsets of each shot's src / rec list (-1: empty)
+};
+
+static void append_list(const Geom& g, const int* pos, int n, std::vector<int>& words, long long& off,
+                        const char* what) {
+    if (n <= 0 || !pos) {
+        off = -1;
+        return;
+    }
+    const int nT = g.tilesZ * g.tilesX;
+    std::vector<int> tileOf(n), local(n), cnt(nT + 1, 0);
+    for (int k = 0; k < n; k++) {
+        const long long p = pos[k];
+        const int iz = (int)(p % g.nz), ix = (int)(p / g.nz);
+        require(p >= 0 && ix < g.nx && iz >= FAT && iz < g.nz - FAT && ix >= FAT && ix < g.nx - FAT,
+                std::string(what) + " position " + std::to_string(p) + " is outside the interior grid");
+        const int z = iz - FAT, x = ix - FAT;
+        tileOf[k] = (x / TX) * g.tilesZ + z / TZ;
+        local[k] = (x % TX) * TZ + (z % TZ);
+        cnt[tileOf[k] + 1]++;
+    }
+    for (int t = 0; t < nT; t++) cnt[t + 1] += cnt[t];
+    const int startWords = (nT + 1 + 1) & ~1;  // keep the entries 8-byte aligned
+    off = (long long)words.size();
+    words.resize(words.size() + startWords + 2 * (size_t)n, 0);
+    int* start = words.data() + off;
+    for (int t = 0; t <= nT; t++) start[t] = cnt[t];
+    std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+    int* ent = start + startWords;
+    for (int k = 0; k < n; k++) {
+        const int slot = fill[tileOf[k]]++;
+        ent[2 * slot] = local[k];
+        ent[2 * slot + 1] = k;
+    }
+}
+
+enum AccMode { ACC_NONE = 0, ACC_FULL = 1, ACC_RING = 2 };
+
+struct Context {
+    aio_params P;
+    Geom g;
+    HostConsts k;
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    DevMem v2, rs, taper;
+    // per-wave buffers
+    DevMem pbuf, ringb, ssb, wf1, wf2, img, lists, desc, sig, dat, aux, model, ext, outv;
+    std::vector<ShotDesc> hdesc;
+    long long launches = 0;
+    long long budget = 0;
+
+    // ------------------------------------------------------------- set-up
+    void init(const aio_params& p, const float* vel2Dtw2, const float* reflScale) {
+        P = p;
+        require(p.nz > 2 * FAT && p.nx > 2 * FAT, "nz and nx must exceed 2*FAT");
+        require(p.nts >= 2, "nts must be >= 2");
+        require(p.sub >= 1 && p.sub < SUB_MAX, "sub must be in [1, 100)");
+        require(p.minPad >= 0 && p.minPad < PAD_MAX, "minPad must be in [0, 200)");
+        require(p.nExt >= 1 && (p.nExt % 2) == 1, "nExt must be a positive odd number");
+        require(p.wavefieldPrecision == AIO_WFLD_FP32, "only FP32 stored wavefields are available in this build");
+        g = make_geom(p.nz, p.nx, p.nts, p.sub, p.minPad, p.nExt);
+        k = make_consts(p);
+        dev = p.device;
+        AIO_CK(cudaSetDevice(dev));
+        AIO_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        v2.ensure(g.isz * 4);
+        rs.ensure(g.isz * 4);
+        taper.ensure(PAD_MAX * 4);
+        AIO_CK(cudaMemcpyAsync(taper.p, k.taper, PAD_MAX * 4, cudaMemcpyHostToDevice, st));
+        set_velocity(vel2Dtw2, reflScale);
+        size_t fr = 0, tot = 0;
+        AIO_CK(cudaMemGetInfo(&fr, &tot));
+        budget = p.memBudgetBytes > 0 ? p.memBudgetBytes : (long long)(0.9 * (double)fr);
+    }
+
+    void set_velocity(const float* vel2Dtw2, const float* reflScale) {
+        AIO_CK(cudaSetDevice(dev));
+        AIO_CK(cudaMemsetAsync(v2.p, 0, g.isz * 4, st));
+        AIO_CK(cudaMemsetAsync(rs.p, 0, g.isz * 4, st));
+        if (vel2Dtw2) to_interior(v2.as<float>(), vel2Dtw2, 1, AIO_MEM_HOST);
+        if (reflScale) to_interior(rs.as<float>(), reflScale, 1, AIO_MEM_HOST);
+        AIO_CK(cudaStreamSynchronize(st));
+    }
+
+    void destroy() {
+        if (st) cudaStreamDestroy(st);
+        st = nullptr;
+    }
+
+    // full nz*nx (per slice) <-> interior pitched slices
+    void to_interior(float* dst, const float* src, int nSlices, int mem) {
+        const cudaMemcpyKind kind = mem == AIO_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+        for (int e = 0; e < nSlices; e++)
+            AIO_CK(cudaMemcpy2DAsync(dst + (long long)e * g.isz, (size_t)g.ip * 4,
+                                     src + (long long)e * g.nz * g.nx + (long long)FAT * g.nz + FAT, (size_t)g.nz * 4,
+                                     (size_t)g.nzi * 4, g.nxi, kind, st));
+    }
+    void from_interior(float* dst, const float* src, int nSlices, int mem) {
+        const cudaMemcpyKind kind = mem == AIO_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+        for (int e = 0; e < nSlices; e++)
+            AIO_CK(cudaMemcpy2DAsync(dst + (long long)e * g.nz * g.nx + (long long)FAT * g.nz + FAT, (size_t)g.nz * 4,
+                                     src + (long long)e * g.isz, (size_t)g.ip * 4, (size_t)g.nzi * 4, g.nxi, kind, st));
+    }
+
+    // ------------------------------------------------------------- waves
+    struct Needs {
+        int nWavefields = 0;  // full coarse wavefields per shot (FP32)
+        int nImg = 0;         // per-shot image slices
+        bool ss = false;
+    };
+
+    long long per_shot_bytes(const Needs& n, int maxSrc, int maxRec) const {
+        long long b = 2 * g.hsz * 4 + 2 * g.isz * 4;  // fine levels + accumulation ring
+        if (n.ss) b += 2 * g.isz * 4;
+        b += (long long)n.nWavefields * g.nts * g.isz * 4;
+        b += (long long)n.nImg * g.isz * (P.imageFp64 ? 8 : 4);
+        b += (long long)maxSrc * g.ntw * 4 + 2LL * maxRec * g.nts * 4;
+        b += 16LL * (g.tilesZ * g.tilesX + 2) + 16LL * (maxSrc + maxRec);
+        return b;
+    }
+
+    int capacity(const Needs& n, int maxSrc, int maxRec) const {
+        long long shared = 2 * g.isz * 4 + (long long)g.nExt * g.isz * 4 * 2 + (long long)g.nExt * g.isz * 8;
+        long long avail = budget - shared;
+        long long per = per_shot_bytes(n, maxSrc, maxRec);
+        long long c = avail / per;
+        return (int)std::max(0LL, std::min(c, 4096LL));
+    }
+
+    int wave_size(const Needs& n, int nShots, const aio_shot* shots) {
+        int maxSrc = 1, maxRec = 1;
+        for (int s = 0; s < nShots; s++) {
+            maxSrc = std::max(maxSrc, shots[s].nSourcesReg);
+            maxRec = std::max(maxRec, shots[s].nReceiversReg);
+        }
+        int cap = capacity(n, maxSrc, maxRec);
+        require(cap >= 1, "device memory budget cannot hold one shot for this operator");
+        return std::min(cap, nShots);
+    }
+
+    // Allocate wave buffers for nb shots and fill descriptors; traces are staged
+    // (host mode) or referenced in place (device mode).
+    void setup_wave(const Needs& n, int nb, const aio_shot* shots, int mem, bool dataIsInput, bool needWemvaData) {
+        int maxSrc = 1, maxRec = 1;
+        for (int s = 0; s < nb; s++) {
+            maxSrc = std::max(maxSrc, shots[s].nSourcesReg);
+            maxRec = std::max(maxRec, shots[s].nReceiversReg);
+        }
+        pbuf.ensure((size_t)nb * 2 * g.hsz * 4);
+        ringb.ensure((size_t)nb * 2 * g.isz * 4);
+        if (n.ss) ssb.ensure((size_t)nb * 2 * g.isz * 4);
+        if (n.nWavefields >= 1) wf1.ensure((size_t)nb * g.nts * g.isz * 4);
+        if (n.nWavefields >= 2) wf2.ensure((size_t)nb * g.nts * g.isz * 4);
+        if (n.nImg) img.ensure((size_t)nb * n.nImg * g.isz * (P.imageFp64 ? 8 : 4));
+        AIO_CK(cudaMemsetAsync(pbuf.p, 0, (size_t)nb * 2 * g.hsz * 4, st));
+        AIO_CK(cudaMemsetAsync(ringb.p, 0, (size_t)nb * 2 * g.isz * 4, st));
+
+        WaveLists L;
+        L.srcOff.resize(nb);
+        L.recOff.resize(nb);
+        for (int s = 0; s < nb; s++) {
+            append_list(g, shots[s].sourcesPositionReg, shots[s].nSourcesReg, L.words, L.srcOff[s], "source");
+            append_list(g, shots[s].receiversPositionReg, shots[s].nReceiversReg, L.words, L.recOff[s], "receiver");
+        }
+        lists.ensure(std::max<size_t>(L.words.size(), 2) * 4);
+        if (!L.words.empty())
+            AIO_CK(cudaMemcpyAsync(lists.p, L.words.data(), L.words.size() * 4, cudaMemcpyHostToDevice, st));
+
+        if (mem == AIO_MEM_HOST) {
+            sig.ensure((size_t)nb * maxSrc * g.ntw * 4);
+            dat.ensure((size_t)nb * maxRec * g.nts * 4);
+            if (needWemvaData) aux.ensure((size_t)nb * maxRec * g.nts * 4);
+        }
+        hdesc.assign(nb, ShotDesc{});
+        const int nT = g.tilesZ * g.tilesX;
+        const int startWords = (nT + 1 + 1) & ~1;
+        srcLists.assign(nb, SparseList{nullptr, nullptr});
+        recLists.assign(nb, SparseList{nullptr, nullptr});
+        srcSig.assign(nb, nullptr);
+        dataPtr.assign(nb, nullptr);
+        wdataPtr.assign(nb, nullptr);
+        for (int s = 0; s < nb; s++) {
+            ShotDesc& d = hdesc[s];
+            d.p[0] = pbuf.as<float>() + (long long)s * 2 * g.hsz;
+            d.p[1] = d.p[0] + g.hsz;
+            d.ss = n.ss ? ssb.as<float>() + (long long)s * 2 * g.isz : nullptr;
+            d.acc = ringb.as<float>() + (long long)s * 2 * g.isz;
+            if (L.srcOff[s] >= 0) {
+                const int* base = lists.as<int>() + L.srcOff[s];
+                srcLists[s] = SparseList{base, (const int2*)(base + startWords)};
+            }
+            if (L.recOff[s] >= 0) {
+                const int* base = lists.as<int>() + L.recOff[s];
+                recLists[s] = SparseList{base, (const int2*)(base + startWords)};
+            }
+            const aio_shot& sh = shots[s];
+            if (mem == AIO_MEM_HOST) {
+                float* sp = sig.as<float>() + (long long)s * maxSrc * g.ntw;
+                float* dp = dat.as<float>() + (long long)s * maxRec * g.nts;
+                if (sh.sourcesSignals && sh.nSourcesReg > 0)
+                    AIO_CK(cudaMemcpyAsync(sp, sh.sourcesSignals, (size_t)sh.nSourcesReg * g.ntw * 4,
+                                           cudaMemcpyHostToDevice, st));
+                if (dataIsInput) {
+                    require(sh.data != nullptr || sh.nReceiversReg == 0, "adjoint input data missing");
+                    if (sh.nReceiversReg > 0)
+                        AIO_CK(cudaMemcpyAsync(dp, sh.data, (size_t)sh.nReceiversReg * g.nts * 4,
+                                               cudaMemcpyHostToDevice, st));
+                } else {
+                    AIO_CK(cudaMemsetAsync(dp, 0, (size_t)std::max(sh.nReceiversReg, 0) * g.nts * 4, st));
+                }
+                srcSig[s] = sp;
+                dataPtr[s] = dp;
+                if (needWemvaData) {
+                    float* wp = aux.as<float>() + (long long)s * maxRec * g.nts;
+                    require(sh.wemvaData != nullptr, "WEMVA data missing");
+                    AIO_CK(cudaMemcpyAsync(wp, sh.wemvaData, (size_t)sh.nReceiversReg * g.nts * 4,
+                                           cudaMemcpyHostToDevice, st));
+                    wdataPtr[s] = wp;
+                }
+            } else {
+                srcSig[s] = sh.sourcesSignals;
+                dataPtr[s] = sh.data;
+                if (!dataIsInput && sh.data && sh.nReceiversReg > 0)
+                    AIO_CK(cudaMemsetAsync(sh.data, 0, (size_t)sh.nReceiversReg * g.nts * 4, st));
+                if (needWemvaData) wdataPtr[s] = sh.wemvaData;
+            }
+        }
+        desc.ensure((size_t)nb * sizeof(ShotDesc));
+    }
+    std::vector<SparseList> srcLists, recLists;
+    std::vector<const float*> srcSig, wdataPtr;
+    std::vector<float*> dataPtr;
+
+    void upload_desc(int nb) {
+        AIO_CK(cudaMemcpyAsync(desc.p, hdesc.data(), (size_t)nb * sizeof(ShotDesc), cudaMemcpyHostToDevice, st));
+    }
+
+    // Copy forward-modelled data of a wave back to the caller (host mode).
+    void download_data(int nb, const aio_shot* shots, int mem) {
+        if (mem != AIO_MEM_HOST) return;
+        for (int s = 0; s < nb; s++)
+            if (shots[s].nReceiversReg > 0 && shots[s].data)
+                AIO_CK(cudaMemcpyAsync(shots[s].data, dataPtr[s], (size_t)shots[s].nReceiversReg * g.nts * 4,
+                                       cudaMemcpyDeviceToHost, st));
+    }
+
+    // ------------------------------------------------------------- stepper
+    StepArgs base_args() const {
+        StepArgs a;
+        std::memset(&a, 0, sizeof(a));
+        a.g = g;
+        a.c = k.c;
+        a.v2 = v2.as<float>();
+        a.taper = taper.as<float>();
+        a.shots = desc.as<ShotDesc>();
+        a.injTB = -1;
+        a.recTB = -1;
+        return a;
+    }
+
+    void launch(int nb, bool adj, int inj, bool rec, bool acc, const StepArgs& a) {
+        dim3 grid(g.tilesZ, g.tilesX, nb), block(TZ, TY);
+        const int key = (adj ? 1 : 0) | (inj << 1) | ((rec ? 1 : 0) << 3) | ((acc ? 1 : 0) << 4);
+        switch (key) {
+#define AIO_CASE(A, I, R, C) \
+    case ((A) | ((I) << 1) | ((R) << 3) | ((C) << 4)): k_step<(A) != 0, (I), (R) != 0, (C) != 0><<<grid, block, 0, st>>>(a); break;
+            AIO_CASE(0, 0, 0, 0) AIO_CASE(1, 0, 0, 0) AIO_CASE(0, 1, 0, 0) AIO_CASE(1, 1, 0, 0)
+            AIO_CASE(0, 2, 0, 0) AIO_CASE(1, 2, 0, 0) AIO_CASE(0, 0, 1, 0) AIO_CASE(1, 0, 1, 0)
+            AIO_CASE(0, 1, 1, 0) AIO_CASE(1, 1, 1, 0) AIO_CASE(0, 2, 1, 0) AIO_CASE(1, 2, 1, 0)
+            AIO_CASE(0, 0, 0, 1) AIO_CASE(1, 0, 0, 1) AIO_CASE(0, 1, 0, 1) AIO_CASE(1, 1, 0, 1)
+            AIO_CASE(0, 2, 0, 1) AIO_CASE(1, 2, 0, 1) AIO_CASE(0, 0, 1, 1) AIO_CASE(1, 0, 1, 1)
+            AIO_CASE(0, 1, 1, 1) AIO_CASE(1, 1, 1, 1) AIO_CASE(0, 2, 1, 1) AIO_CASE(1, 2, 1, 1)
+#undef AIO_CASE
+            default: throw Error{AIO_ERR_ARGUMENT, "unsupported stepper variant"};
+        }
+        AIO_CK(cudaGetLastError());
+        launches++;
+    }
+
+    float hf(int i) const { return k.h[i]; }
+
+    // Sets injection from sources (fine traces) and recording into receivers.
+    void desc_sources_in(int nb, bool recordData) {
+        for (int s = 0; s < nb; s++) {
+            ShotDesc& d = hdesc[s];
+            d.inj = srcLists[s];
+            d.injSig = srcSig[s];
+            d.injLd = g.ntw;
+            d.rec = recordData ? recLists[s] : SparseList{nullptr, nullptr};
+            d.recSig = recordData ? dataPtr[s] : nullptr;
+            d.recLd = g.nts;
+        }
+    }
+    // Sets injection of receiver data (coarse traces) and optional recording at sources.
+    void desc_data_in(int nb, const std::vector<const float*>& data, const std::vector<float*>* srcOut) {
+        for (int s = 0; s < nb; s++) {
+            ShotDesc& d = hdesc[s];
+            d.inj = recLists[s];
+            d.injSig = data[s];
+            d.injLd = g.nts;
+            d.rec = srcOut ? srcLists[s] : SparseList{nullptr, nullptr};
+            d.recSig = srcOut ? (*srcOut)[s] : nullptr;
+            d.recLd = g.ntw;
+        }
+    }
+    void desc_acc(int nb, DevMem* full) {
+        for (int s = 0; s < nb; s++)
+            hdesc[s].acc = full ? full->as<float>() + (long long)s * g.nts * g.isz
+                                : ringb.as<float>() + (long long)s * 2 * g.isz;
+    }
+    void desc_dense(int nb, bool recordData) {
+        for (int s = 0; s < nb; s++) {
+            ShotDesc& d = hdesc[s];
+            d.inj = SparseList{nullptr, nullptr};
+            d.injSig = nullptr;
+            d.rec = recordData ? recLists[s] : SparseList{nullptr, nullptr};
+            d.recSig = recordData ? dataPtr[s] : nullptr;
+            d.recLd = g.nts;
+        }
+    }
+
+    void zero_levels(int nb) { AIO_CK(cudaMemsetAsync(pbuf.p, 0, (size_t)nb * 2 * g.hsz * 4, st)); }
+    void zero_ring(int nb) { AIO_CK(cudaMemsetAsync(ringb.p, 0, (size_t)nb * 2 * g.isz * 4, st)); }
+    void zero_ss(int nb) { AIO_CK(cudaMemsetAsync(ssb.p, 0, (size_t)nb * 2 * g.isz * 4, st)); }
+
+    // Forward-time propagation of sparse injected traces (sources), optional
+    // receiver recording and optional accumulation into a full coarse wavefield.
+    // F/src/nonlinearShotsGpuFunctions.cu:269-295 and :351-380,
+    // F/src/BornShotsGpuFunctions.cu:297-321.
+    void fwd_sparse_pass(int nb, bool recordData, DevMem* wfld) {
+        desc_sources_in(nb, recordData);
+        desc_acc(nb, wfld);
+        upload_desc(nb);
+        zero_levels(nb);
+        if (wfld) AIO_CK(cudaMemsetAsync(wfld->p, 0, (size_t)nb * g.nts * g.isz * 4, st));
+        StepArgs a = base_args();
+        int parity = 0;
+        for (int its = 0; its < g.nts - 1; its++)
+            for (int it2 = 1; it2 < g.sub + 1; it2++) {
+                a.parity = parity;
+                a.injTA = its * g.sub + it2 - 1;
+                a.injTB = -1;
+                a.recTA = its; a.recTB = its + 1; a.recCA = hf(it2); a.recCB = hf(g.H + it2);
+                a.accOffA = (long long)its * g.isz; a.accOffB = (long long)(its + 1) * g.isz;
+                a.hAccA = hf(it2); a.hAccB = hf(g.H + it2);
+                launch(nb, false, 1, recordData, wfld != nullptr, a);
+                parity ^= 1;
+            }
+    }
+
+    // Adjoint-time propagation of injected receiver data with optional source
+    // recording and accumulation (full wavefield or a 2-slice ring whose complete
+    // coarse sample t is handed to post(t, slotOffset)).
+    // F/src/nonlinearShotsGpuFunctions.cu:616-641, F/src/BornShotsGpuFunctions.cu:906-937,
+    // F/src/tomoExtShotsGpuFunctions.cu:1481-1515.
+    void adj_sparse_pass(int nb, const std::vector<const float*>& data, const std::vector<float*>* srcOut, AccMode am,
+                         DevMem* wfld, const std::function<void(int, long long)>& post) {
+        desc_data_in(nb, data, srcOut);
+        desc_acc(nb, am == ACC_FULL ? wfld : nullptr);
+        upload_desc(nb);
+        zero_levels(nb);
+        if (am == ACC_FULL) AIO_CK(cudaMemsetAsync(wfld->p, 0, (size_t)nb * g.nts * g.isz * 4, st));
+        if (am == ACC_RING) zero_ring(nb);
+        StepArgs a = base_args();
+        int parity = 0;
+        for (int its = g.nts - 2; its > -1; its--) {
+            for (int it2 = g.sub - 1; it2 > -1; it2--) {
+                a.parity = parity;
+                a.injTA = its; a.injTB = its + 1; a.injCA = hf(it2 + 1); a.injCB = hf(g.H + it2 + 1);
+                a.recTA = its * g.sub + it2; a.recTB = -1; a.recCA = 1.f;
+                if (am == ACC_FULL) {
+                    a.accOffA = (long long)its * g.isz; a.accOffB = (long long)(its + 1) * g.isz;
+                } else {
+                    a.accOffA = (long long)(its % 2) * g.isz; a.accOffB = (long long)((its + 1) % 2) * g.isz;
+                }
+                a.hAccA = hf(it2); a.hAccB = hf(g.H + it2);
+                launch(nb, true, 1, srcOut != nullptr, am != ACC_NONE, a);
+                parity ^= 1;
+            }
+            if (am == ACC_RING) post(its + 1, (long long)((its + 1) % 2) * g.isz);
+        }
+        if (am == ACC_RING) post(0, 0);
+    }
+
+    // Forward-time scattered propagation driven by a coarse secondary-source ring
+    // (make_ss(t, slotOffset) fills slot t%2); optional data recording and
+    // accumulation (full wavefield, or ring with post(t, slotOffset)).
+    // F/src/BornShotsGpuFunctions.cu:342-374, F/src/tomoExtShotsGpuFunctions.cu:1554-1656,2442-2527.
+    void fwd_dense_pass(int nb, const std::function<void(int, long long)>& make_ss, bool resetSS, bool recordData,
+                        AccMode am, DevMem* wfld, const std::function<void(int, long long)>& post) {
+        desc_dense(nb, recordData);
+        desc_acc(nb, am == ACC_FULL ? wfld : nullptr);
+        upload_desc(nb);
+        zero_levels(nb);
+        zero_ss(nb);
+        if (am == ACC_FULL) AIO_CK(cudaMemsetAsync(wfld->p, 0, (size_t)nb * g.nts * g.isz * 4, st));
+        if (am == ACC_RING) zero_ring(nb);
+        StepArgs a = base_args();
+        int parity = 0;
+        make_ss(0, 0);
+        for (int its = 0; its < g.nts - 1; its++) {
+            const long long sL = (long long)(its % 2) * g.isz, sR = (long long)((its + 1) % 2) * g.isz;
+            make_ss(its + 1, sR);
+            for (int it2 = 1; it2 < g.sub + 1; it2++) {
+                a.parity = parity;
+                a.ssOffA = sL; a.ssOffB = sR; a.hInjA = hf(it2 - 1); a.hInjB = hf(g.H + it2 - 1);
+                a.recTA = its; a.recTB = its + 1; a.recCA = hf(it2); a.recCB = hf(g.H + it2);
+                if (am == ACC_FULL) {
+                    a.accOffA = (long long)its * g.isz; a.accOffB = (long long)(its + 1) * g.isz;
+                } else {
+                    a.accOffA = sL; a.accOffB = sR;
+                }
+                a.hAccA = hf(it2); a.hAccB = hf(g.H + it2);
+                launch(nb, false, 2, recordData, am != ACC_NONE, a);
+                parity ^= 1;
+            }
+            if (am == ACC_RING) post(its, sL);
+            if (resetSS) zero_slot(ssb, nb, sL);
+        }
+        if (am == ACC_RING) post(g.nts - 1, (long long)((g.nts - 1) % 2) * g.isz);
+    }
+
+    // Adjoint-time scattered propagation driven by a coarse secondary-source ring,
+    // injected with h[it2+1]; the completed ring slot of coarse time t goes to post.
+    // F/src/tomoExtShotsGpuFunctions.cu:2619-2700, F/src/wemvaExtShotsGpuFunctions.cu:1038-1121.
+    void adj_dense_pass(int nb, const std::function<void(int, long long)>& make_ss, bool resetSS,
+                        const std::function<void(int, long long)>& post) {
+        desc_dense(nb, false);
+        desc_acc(nb, nullptr);
+        upload_desc(nb);
+        zero_levels(nb);
+        zero_ss(nb);
+        zero_ring(nb);
+        StepArgs a = base_args();
+        int parity = 0;
+        make_ss(g.nts - 1, (long long)((g.nts - 1) % 2) * g.isz);
+        for (int its = g.nts - 2; its > -1; its--) {
+            const long long sL = (long long)(its % 2) * g.isz, sR = (long long)((its + 1) % 2) * g.isz;
+            make_ss(its, sL);
+            for (int it2 = g.sub - 1; it2 > -1; it2--) {
+                a.parity = parity;
+                a.ssOffA = sL; a.ssOffB = sR; a.hInjA = hf(it2 + 1); a.hInjB = hf(g.H + it2 + 1);
+                a.accOffA = sL; a.accOffB = sR; a.hAccA = hf(it2); a.hAccB = hf(g.H + it2);
+                launch(nb, true, 2, false, true, a);
+                parity ^= 1;
+            }
+            post(its + 1, sR);
+            if (resetSS) zero_slot(ssb, nb, sR);
+        }
+        post(0, 0);
+    }
+
+    void zero_slot(DevMem& ring, int nb, long long off) {
+        AIO_CK(cudaMemset2DAsync(ring.as<float>() + off, (size_t)2 * g.isz * 4, 0, (size_t)g.isz * 4, nb, st));
+    }
+
+    // ------------------------------------------------------------- coarse ops
+    dim3 ew_grid(int nb, long long n) const {
+        long long blocks = (n + 255) / 256;
+        blocks = std::min<long long>(blocks, 1184);
+        return dim3((unsigned)std::max<long long>(blocks, 1), nb, 1);
+    }
+    float* ss_ptr(long long off) { return ssb.as<float>() + off; }
+    float* ring_ptr(long long off) { return ringb.as<float>() + off; }
+    long long pairSt() const { return 2 * g.isz; }
+    long long wfSt() const { return (long long)g.nts * g.isz; }
+
+    // ss[slot] = m * W[t]  (imagingFwdGpu)
+    void img_fwd(int nb, long long slot, const float* m, long long mSt, const float* W, int t) {
+        k_img_fwd<<<ew_grid(nb, g.isz), 256, 0, st>>>(ss_ptr(slot), pairSt(), m, mSt, W + (long long)t * g.isz,
+                                                       wfSt(), g.isz);
+        AIO_CK(cudaGetLastError());
+    }
+    // image += W[t] * ring[slot]; ring[slot] = 0  (imagingAdjGpu)
+    void img_adj(int nb, long long slot, const float* W, int t) {
+        if (P.imageFp64)
+            k_img_adj<double><<<ew_grid(nb, g.isz), 256, 0, st>>>(img.as<double>(), g.isz, ring_ptr(slot), pairSt(),
+                                                                  W + (long long)t * g.isz, wfSt(), g.isz, 1);
+        else
+            k_img_adj<float><<<ew_grid(nb, g.isz), 256, 0, st>>>(img.as<float>(), g.isz, ring_ptr(slot), pairSt(),
+                                                                 W + (long long)t * g.isz, wfSt(), g.isz, 1);
+        AIO_CK(cudaGetLastError());
+    }
+    // Lag bounds with C truncating division (F/src/BornExtShotsGpuFunctions.cu:366-383;
+    // F/src/tomoExtShotsGpuFunctions.cu:2631-2650).
+    void bounds_src(int t, int& e0, int& e1) const {
+        e0 = std::max((t + 1 - g.nts) / 2, -g.hExt) + g.hExt;
+        e1 = std::min(t / 2, g.hExt) + g.hExt + 1;
+    }
+    void bounds_rec(int t, int& e0, int& e1) const {
+        e0 = std::max((-t) / 2, -g.hExt) + g.hExt;
+        e1 = std::min((g.nts - 1 - t) / 2, g.hExt) + g.hExt + 1;
+    }
+    // ss[slot] += sum_e ext[e] W[t-2(e-h)]  (imagingTimeFwdGpu)
+    void img_time_fwd(int nb, long long slot, const float* ext, const float* W, int t) {
+        int e0, e1;
+        bounds_src(t, e0, e1);
+        k_img_time_fwd<<<ew_grid(nb, g.isz), 256, 0, st>>>(ss_ptr(slot), pairSt(), ext, 0, W, wfSt(), g.isz, t, e0,
+                                                            e1, g.hExt);
+        AIO_CK(cudaGetLastError());
+    }
+    // ss[slot] += sum_e ext[e] R[t+2(e-h)]  (imagingTimeTomoAdjGpu)
+    void img_time_tomo_adj(int nb, long long slot, const float* ext, const float* R, int t) {
+        int e0, e1;
+        bounds_rec(t, e0, e1);
+        k_img_time_tomo_adj<<<ew_grid(nb, g.isz), 256, 0, st>>>(ss_ptr(slot), pairSt(), ext, 0, R, wfSt(), g.isz, t,
+                                                                 e0, e1, g.hExt);
+        AIO_CK(cudaGetLastError());
+    }
+    // image[e] += ring[slot] * W[t -/+ 2(e-h)]; ring[slot] = 0
+    //   sign=+1: imagingTimeAdjGpu (source side); sign=-1: imagingWemvaTimeAdjGpu.
+    void img_time_adj(int nb, long long slot, const float* W, int t, int sign) {
+        int e0, e1;
+        if (sign > 0) bounds_src(t, e0, e1);
+        else bounds_rec(t, e0, e1);
+        const long long mSt = (long long)g.nExt * g.isz;
+        if (P.imageFp64)
+            k_img_time_adj<double><<<ew_grid(nb, g.isz), 256, 0, st>>>(img.as<double>(), mSt, ring_ptr(slot), pairSt(),
+                                                                       W, wfSt(), g.isz, t, e0, e1, g.hExt, sign, 1);
+        else
+            k_img_time_adj<float><<<ew_grid(nb, g.isz), 256, 0, st>>>(img.as<float>(), mSt, ring_ptr(slot), pairSt(),
+                                                                      W, wfSt(), g.isz, t, e0, e1, g.hExt, sign, 1);
+        AIO_CK(cudaGetLastError());
+    }
+
+    void scale_shared(float* m, int nSlices, int mode) {
+        k_scale<<<ew_grid(1, (long long)nSlices * g.isz), 256, 0, st>>>(m, 0, nSlices, v2.as<float>(), rs.as<float>(),
+                                                                         g.isz, mode);
+        AIO_CK(cudaGetLastError());
+    }
+
+    // Scale per-shot images (reference scales each shot's model before the host
+    // stack, F/src/BornShotsGpu.cpp:325-332) and sum them into out (interior slices).
+    void reduce_images(int nb, int nSlices, int mode, float* out, bool add) {
+        const long long n = (long long)nSlices * g.isz;
+        if (P.imageFp64) {
+            k_scale_d<<<ew_grid(nb, n), 256, 0, st>>>(img.as<double>(), n, nSlices, v2.as<float>(), rs.as<float>(),
+                                                      g.isz, mode);
+            AIO_CK(cudaGetLastError());
+            k_sum_shots<double><<<ew_grid(1, n), 256, 0, st>>>(out, img.as<double>(), n, nb, n, add ? 1 : 0);
+        } else {
+            k_scale<<<ew_grid(nb, n), 256, 0, st>>>(img.as<float>(), n, nSlices, v2.as<float>(), rs.as<float>(), g.isz,
+                                                    mode);
+            AIO_CK(cudaGetLastError());
+            k_sum_shots<float><<<ew_grid(1, n), 256, 0, st>>>(out, img.as<float>(), n, nb, n, add ? 1 : 0);
+        }
+        AIO_CK(cudaGetLastError());
+    }
+    void zero_images(int nb, int nSlices) {
+        AIO_CK(cudaMemsetAsync(img.p, 0, (size_t)nb * nSlices * g.isz * (P.imageFp64 ? 8 : 4), st));
+    }
+
+    // Model staging: shared interior slices for models, extended reflectivity
+    // and the summed output.
+    float* stage_model(const float* m, int nSlices, int mem, DevMem& buf) {
+        buf.ensure((size_t)nSlices * g.isz * 4);
+        AIO_CK(cudaMemsetAsync(buf.p, 0, (size_t)nSlices * g.isz * 4, st));
+        to_interior(buf.as<float>(), m, nSlices, mem);
+        return buf.as<float>();
+    }
+    void write_model(float* dst, int nSlices, int add, int mem, float* outInterior) {
+        // outInterior already holds (add ? dst + result : result) on interior points.
+        if (!add) {
+            if (mem == AIO_MEM_HOST) std::memset(dst, 0, (size_t)nSlices * g.nz * g.nx * 4);
+            else AIO_CK(cudaMemsetAsync(dst, 0, (size_t)nSlices * g.nz * g.nx * 4, st));
+        }
+        from_interior(dst, outInterior, nSlices, mem);
+    }
+    void sync() { AIO_CK(cudaStreamSynchronize(st)); }
+
+    void begin_call() {
+        AIO_CK(cudaSetDevice(dev));
+        launches = 0;
+    }
+
+    // ============================================================ operators
+
+    // Nonlinear forward (F/src/nonlinearShotsGpuFunctions.cu:227-309; with a
+    // wavefield, :310-395 — only a batch of one shot returns it).
+    void nonlinear_forward(int nShots, const aio_shot* shots, int mem, float* wavefieldOut) {
+        begin_call();
+        Needs n;
+        n.nWavefields = wavefieldOut ? 1 : 0;
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = wave_size(n, nShots - s0, shots + s0);
+            setup_wave(n, nb, shots + s0, mem, false, false);
+            fwd_sparse_pass(nb, true, wavefieldOut ? &wf1 : nullptr);
+            download_data(nb, shots + s0, mem);
+            if (wavefieldOut) download_wavefield(wavefieldOut, wf1.as<float>());
+            sync();
+            s0 += nb;
+        }
+    }
+
+    // Nonlinear adjoint (F/src/nonlinearShotsGpuFunctions.cu:579-652 / :653-737).
+    void nonlinear_adjoint(int nShots, const aio_shot* shots, int mem, float* wavefieldOut) {
+        begin_call();
+        Needs n;
+        n.nWavefields = wavefieldOut ? 1 : 0;
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = wave_size(n, nShots - s0, shots + s0);
+            setup_wave(n, nb, shots + s0, mem, true, false);
+            std::vector<float*> srcOut(nb);
+            std::vector<const float*> din(dataPtr.begin(), dataPtr.end());
+            // source traces output: staged in the `sig` buffer (host) or caller memory (device)
+            for (int s = 0; s < nb; s++) {
+                const aio_shot& sh = shots[s0 + s];
+                float* o = mem == AIO_MEM_HOST ? const_cast<float*>(srcSig[s]) : sh.sourcesOut;
+                require(o != nullptr || sh.nSourcesReg == 0, "nonlinear adjoint output traces missing");
+                if (sh.nSourcesReg > 0) AIO_CK(cudaMemsetAsync(o, 0, (size_t)sh.nSourcesReg * g.ntw * 4, st));
+                srcOut[s] = o;
+            }
+            adj_sparse_pass(nb, din, &srcOut, wavefieldOut ? ACC_FULL : ACC_NONE, wavefieldOut ? &wf1 : nullptr,
+                            [](int, long long) {});
+            if (mem == AIO_MEM_HOST)
+                for (int s = 0; s < nb; s++) {
+                    const aio_shot& sh = shots[s0 + s];
+                    if (sh.nSourcesReg > 0)
+                        AIO_CK(cudaMemcpyAsync(sh.sourcesOut, srcOut[s], (size_t)sh.nSourcesReg * g.ntw * 4,
+                                               cudaMemcpyDeviceToHost, st));
+                }
+            if (wavefieldOut) download_wavefield(wavefieldOut, wf1.as<float>());
+            sync();
+            s0 += nb;
+        }
+    }
+
+    void download_wavefield(float* host, const float* dev) {
+        // interior pitched [nts] slices -> full [nts][nx][nz] host array (zero outside interior)
+        std::memset(host, 0, (size_t)g.nts * g.nz * g.nx * 4);
+        for (int t = 0; t < g.nts; t++)
+            AIO_CK(cudaMemcpy2DAsync(host + (long long)t * g.nz * g.nx + (long long)FAT * g.nz + FAT, (size_t)g.nz * 4,
+                                     dev + (long long)t * g.isz, (size_t)g.ip * 4, (size_t)g.nzi * 4, g.nxi,
+                                     cudaMemcpyDeviceToHost, st));
+    }
+
+    // Source pass storing the coarse source wavefield W[nts] of every shot of the wave.
+    // F/src/BornShotsGpuFunctions.cu:297-321.
+    void source_wavefield(int nb, DevMem& W) { fwd_sparse_pass(nb, false, &W); }
+
+    // Born forward (F/src/BornShotsGpuFunctions.cu:260-388).
+    void born_forward(const float* model, int nShots, const aio_shot* shots, int mem) {
+        begin_call();
+        Needs n;
+        n.nWavefields = 1;
+        n.ss = true;
+        float* dm = stage_model(model, 1, mem, this->model);
+        scale_shared(dm, 1, 0);
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = wave_size(n, nShots - s0, shots + s0);
+            setup_wave(n, nb, shots + s0, mem, false, false);
+            source_wavefield(nb, wf1);
+            const float* W = wf1.as<float>();
+            fwd_dense_pass(
+                nb, [&](int t, long long slot) { img_fwd(nb, slot, dm, 0, W, t); }, false, true, ACC_NONE, nullptr,
+                [](int, long long) {});
+            download_data(nb, shots + s0, mem);
+            sync();
+            s0 += nb;
+        }
+    }
+
+    // Born adjoint (F/src/BornShotsGpuFunctions.cu:829-957), per-shot images
+    // summed on the device.
+    void born_adjoint(float* modelOut, int add, int nShots, const aio_shot* shots, int mem) {
+        begin_call();
+        Needs n;
+        n.nWavefields = 1;
+        n.nImg = 1;
+        float* out = stage_out(modelOut, 1, add, mem);
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = wave_size(n, nShots - s0, shots + s0);
+            setup_wave(n, nb, shots + s0, mem, true, false);
+            source_wavefield(nb, wf1);
+            zero_images(nb, 1);
+            const float* W = wf1.as<float>();
+            std::vector<const float*> din(dataPtr.begin(), dataPtr.end());
+            adj_sparse_pass(nb, din, nullptr, ACC_RING, nullptr,
+                            [&](int t, long long slot) { img_adj(nb, slot, W, t); });
+            reduce_images(nb, 1, 0, out, true);
+            sync();
+            s0 += nb;
+        }
+        write_model(modelOut, 1, add, mem, out);
+        sync();
+    }
+
+    float* stage_out(float* dst, int nSlices, int add, int mem) {
+        outv.ensure((size_t)nSlices * g.isz * 4);
+        AIO_CK(cudaMemsetAsync(outv.p, 0, (size_t)nSlices * g.isz * 4, st));
+        if (add) to_interior(outv.as<float>(), dst, nSlices, mem);
+        return outv.as<float>();
+    }
+
+    // Extended (time-lag) Born forward (F/src/BornExtShotsGpuFunctions.cu:269-419).
+    void born_ext_forward(const float* model, int nShots, const aio_shot* shots, int mem) {
+        begin_call();
+        Needs n;
+        n.nWavefields = 1;
+        n.ss = true;
+        float* dm = stage_model(model, g.nExt, mem, this->model);
+        scale_shared(dm, g.nExt, P.sloth ? 2 : 1);
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = wave_size(n, nShots - s0, shots + s0);
+            setup_wave(n, nb, shots + s0, mem, false, false);
+            source_wavefield(nb, wf1);
+            const float* W = wf1.as<float>();
+            fwd_dense_pass(
+                nb, [&](int t, long long slot) { img_time_fwd(nb, slot, dm, W, t); }, true, true, ACC_NONE, nullptr,
+                [](int, long long) {});
+            download_data(nb, shots + s0, mem);
+            sync();
+            s0 += nb;
+        }
+    }
+
+    // Extended (time-lag) Born adjoint (F/src/BornExtShotsGpuFunctions.cu:1525-1675).
+    void born_ext_adjoint(float* modelOut, int add, int nShots, const aio_shot* shots, int mem) {
+        begin_call();
+        Needs n;
+        n.nWavefields = 1;
+        n.nImg = g.nExt;
+        float* out = stage_out(modelOut, g.nExt, add, mem);
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = wave_size(n, nShots - s0, shots + s0);
+            setup_wave(n, nb, shots + s0, mem, true, false);
+            source_wavefield(nb, wf1);
+            zero_images(nb, g.nExt);
+            const float* W = wf1.as<float>();
+            std::vector<const float*> din(dataPtr.begin(), dataPtr.end());
+            adj_sparse_pass(nb, din, nullptr, ACC_RING, nullptr,
+                            [&](int t, long long slot) { img_time_adj(nb, slot, W, t, +1); });
+            reduce_images(nb, g.nExt, P.sloth ? 2 : 1, out, true);
+            sync();
+            s0 += nb;
+        }
+        write_model(modelOut, g.nExt, add, mem, out);
+        sync();
+    }
+
+    // Source wavefield with coarse second time derivative (computeTomoSrcWfldDt2,
+    // F/src/tomoExtShotsGpuFunctions.cu:1251-1361).
+    void source_wavefield_dt2(int nb, DevMem& W) {
+        fwd_sparse_pass(nb, false, &W);
+        k_dt2<<<ew_grid(nb, g.isz), 256, 0, st>>>(W.as<float>(), wfSt(), g.isz, g.nts, k.cSide, k.cCenter);
+        AIO_CK(cudaGetLastError());
+    }
+    // Receiver wavefield (computeTomoRecWfld, F/src/tomoExtShotsGpuFunctions.cu:1481-1515).
+    void receiver_wavefield(int nb, const std::vector<const float*>& data, DevMem& R) {
+        adj_sparse_pass(nb, data, nullptr, ACC_FULL, &R, [](int, long long) {});
+    }
+
+    // Extended tomo forward (F/src/tomoExtShotsGpuFunctions.cu:355-465, legs :1554-1881).
+    void tomo_forward(const float* model, const float* extRefl, int nShots, const aio_shot* shots, int mem) {
+        begin_call();
+        Needs n;
+        n.nWavefields = 2;
+        n.ss = true;
+        float* dm = stage_model(model, 1, mem, this->model);
+        scale_shared(dm, 1, 0);
+        float* ex = stage_model(extRefl, g.nExt, mem, this->ext);
+        scale_shared(ex, g.nExt, P.sloth ? 2 : 1);
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = wave_size(n, nShots - s0, shots + s0);
+            setup_wave(n, nb, shots + s0, mem, false, false);
+            source_wavefield_dt2(nb, wf2);
+            const float* W2 = wf2.as<float>();
+            const float* W1 = wf1.as<float>();
+            auto nop = [](int, long long) {};
+            if (P.leg1) {
+                fwd_dense_pass(
+                    nb, [&](int t, long long slot) { img_time_fwd(nb, slot, ex, W2, t); }, true, false, ACC_FULL, &wf1,
+                    nop);
+                fwd_dense_pass(
+                    nb, [&](int t, long long slot) { img_fwd(nb, slot, dm, 0, W1, t); }, false, true, ACC_NONE,
+                    nullptr, nop);
+            }
+            if (P.leg2) {
+                fwd_dense_pass(
+                    nb, [&](int t, long long slot) { img_fwd(nb, slot, dm, 0, W2, t); }, false, false, ACC_FULL, &wf1,
+                    nop);
+                fwd_dense_pass(
+                    nb, [&](int t, long long slot) { img_time_fwd(nb, slot, ex, W1, t); }, true, true, ACC_NONE,
+                    nullptr, nop);
+            }
+            download_data(nb, shots + s0, mem);
+            sync();
+            s0 += nb;
+        }
+    }
+
+    // Extended tomo adjoint (F/src/tomoExtShotsGpuFunctions.cu:797-910, legs :2442-2701).
+    void tomo_adjoint(float* modelOut, int add, const float* extRefl, int nShots, const aio_shot* shots, int mem) {
+        begin_call();
+        Needs n;
+        n.nWavefields = 2;
+        n.ss = true;
+        n.nImg = 1;
+        float* ex = stage_model(extRefl, g.nExt, mem, this->ext);
+        scale_shared(ex, g.nExt, P.sloth ? 2 : 1);
+        float* out = stage_out(modelOut, 1, add, mem);
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = wave_size(n, nShots - s0, shots + s0);
+            setup_wave(n, nb, shots + s0, mem, true, false);
+            source_wavefield_dt2(nb, wf2);
+            std::vector<const float*> din(dataPtr.begin(), dataPtr.end());
+            receiver_wavefield(nb, din, wf1);
+            zero_images(nb, 1);
+            const float* W2 = wf2.as<float>();
+            const float* R = wf1.as<float>();
+            if (P.leg1)
+                fwd_dense_pass(
+                    nb, [&](int t, long long slot) { img_time_fwd(nb, slot, ex, W2, t); }, true, false, ACC_RING,
+                    nullptr, [&](int t, long long slot) { img_adj(nb, slot, R, t); });
+            if (P.leg2)
+                adj_dense_pass(
+                    nb, [&](int t, long long slot) { img_time_tomo_adj(nb, slot, ex, R, t); }, true,
+                    [&](int t, long long slot) { img_adj(nb, slot, W2, t); });
+            reduce_images(nb, 1, 0, out, true);
+            sync();
+            s0 += nb;
+        }
+        write_model(modelOut, 1, add, mem, out);
+        sync();
+    }
+
+    // Extended WEMVA forward (F/src/wemvaExtShotsGpuFunctions.cu:344-456, legs :961-1122).
+    void wemva_forward(const float* model, float* imageOut, int add, int nShots, const aio_shot* shots, int mem) {
+        begin_call();
+        Needs n;
+        n.nWavefields = 2;
+        n.ss = true;
+        n.nImg = g.nExt;
+        float* dm = stage_model(model, 1, mem, this->model);
+        scale_shared(dm, 1, 0);
+        float* out = stage_out(imageOut, g.nExt, add, mem);
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = wave_size(n, nShots - s0, shots + s0);
+            setup_wave(n, nb, shots + s0, mem, false, true);
+            source_wavefield_dt2(nb, wf2);
+            receiver_wavefield(nb, wdataPtr, wf1);
+            zero_images(nb, g.nExt);
+            const float* W2 = wf2.as<float>();
+            const float* R = wf1.as<float>();
+            if (P.leg1)
+                fwd_dense_pass(
+                    nb, [&](int t, long long slot) { img_fwd(nb, slot, dm, 0, W2, t); }, false, false, ACC_RING,
+                    nullptr, [&](int t, long long slot) { img_time_adj(nb, slot, R, t, -1); });
+            if (P.leg2)
+                adj_dense_pass(
+                    nb, [&](int t, long long slot) { img_fwd(nb, slot, dm, 0, R, t); }, false,
+                    [&](int t, long long slot) { img_time_adj(nb, slot, W2, t, +1); });
+            reduce_images(nb, g.nExt, 1, out, true);
+            sync();
+            s0 += nb;
+        }
+        write_model(imageOut, g.nExt, add, mem, out);
+        sync();
+    }
+
+    // Extended WEMVA adjoint (F/src/wemvaExtShotsGpuFunctions.cu:575-688, legs :1270-1426).
+    void wemva_adjoint(float* modelOut, int add, const float* image, int nShots, const aio_shot* shots, int mem) {
+        begin_call();
+        Needs n;
+        n.nWavefields = 2;
+        n.ss = true;
+        n.nImg = 1;
+        float* im = stage_model(image, g.nExt, mem, this->ext);
+        scale_shared(im, g.nExt, 1);
+        float* out = stage_out(modelOut, 1, add, mem);
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = wave_size(n, nShots - s0, shots + s0);
+            setup_wave(n, nb, shots + s0, mem, false, true);
+            source_wavefield_dt2(nb, wf2);
+            receiver_wavefield(nb, wdataPtr, wf1);
+            zero_images(nb, 1);
+            const float* W2 = wf2.as<float>();
+            const float* R = wf1.as<float>();
+            if (P.leg1)
+                adj_dense_pass(
+                    nb, [&](int t, long long slot) { img_time_tomo_adj(nb, slot, im, R, t); }, true,
+                    [&](int t, long long slot) { img_adj(nb, slot, W2, t); });
+            if (P.leg2)
+                fwd_dense_pass(
+                    nb, [&](int t, long long slot) { img_time_fwd(nb, slot, im, W2, t); }, true, false, ACC_RING,
+                    nullptr, [&](int t, long long slot) { img_adj(nb, slot, R, t); });
+            reduce_images(nb, 1, 0, out, true);
+            sync();
+            s0 += nb;
+        }
+        write_model(modelOut, 1, add, mem, out);
+        sync();
+    }
+};
+
+// ----------------------------------------------------------------------------
+// Reference-seam state: one parameter block and one context per (family, iGpu)
+// slot, the counterpart of the reference's per-translation-unit globals
+// (F/include/varDeclare.h:22-93).
+// ----------------------------------------------------------------------------
+struct SeamSlot {
+    aio_params P{};
+    bool inited = false;
+    Context* ctx = nullptr;
+};
+static std::mutex g_seam_mu;
+static std::map<std::pair<int, int>, SeamSlot> g_seam;
+
+static SeamSlot& seam(int family, int iGpu) { return g_seam[{family, iGpu}]; }
+
+static void seam_init(int family, float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad,
+                      float alphaCos, int nExt, int leg1, int leg2, int nGpu, int iGpuId) {
+    require(nGpu >= 1, "nGpu must be >= 1");
+    std::lock_guard<std::mutex> lk(g_seam_mu);
+    aio_params P{};
+    P.nz = nz; P.nx = nx; P.nts = nts; P.sub = sub; P.minPad = minPad; P.nExt = nExt;
+    P.dz = dz; P.dx = dx; P.dts = dts; P.alphaCos = alphaCos; P.leg1 = leg1; P.leg2 = leg2;
+    P.wavefieldPrecision = AIO_WFLD_FP32; P.imageFp64 = 0; P.device = iGpuId;
+    // The reference's slot index is iGpu (0..nGpu-1) while init is called per
+    // device id; the parameters are identical for every slot of a family.
+    for (int i = 0; i < nGpu; i++) {
+        SeamSlot& s = seam(family, i);
+        s.P = P;
+        s.inited = true;
+    }
+}
+
+static void seam_allocate(int family, float* vel2Dtw2, float* reflScale, int iGpu, int iGpuId) {
+    std::lock_guard<std::mutex> lk(g_seam_mu);
+    SeamSlot& s = seam(family, iGpu);
+    if (!s.inited) throw Error{AIO_ERR_STATE, "allocate called before init"};
+    if (s.ctx) {
+        s.ctx->destroy();
+        delete s.ctx;
+        s.ctx = nullptr;
+    }
+    s.P.device = iGpuId;
+    Context* c = new Context();
+    try {
+        c->init(s.P, vel2Dtw2, reflScale);
+    } catch (...) {
+        delete c;
+        throw;
+    }
+    s.ctx = c;
+}
+
+static void seam_deallocate(int family, int iGpu) {
+    std::lock_guard<std::mutex> lk(g_seam_mu);
+    SeamSlot& s = seam(family, iGpu);
+    if (s.ctx) {
+        s.ctx->destroy();
+        delete s.ctx;
+    }
+    s.ctx = nullptr;
+}
+
+static Context& seam_ctx(int family, int iGpu) {
+    std::lock_guard<std::mutex> lk(g_seam_mu);
+    SeamSlot& s = seam(family, iGpu);
+    if (!s.ctx) throw Error{AIO_ERR_STATE, "operator call before allocate"};
+    return *s.ctx;
+}
+
+static aio_shot one_shot(float* sig, int* sp, int ns, int* rp, int nr, float* data) {
+    aio_shot s{};
+    s.sourcesPositionReg = sp; s.nSourcesReg = ns;
+    s.receiversPositionReg = rp; s.nReceiversReg = nr;
+    s.sourcesSignals = sig; s.data = data;
+    return s;
+}
+
+}  // namespace aio
+
+using namespace aio;
+
+struct aio_context {
+    Context c;
+};
+
+#define AIO_API extern "C" __attribute__((visibility("default")))
+
+AIO_API const char* aio_last_error(void) { return g_err.c_str(); }
+
+AIO_API int aio_context_create(const aio_params* params, const float* vel2Dtw2, const float* reflectivityScale,
+                               aio_context** out) {
+    return guard([&] {
+        require(params && out, "null argument");
+        aio_context* c = new aio_context();
+        try {
+            c->c.init(*params, vel2Dtw2, reflectivityScale);
+        } catch (...) {
+            delete c;
+            throw;
+        }
+        *out = c;
+    });
+}
+AIO_API int aio_context_destroy(aio_context* ctx) {
+    return guard([&] {
+        if (!ctx) return;
+        cudaSetDevice(ctx->c.dev);
+        ctx->c.destroy();
+        delete ctx;
+    });
+}
+AIO_API int aio_context_set_velocity(aio_context* ctx, const float* vel2Dtw2, const float* reflectivityScale) {
+    return guard([&] { ctx->c.set_velocity(vel2Dtw2, reflectivityScale); });
+}
+AIO_API int aio_context_wave_capacity(aio_context* ctx, int family) {
+    Context::Needs n;
+    switch (family) {
+        case AIO_NONLINEAR: break;
+        case AIO_BORN: n.nWavefields = 1; n.ss = true; n.nImg = 1; break;
+        case AIO_BORN_EXT: n.nWavefields = 1; n.ss = true; n.nImg = ctx->c.g.nExt; break;
+        default: n.nWavefields = 2; n.ss = true; n.nImg = ctx->c.g.nExt; break;
+    }
+    return ctx->c.capacity(n, 4, 4096);
+}
+AIO_API long long aio_context_last_launches(aio_context* ctx) { return ctx->c.launches; }
+
+AIO_API int aio_nonlinear_forward(aio_context* ctx, int nShots, const aio_shot* shots, int memSpace) {
+    return guard([&] { ctx->c.nonlinear_forward(nShots, shots, memSpace, nullptr); });
+}
+AIO_API int aio_nonlinear_adjoint(aio_context* ctx, int nShots, const aio_shot* shots, int memSpace) {
+    return guard([&] { ctx->c.nonlinear_adjoint(nShots, shots, memSpace, nullptr); });
+}
+AIO_API int aio_born_forward(aio_context* ctx, const float* model, int nShots, const aio_shot* shots, int memSpace) {
+    return guard([&] { ctx->c.born_forward(model, nShots, shots, memSpace); });
+}
+AIO_API int aio_born_adjoint(aio_context* ctx, float* model, int add, int nShots, const aio_shot* shots,
+                             int memSpace) {
+    return guard([&] { ctx->c.born_adjoint(model, add, nShots, shots, memSpace); });
+}
+AIO_API int aio_born_ext_forward(aio_context* ctx, const float* model, int nShots, const aio_shot* shots,
+                                 int memSpace) {
+    return guard([&] { ctx->c.born_ext_forward(model, nShots, shots, memSpace); });
+}
+AIO_API int aio_born_ext_adjoint(aio_context* ctx, float* model, int add, int nShots, const aio_shot* shots,
+                                 int memSpace) {
+    return guard([&] { ctx->c.born_ext_adjoint(model, add, nShots, shots, memSpace); });
+}
+AIO_API int aio_tomo_ext_forward(aio_context* ctx, const float* model, const float* extReflectivity, int nShots,
+                                 const aio_shot* shots, int memSpace) {
+    return guard([&] { ctx->c.tomo_forward(model, extReflectivity, nShots, shots, memSpace); });
+}
+AIO_API int aio_tomo_ext_adjoint(aio_context* ctx, float* model, int add, const float* extReflectivity, int nShots,
+                                 const aio_shot* shots, int memSpace) {
+    return guard([&] { ctx->c.tomo_adjoint(model, add, extReflectivity, nShots, shots, memSpace); });
+}
+AIO_API int aio_wemva_ext_forward(aio_context* ctx, const float* model, float* image, int add, int nShots,
+                                  const aio_shot* shots, int memSpace) {
+    return guard([&] { ctx->c.wemva_forward(model, image, add, nShots, shots, memSpace); });
+}
+AIO_API int aio_wemva_ext_adjoint(aio_context* ctx, float* model, int add, const float* image, int nShots,
+                                  const aio_shot* shots, int memSpace) {
+    return guard([&] { ctx->c.wemva_adjoint(model, add, image, nShots, shots, memSpace); });
+}
+
+// ------------------------------------------------------------ reference seam
+AIO_API int aio_getGpuInfo(const int* gpuList, int nGpuList, int info, int deviceNumberInfo) {
+    (void)info; (void)deviceNumberInfo;
+    return guard([&] {
+        int nDev = 0;
+        AIO_CK(cudaGetDeviceCount(&nDev));
+        require(nGpuList <= nDev, "number of requested GPUs greater than available GPUs");
+        for (int i = 0; i < nGpuList; i++)
+            require(gpuList[i] >= 0 && gpuList[i] < nDev, "GPU id list holds an invalid id");
+    });
+}
+
+AIO_API int aio_initNonlinearGpu(float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad,
+                                 int blockSize, float alphaCos, int nGpu, int iGpuId, int iGpuAlloc) {
+    (void)blockSize; (void)iGpuAlloc;
+    return guard([&] { seam_init(AIO_NONLINEAR, dz, dx, nz, nx, nts, dts, sub, minPad, alphaCos, 1, 1, 1, nGpu, iGpuId); });
+}
+AIO_API int aio_allocateNonlinearGpu(float* vel2Dtw2, int iGpu, int iGpuId) {
+    return guard([&] { seam_allocate(AIO_NONLINEAR, vel2Dtw2, nullptr, iGpu, iGpuId); });
+}
+AIO_API int aio_deallocateNonlinearGpu(int iGpu, int iGpuId) {
+    (void)iGpuId;
+    return guard([&] { seam_deallocate(AIO_NONLINEAR, iGpu); });
+}
+AIO_API int aio_propShotsFwdGpu(float* modelRegDtw, float* dataRegDts, int* sp, int ns, int* rp, int nr,
+                                float* wavefieldDts, int iGpu, int iGpuId) {
+    (void)wavefieldDts; (void)iGpuId;
+    return guard([&] {
+        aio_shot s = one_shot(modelRegDtw, sp, ns, rp, nr, dataRegDts);
+        seam_ctx(AIO_NONLINEAR, iGpu).nonlinear_forward(1, &s, AIO_MEM_HOST, nullptr);
+    });
+}
+AIO_API int aio_propShotsFwdGpuWavefield(float* modelRegDtw, float* dataRegDts, int* sp, int ns, int* rp, int nr,
+                                         float* wavefieldDts, int iGpu, int iGpuId) {
+    (void)iGpuId;
+    return guard([&] {
+        aio_shot s = one_shot(modelRegDtw, sp, ns, rp, nr, dataRegDts);
+        seam_ctx(AIO_NONLINEAR, iGpu).nonlinear_forward(1, &s, AIO_MEM_HOST, wavefieldDts);
+    });
+}
+AIO_API int aio_propShotsAdjGpu(float* modelRegDtw, float* dataRegDts, int* sp, int ns, int* rp, int nr,
+                                float* wavefieldDts, int iGpu, int iGpuId) {
+    (void)wavefieldDts; (void)iGpuId;
+    return guard([&] {
+        aio_shot s = one_shot(nullptr, sp, ns, rp, nr, dataRegDts);
+        s.sourcesOut = modelRegDtw;
+        seam_ctx(AIO_NONLINEAR, iGpu).nonlinear_adjoint(1, &s, AIO_MEM_HOST, nullptr);
+    });
+}
+AIO_API int aio_propShotsAdjGpuWavefield(float* modelRegDtw, float* dataRegDts, int* sp, int ns, int* rp, int nr,
+                                         float* wavefieldDts, int iGpu, int iGpuId) {
+    (void)iGpuId;
+    return guard([&] {
+        aio_shot s = one_shot(nullptr, sp, ns, rp, nr, dataRegDts);
+        s.sourcesOut = modelRegDtw;
+        seam_ctx(AIO_NONLINEAR, iGpu).nonlinear_adjoint(1, &s, AIO_MEM_HOST, wavefieldDts);
+    });
+}
+
+AIO_API int aio_initBornGpu(float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad, int blockSize,
+                            float alphaCos, int nGpu, int iGpuId, int iGpuAlloc) {
+    (void)blockSize; (void)iGpuAlloc;
+    return guard([&] { seam_init(AIO_BORN, dz, dx, nz, nx, nts, dts, sub, minPad, alphaCos, 1, 1, 1, nGpu, iGpuId); });
+}
+AIO_API int aio_allocateBornShotsGpu(float* vel2Dtw2, float* reflectivityScale, int iGpu, int iGpuId) {
+    return guard([&] { seam_allocate(AIO_BORN, vel2Dtw2, reflectivityScale, iGpu, iGpuId); });
+}
+AIO_API int aio_deallocateBornShotsGpu(int iGpu, int iGpuId) {
+    (void)iGpuId;
+    return guard([&] { seam_deallocate(AIO_BORN, iGpu); });
+}
+AIO_API int aio_BornShotsFwdGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sp, int ns, int* rp,
+                                int nr, float* srcWavefield, float* scatWavefield, int iGpu, int iGpuId) {
+    (void)srcWavefield; (void)scatWavefield; (void)iGpuId;
+    return guard([&] {
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
+        seam_ctx(AIO_BORN, iGpu).born_forward(model, 1, &s, AIO_MEM_HOST);
+    });
+}
+AIO_API int aio_BornShotsAdjGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sp, int ns, int* rp,
+                                int nr, float* srcWavefield, float* recWavefield, int iGpu, int iGpuId) {
+    (void)srcWavefield; (void)recWavefield; (void)iGpuId;
+    return guard([&] {
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
+        seam_ctx(AIO_BORN, iGpu).born_adjoint(model, 0, 1, &s, AIO_MEM_HOST);
+    });
+}
+
+AIO_API int aio_initBornExtGpu(float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad,
+                               int blockSize, float alphaCos, int nExt, int nGpu, int iGpuId, int iGpuAlloc) {
+    (void)blockSize; (void)iGpuAlloc;
+    return guard(
+        [&] { seam_init(AIO_BORN_EXT, dz, dx, nz, nx, nts, dts, sub, minPad, alphaCos, nExt, 1, 1, nGpu, iGpuId); });
+}
+AIO_API int aio_allocateBornExtShotsGpu(float* vel2Dtw2, float* reflectivityScale, int iGpu, int iGpuId) {
+    return guard([&] { seam_allocate(AIO_BORN_EXT, vel2Dtw2, reflectivityScale, iGpu, iGpuId); });
+}
+AIO_API int aio_deallocateBornExtShotsGpu(int iGpu, int iGpuId) {
+    (void)iGpuId;
+    return guard([&] { seam_deallocate(AIO_BORN_EXT, iGpu); });
+}
+AIO_API int aio_BornTimeShotsFwdGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sp, int ns, int* rp,
+                                    int nr, float* srcWavefield, float* scatWavefield, int sloth, int iGpu,
+                                    int iGpuId) {
+    (void)srcWavefield; (void)scatWavefield; (void)iGpuId;
+    return guard([&] {
+        Context& c = seam_ctx(AIO_BORN_EXT, iGpu);
+        c.P.sloth = sloth;
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
+        c.born_ext_forward(model, 1, &s, AIO_MEM_HOST);
+    });
+}
+AIO_API int aio_BornTimeShotsAdjGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sp, int ns, int* rp,
+                                    int nr, float* srcWavefield, float* recWavefield, int sloth, int iGpu,
+                                    int iGpuId) {
+    (void)srcWavefield; (void)recWavefield; (void)iGpuId;
+    return guard([&] {
+        Context& c = seam_ctx(AIO_BORN_EXT, iGpu);
+        c.P.sloth = sloth;
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
+        c.born_ext_adjoint(model, 0, 1, &s, AIO_MEM_HOST);
+    });
+}
+
+AIO_API int aio_initTomoExtGpu(float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad,
+                               int blockSize, float alphaCos, int nExt, int leg1, int leg2, int nGpu, int iGpuId,
+                               int iGpuAlloc) {
+    (void)blockSize; (void)iGpuAlloc;
+    return guard([&] {
+        seam_init(AIO_TOMO_EXT, dz, dx, nz, nx, nts, dts, sub, minPad, alphaCos, nExt, leg1, leg2, nGpu, iGpuId);
+    });
+}
+AIO_API int aio_allocateTomoExtShotsGpu(float* vel2Dtw2, float* reflectivityScale, int iGpu, int iGpuId) {
+    return guard([&] { seam_allocate(AIO_TOMO_EXT, vel2Dtw2, reflectivityScale, iGpu, iGpuId); });
+}
+AIO_API int aio_deallocateTomoExtShotsGpu(int iGpu, int iGpuId) {
+    (void)iGpuId;
+    return guard([&] { seam_deallocate(AIO_TOMO_EXT, iGpu); });
+}
+AIO_API int aio_tomoTimeShotsFwdGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
+                                    int* sp, int ns, int* rp, int nr, float* w0, float* w1, float* w2, int sloth,
+                                    int iGpu, int iGpuId, int saveWavefield) {
+    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    return guard([&] {
+        require(saveWavefield == 0, "saveWavefield=1 is not available for tomo in this build");
+        Context& c = seam_ctx(AIO_TOMO_EXT, iGpu);
+        c.P.sloth = sloth;
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
+        c.tomo_forward(model, extReflectivity, 1, &s, AIO_MEM_HOST);
+    });
+}
+AIO_API int aio_tomoTimeShotsAdjGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
+                                    int* sp, int ns, int* rp, int nr, float* w0, float* w1, float* w2, int sloth,
+                                    int iGpu, int iGpuId, int saveWavefield) {
+    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    return guard([&] {
+        require(saveWavefield == 0, "saveWavefield=1 is not available for tomo in this build");
+        Context& c = seam_ctx(AIO_TOMO_EXT, iGpu);
+        c.P.sloth = sloth;
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
+        c.tomo_adjoint(model, 0, extReflectivity, 1, &s, AIO_MEM_HOST);
+    });
+}
+
+AIO_API int aio_initWemvaExtGpu(float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad,
+                                int blockSize, float alphaCos, int nExt, int leg1, int leg2, int nGpu, int iGpuId,
+                                int iGpuAlloc) {
+    (void)blockSize; (void)iGpuAlloc;
+    return guard([&] {
+        seam_init(AIO_WEMVA_EXT, dz, dx, nz, nx, nts, dts, sub, minPad, alphaCos, nExt, leg1, leg2, nGpu, iGpuId);
+    });
+}
+AIO_API int aio_allocateWemvaExtShotsGpu(float* vel2Dtw2, float* reflectivityScale, int iGpu, int iGpuId) {
+    return guard([&] { seam_allocate(AIO_WEMVA_EXT, vel2Dtw2, reflectivityScale, iGpu, iGpuId); });
+}
+AIO_API int aio_deallocateWemvaExtShotsGpu(int iGpu, int iGpuId) {
+    (void)iGpuId;
+    return guard([&] { seam_deallocate(AIO_WEMVA_EXT, iGpu); });
+}
+AIO_API int aio_wemvaTimeShotsFwdGpu(float* model, float* wemvaExtImage, float* sourcesSignals, int* sp, int ns,
+                                     float* wemvaDataRegDts, int* rp, int nr, float* w0, float* w1, float* w2,
+                                     int iGpu, int iGpuId, int saveWavefield) {
+    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    return guard([&] {
+        require(saveWavefield == 0, "saveWavefield=1 is not available for WEMVA in this build");
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, nullptr);
+        s.wemvaData = wemvaDataRegDts;
+        seam_ctx(AIO_WEMVA_EXT, iGpu).wemva_forward(model, wemvaExtImage, 0, 1, &s, AIO_MEM_HOST);
+    });
+}
+AIO_API int aio_wemvaTimeShotsAdjGpu(float* model, float* wemvaExtImage, float* sourcesSignals, int* sp, int ns,
+                                     float* wemvaDataRegDts, int* rp, int nr, float* w0, float* w1, float* w2,
+                                     int iGpu, int iGpuId, int saveWavefield) {
+    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    return guard([&] {
+        require(saveWavefield == 0, "saveWavefield=1 is not available for WEMVA in this build");
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, nullptr);
+        s.wemvaData = wemvaDataRegDts;
+        seam_ctx(AIO_WEMVA_EXT, iGpu).wemva_adjoint(model, 0, wemvaExtImage, 1, &s, AIO_MEM_HOST);
+    });
+}

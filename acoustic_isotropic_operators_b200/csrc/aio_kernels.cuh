@@ -1,0 +1,278 @@
+// Device kernels of the B200 acoustic-isotropic engine.
+//
+// One fused kernel advances every shot of a batch by one fine time step
+// (gridDim.z = shot): 10th-order stencil, damping of both time levels, sparse
+// source/data injection, dense secondary-source injection, sparse receiver /
+// source recording and fine->coarse accumulation all happen in the same pass
+// over the grid. The reference runs each of these as a separate launch
+// (F/src/kernelsGpu.cu:88-239,513-610) per step and per shot.
+//
+// Damping of the current level. The reference damps both p_new and p_cur after
+// every step (dampCosineEdge, F/src/kernelsGpu.cu:202-219); the damped p_cur is
+// only ever used again point-wise as next step's p_old. The stepper therefore
+// stores each level once (damped once) and applies the second damping factor
+// when it reads p_old, which produces the same values with one store per point.
+#pragma once
+#include "aio_common.cuh"
+
+namespace aio {
+
+__device__ __forceinline__ float v2_scaled(float v, const float* __restrict__ v2, const Geom& g, int z, int x) {
+    // v is zero outside the interior (FAT ring / padding never written).
+    if (z >= 0 && z < g.nzi && x >= 0 && x < g.nxi) v *= __ldg(v2 + (long long)x * g.ip + z);
+    return v;
+}
+
+// ADJ=false: n = v2*L(c) + 2c - D*o    (stepFwdGpu,  F/src/kernelsGpu.cu:513-552)
+// ADJ=true : n = L(v2*c) + 2c - D*o    (stepAdjGpu,  F/src/kernelsGpu.cu:574-610)
+// then      S = D * (n + injection), written over o.
+// INJ: 0 none, 1 sparse traces (injectSource / interpInjectData, :88-99),
+//      2 dense secondary source ssA*hA + ssB*hB (injectSecondarySource, :102-107).
+// REC: sparse recording of S (recordInterpData / recordSource, :113-127).
+// ACC: accA += S*hA, accB += S*hB (interpWavefield / extractInterpAdjointWavefield /
+//      interpFineToCoarseSlice, :132-182).
+template <bool ADJ, int INJ, bool REC, bool ACC>
+__global__ void __launch_bounds__(TZ* TY) k_step(const StepArgs a) {
+    __shared__ float s[TX + 2 * FAT][TZ + 2 * FAT];
+    const Geom& g = a.g;
+    const ShotDesc& sd = a.shots[blockIdx.z];
+    const int lane = threadIdx.x, ty = threadIdx.y;
+    const int z0 = blockIdx.x * TZ, x0 = blockIdx.y * TX;
+    const float* __restrict__ cur = sd.p[a.parity];
+    float* __restrict__ old = sd.p[a.parity ^ 1];
+
+    // Stage the current level (times v^2 dtw^2 for the adjoint) with its halo.
+    for (int r = ty; r < TX + 2 * FAT; r += TY) {
+        const int x = x0 - FAT + r;
+        const float* col = cur + (long long)(x + FAT) * g.hp + ZOFF;
+        float v = col[z0 + lane];
+        if (ADJ) v = v2_scaled(v, a.v2, g, z0 + lane, x);
+        s[r][FAT + lane] = v;
+        if (lane < 2 * FAT) {
+            const int zz = lane < FAT ? z0 - FAT + lane : z0 + TZ + (lane - FAT);
+            float hv = col[zz];
+            if (ADJ) hv = v2_scaled(hv, a.v2, g, zz, x);
+            s[r][lane < FAT ? lane : TZ + lane] = hv;
+        }
+    }
+    __syncthreads();
+
+    const int zi = z0 + lane;
+    const int xb = x0 + ty * PX;
+    float inj[PX];
+#pragma unroll
+    for (int j = 0; j < PX; j++) inj[j] = 0.f;
+
+    const int tile = blockIdx.y * gridDim.x + blockIdx.x;
+    if (INJ == 1 && sd.inj.tileStart) {
+        const int b = sd.inj.tileStart[tile], e = sd.inj.tileStart[tile + 1];
+        for (int k = b; k < e; k++) {
+            const int2 en = sd.inj.ent[k];
+            const int lz = en.x & (TZ - 1), lx = en.x / TZ;
+            if (lz == lane && (lx / PX) == ty) {
+                const float* tr = sd.injSig + (long long)en.y * sd.injLd;
+                float v = a.injTB >= 0 ? tr[a.injTA] * a.injCA + tr[a.injTB] * a.injCB : tr[a.injTA];
+#pragma unroll
+                for (int j = 0; j < PX; j++)
+                    if (j == (lx % PX)) inj[j] += v;
+            }
+        }
+    }
+
+    const float* __restrict__ ssA = (INJ == 2) ? sd.ss + a.ssOffA : nullptr;
+    const float* __restrict__ ssB = (INJ == 2) ? sd.ss + a.ssOffB : nullptr;
+    float* __restrict__ accA = ACC ? sd.acc + a.accOffA : nullptr;
+    float* __restrict__ accB = ACC ? sd.acc + a.accOffB : nullptr;
+
+    float w[PX + 2 * FAT];
+#pragma unroll
+    for (int k = 0; k < PX + 2 * FAT; k++) w[k] = s[ty * PX + k][FAT + lane];
+
+    const int dzd = min(zi, g.nzi - 1 - zi);
+    float S[PX];
+#pragma unroll
+    for (int j = 0; j < PX; j++) {
+        const int xi = xb + j;
+        const float* row = s[FAT + ty * PX + j];
+        const float c = w[FAT + j];
+        const float lap = a.c.zc[0] * c + a.c.zc[1] * (row[FAT + lane - 1] + row[FAT + lane + 1]) +
+                          a.c.zc[2] * (row[FAT + lane - 2] + row[FAT + lane + 2]) +
+                          a.c.zc[3] * (row[FAT + lane - 3] + row[FAT + lane + 3]) +
+                          a.c.zc[4] * (row[FAT + lane - 4] + row[FAT + lane + 4]) +
+                          a.c.zc[5] * (row[FAT + lane - 5] + row[FAT + lane + 5]) + a.c.xc[0] * c +
+                          a.c.xc[1] * (w[FAT + j + 1] + w[FAT + j - 1]) +
+                          a.c.xc[2] * (w[FAT + j + 2] + w[FAT + j - 2]) +
+                          a.c.xc[3] * (w[FAT + j + 3] + w[FAT + j - 3]) +
+                          a.c.xc[4] * (w[FAT + j + 4] + w[FAT + j - 4]) +
+                          a.c.xc[5] * (w[FAT + j + 5] + w[FAT + j - 5]);
+        S[j] = 0.f;
+        if (zi < g.nzi && xi < g.nxi) {
+            const long long hidx = (long long)(xi + FAT) * g.hp + ZOFF + zi;
+            const long long iidx = (long long)xi * g.ip + zi;
+            const int d = min(dzd, min(xi, g.nxi - 1 - xi));
+            const float D = d < g.minPad ? __ldg(a.taper + d) : 1.f;
+            const float o = D * old[hidx];
+            float n;
+            if (ADJ) {
+                const float cr = cur[hidx];
+                n = lap + cr + cr - o;
+            } else {
+                n = __ldg(a.v2 + iidx) * lap + c + c - o;
+            }
+            if (INJ == 1) n = n + inj[j];
+            if (INJ == 2) n = n + (ssA[iidx] * a.hInjA + ssB[iidx] * a.hInjB);
+            const float sv = n * D;
+            S[j] = sv;
+            old[hidx] = sv;
+            if (ACC) {
+                accA[iidx] += sv * a.hAccA;
+                accB[iidx] += sv * a.hAccB;
+            }
+        }
+    }
+
+    if (REC && sd.rec.tileStart) {
+        const int b = sd.rec.tileStart[tile], e = sd.rec.tileStart[tile + 1];
+        for (int k = b; k < e; k++) {
+            const int2 en = sd.rec.ent[k];
+            const int lz = en.x & (TZ - 1), lx = en.x / TZ;
+            if (lz == lane && (lx / PX) == ty) {
+                float v = 0.f;
+#pragma unroll
+                for (int j = 0; j < PX; j++)
+                    if (j == (lx % PX)) v = S[j];
+                float* tr = sd.recSig + (long long)en.y * sd.recLd;
+                tr[a.recTA] += v * a.recCA;
+                if (a.recTB >= 0) tr[a.recTB] += v * a.recCB;
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Coarse-time kernels on interior slices. blockIdx.y = shot; `*St` are per-shot
+// strides in floats (0 for arrays shared by every shot of the batch). Slices
+// are swept whole (padding lanes are zero in every operand).
+// ----------------------------------------------------------------------------
+#define AIO_GRID_STRIDE(i, n) \
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
+
+// imagingFwdGpu (F/src/kernelsGpu.cu:309-316): ss = m * W.
+__global__ void k_img_fwd(float* ss, long long ssSt, const float* m, long long mSt, const float* W, long long WSt,
+                          long long n) {
+    const int b = blockIdx.y;
+    ss += b * ssSt; m += b * mSt; W += b * WSt;
+    AIO_GRID_STRIDE(i, n) ss[i] = m[i] * W[i];
+}
+
+// imagingAdjGpu (F/src/kernelsGpu.cu:318-325): m += W * r; optionally r = 0 afterwards.
+template <typename Acc>
+__global__ void k_img_adj(Acc* m, long long mSt, float* r, long long rSt, const float* W, long long WSt, long long n,
+                          int zeroR) {
+    const int b = blockIdx.y;
+    m += b * mSt; r += b * rSt; W += b * WSt;
+    AIO_GRID_STRIDE(i, n) {
+        const float rv = r[i];
+        m[i] += (Acc)(W[i] * rv);
+        if (zeroR) r[i] = 0.f;
+    }
+}
+
+// imagingTimeFwdGpu (:337-350): ss += sum_e ext[e] * W[t - 2(e-h)].
+__global__ void k_img_time_fwd(float* ss, long long ssSt, const float* ext, long long extSt, const float* W,
+                               long long WSt, long long isz, int t, int e0, int e1, int hExt) {
+    const int b = blockIdx.y;
+    ss += b * ssSt; ext += b * extSt; W += b * WSt;
+    AIO_GRID_STRIDE(i, isz) {
+        float acc = ss[i];
+        for (int e = e0; e < e1; e++) acc += ext[(long long)e * isz + i] * W[(long long)(t - 2 * (e - hExt)) * isz + i];
+        ss[i] = acc;
+    }
+}
+
+// imagingTimeTomoAdjGpu (:445-458): ss += sum_e ext[e] * R[t + 2(e-h)].
+__global__ void k_img_time_tomo_adj(float* ss, long long ssSt, const float* ext, long long extSt, const float* R,
+                                    long long RSt, long long isz, int t, int e0, int e1, int hExt) {
+    const int b = blockIdx.y;
+    ss += b * ssSt; ext += b * extSt; R += b * RSt;
+    AIO_GRID_STRIDE(i, isz) {
+        float acc = ss[i];
+        for (int e = e0; e < e1; e++) acc += ext[(long long)e * isz + i] * R[(long long)(t + 2 * (e - hExt)) * isz + i];
+        ss[i] = acc;
+    }
+}
+
+// imagingTimeAdjGpu (:352-364): m[e] += r * W[t - 2(e-h)]; sign=-1 gives
+// imagingWemvaTimeAdjGpu (:366-378): m[e] += r * W[t + 2(e-h)]. Optionally r = 0.
+template <typename Acc>
+__global__ void k_img_time_adj(Acc* m, long long mSt, float* r, long long rSt, const float* W, long long WSt,
+                               long long isz, int t, int e0, int e1, int hExt, int sign, int zeroR) {
+    const int b = blockIdx.y;
+    m += b * mSt; r += b * rSt; W += b * WSt;
+    AIO_GRID_STRIDE(i, isz) {
+        const float rv = r[i];
+        for (int e = e0; e < e1; e++)
+            m[(long long)e * isz + i] += (Acc)(rv * W[(long long)(t - sign * 2 * (e - hExt)) * isz + i]);
+        if (zeroR) r[i] = 0.f;
+    }
+}
+
+// Scalings (F/src/kernelsGpu.cu:246-252, 278-303). mode 0: m *= v2*rs;
+// mode 1: m *= rs*v2 (extended); mode 2: m = -(m*v2) (sloth).
+__global__ void k_scale(float* m, long long mSt, int nSlices, const float* v2, const float* rs, long long isz,
+                        int mode) {
+    const int b = blockIdx.y;
+    m += b * mSt;
+    const long long n = (long long)nSlices * isz;
+    AIO_GRID_STRIDE(k, n) {
+        const long long i = k % isz;
+        const float v = v2[i], r = rs[i];
+        if (mode == 0) m[k] *= v * r;
+        else if (mode == 1) m[k] *= r * v;
+        else m[k] = -(m[k] * v);
+    }
+}
+
+// Coarse second time derivative in place along the slice stack, zero outside
+// [0, nts): srcWfldSecondTimeDerivative (F/src/kernelsGpu.cu:188-197) applied at
+// every coarse sample as computeTomoSrcWfldDt2 does (F/src/tomoExtShotsGpuFunctions.cu:1251-1361).
+__global__ void k_dt2(float* W, long long WSt, long long isz, int nts, float cSide, float cCenter) {
+    const int b = blockIdx.y;
+    W += b * WSt;
+    AIO_GRID_STRIDE(i, isz) {
+        float prev = 0.f, c = W[i];
+        for (int t = 0; t < nts; t++) {
+            const float nx = (t + 1 < nts) ? W[(long long)(t + 1) * isz + i] : 0.f;
+            W[(long long)t * isz + i] = cSide * (prev + nx) + cCenter * c;
+            prev = c;
+            c = nx;
+        }
+    }
+}
+
+// Sum of per-shot images into one output: out[i] (+)= sum_b in[b][i].
+template <typename Acc>
+__global__ void k_sum_shots(float* out, const Acc* in, long long inSt, int nShots, long long n, int add) {
+    AIO_GRID_STRIDE(i, n) {
+        Acc s = 0;
+        for (int b = 0; b < nShots; b++) s += in[b * inSt + i];
+        out[i] = add ? out[i] + (float)s : (float)s;
+    }
+}
+
+// FP64 -> FP32 with scaling for per-shot images kept in FP64.
+__global__ void k_scale_d(double* m, long long mSt, int nSlices, const float* v2, const float* rs, long long isz,
+                          int mode) {
+    const int b = blockIdx.y;
+    m += b * mSt;
+    const long long n = (long long)nSlices * isz;
+    AIO_GRID_STRIDE(k, n) {
+        const long long i = k % isz;
+        const double v = v2[i], r = rs[i];
+        if (mode == 0) m[k] *= (double)(float)(v * r);
+        else if (mode == 1) m[k] *= (double)(float)(r * v);
+        else m[k] = -(m[k] * v);
+    }
+}
+
+}  // namespace aio

@@ -1,0 +1,188 @@
+/*
+ * aio_b200.h — C ABI of the B200 (sm_100a) acoustic isotropic operators.
+ *
+ * Two layers, both plain C (pointers, sizes, int status codes; 0 = success):
+ *
+ *  1. Reference seam. Drop-in replacements for the free functions the
+ *     reference's per-shot operators call (F/include/*ShotsGpuFunctions.h,
+ *     F = acoustic_iso_lib/acoustic_iso_float), same argument lists, prefixed
+ *     `aio_`, returning a status instead of throwing / exit(-1). Each family
+ *     keeps its own state per iGpu slot, so the families are re-entrant with
+ *     respect to one another (the reference shares one set of globals).
+ *
+ *  2. Batched API. An `aio_context` holds one operator instance (one grid,
+ *     velocity and device). Every call takes a whole batch of shots and runs
+ *     them together: one fused stepper launch advances every shot of a wave by
+ *     one fine step. `memSpace` says whether the per-shot trace / model arrays
+ *     are host (AIO_MEM_HOST) or device (AIO_MEM_DEVICE) pointers; device
+ *     position arrays are always host arrays.
+ *
+ * Conventions (identical to the reference): slices are nz*nx floats with z
+ * fastest (index ix*nz+iz, FAT=5 ring included); device positions are such
+ * linear indices ("regular" grid points, unique per list); traces are
+ * [nDevice][nt] with time fastest; fine time has ntw=(nts-1)*sub+1 samples.
+ * Source / receiver positions must lie inside the interior
+ * [5,nz-5) x [5,nx-5); other positions return AIO_ERR_ARGUMENT.
+ */
+#ifndef AIO_B200_H
+#define AIO_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AIO_OK 0
+#define AIO_ERR_ARGUMENT 1   /* invalid parameter / geometry (reference: std::runtime_error) */
+#define AIO_ERR_CUDA 2       /* CUDA runtime error (reference: exit(-1)) */
+#define AIO_ERR_MEMORY 3     /* device allocation failed */
+#define AIO_ERR_STATE 4      /* call order (e.g. shot call before allocate) */
+
+#define AIO_MEM_HOST 0
+#define AIO_MEM_DEVICE 1
+
+#define AIO_NONLINEAR 0
+#define AIO_BORN 1
+#define AIO_BORN_EXT 2
+#define AIO_TOMO_EXT 3
+#define AIO_WEMVA_EXT 4
+
+#define AIO_WFLD_FP32 0  /* stored source wavefield in FP32 (reference behaviour) */
+#define AIO_WFLD_BF16 1  /* BF16 with a per-time-slice FP32 scale */
+#define AIO_WFLD_FP16 2  /* FP16 with a per-time-slice FP32 scale */
+
+typedef struct aio_context aio_context;
+
+typedef struct {
+    int nz, nx;          /* padded grid including FAT (reference par nz, nx) */
+    int nts, sub;        /* coarse samples, fine sub-steps per coarse step */
+    int minPad;          /* sponge width, min(zPad, xPad) (F/src/fdParam.cpp:93) */
+    int nExt;            /* extension length (odd), 1 for non-extended operators */
+    float dz, dx, dts;   /* spacings (m) and coarse sampling (s) */
+    float alphaCos;      /* taper floor, reference default 0.99 */
+    int leg1, leg2;      /* tomo / WEMVA legs (reference par leg1, leg2) */
+    int sloth;           /* extended Born / tomo: slowness-squared perturbation */
+    int wavefieldPrecision;  /* AIO_WFLD_* for the stored source wavefield */
+    int imageFp64;       /* 1: accumulate imaging conditions in FP64 on the GPU */
+    int device;          /* CUDA device ordinal */
+    long long memBudgetBytes; /* cap on device memory for shot buffers; 0 = 90% of free */
+} aio_params;
+
+typedef struct {
+    const int* sourcesPositionReg;   /* host array, nSourcesReg */
+    int nSourcesReg;
+    const int* receiversPositionReg; /* host array, nReceiversReg */
+    int nReceiversReg;
+    const float* sourcesSignals;     /* [nSourcesReg][ntw]: Born-family d2/dt2-scaled-interpolated
+                                        wavelet; nonlinear forward: the model traces */
+    float* data;                     /* [nReceiversReg][nts]: output (forward) / input (adjoint) */
+    const float* wemvaData;          /* WEMVA only: [nReceiversReg][nts] data driving the receiver wavefield */
+    float* sourcesOut;               /* nonlinear adjoint only: [nSourcesReg][ntw] output traces */
+} aio_shot;
+
+/* ---------------------------------------------------------------- batched API */
+int aio_context_create(const aio_params* params, const float* vel2Dtw2, const float* reflectivityScale,
+                       aio_context** out);
+int aio_context_destroy(aio_context* ctx);
+/* Replace the velocity-derived fields (reference setVel + fdParam precompute). */
+int aio_context_set_velocity(aio_context* ctx, const float* vel2Dtw2, const float* reflectivityScale);
+/* Maximum number of shots one wave can hold for operator `family` under the memory budget. */
+int aio_context_wave_capacity(aio_context* ctx, int family);
+/* Number of stepper launches issued by the most recent operator call. */
+long long aio_context_last_launches(aio_context* ctx);
+const char* aio_last_error(void);
+
+/* Nonlinear: model = source traces (sourcesSignals), data per shot. */
+int aio_nonlinear_forward(aio_context* ctx, int nShots, const aio_shot* shots, int memSpace);
+int aio_nonlinear_adjoint(aio_context* ctx, int nShots, const aio_shot* shots, int memSpace);
+/* Born: model nz*nx (shared by all shots). adjoint: add=0 overwrites, add=1 accumulates. */
+int aio_born_forward(aio_context* ctx, const float* model, int nShots, const aio_shot* shots, int memSpace);
+int aio_born_adjoint(aio_context* ctx, float* model, int add, int nShots, const aio_shot* shots, int memSpace);
+/* Extended (time-lag) Born: model nExt*nz*nx. */
+int aio_born_ext_forward(aio_context* ctx, const float* model, int nShots, const aio_shot* shots, int memSpace);
+int aio_born_ext_adjoint(aio_context* ctx, float* model, int add, int nShots, const aio_shot* shots, int memSpace);
+/* Extended tomo: model nz*nx, background extended reflectivity nExt*nz*nx. */
+int aio_tomo_ext_forward(aio_context* ctx, const float* model, const float* extReflectivity, int nShots,
+                         const aio_shot* shots, int memSpace);
+int aio_tomo_ext_adjoint(aio_context* ctx, float* model, int add, const float* extReflectivity, int nShots,
+                         const aio_shot* shots, int memSpace);
+/* Extended WEMVA: model nz*nx, data = extended image nExt*nz*nx. */
+int aio_wemva_ext_forward(aio_context* ctx, const float* model, float* image, int add, int nShots,
+                          const aio_shot* shots, int memSpace);
+int aio_wemva_ext_adjoint(aio_context* ctx, float* model, int add, const float* image, int nShots,
+                          const aio_shot* shots, int memSpace);
+
+/* -------------------------------------------------------------- reference seam
+ * Each replaces the reference function of the same name without the prefix;
+ * blockSize is accepted and ignored (the reference requires 16; tiles here are
+ * fixed by the kernels). nGpu / iGpuAlloc are accepted for signature parity.
+ */
+/* F/include/nonlinearShotsGpuFunctions.h:7-24 */
+int aio_initNonlinearGpu(float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad, int blockSize,
+                         float alphaCos, int nGpu, int iGpuId, int iGpuAlloc);
+int aio_allocateNonlinearGpu(float* vel2Dtw2, int iGpu, int iGpuId);
+int aio_deallocateNonlinearGpu(int iGpu, int iGpuId);
+int aio_propShotsFwdGpu(float* modelRegDtw, float* dataRegDts, int* sourcesPositionReg, int nSourcesReg,
+                        int* receiversPositionReg, int nReceiversReg, float* wavefieldDts, int iGpu, int iGpuId);
+int aio_propShotsFwdGpuWavefield(float* modelRegDtw, float* dataRegDts, int* sourcesPositionReg, int nSourcesReg,
+                                 int* receiversPositionReg, int nReceiversReg, float* wavefieldDts, int iGpu,
+                                 int iGpuId);
+int aio_propShotsAdjGpu(float* modelRegDtw, float* dataRegDts, int* sourcesPositionReg, int nSourcesReg,
+                        int* receiversPositionReg, int nReceiversReg, float* wavefieldDts, int iGpu, int iGpuId);
+int aio_propShotsAdjGpuWavefield(float* modelRegDtw, float* dataRegDts, int* sourcesPositionReg, int nSourcesReg,
+                                 int* receiversPositionReg, int nReceiversReg, float* wavefieldDts, int iGpu,
+                                 int iGpuId);
+/* F/include/BornShotsGpuFunctions.h:7-33 */
+int aio_initBornGpu(float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad, int blockSize,
+                    float alphaCos, int nGpu, int iGpuId, int iGpuAlloc);
+int aio_allocateBornShotsGpu(float* vel2Dtw2, float* reflectivityScale, int iGpu, int iGpuId);
+int aio_deallocateBornShotsGpu(int iGpu, int iGpuId);
+int aio_BornShotsFwdGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                        int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
+                        float* scatWavefield, int iGpu, int iGpuId);
+int aio_BornShotsAdjGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                        int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
+                        float* recWavefield, int iGpu, int iGpuId);
+/* F/include/BornExtShotsGpuFunctions.h:6-54 (time-lag extension) */
+int aio_initBornExtGpu(float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad, int blockSize,
+                       float alphaCos, int nExt, int nGpu, int iGpuId, int iGpuAlloc);
+int aio_allocateBornExtShotsGpu(float* vel2Dtw2, float* reflectivityScale, int iGpu, int iGpuId);
+int aio_deallocateBornExtShotsGpu(int iGpu, int iGpuId);
+int aio_BornTimeShotsFwdGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                            int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
+                            float* scatWavefield, int sloth, int iGpu, int iGpuId);
+int aio_BornTimeShotsAdjGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                            int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
+                            float* recWavefield, int sloth, int iGpu, int iGpuId);
+/* F/include/tomoExtShotsGpuFunctions.h:6-33 (time-lag extension) */
+int aio_initTomoExtGpu(float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad, int blockSize,
+                       float alphaCos, int nExt, int leg1, int leg2, int nGpu, int iGpuId, int iGpuAlloc);
+int aio_allocateTomoExtShotsGpu(float* vel2Dtw2, float* reflectivityScale, int iGpu, int iGpuId);
+int aio_deallocateTomoExtShotsGpu(int iGpu, int iGpuId);
+int aio_tomoTimeShotsFwdGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
+                            int* sourcesPositionReg, int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
+                            float* tomoSrcWavefieldDt2, float* tomoSecWavefield1, float* tomoSecWavefield2,
+                            int sloth, int iGpu, int iGpuId, int saveWavefield);
+int aio_tomoTimeShotsAdjGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
+                            int* sourcesPositionReg, int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
+                            float* tomoSrcWavefieldDt2, float* tomoSecWavefield1, float* tomoSecWavefield2,
+                            int sloth, int iGpu, int iGpuId, int saveWavefield);
+/* F/include/wemvaExtShotsGpuFunctions.h:6-17 (time-lag extension) */
+int aio_initWemvaExtGpu(float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad, int blockSize,
+                        float alphaCos, int nExt, int leg1, int leg2, int nGpu, int iGpuId, int iGpuAlloc);
+int aio_allocateWemvaExtShotsGpu(float* vel2Dtw2, float* reflectivityScale, int iGpu, int iGpuId);
+int aio_deallocateWemvaExtShotsGpu(int iGpu, int iGpuId);
+int aio_wemvaTimeShotsFwdGpu(float* model, float* wemvaExtImage, float* sourcesSignals, int* sourcesPositionReg,
+                             int nSourcesReg, float* wemvaDataRegDts, int* receiversPositionReg, int nReceiversReg,
+                             float* wemvaSrcWavefieldDt2, float* wemvaSecWavefield1, float* wemvaSecWavefield2,
+                             int iGpu, int iGpuId, int saveWavefield);
+int aio_wemvaTimeShotsAdjGpu(float* model, float* wemvaExtImage, float* sourcesSignals, int* sourcesPositionReg,
+                             int nSourcesReg, float* wemvaDataRegDts, int* receiversPositionReg, int nReceiversReg,
+                             float* wemvaSrcWavefieldDt2, float* wemvaSecWavefield1, float* wemvaSecWavefield2,
+                             int iGpu, int iGpuId, int saveWavefield);
+/* F/src/nonlinearShotsGpuFunctions.cu:18-84: validates a GPU id list (info printing dropped). */
+int aio_getGpuInfo(const int* gpuList, int nGpuList, int info, int deviceNumberInfo);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AIO_B200_H */

@@ -1,0 +1,204 @@
+"""ctypes binding of the CPU oracle (oracle/aio_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py as the checker. The product path never uses it.
+
+Every function works at the reference's regular-grid seam: slices are
+(nx, nz) float arrays with z fastest (the reference's ``index = ix*nz + iz``),
+traces are (nDevice, nt) with time fastest, device positions are linear grid
+indices. ``dtype`` selects the FP32 restatement (float32) or the FP64 one
+(float64, the reference's acoustic_iso_double scheme).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+class OrcParams(C.Structure):
+    _fields_ = [("nz", C.c_int), ("nx", C.c_int), ("nts", C.c_int), ("sub", C.c_int),
+                ("minPad", C.c_int), ("nExt", C.c_int), ("dz", C.c_double), ("dx", C.c_double),
+                ("dts", C.c_double), ("alphaCos", C.c_double)]
+
+
+def build() -> str:
+    """Compile liboracle.so with g++ (no GPU needed)."""
+    subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so"])
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = C.CDLL(_LIB_PATH)
+    return _lib
+
+
+@dataclass
+class Scheme:
+    """Grid and time parameters of one operator instance (reference par keys)."""
+    nz: int
+    nx: int
+    nts: int
+    dts: float
+    sub: int
+    dz: float
+    dx: float
+    minPad: int
+    alphaCos: float = 0.99
+    nExt: int = 1
+
+    @property
+    def ntw(self) -> int:
+        return (self.nts - 1) * self.sub + 1
+
+    def c(self) -> OrcParams:
+        return OrcParams(self.nz, self.nx, self.nts, self.sub, self.minPad, self.nExt,
+                         self.dz, self.dx, self.dts, self.alphaCos)
+
+
+def _suf(dtype) -> str:
+    return "f64" if np.dtype(dtype) == np.float64 else "f32"
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _ip(a):
+    return np.ascontiguousarray(a, dtype=np.int32).ctypes.data_as(C.c_void_p)
+
+
+def _arr(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def constants(s: Scheme, vel, dtype=np.float64):
+    vel = _arr(vel, dtype)
+    zc = np.zeros(6, dtype); xc = np.zeros(6, dtype)
+    h = np.zeros(2 * (s.sub + 1), dtype); taper = np.zeros(max(s.minPad, 1), dtype)
+    v2 = np.zeros_like(vel); rs = np.zeros_like(vel)
+    getattr(lib(), "orc_constants_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(zc), _p(xc), _p(h), _p(taper),
+                                                   _p(v2), _p(rs))
+    return dict(zc=zc, xc=xc, h=h, taper=taper[: s.minPad], v2=v2, rs=rs)
+
+
+def nl_fwd(s, vel, model_dtw, src_pos, rec_pos, dtype=np.float64, wavefield=False):
+    vel = _arr(vel, dtype); m = _arr(model_dtw, dtype)
+    nr = len(rec_pos)
+    d = np.zeros((nr, s.nts), dtype)
+    W = np.zeros((s.nts, s.nx, s.nz), dtype) if wavefield else None
+    getattr(lib(), "orc_nl_fwd_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _ip(src_pos), len(src_pos),
+                                                _ip(rec_pos), nr, _p(d), _p(W) if W is not None else None)
+    return (d, W) if wavefield else d
+
+
+def nl_adj(s, vel, data, src_pos, rec_pos, dtype=np.float64, wavefield=False):
+    vel = _arr(vel, dtype); d = _arr(data, dtype)
+    m = np.zeros((len(src_pos), s.ntw), dtype)
+    W = np.zeros((s.nts, s.nx, s.nz), dtype) if wavefield else None
+    getattr(lib(), "orc_nl_adj_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _ip(src_pos), len(src_pos),
+                                                _ip(rec_pos), len(rec_pos), _p(d), _p(W) if W is not None else None)
+    return (m, W) if wavefield else m
+
+
+def born_fwd(s, vel, model, sig_dtw, src_pos, rec_pos, dtype=np.float64, wavefield=False):
+    vel = _arr(vel, dtype); m = _arr(model, dtype); sig = _arr(sig_dtw, dtype)
+    d = np.zeros((len(rec_pos), s.nts), dtype)
+    W = np.zeros((s.nts, s.nx, s.nz), dtype) if wavefield else None
+    getattr(lib(), "orc_born_fwd_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(sig), _ip(src_pos),
+                                                  len(src_pos), _ip(rec_pos), len(rec_pos), _p(d),
+                                                  _p(W) if W is not None else None)
+    return (d, W) if wavefield else d
+
+
+def born_adj(s, vel, data, sig_dtw, src_pos, rec_pos, dtype=np.float64, wavefield=False):
+    vel = _arr(vel, dtype); d = _arr(data, dtype); sig = _arr(sig_dtw, dtype)
+    m = np.zeros((s.nx, s.nz), dtype)
+    W = np.zeros((s.nts, s.nx, s.nz), dtype) if wavefield else None
+    getattr(lib(), "orc_born_adj_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(sig), _ip(src_pos),
+                                                  len(src_pos), _ip(rec_pos), len(rec_pos), _p(d),
+                                                  _p(W) if W is not None else None)
+    return (m, W) if wavefield else m
+
+
+def bornext_fwd(s, vel, model_ext, sig_dtw, src_pos, rec_pos, dtype=np.float64, sloth=0):
+    vel = _arr(vel, dtype); m = _arr(model_ext, dtype); sig = _arr(sig_dtw, dtype)
+    d = np.zeros((len(rec_pos), s.nts), dtype)
+    getattr(lib(), "orc_bornext_fwd_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(sig), _ip(src_pos),
+                                                     len(src_pos), _ip(rec_pos), len(rec_pos), _p(d), sloth)
+    return d
+
+
+def bornext_adj(s, vel, data, sig_dtw, src_pos, rec_pos, dtype=np.float64, sloth=0):
+    vel = _arr(vel, dtype); d = _arr(data, dtype); sig = _arr(sig_dtw, dtype)
+    m = np.zeros((s.nExt, s.nx, s.nz), dtype)
+    getattr(lib(), "orc_bornext_adj_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(sig), _ip(src_pos),
+                                                     len(src_pos), _ip(rec_pos), len(rec_pos), _p(d), sloth)
+    return m
+
+
+def tomo_fwd(s, vel, model, ext_refl, sig_dtw, src_pos, rec_pos, dtype=np.float64, sloth=0, leg1=1, leg2=1):
+    vel = _arr(vel, dtype); m = _arr(model, dtype); e = _arr(ext_refl, dtype); sig = _arr(sig_dtw, dtype)
+    d = np.zeros((len(rec_pos), s.nts), dtype)
+    getattr(lib(), "orc_tomo_fwd_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(e), _p(sig), _ip(src_pos),
+                                                  len(src_pos), _ip(rec_pos), len(rec_pos), _p(d), sloth, leg1, leg2)
+    return d
+
+
+def tomo_adj(s, vel, data, ext_refl, sig_dtw, src_pos, rec_pos, dtype=np.float64, sloth=0, leg1=1, leg2=1):
+    vel = _arr(vel, dtype); d = _arr(data, dtype); e = _arr(ext_refl, dtype); sig = _arr(sig_dtw, dtype)
+    m = np.zeros((s.nx, s.nz), dtype)
+    getattr(lib(), "orc_tomo_adj_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(e), _p(sig), _ip(src_pos),
+                                                  len(src_pos), _ip(rec_pos), len(rec_pos), _p(d), sloth, leg1, leg2)
+    return m
+
+
+def wemva_fwd(s, vel, model, sig_dtw, src_pos, rec_pos, rdata, dtype=np.float64, leg1=1, leg2=1):
+    vel = _arr(vel, dtype); m = _arr(model, dtype); sig = _arr(sig_dtw, dtype); r = _arr(rdata, dtype)
+    img = np.zeros((s.nExt, s.nx, s.nz), dtype)
+    getattr(lib(), "orc_wemva_fwd_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(sig), _ip(src_pos),
+                                                   len(src_pos), _ip(rec_pos), len(rec_pos), _p(r), _p(img),
+                                                   leg1, leg2)
+    return img
+
+
+def wemva_adj(s, vel, image, sig_dtw, src_pos, rec_pos, rdata, dtype=np.float64, leg1=1, leg2=1):
+    vel = _arr(vel, dtype); img = _arr(image, dtype); sig = _arr(sig_dtw, dtype); r = _arr(rdata, dtype)
+    m = np.zeros((s.nx, s.nz), dtype)
+    getattr(lib(), "orc_wemva_adj_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(sig), _ip(src_pos),
+                                                   len(src_pos), _ip(rec_pos), len(rec_pos), _p(r), _p(img),
+                                                   leg1, leg2)
+    return m
+
+
+def time_interp_fwd(nts, dts, sub, m, ots=0.0, dtype=np.float64):
+    m = _arr(m, dtype)
+    ntw = (nts - 1) * sub + 1
+    d = np.zeros((m.shape[0], ntw), dtype)
+    getattr(lib(), "orc_time_interp_fwd_" + _suf(dtype))(nts, C.c_double(dts), C.c_double(ots), sub, m.shape[0], _p(m), _p(d))
+    return d
+
+
+def time_interp_adj(nts, dts, sub, d, ots=0.0, dtype=np.float64):
+    d = _arr(d, dtype)
+    m = np.zeros((d.shape[0], nts), dtype)
+    getattr(lib(), "orc_time_interp_adj_" + _suf(dtype))(nts, C.c_double(dts), C.c_double(ots), sub, d.shape[0], _p(m), _p(d))
+    return m
+
+
+def second_deriv(nt, dt, m, dtype=np.float64):
+    m = _arr(m, dtype)
+    d = np.zeros_like(m)
+    getattr(lib(), "orc_second_deriv_" + _suf(dtype))(nt, C.c_double(dt), m.shape[0], _p(m), _p(d))
+    return d
