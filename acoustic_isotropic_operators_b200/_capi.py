@@ -26,11 +26,14 @@ AIO_WFLD_FP32, AIO_WFLD_BF16, AIO_WFLD_FP16 = range(3)
 
 EXPORTED = [
     "aio_last_error", "aio_context_create", "aio_context_destroy", "aio_context_set_velocity",
-    "aio_context_wave_capacity", "aio_context_last_launches",
+    "aio_context_wave_capacity", "aio_context_last_launches", "aio_context_stream", "aio_context_profile",
+    "aio_context_stats", "aio_context_reset_stats",
     "aio_nonlinear_forward", "aio_nonlinear_adjoint", "aio_born_forward", "aio_born_adjoint",
     "aio_born_ext_forward", "aio_born_ext_adjoint", "aio_tomo_ext_forward", "aio_tomo_ext_adjoint",
     "aio_wemva_ext_forward", "aio_wemva_ext_adjoint",
     "aio_getGpuInfo",
+    "aio_fd_precompute", "aio_time_interp_forward", "aio_time_interp_adjoint", "aio_second_time_derivative",
+    "aio_scale_seismic_source", "aio_device_spread", "aio_device_gather", "aio_prepare_source",
     "aio_initNonlinearGpu", "aio_allocateNonlinearGpu", "aio_deallocateNonlinearGpu", "aio_propShotsFwdGpu",
     "aio_propShotsFwdGpuWavefield", "aio_propShotsAdjGpu", "aio_propShotsAdjGpuWavefield",
     "aio_initBornGpu", "aio_allocateBornShotsGpu", "aio_deallocateBornShotsGpu", "aio_BornShotsFwdGpu",
@@ -81,6 +84,8 @@ def lib():
         L.aio_context_last_launches.restype = C.c_longlong
         L.aio_context_last_launches.argtypes = [C.c_void_p]
         L.aio_context_wave_capacity.argtypes = [C.c_void_p, C.c_int]
+        L.aio_context_stream.restype = C.c_void_p
+        L.aio_context_stream.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 

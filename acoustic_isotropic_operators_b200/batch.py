@@ -78,6 +78,42 @@ class Context:
     def capacity(self, family: int) -> int:
         return int(A.lib().aio_context_wave_capacity(self._h, family))
 
+    @property
+    def stream_ptr(self) -> int:
+        return int(A.lib().aio_context_stream(self._h) or 0)
+
+    def profile(self, sample_every: int) -> None:
+        A.check(A.lib().aio_context_profile(self._h, int(sample_every)))
+
+    def stats(self):
+        """(kernels launched, timed stepper ms, timed stepper launches, their point-updates) since reset."""
+        k, n = C.c_longlong(), C.c_longlong()
+        ms, pts = C.c_double(), C.c_double()
+        A.check(A.lib().aio_context_stats(self._h, C.byref(k), C.byref(ms), C.byref(n), C.byref(pts)))
+        return int(k.value), float(ms.value), int(n.value), float(pts.value)
+
+    def reset_stats(self) -> None:
+        A.check(A.lib().aio_context_reset_stats(self._h))
+
+    # ------------------------------------------------------ device-resident calls
+    def device_call(self, name: str, *args, shots=None):
+        """Call aio_<name>(ctx, *args, nShots, shots, AIO_MEM_DEVICE) with raw device pointers.
+
+        ``args`` are ctypes values (``ctypes.c_void_p(device_address)``, ``ctypes.c_int``...).
+        ``shots`` is a list of (src_pos, rec_pos, sig_ptr, data_ptr, wemva_ptr, src_out_ptr) with
+        host int32 position arrays and device addresses (ints, 0 for none).
+        """
+        arr = (A.AioShot * len(shots))()
+        keep = []
+        for i, (sp, rp, sig, dat, wd, so) in enumerate(shots):
+            sp = np.ascontiguousarray(sp, np.int32)
+            rp = np.ascontiguousarray(rp, np.int32)
+            keep += [sp, rp]
+            arr[i] = A.AioShot(A.iptr(sp), len(sp), A.iptr(rp), len(rp), sig or None, dat or None, wd or None,
+                               so or None)
+        fn = getattr(A.lib(), "aio_" + name)
+        A.check(fn(self._h, *args, len(shots), arr, A.AIO_MEM_DEVICE))
+
     # ------------------------------------------------------------------ helpers
     def _shots(self, shots: Sequence[Shot], *, data_out: bool, need_sig=True, src_out=False):
         arr = (A.AioShot * len(shots))()

@@ -170,8 +170,17 @@ struct Context {
     // per-wave buffers
     DevMem pbuf, ringb, ssb, wf1, wf2, img, lists, desc, sig, dat, aux, model, ext, outv;
     std::vector<ShotDesc> hdesc;
-    long long launches = 0;
+    long long launches = 0;      // stepper launches of the last operator call
+    long long kernels = 0;       // every kernel launched since the last stats reset
     long long budget = 0;
+    // Live stepper timing: every profEvery-th stepper launch is bracketed by a
+    // pair of CUDA events on the engine stream; pairs are read back at sync().
+    int profEvery = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evFree, evBusy;
+    std::vector<long long> evPoints;   // interior points advanced by each timed launch
+    double stepMs = 0.0;
+    long long stepTimed = 0;
+    double stepPoints = 0.0;
 
     // ------------------------------------------------------------- set-up
     void init(const aio_params& p, const float* vel2Dtw2, const float* reflScale) {
@@ -207,8 +216,16 @@ struct Context {
     }
 
     void destroy() {
+        for (auto& e : evFree) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+        for (auto& e : evBusy) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+        evFree.clear();
+        evBusy.clear();
         if (st) cudaStreamDestroy(st);
         st = nullptr;
+    }
+    void kcheck() {
+        AIO_CK(cudaGetLastError());
+        kernels++;
     }
 
     // full nz*nx (per slice) <-> interior pitched slices
@@ -382,7 +399,38 @@ struct Context {
         return a;
     }
 
+    std::pair<cudaEvent_t, cudaEvent_t> take_events() {
+        if (evFree.empty()) {
+            cudaEvent_t a, b;
+            AIO_CK(cudaEventCreate(&a));
+            AIO_CK(cudaEventCreate(&b));
+            evFree.push_back({a, b});
+        }
+        auto e = evFree.back();
+        evFree.pop_back();
+        return e;
+    }
+    void collect_events() {
+        for (size_t i = 0; i < evBusy.size(); i++) {
+            auto& e = evBusy[i];
+            float ms = 0.f;
+            AIO_CK(cudaEventElapsedTime(&ms, e.first, e.second));
+            stepMs += ms;
+            stepTimed++;
+            stepPoints += (double)evPoints[i];
+            evFree.push_back(e);
+        }
+        evBusy.clear();
+        evPoints.clear();
+    }
+
     void launch(int nb, bool adj, int inj, bool rec, bool acc, const StepArgs& a) {
+        const bool timed = profEvery > 0 && (launches % profEvery) == 0;
+        std::pair<cudaEvent_t, cudaEvent_t> ev{};
+        if (timed) {
+            ev = take_events();
+            AIO_CK(cudaEventRecord(ev.first, st));
+        }
         dim3 grid(g.tilesZ, g.tilesX, nb), block(TZ, TY);
         const int key = (adj ? 1 : 0) | (inj << 1) | ((rec ? 1 : 0) << 3) | ((acc ? 1 : 0) << 4);
         switch (key) {
@@ -398,7 +446,13 @@ struct Context {
             default: throw Error{AIO_ERR_ARGUMENT, "unsupported stepper variant"};
         }
         AIO_CK(cudaGetLastError());
+        if (timed) {
+            AIO_CK(cudaEventRecord(ev.second, st));
+            evBusy.push_back(ev);
+            evPoints.push_back((long long)nb * g.nzi * g.nxi);
+        }
         launches++;
+        kernels++;
     }
 
     float hf(int i) const { return k.h[i]; }
@@ -593,7 +647,7 @@ struct Context {
     void img_fwd(int nb, long long slot, const float* m, long long mSt, const float* W, int t) {
         k_img_fwd<<<ew_grid(nb, g.isz), 256, 0, st>>>(ss_ptr(slot), pairSt(), m, mSt, W + (long long)t * g.isz,
                                                        wfSt(), g.isz);
-        AIO_CK(cudaGetLastError());
+        kcheck();
     }
     // image += W[t] * ring[slot]; ring[slot] = 0  (imagingAdjGpu)
     void img_adj(int nb, long long slot, const float* W, int t) {
@@ -603,7 +657,7 @@ struct Context {
         else
             k_img_adj<float><<<ew_grid(nb, g.isz), 256, 0, st>>>(img.as<float>(), g.isz, ring_ptr(slot), pairSt(),
                                                                  W + (long long)t * g.isz, wfSt(), g.isz, 1);
-        AIO_CK(cudaGetLastError());
+        kcheck();
     }
     // Lag bounds with C truncating division (F/src/BornExtShotsGpuFunctions.cu:366-383;
     // F/src/tomoExtShotsGpuFunctions.cu:2631-2650).
@@ -621,7 +675,7 @@ struct Context {
         bounds_src(t, e0, e1);
         k_img_time_fwd<<<ew_grid(nb, g.isz), 256, 0, st>>>(ss_ptr(slot), pairSt(), ext, 0, W, wfSt(), g.isz, t, e0,
                                                             e1, g.hExt);
-        AIO_CK(cudaGetLastError());
+        kcheck();
     }
     // ss[slot] += sum_e ext[e] R[t+2(e-h)]  (imagingTimeTomoAdjGpu)
     void img_time_tomo_adj(int nb, long long slot, const float* ext, const float* R, int t) {
@@ -629,7 +683,7 @@ struct Context {
         bounds_rec(t, e0, e1);
         k_img_time_tomo_adj<<<ew_grid(nb, g.isz), 256, 0, st>>>(ss_ptr(slot), pairSt(), ext, 0, R, wfSt(), g.isz, t,
                                                                  e0, e1, g.hExt);
-        AIO_CK(cudaGetLastError());
+        kcheck();
     }
     // image[e] += ring[slot] * W[t -/+ 2(e-h)]; ring[slot] = 0
     //   sign=+1: imagingTimeAdjGpu (source side); sign=-1: imagingWemvaTimeAdjGpu.
@@ -644,13 +698,13 @@ struct Context {
         else
             k_img_time_adj<float><<<ew_grid(nb, g.isz), 256, 0, st>>>(img.as<float>(), mSt, ring_ptr(slot), pairSt(),
                                                                       W, wfSt(), g.isz, t, e0, e1, g.hExt, sign, 1);
-        AIO_CK(cudaGetLastError());
+        kcheck();
     }
 
     void scale_shared(float* m, int nSlices, int mode) {
         k_scale<<<ew_grid(1, (long long)nSlices * g.isz), 256, 0, st>>>(m, 0, nSlices, v2.as<float>(), rs.as<float>(),
                                                                          g.isz, mode);
-        AIO_CK(cudaGetLastError());
+        kcheck();
     }
 
     // Scale per-shot images (reference scales each shot's model before the host
@@ -660,15 +714,15 @@ struct Context {
         if (P.imageFp64) {
             k_scale_d<<<ew_grid(nb, n), 256, 0, st>>>(img.as<double>(), n, nSlices, v2.as<float>(), rs.as<float>(),
                                                       g.isz, mode);
-            AIO_CK(cudaGetLastError());
+            kcheck();
             k_sum_shots<double><<<ew_grid(1, n), 256, 0, st>>>(out, img.as<double>(), n, nb, n, add ? 1 : 0);
         } else {
             k_scale<<<ew_grid(nb, n), 256, 0, st>>>(img.as<float>(), n, nSlices, v2.as<float>(), rs.as<float>(), g.isz,
                                                     mode);
-            AIO_CK(cudaGetLastError());
+            kcheck();
             k_sum_shots<float><<<ew_grid(1, n), 256, 0, st>>>(out, img.as<float>(), n, nb, n, add ? 1 : 0);
         }
-        AIO_CK(cudaGetLastError());
+        kcheck();
     }
     void zero_images(int nb, int nSlices) {
         AIO_CK(cudaMemsetAsync(img.p, 0, (size_t)nb * nSlices * g.isz * (P.imageFp64 ? 8 : 4), st));
@@ -690,7 +744,10 @@ struct Context {
         }
         from_interior(dst, outInterior, nSlices, mem);
     }
-    void sync() { AIO_CK(cudaStreamSynchronize(st)); }
+    void sync() {
+        AIO_CK(cudaStreamSynchronize(st));
+        collect_events();
+    }
 
     void begin_call() {
         AIO_CK(cudaSetDevice(dev));
@@ -867,7 +924,7 @@ struct Context {
     void source_wavefield_dt2(int nb, DevMem& W) {
         fwd_sparse_pass(nb, false, &W);
         k_dt2<<<ew_grid(nb, g.isz), 256, 0, st>>>(W.as<float>(), wfSt(), g.isz, g.nts, k.cSide, k.cCenter);
-        AIO_CK(cudaGetLastError());
+        kcheck();
     }
     // Receiver wavefield (computeTomoRecWfld, F/src/tomoExtShotsGpuFunctions.cu:1481-1515).
     void receiver_wavefield(int nb, const std::vector<const float*>& data, DevMem& R) {
@@ -1142,6 +1199,28 @@ AIO_API int aio_context_wave_capacity(aio_context* ctx, int family) {
     return ctx->c.capacity(n, 4, 4096);
 }
 AIO_API long long aio_context_last_launches(aio_context* ctx) { return ctx->c.launches; }
+AIO_API void* aio_context_stream(aio_context* ctx) { return (void*)ctx->c.st; }
+AIO_API int aio_context_profile(aio_context* ctx, int sampleEvery) {
+    return guard([&] {
+        require(sampleEvery >= 0, "sampleEvery must be >= 0");
+        ctx->c.profEvery = sampleEvery;
+    });
+}
+AIO_API int aio_context_stats(aio_context* ctx, long long* kernels, double* stepperMs, long long* stepperTimed,
+                              double* stepperPoints) {
+    if (kernels) *kernels = ctx->c.kernels;
+    if (stepperMs) *stepperMs = ctx->c.stepMs;
+    if (stepperTimed) *stepperTimed = ctx->c.stepTimed;
+    if (stepperPoints) *stepperPoints = ctx->c.stepPoints;
+    return AIO_OK;
+}
+AIO_API int aio_context_reset_stats(aio_context* ctx) {
+    ctx->c.kernels = 0;
+    ctx->c.stepMs = 0.0;
+    ctx->c.stepTimed = 0;
+    ctx->c.stepPoints = 0.0;
+    return AIO_OK;
+}
 
 AIO_API int aio_nonlinear_forward(aio_context* ctx, int nShots, const aio_shot* shots, int memSpace) {
     return guard([&] { ctx->c.nonlinear_forward(nShots, shots, memSpace, nullptr); });

@@ -1,0 +1,318 @@
+#!/usr/bin/env python
+"""Benchmark: batched Born forward + adjoint (400 x 1200 physical grid at 10 m,
+32 shots, nts = 2000 at 4 ms, 15 Hz Ricker, 1200 receivers, smoothed-gradient
+background, 20-interface reflectivity) on the B200 engine.
+
+One step = Born forward of every shot (model -> data) followed by Born adjoint
+of that data (data -> image): 4 propagation passes per shot. The metric is
+grid-point updates per second: interior points x fine steps x 4 passes x shots.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+`value` is measured with inputs resident in HBM (C ABI, device pointers);
+`e2e` is the same metric through the C ABI with host buffers (host<->device
+copies inside the timed region). Under torchrun each rank owns its own 32
+shots (weak scaling) and the images are summed with one NCCL all-reduce.
+`--impl reference` times the reference scheme's CPU implementation (this
+repository's CPU port of it; the reference itself has no CPU path) on a
+bounded sample of the same workload, on all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gpts/s (grid-point updates per second), batched Born forward+adjoint"
+UNIT = "Gpts/s"
+PASSES = 4
+BYTES_PER_POINT = 16  # algorithmic bytes per point update: read p_old, p_cur, v2dtw2; write p_new (FP32)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--shots", type=int, default=32, help="shots per GPU")
+    ap.add_argument("--nts", type=int, default=2000)
+    ap.add_argument("--wavefield", default="fp32", choices=["fp32", "bf16", "fp16"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-nts", type=int, default=0, help="coarse samples of the CPU sample (0 = auto)")
+    return ap.parse_args()
+
+
+def workload(args, nshots):
+    from acoustic_isotropic_operators_b200 import synthetic as S
+    return S.born_workload(nshots=nshots, nts=args.nts)
+
+
+def prepare_signals(w, lib):
+    """Born-family source chain in the product's C++ host code (per shot)."""
+    sigs = []
+    velf = np.ascontiguousarray(w.vel.reshape(-1), np.float32)
+    for a in w.shots:
+        wav = np.repeat(w.wavelet[None, :], a.src_cidx.shape[0], axis=0).astype(np.float32)
+        out = np.zeros((len(a.src_pos), w.ntw), np.float32)
+        rc = lib.aio_prepare_source(1, a.src_cidx.shape[0], a.src_cidx.shape[1],
+                                    a.src_cidx.ctypes.data_as(C.c_void_p), a.src_w.ctypes.data_as(C.c_void_p),
+                                    len(a.src_pos), a.src_pos.ctypes.data_as(C.c_void_p), w.nts, C.c_float(w.dts),
+                                    w.sub, velf.ctypes.data_as(C.c_void_p), wav.ctypes.data_as(C.c_void_p),
+                                    out.ctypes.data_as(C.c_void_p))
+        assert rc == 0
+        sigs.append(out)
+    return sigs
+
+
+class Clocks:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            self.p.wait()
+
+    def summary(self):
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if "Active" in v and "Not" not in v})
+        load = [x for x in sm if x > 0.5 * (max(mx) if mx else 0)] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_sample(w, sigs, nts_sample, threads):
+    """Time the CPU port (FP32 restatement of the reference scheme) on one shot and a
+    shortened time axis of the same grid; returns Gpts/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
+    s = orc.Scheme(nz=w.nz, nx=w.nx, nts=nts_sample, dts=w.dts, sub=w.sub, dz=w.dz, dx=w.dx, minPad=w.minPad)
+    a = w.shots[0]
+    sig = np.ascontiguousarray(sigs[0][:, : s.ntw])
+    t0 = time.perf_counter()
+    d = orc.born_fwd(s, w.vel, w.model, sig, a.src_pos, a.rec_pos, dtype=np.float32)
+    orc.born_adj(s, w.vel, d, sig, a.src_pos, a.rec_pos, dtype=np.float32)
+    dt = time.perf_counter() - t0
+    pts = w.n_interior * (nts_sample - 1) * w.sub * PASSES
+    return pts / dt / 1e9, dt, pts
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    w = workload(args, 1)
+    from acoustic_isotropic_operators_b200 import _capi
+    sigs = prepare_signals(w, _capi.lib())
+    nts_sample = args.cpu_nts or 150
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, dt, pts = cpu_sample(w, sigs, nts_sample, threads)
+        if i >= args.warmup:
+            vals.append((v, dt))
+    value = statistics.mean(v for v, _ in vals)
+    ms = 1000 * statistics.mean(dt for _, dt in vals)
+    sample = (f"1 of {args.shots} shots, Born forward+adjoint, full {w.nz}x{w.nx} grid, "
+              f"nts={nts_sample} of {args.nts} coarse samples ({(nts_sample - 1) * w.sub} fine steps)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_dict(args, w),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def config_dict(args, w):
+    return {"workload": "batched Born forward+adjoint, 400x1200 at 10 m, nts=2000, 15 Hz Ricker",
+            "shots_per_gpu": args.shots, "grid_padded": [w.nz, w.nx],
+            "interior": [w.nz - 10, w.nx - 10], "nts": w.nts, "sub": w.sub, "fine_steps": w.fine_steps,
+            "passes_per_shot": PASSES, "wavefield": args.wavefield, "receivers_per_shot": 1200,
+            "parallelism": f"dp{args.gpus} (shots)", "l2": "inputs larger than L2 (5.4 GB wavefield per shot)"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from acoustic_isotropic_operators_b200 import _capi
+    from acoustic_isotropic_operators_b200.batch import Context
+    from acoustic_isotropic_operators_b200 import synthetic as S
+
+    full = workload(args, args.shots * world)
+    mine = full.shots[rank::world]
+    w = full
+    lib = _capi.lib()
+    v2 = np.zeros(w.nz * w.nx, np.float32)
+    rs = np.zeros(w.nz * w.nx, np.float32)
+    velf = np.ascontiguousarray(w.vel.reshape(-1), np.float32)
+    assert lib.aio_fd_precompute(w.nz, w.nx, C.c_float(w.dts), w.sub, velf.ctypes.data_as(C.c_void_p),
+                                 v2.ctypes.data_as(C.c_void_p), rs.ctypes.data_as(C.c_void_p)) == 0
+    w_mine = S.Workload(w.name, w.pad, w.nts, w.dts, w.sub, w.dz, w.dx, w.vel, w.wavelet, mine, model=w.model)
+    sigs = prepare_signals(w_mine, lib)
+
+    ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs, wavefield=args.wavefield,
+                  image_fp64=True, device=local)
+    dev = torch.device("cuda", local)
+    model_d = torch.from_numpy(np.ascontiguousarray(w.model, np.float32)).to(dev)
+    image_d = torch.zeros((w.nx, w.nz), dtype=torch.float32, device=dev)
+    sig_d = [torch.from_numpy(s).to(dev) for s in sigs]
+    dat_d = [torch.zeros((len(a.rec_pos), w.nts), dtype=torch.float32, device=dev) for a in mine]
+    torch.cuda.synchronize()
+    shots = [(a.src_pos, a.rec_pos, s.data_ptr(), d.data_ptr(), 0, 0) for a, s, d in zip(mine, sig_d, dat_d)]
+
+    def step():
+        ctx.device_call("born_forward", C.c_void_p(model_d.data_ptr()), shots=shots)
+        ctx.device_call("born_adjoint", C.c_void_p(image_d.data_ptr()), C.c_int(0), shots=shots)
+
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=dev)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    ctx.reset_stats()
+    ctx.profile(16)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        barrier()
+    ctx.profile(0)
+    kernels, step_ms, n_timed, step_pts = ctx.stats()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.all_reduce(image_d)  # the image stack across ranks (one reduction per adjoint)
+    ms_per_step = ms / args.steps
+    pts_per_step = w.n_interior * w.fine_steps * PASSES * args.shots * world
+    value = pts_per_step / (ms_per_step / 1e3) / 1e9
+
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    hbm_peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if hbm_peak else "fallback"
+    hbm_peak = hbm_peak or 6650.0
+    achieved = (BYTES_PER_POINT * step_pts / 1e9) / (step_ms / 1e3) if step_ms > 0 else None
+    traffic = None
+    tr = os.path.join(ROOT, "profiles", "stepper_traffic.json")
+    if os.path.exists(tr):
+        try:
+            traffic = json.load(open(tr)).get("bytes_per_point_update")
+        except Exception:
+            traffic = None
+
+    # ------------------------------------------------ e2e through the C ABI (host buffers)
+    e2e = None
+    if not args.no_e2e:
+        from acoustic_isotropic_operators_b200.batch import Shot
+        host_shots = [Shot(a.src_pos, a.rec_pos, s) for a, s in zip(mine, sigs)]
+        model_h = np.ascontiguousarray(w.model, np.float32)
+        ctx.born_forward(model_h, host_shots)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(max(1, args.steps)):
+            ctx.born_forward(model_h, host_shots)
+            img = ctx.born_adjoint(host_shots)
+        barrier()
+        e_ms = (time.perf_counter() - t0) * 1e3 / max(1, args.steps)
+        if dist:
+            t = torch.tensor([e_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+        h2d = model_h.nbytes + 2 * sum(s.nbytes for s in sigs) + sum(len(a.rec_pos) * w.nts * 4 for a in mine)
+        d2h = sum(len(a.rec_pos) * w.nts * 4 for a in mine) + img.nbytes
+        e2e = {"value": pts_per_step / (e_ms / 1e3) / 1e9, "unit": UNIT, "ms_per_step": e_ms,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        nts_sample = args.cpu_nts or 150
+        v, dt, _ = cpu_sample(w_mine, sigs, nts_sample, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"1 shot, Born forward+adjoint, full grid, nts={nts_sample} ({dt:.1f} s)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, BASELINE shapes)",
+                "config": config_dict(args, w),
+                "roofline": {"bound": "hbm", "kernel": "k_step (fused fine-time stepper)",
+                             "achieved": achieved, "peak": hbm_peak, "peak_source": peak_src, "unit": "GB/s",
+                             "frac": (achieved / hbm_peak) if achieved else None,
+                             "traffic": traffic, "timed_launches": n_timed,
+                             "stepper_ms_share": (step_ms * 16 / ms) if ms > 0 else None},
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": kernels, "clocks": clk.summary()}
+        print(json.dumps(line))
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -90,6 +90,15 @@ int aio_context_wave_capacity(aio_context* ctx, int family);
 /* Number of stepper launches issued by the most recent operator call. */
 long long aio_context_last_launches(aio_context* ctx);
 const char* aio_last_error(void);
+/* The CUDA stream (cudaStream_t) every kernel of this context runs on. */
+void* aio_context_stream(aio_context* ctx);
+/* Live stepper timing: bracket every sampleEvery-th stepper launch with CUDA events (0 = off). */
+int aio_context_profile(aio_context* ctx, int sampleEvery);
+/* Kernels launched, and timed-stepper totals (milliseconds, launches, interior
+ * point-updates of those launches) since the last reset. */
+int aio_context_stats(aio_context* ctx, long long* kernels, double* stepperMs, long long* stepperTimed,
+                      double* stepperPoints);
+int aio_context_reset_stats(aio_context* ctx);
 
 /* Nonlinear: model = source traces (sourcesSignals), data per shot. */
 int aio_nonlinear_forward(aio_context* ctx, int nShots, const aio_shot* shots, int memSpace);
@@ -110,6 +119,30 @@ int aio_wemva_ext_forward(aio_context* ctx, const float* model, float* image, in
                           const aio_shot* shots, int memSpace);
 int aio_wemva_ext_adjoint(aio_context* ctx, float* model, int add, const float* image, int nShots,
                           const aio_shot* shots, int memSpace);
+
+/* ------------------------------------------------------------ host preparation
+ * The reference's host-side numerics, FP32 expressions unchanged; arrays are
+ * host memory. add=0 overwrites the output, add=1 accumulates.
+ */
+/* fdParam: v^2*dtw^2 and 2/v^3 over the padded grid (F/src/fdParam.cpp:124-139). Either output may be NULL. */
+int aio_fd_precompute(int nz, int nx, float dts, int sub, const float* vel, float* vel2Dtw2, float* reflectivityScale);
+/* interpTimeLinTbb forward / adjoint: coarse [nDev][nts] <-> fine [nDev][ntw] (F/src/interpTimeLinTbb.cpp:26-102). */
+int aio_time_interp_forward(int add, int nts, float dts, float ots, int sub, int nDev, const float* coarse, float* fine);
+int aio_time_interp_adjoint(int add, int nts, float dts, float ots, int sub, int nDev, float* coarse, const float* fine);
+/* secondTimeDerivative forward (= adjoint), [nDev][nt] (F/src/secondTimeDerivative.cpp:14-39). */
+int aio_second_time_derivative(int add, int nt, float dt, int nDev, const float* in, float* out);
+/* seismicOperator2D::scaleSeismicSource: signal[k][:] *= dtw^2 v(pos[k])^2 (F/include/seismicOperator2D.cpp:72-86). */
+int aio_scale_seismic_source(int nDevReg, const int* posReg, int nt, float dts, int sub, const float* vel, float* signal);
+/* deviceGpu adjoint / forward on unique grid points (F/src/deviceGpu.cpp:227-261). */
+int aio_device_spread(int add, int nDevIrreg, int nCorner, const int* cornerIdx, const float* weights, int nDevReg,
+                      int nt, const float* irreg, float* reg);
+int aio_device_gather(int add, int nDevIrreg, int nCorner, const int* cornerIdx, const float* weights, int nDevReg,
+                      int nt, const float* reg, float* irreg);
+/* seismicOperator2D::setSources chain: spread, [d2/dt2], dtw^2 v^2 scale, interpolate to fine time
+ * (F/include/seismicOperator2D.cpp:10-39; secondDerivative=0 gives F/src/nonlinearPropGpu.cpp:44-51). */
+int aio_prepare_source(int secondDerivative, int nDevIrreg, int nCorner, const int* cornerIdx, const float* weights,
+                       int nDevReg, const int* posReg, int nts, float dts, int sub, const float* vel,
+                       const float* wavelets, float* out);
 
 /* -------------------------------------------------------------- reference seam
  * Each replaces the reference function of the same name without the prefix;
