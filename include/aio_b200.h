@@ -212,6 +212,24 @@ int aio_wemvaTimeShotsAdjGpu(float* model, float* wemvaExtImage, float* sourcesS
                              int nSourcesReg, float* wemvaDataRegDts, int* receiversPositionReg, int nReceiversReg,
                              float* wemvaSrcWavefieldDt2, float* wemvaSecWavefield1, float* wemvaSecWavefield2,
                              int iGpu, int iGpuId, int saveWavefield);
+/* Allocation-free nonlinear forward of one shot. No counterpart in the reference.
+ * For callers that cannot let a library allocate device memory: work recorded
+ * into a CUDA graph (cudaMalloc is not allowed during stream capture), services
+ * that plan all device memory ahead and forbid allocation on the request path,
+ * and hosts whose own allocator owns the device heap. Inputs and output are
+ * device pointers (vel2Dtw2: nz*nx; modelRegDtw: [nSourcesReg][ntw]; dataRegDts:
+ * [nReceiversReg][nts], overwritten); positions are host arrays; work is queued
+ * on `stream` (a cudaStream_t, NULL = default stream) and not waited for.
+ * Every temporary lives in one fixed 48 MiB __device__ array that each GPU
+ * loading the library holds until exit; grids needing more return
+ * AIO_ERR_ARGUMENT. The first call on a device looks up that array's device
+ * address (make it before any stream capture). All calls share the array:
+ * calls whose GPU work overlaps race and must be serialised by the caller.
+ * Errors are returned as codes and described on stderr. */
+int aio_propShotsFwdGpu_noalloc(float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad,
+                                float alphaCos, const float* vel2Dtw2, const float* modelRegDtw,
+                                const int* sourcesPositionReg, int nSourcesReg, const int* receiversPositionReg,
+                                int nReceiversReg, float* dataRegDts, void* stream);
 /* F/src/nonlinearShotsGpuFunctions.cu:18-84: validates a GPU id list (info printing dropped). */
 int aio_getGpuInfo(const int* gpuList, int nGpuList, int info, int deviceNumberInfo);
 
