@@ -23,6 +23,7 @@ AIO_MEM_HOST = 0
 AIO_MEM_DEVICE = 1
 AIO_NONLINEAR, AIO_BORN, AIO_BORN_EXT, AIO_TOMO_EXT, AIO_WEMVA_EXT = range(5)
 AIO_WFLD_FP32, AIO_WFLD_BF16, AIO_WFLD_FP16 = range(3)
+AIO_STEPPER_AUTO, AIO_STEPPER_FINE, AIO_STEPPER_BLOCKED = range(3)
 
 EXPORTED = [
     "aio_last_error", "aio_context_create", "aio_context_destroy", "aio_context_set_velocity",
@@ -52,7 +53,7 @@ class AioParams(C.Structure):
                 ("nExt", C.c_int), ("dz", C.c_float), ("dx", C.c_float), ("dts", C.c_float),
                 ("alphaCos", C.c_float), ("leg1", C.c_int), ("leg2", C.c_int), ("sloth", C.c_int),
                 ("wavefieldPrecision", C.c_int), ("imageFp64", C.c_int), ("device", C.c_int),
-                ("memBudgetBytes", C.c_longlong)]
+                ("memBudgetBytes", C.c_longlong), ("stepper", C.c_int), ("chunkColumns", C.c_int)]
 
 
 class AioShot(C.Structure):

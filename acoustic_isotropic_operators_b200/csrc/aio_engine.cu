@@ -19,6 +19,7 @@
 
 #include "aio_b200.h"
 #include "aio_kernels.cuh"
+#include "aio_tb.cuh"
 
 namespace aio {
 
@@ -190,9 +191,17 @@ struct Context {
         require(p.sub >= 1 && p.sub < SUB_MAX, "sub must be in [1, 100)");
         require(p.minPad >= 0 && p.minPad < PAD_MAX, "minPad must be in [0, 200)");
         require(p.nExt >= 1 && (p.nExt % 2) == 1, "nExt must be a positive odd number");
-        require(p.wavefieldPrecision == AIO_WFLD_FP32, "only FP32 stored wavefields are available in this build");
+        require(p.wavefieldPrecision == AIO_WFLD_FP32 || p.wavefieldPrecision == AIO_WFLD_BF16,
+                "stored wavefield precision must be AIO_WFLD_FP32 or AIO_WFLD_BF16");
+        require(p.stepper >= AIO_STEPPER_AUTO && p.stepper <= AIO_STEPPER_BLOCKED, "unknown stepper");
+        require(p.stepper != AIO_STEPPER_BLOCKED || p.sub == 4, "the interval-blocked stepper requires sub == 4");
+        require(p.wavefieldPrecision == AIO_WFLD_FP32 || (p.stepper != AIO_STEPPER_FINE && p.sub == 4),
+                "compressed stored wavefields need the interval-blocked stepper (sub == 4)");
         g = make_geom(p.nz, p.nx, p.nts, p.sub, p.minPad, p.nExt);
         k = make_consts(p);
+        // the blocked stepper evaluates taper[min(a, b)] as min(taper[a], taper[b])
+        for (int i = 1; i < p.minPad; i++)
+            require(k.taper[i] >= k.taper[i - 1] && k.taper[i] <= 1.f, "cosine taper must be monotone and <= 1");
         dev = p.device;
         AIO_CK(cudaSetDevice(dev));
         AIO_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -754,12 +763,234 @@ struct Context {
         launches = 0;
     }
 
+
+    // ============================================================ blocked stepper
+    // One launch per coarse interval (aio_tb.cuh). State, partial sums and
+    // images use interior slices; the stored wavefield is FP32 or BF16.
+    DevMem tbState, tbPart, tbImg, tbW, tbEnt, tbStart, tbDesc;
+    struct TBPlan {
+        int T = 4, HZ = 0, nStrips = 0, LX = 0, nChunks = 0, iters = 0, threads = 0;
+    };
+
+    bool tb_enabled() const { return P.stepper != AIO_STEPPER_FINE && g.sub == 4; }
+    int wbytes() const { return P.wavefieldPrecision == AIO_WFLD_BF16 ? 2 : 4; }
+
+    TBPlan tb_plan() const {
+        TBPlan pl;
+        const int maxHZ = TB_MAXROWS - 10 * pl.T;
+        pl.nStrips = (g.nzi + maxHZ - 1) / maxHZ;
+        pl.HZ = (g.nzi + pl.nStrips - 1) / pl.nStrips;
+        pl.threads = round_up(pl.HZ + 10 * pl.T, 32);
+        int target = P.chunkColumns > 0 ? P.chunkColumns : 128;
+        pl.nChunks = std::max(1, (g.nxi + target / 2) / target);
+        pl.LX = (g.nxi + pl.nChunks - 1) / pl.nChunks;
+        pl.iters = round_up(pl.LX + 10 * pl.T + TBD, TBQ);
+        return pl;
+    }
+
+    // Per-CTA sparse lists of every shot of a wave. inj: 0 none, 1 sources, 2 receivers
+    // (over the CTA's recomputed halo region); rec: record receivers (output region).
+    int tb_lists(const TBPlan& pl, int nb, const aio_shot* shots, int inj, bool rec) {
+        std::vector<TBEnt> ents;
+        std::vector<int4> starts((size_t)nb * pl.nStrips * pl.nChunks);
+        const int h = 5 * (pl.T - 1);
+        int maxEnt = 1;
+        for (int s = 0; s < nb; s++) {
+            std::vector<std::pair<int, int>> ipos, rpos;  // (interior x, interior z) per device
+            auto collect = [&](const int* pos, int n, std::vector<std::pair<int, int>>& out, const char* what) {
+                out.resize(n);
+                for (int k2 = 0; k2 < n; k2++) {
+                    const long long p = pos[k2];
+                    const int iz = (int)(p % g.nz), ix = (int)(p / g.nz);
+                    require(p >= 0 && ix < g.nx && iz >= FAT && iz < g.nz - FAT && ix >= FAT && ix < g.nx - FAT,
+                            std::string(what) + " position " + std::to_string(p) + " is outside the interior grid");
+                    out[k2] = {ix - FAT, iz - FAT};
+                }
+            };
+            if (inj == 1) collect(shots[s].sourcesPositionReg, shots[s].nSourcesReg, ipos, "source");
+            if (inj == 2) collect(shots[s].receiversPositionReg, shots[s].nReceiversReg, ipos, "receiver");
+            if (rec) collect(shots[s].receiversPositionReg, shots[s].nReceiversReg, rpos, "receiver");
+            for (int st2 = 0; st2 < pl.nStrips; st2++)
+                for (int ch = 0; ch < pl.nChunks; ch++) {
+                    const int z0 = st2 * pl.HZ, z1 = std::min(z0 + pl.HZ, g.nzi);
+                    const int x0 = ch * pl.LX, x1 = std::min(x0 + pl.LX, g.nxi);
+                    std::vector<TBEnt> a1, a2;
+                    for (size_t d = 0; d < ipos.size(); d++) {
+                        const int x = ipos[d].first, z = ipos[d].second;
+                        if (x >= x0 - h && x < x1 + h && z >= z0 - h && z < z1 + h) a1.push_back(TBEnt{x, z, (int)d, 0});
+                    }
+                    for (size_t d = 0; d < rpos.size(); d++) {
+                        const int x = rpos[d].first, z = rpos[d].second;
+                        if (x >= x0 && x < x1 && z >= z0 && z < z1) a2.push_back(TBEnt{x, z, (int)d, 0});
+                    }
+                    auto byCol = [](const TBEnt& A, const TBEnt& B) { return A.col < B.col || (A.col == B.col && A.row < B.row); };
+                    std::sort(a1.begin(), a1.end(), byCol);
+                    std::sort(a2.begin(), a2.end(), byCol);
+                    int4 se;
+                    se.x = (int)ents.size();
+                    ents.insert(ents.end(), a1.begin(), a1.end());
+                    se.y = (int)ents.size();
+                    se.z = se.y;
+                    ents.insert(ents.end(), a2.begin(), a2.end());
+                    se.w = (int)ents.size();
+                    starts[((size_t)s * pl.nStrips + st2) * pl.nChunks + ch] = se;
+                    maxEnt = std::max(maxEnt, se.w - se.x);
+                }
+        }
+        require(maxEnt <= 4096, "too many sparse devices inside one blocked-stepper tile");
+        tbEnt.ensure(std::max<size_t>(ents.size(), 1) * sizeof(TBEnt));
+        tbStart.ensure(starts.size() * sizeof(int4));
+        if (!ents.empty())
+            AIO_CK(cudaMemcpyAsync(tbEnt.p, ents.data(), ents.size() * sizeof(TBEnt), cudaMemcpyHostToDevice, st));
+        AIO_CK(cudaMemcpyAsync(tbStart.p, starts.data(), starts.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+        return maxEnt;
+    }
+
+    void tb_alloc(int nb, bool needImg) {
+        require(g.isz < (1LL << 31), "interior slice too large for 32-bit in-slice offsets");
+        tbState.ensure((size_t)nb * 4 * g.isz * 4);
+        tbPart.ensure((size_t)nb * 2 * g.isz * 4);
+        if (needImg) tbImg.ensure((size_t)nb * g.isz * 8);
+        tbDesc.ensure((size_t)2 * nb * sizeof(TBShot));
+    }
+
+    // Descriptor pairs: version v reads state/part set v and writes set 1-v
+    // (partSwap=true: the ADJ part ordering, see tb_adj_pass).
+    void tb_desc(const TBPlan& pl, int nb, bool injSources, bool injData, bool recData, void* W, bool partFlip) {
+        std::vector<TBShot> d(2 * (size_t)nb);
+        const int nCTA = pl.nStrips * pl.nChunks;
+        for (int v = 0; v < 2; v++)
+            for (int s = 0; s < nb; s++) {
+                TBShot& t = d[(size_t)v * nb + s];
+                std::memset(&t, 0, sizeof(t));
+                float* base = tbState.as<float>() + (size_t)s * 4 * g.isz;
+                t.cur = base + (size_t)(2 * v) * g.isz;
+                t.old = base + (size_t)(2 * v + 1) * g.isz;
+                t.ncur = base + (size_t)(2 * (1 - v)) * g.isz;
+                t.nold = base + (size_t)(2 * (1 - v) + 1) * g.isz;
+                float* pb = tbPart.as<float>() + (size_t)s * 2 * g.isz;
+                const int vin = partFlip ? (v ^ 1) : v;
+                t.part = pb + (size_t)vin * g.isz;
+                t.partOut = pb + (size_t)(1 - vin) * g.isz;
+                t.injSig = injSources ? srcSig[s] : (injData ? dataPtr[s] : nullptr);
+                t.injLd = injSources ? g.ntw : g.nts;
+                t.recSig = recData ? dataPtr[s] : nullptr;
+                t.recLd = g.nts;
+                t.entStart = tbStart.as<int4>() + (size_t)s * nCTA;
+                t.ent = tbEnt.as<TBEnt>();
+                t.W = W ? (void*)((char*)W + (size_t)s * g.nts * g.isz * wbytes()) : nullptr;
+                t.img = tbImg.p ? tbImg.as<double>() + (size_t)s * g.isz : nullptr;
+            }
+        AIO_CK(cudaMemcpyAsync(tbDesc.p, d.data(), d.size() * sizeof(TBShot), cudaMemcpyHostToDevice, st));
+    }
+
+    TBArgs tb_args(const TBPlan& pl, int maxEnt, const float* dm) const {
+        TBArgs a;
+        std::memset(&a, 0, sizeof(a));
+        a.g = g;
+        a.c = k.c;
+        a.v2 = v2.as<float>();
+        a.taper = taper.as<float>();
+        a.dm = dm;
+        std::copy(k.h, k.h + 2 * (SUB_MAX + 1), a.h);
+        a.HZ = pl.HZ;
+        a.LX = pl.LX;
+        a.nStrips = pl.nStrips;
+        a.nChunks = pl.nChunks;
+        a.iters = pl.iters;
+        a.maxEnt = maxEnt;
+        a.wStride = g.isz;
+        return a;
+    }
+
+    template <int MODE, int WP>
+    void tb_launch_t(const TBPlan& pl, int nb, TBArgs& a, int v) {
+        const size_t smem = tb_smem_bytes(pl.T, MODE, a.maxEnt);
+        static int attrDev = -1;
+        if (attrDev != dev) {
+            AIO_CK(cudaFuncSetAttribute(k_interval<4, MODE, WP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)tb_smem_bytes(4, MODE, 4096)));
+            attrDev = dev;
+        }
+        a.shots = tbDesc.as<TBShot>() + (size_t)v * nb;
+        const bool timed = profEvery > 0 && (launches % profEvery) == 0;
+        std::pair<cudaEvent_t, cudaEvent_t> ev{};
+        if (timed) {
+            ev = take_events();
+            AIO_CK(cudaEventRecord(ev.first, st));
+        }
+        k_interval<4, MODE, WP><<<dim3(pl.nStrips, pl.nChunks, nb), pl.threads, smem, st>>>(a);
+        AIO_CK(cudaGetLastError());
+        if (timed) {
+            AIO_CK(cudaEventRecord(ev.second, st));
+            evBusy.push_back(ev);
+            evPoints.push_back((long long)nb * g.nzi * g.nxi * pl.T);
+        }
+        launches++;
+        kernels++;
+    }
+    template <int MODE>
+    void tb_launch(const TBPlan& pl, int nb, TBArgs& a, int v) {
+        if (P.wavefieldPrecision == AIO_WFLD_BF16) tb_launch_t<MODE, TBW_BF16>(pl, nb, a, v);
+        else tb_launch_t<MODE, TBW_F32>(pl, nb, a, v);
+    }
+
+    void tb_zero(int nb, bool img) {
+        AIO_CK(cudaMemsetAsync(tbState.p, 0, (size_t)nb * 4 * g.isz * 4, st));
+        AIO_CK(cudaMemsetAsync(tbPart.p, 0, (size_t)nb * 2 * g.isz * 4, st));
+        if (img) AIO_CK(cudaMemsetAsync(tbImg.p, 0, (size_t)nb * g.isz * 8, st));
+    }
+
+    // Source pass storing W[nts] (F/src/BornShotsGpuFunctions.cu:297-321), or the
+    // nonlinear forward when recordData (F/src/nonlinearShotsGpuFunctions.cu:269-295).
+    void tb_src_pass(int nb, const aio_shot* shots, bool nonlinear) {
+        const TBPlan pl = tb_plan();
+        const int maxEnt = tb_lists(pl, nb, shots, 1, nonlinear);
+        tb_zero(nb, false);
+        tb_desc(pl, nb, true, false, nonlinear, nonlinear ? nullptr : tbW.p, false);
+        TBArgs a = tb_args(pl, maxEnt, nullptr);
+        for (int its = 0; its < g.nts - 1; its++) {
+            a.its = its;
+            if (nonlinear) tb_launch<TB_NL>(pl, nb, a, its & 1);
+            else tb_launch<TB_SRC>(pl, nb, a, its & 1);
+        }
+    }
+
+    // Scattered pass with data recording (F/src/BornShotsGpuFunctions.cu:323-376).
+    void tb_scat_pass(int nb, const aio_shot* shots, const float* dm) {
+        const TBPlan pl = tb_plan();
+        const int maxEnt = tb_lists(pl, nb, shots, 0, true);
+        tb_zero(nb, false);
+        tb_desc(pl, nb, false, false, true, tbW.p, false);
+        TBArgs a = tb_args(pl, maxEnt, dm);
+        for (int its = 0; its < g.nts - 1; its++) {
+            a.its = its;
+            tb_launch<TB_SCAT>(pl, nb, a, its & 1);
+        }
+    }
+
+    // Receiver pass with imaging (F/src/BornShotsGpuFunctions.cu:880-950), on U = v2*p.
+    // Launch L handles interval its = nts-2-L: it reads the partial R(its+1) written by
+    // launch L-1 and writes R(its); state ping-pongs with L.
+    void tb_adj_pass(int nb, const aio_shot* shots) {
+        const TBPlan pl = tb_plan();
+        const int maxEnt = tb_lists(pl, nb, shots, 2, false);
+        tb_zero(nb, true);
+        tb_desc(pl, nb, false, true, false, tbW.p, false);
+        TBArgs a = tb_args(pl, maxEnt, nullptr);
+        for (int L = 0; L < g.nts - 1; L++) {
+            a.its = g.nts - 2 - L;
+            tb_launch<TB_ADJ>(pl, nb, a, L & 1);
+        }
+    }
+
     // ============================================================ operators
 
     // Nonlinear forward (F/src/nonlinearShotsGpuFunctions.cu:227-309; with a
     // wavefield, :310-395 — only a batch of one shot returns it).
     void nonlinear_forward(int nShots, const aio_shot* shots, int mem, float* wavefieldOut) {
         begin_call();
+        if (tb_enabled() && !wavefieldOut) return nonlinear_forward_tb(nShots, shots, mem);
         Needs n;
         n.nWavefields = wavefieldOut ? 1 : 0;
         for (int s0 = 0; s0 < nShots;) {
@@ -815,6 +1046,78 @@ struct Context {
                                      cudaMemcpyDeviceToHost, st));
     }
 
+
+    // Wave sizing for the blocked stepper: per shot 4 state + 2 partial slices,
+    // the stored wavefield, an FP64 image, traces.
+    int tb_wave_size(int nShots, const aio_shot* shots, bool wavefield, bool image) {
+        int maxSrc = 1, maxRec = 1;
+        for (int s = 0; s < nShots; s++) {
+            maxSrc = std::max(maxSrc, shots[s].nSourcesReg);
+            maxRec = std::max(maxRec, shots[s].nReceiversReg);
+        }
+        long long per = 6LL * g.isz * 4 + (wavefield ? (long long)g.nts * g.isz * wbytes() : 0) +
+                        (image ? g.isz * 8LL : 0) + (long long)maxSrc * g.ntw * 4 + 2LL * maxRec * g.nts * 4 +
+                        2 * g.hsz * 4 + 2 * g.isz * 4 + (1 << 16);
+        long long shared = 4LL * g.isz * 4 + (64LL << 20);
+        long long cap = (budget - shared) / per;
+        require(cap >= 1, "device memory budget cannot hold one shot for this operator");
+        return (int)std::min<long long>(cap, nShots);
+    }
+
+    void born_forward_tb(const float* model, int nShots, const aio_shot* shots, int mem) {
+        float* dm = stage_model(model, 1, mem, this->model);
+        scale_shared(dm, 1, 0);
+        Needs n;
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = tb_wave_size(nShots - s0, shots + s0, true, false);
+            setup_wave(n, nb, shots + s0, mem, false, false);
+            tb_alloc(nb, false);
+            tbW.ensure((size_t)nb * g.nts * g.isz * wbytes());
+            tb_src_pass(nb, shots + s0, false);
+            tb_scat_pass(nb, shots + s0, dm);
+            download_data(nb, shots + s0, mem);
+            sync();
+            s0 += nb;
+        }
+    }
+
+    void born_adjoint_tb(float* modelOut, int add, int nShots, const aio_shot* shots, int mem) {
+        float* out = stage_out(modelOut, 1, add, mem);
+        Needs n;
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = tb_wave_size(nShots - s0, shots + s0, true, true);
+            setup_wave(n, nb, shots + s0, mem, true, false);
+            tb_alloc(nb, true);
+            tbW.ensure((size_t)nb * g.nts * g.isz * wbytes());
+            tb_src_pass(nb, shots + s0, false);
+            tb_adj_pass(nb, shots + s0);
+            // images of U = v2*p: the reference's v2*(2/v^3) scaling reduces to 2/v^3
+            const long long nI = g.isz;
+            k_scale_d<<<ew_grid(nb, nI), 256, 0, st>>>(tbImg.as<double>(), nI, 1, v2.as<float>(), rs.as<float>(),
+                                                       g.isz, 3);
+            kcheck();
+            k_sum_shots<double><<<ew_grid(1, nI), 256, 0, st>>>(out, tbImg.as<double>(), nI, nb, nI, 1);
+            kcheck();
+            sync();
+            s0 += nb;
+        }
+        write_model(modelOut, 1, add, mem, out);
+        sync();
+    }
+
+    void nonlinear_forward_tb(int nShots, const aio_shot* shots, int mem) {
+        Needs n;
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = tb_wave_size(nShots - s0, shots + s0, false, false);
+            setup_wave(n, nb, shots + s0, mem, false, false);
+            tb_alloc(nb, false);
+            tb_src_pass(nb, shots + s0, true);
+            download_data(nb, shots + s0, mem);
+            sync();
+            s0 += nb;
+        }
+    }
+
     // Source pass storing the coarse source wavefield W[nts] of every shot of the wave.
     // F/src/BornShotsGpuFunctions.cu:297-321.
     void source_wavefield(int nb, DevMem& W) { fwd_sparse_pass(nb, false, &W); }
@@ -822,6 +1125,7 @@ struct Context {
     // Born forward (F/src/BornShotsGpuFunctions.cu:260-388).
     void born_forward(const float* model, int nShots, const aio_shot* shots, int mem) {
         begin_call();
+        if (tb_enabled()) return born_forward_tb(model, nShots, shots, mem);
         Needs n;
         n.nWavefields = 1;
         n.ss = true;
@@ -845,6 +1149,7 @@ struct Context {
     // summed on the device.
     void born_adjoint(float* modelOut, int add, int nShots, const aio_shot* shots, int mem) {
         begin_call();
+        if (tb_enabled()) return born_adjoint_tb(modelOut, add, nShots, shots, mem);
         Needs n;
         n.nWavefields = 1;
         n.nImg = 1;

@@ -35,11 +35,21 @@ template <bool ADJ, int INJ, bool REC, bool ACC>
 __global__ void __launch_bounds__(TZ* TY) k_step(const StepArgs a) {
     __shared__ float s[TX + 2 * FAT][TZ + 2 * FAT];
     const Geom& g = a.g;
-    const ShotDesc& sd = a.shots[blockIdx.z];
+    // Descriptor fields are read once into registers: stores below could
+    // otherwise alias the descriptor and force reloads.
+    const ShotDesc* sdp = a.shots + blockIdx.z;
+    float* const p0 = sdp->p[0];
+    float* const p1 = sdp->p[1];
+    const SparseList injL = sdp->inj, recL = sdp->rec;
+    const float* __restrict__ injSig = sdp->injSig;
+    float* __restrict__ recSig = sdp->recSig;
+    const int injLd = sdp->injLd, recLd = sdp->recLd;
+    float* const ssBase = sdp->ss;
+    float* const accBase = sdp->acc;
     const int lane = threadIdx.x, ty = threadIdx.y;
     const int z0 = blockIdx.x * TZ, x0 = blockIdx.y * TX;
-    const float* __restrict__ cur = sd.p[a.parity];
-    float* __restrict__ old = sd.p[a.parity ^ 1];
+    const float* __restrict__ cur = a.parity ? p1 : p0;
+    float* __restrict__ old = a.parity ? p0 : p1;
 
     // Stage the current level (times v^2 dtw^2 for the adjoint) with its halo.
     for (int r = ty; r < TX + 2 * FAT; r += TY) {
@@ -64,13 +74,13 @@ __global__ void __launch_bounds__(TZ* TY) k_step(const StepArgs a) {
     for (int j = 0; j < PX; j++) inj[j] = 0.f;
 
     const int tile = blockIdx.y * gridDim.x + blockIdx.x;
-    if (INJ == 1 && sd.inj.tileStart) {
-        const int b = sd.inj.tileStart[tile], e = sd.inj.tileStart[tile + 1];
+    if (INJ == 1 && injL.tileStart) {
+        const int b = injL.tileStart[tile], e = injL.tileStart[tile + 1];
         for (int k = b; k < e; k++) {
-            const int2 en = sd.inj.ent[k];
+            const int2 en = injL.ent[k];
             const int lz = en.x & (TZ - 1), lx = en.x / TZ;
             if (lz == lane && (lx / PX) == ty) {
-                const float* tr = sd.injSig + (long long)en.y * sd.injLd;
+                const float* tr = injSig + (long long)en.y * injLd;
                 float v = a.injTB >= 0 ? tr[a.injTA] * a.injCA + tr[a.injTB] * a.injCB : tr[a.injTA];
 #pragma unroll
                 for (int j = 0; j < PX; j++)
@@ -79,10 +89,10 @@ __global__ void __launch_bounds__(TZ* TY) k_step(const StepArgs a) {
         }
     }
 
-    const float* __restrict__ ssA = (INJ == 2) ? sd.ss + a.ssOffA : nullptr;
-    const float* __restrict__ ssB = (INJ == 2) ? sd.ss + a.ssOffB : nullptr;
-    float* __restrict__ accA = ACC ? sd.acc + a.accOffA : nullptr;
-    float* __restrict__ accB = ACC ? sd.acc + a.accOffB : nullptr;
+    const float* __restrict__ ssA = (INJ == 2) ? ssBase + a.ssOffA : nullptr;
+    const float* __restrict__ ssB = (INJ == 2) ? ssBase + a.ssOffB : nullptr;
+    float* __restrict__ accA = ACC ? accBase + a.accOffA : nullptr;
+    float* __restrict__ accB = ACC ? accBase + a.accOffB : nullptr;
 
     float w[PX + 2 * FAT];
 #pragma unroll
@@ -131,17 +141,17 @@ __global__ void __launch_bounds__(TZ* TY) k_step(const StepArgs a) {
         }
     }
 
-    if (REC && sd.rec.tileStart) {
-        const int b = sd.rec.tileStart[tile], e = sd.rec.tileStart[tile + 1];
+    if (REC && recL.tileStart) {
+        const int b = recL.tileStart[tile], e = recL.tileStart[tile + 1];
         for (int k = b; k < e; k++) {
-            const int2 en = sd.rec.ent[k];
+            const int2 en = recL.ent[k];
             const int lz = en.x & (TZ - 1), lx = en.x / TZ;
             if (lz == lane && (lx / PX) == ty) {
                 float v = 0.f;
 #pragma unroll
                 for (int j = 0; j < PX; j++)
                     if (j == (lx % PX)) v = S[j];
-                float* tr = sd.recSig + (long long)en.y * sd.recLd;
+                float* tr = recSig + (long long)en.y * recLd;
                 tr[a.recTA] += v * a.recCA;
                 if (a.recTB >= 0) tr[a.recTB] += v * a.recCB;
             }
@@ -271,6 +281,7 @@ __global__ void k_scale_d(double* m, long long mSt, int nSlices, const float* v2
         const double v = v2[i], r = rs[i];
         if (mode == 0) m[k] *= (double)(float)(v * r);
         else if (mode == 1) m[k] *= (double)(float)(r * v);
+        else if (mode == 3) m[k] *= r;   // images of v2-weighted (adjoint U-form) wavefields
         else m[k] = -(m[k] * v);
     }
 }

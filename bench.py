@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-nts", type=int, default=0, help="coarse samples of the CPU sample (0 = auto)")
+    ap.add_argument("--stepper", default="auto", choices=["auto", "fine", "blocked"])
+    ap.add_argument("--chunk", type=int, default=0, help="blocked-stepper chunk width (0 = automatic)")
     return ap.parse_args()
 
 
@@ -168,6 +170,7 @@ def config_dict(args, w):
             "shots_per_gpu": args.shots, "grid_padded": [w.nz, w.nx],
             "interior": [w.nz - 10, w.nx - 10], "nts": w.nts, "sub": w.sub, "fine_steps": w.fine_steps,
             "passes_per_shot": PASSES, "wavefield": args.wavefield, "receivers_per_shot": 1200,
+            "stepper": args.stepper, "chunk": args.chunk,
             "parallelism": f"dp{args.gpus} (shots)", "l2": "inputs larger than L2 (5.4 GB wavefield per shot)"}
 
 
@@ -204,7 +207,7 @@ def main():
     sigs = prepare_signals(w_mine, lib)
 
     ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs, wavefield=args.wavefield,
-                  image_fp64=True, device=local)
+                  image_fp64=True, device=local, stepper=args.stepper, chunk_columns=args.chunk)
     dev = torch.device("cuda", local)
     model_d = torch.from_numpy(np.ascontiguousarray(w.model, np.float32)).to(dev)
     image_d = torch.zeros((w.nx, w.nz), dtype=torch.float32, device=dev)

@@ -65,7 +65,13 @@ typedef struct {
     int imageFp64;       /* 1: accumulate imaging conditions in FP64 on the GPU */
     int device;          /* CUDA device ordinal */
     long long memBudgetBytes; /* cap on device memory for shot buffers; 0 = 90% of free */
+    int stepper;         /* AIO_STEPPER_*: how Born / nonlinear passes advance time */
+    int chunkColumns;    /* blocked stepper x-chunk width (0 = automatic) */
 } aio_params;
+
+#define AIO_STEPPER_AUTO 0      /* interval-blocked where available (sub == 4), else per fine step */
+#define AIO_STEPPER_FINE 1      /* one fused launch per fine step (the reference's schedule) */
+#define AIO_STEPPER_BLOCKED 2   /* one launch per coarse interval (requires sub == 4) */
 
 typedef struct {
     const int* sourcesPositionReg;   /* host array, nSourcesReg */

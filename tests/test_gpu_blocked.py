@@ -1,0 +1,107 @@
+"""Interval-blocked stepper (one launch per coarse interval, sub = 4) vs the CPU
+oracle and vs the per-fine-step stepper.
+
+The grid is chosen so the blocked kernel runs several z-strips and x-chunks,
+with sources on strip / chunk boundaries (the recomputed halo regions must
+inject too). Tolerances: relative L2 1e-5 vs the FP32 oracle for FP32 storage;
+BF16 storage of the source wavefield is checked against the FP64 oracle at
+1e-2 (8-bit significand) and reported.
+"""
+import numpy as np
+import pytest
+
+import orc
+from cases import Case, interior_mask, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def blocked_case(seed=4, nzi=320, nxi=288, nts=30, nshots=2):
+    rng = np.random.default_rng(seed)
+    nz, nx = nzi + 10, nxi + 10
+    s = orc.Scheme(nz=nz, nx=nx, nts=nts, dts=0.004, sub=4, dz=10.0, dx=10.0, minPad=20)
+    zz = np.linspace(0, 1, nz)[None, :]
+    vel = (2000.0 + 800.0 * zz + 100.0 * rng.random((nx, nz))).astype(np.float32)
+    src_pos, rec_pos, sig = [], [], []
+    # strip boundary at interior z = 160, chunk boundaries at multiples of 64 (chunk_columns=64)
+    src_pts = [[(5 + 63, 5 + 159), (5 + 64, 5 + 160), (5 + 140, 5 + 12)],
+               [(5 + 127, 5 + 161), (5 + 200, 5 + 158), (5 + 30, 5 + 300)]]
+    for k in range(nshots):
+        sp = np.array([ix * nz + iz for ix, iz in src_pts[k % 2]], np.int32)
+        rp = np.array([ix * nz + 5 + 9 for ix in range(5, nx - 5)] +
+                      [ix * nz + 5 + 165 for ix in range(5, nx - 5, 3)], np.int32)
+        src_pos.append(sp)
+        rec_pos.append(rp)
+        sig.append((rng.standard_normal((len(sp), s.ntw)) * 1e-2).astype(np.float32))
+    return Case(s, vel, src_pos, rec_pos, sig, rng)
+
+
+@pytest.fixture(scope="module")
+def case():
+    return blocked_case()
+
+
+def ctx(case, **kw):
+    from acoustic_isotropic_operators_b200.batch import Context
+    s = case.scheme
+    k = orc.constants(s, case.vel, dtype=np.float32)
+    return Context(s.nz, s.nx, s.nts, s.dts, s.sub, s.dz, s.dx, s.minPad, k["v2"], k["rs"], chunk_columns=64, **kw)
+
+
+def shots(case, data=None):
+    from acoustic_isotropic_operators_b200.batch import Shot
+    return [Shot(case.src_pos[i], case.rec_pos[i], case.sig[i], None if data is None else data[i])
+            for i in range(len(case.src_pos))]
+
+
+def test_nonlinear_forward_blocked(case):
+    got = ctx(case, stepper="blocked").nonlinear_forward(shots(case))
+    fine = ctx(case, stepper="fine").nonlinear_forward(shots(case))
+    for i in range(len(got)):
+        r32 = orc.nl_fwd(case.scheme, case.vel, case.sig[i], case.src_pos[i], case.rec_pos[i], dtype=np.float32)
+        assert rel_l2(got[i], r32) < 1e-5
+        assert rel_l2(got[i], fine[i]) < 1e-5
+
+
+def test_born_forward_blocked(case):
+    m = case.rng.standard_normal((case.nx, case.nz)).astype(np.float32) * interior_mask(case.nx, case.nz)
+    c = ctx(case, stepper="blocked")
+    got = c.born_forward(m, shots(case))
+    assert c.last_launches == 2 * (case.scheme.nts - 1)
+    for i in range(len(got)):
+        r32 = orc.born_fwd(case.scheme, case.vel, m, case.sig[i], case.src_pos[i], case.rec_pos[i], dtype=np.float32)
+        assert rel_l2(got[i], r32) < 1e-5
+
+
+def test_born_adjoint_blocked(case):
+    d = [case.rng.standard_normal((len(r), case.scheme.nts)).astype(np.float32) for r in case.rec_pos]
+    got = ctx(case, stepper="blocked").born_adjoint(shots(case, d))
+    r32 = sum(orc.born_adj(case.scheme, case.vel, d[i], case.sig[i], case.src_pos[i], case.rec_pos[i],
+                           dtype=np.float32) for i in range(len(d)))
+    assert rel_l2(got, r32) < 1e-5
+    assert np.all(got[~interior_mask(case.nx, case.nz)] == 0)
+
+
+def test_born_dot_blocked(case):
+    c = ctx(case, stepper="blocked")
+    m = case.rng.standard_normal((case.nx, case.nz)).astype(np.float32) * interior_mask(case.nx, case.nz)
+    d = [case.rng.standard_normal((len(r), case.scheme.nts)).astype(np.float32) for r in case.rec_pos]
+    fm = c.born_forward(m, shots(case))
+    ad = c.born_adjoint(shots(case, d))
+    a = sum(float(np.sum(fm[i].astype(np.float64) * d[i])) for i in range(len(d)))
+    b = float(np.sum(m.astype(np.float64) * ad))
+    assert abs(a - b) / abs(b) < 1e-5
+
+
+def test_born_bf16_error(case):
+    m = case.rng.standard_normal((case.nx, case.nz)).astype(np.float32) * interior_mask(case.nx, case.nz)
+    got = ctx(case, stepper="blocked", wavefield="bf16").born_forward(m, shots(case))
+    v64 = case.vel.astype(np.float64)
+    for i in range(len(got)):
+        r64 = orc.born_fwd(case.scheme, v64, m, case.sig[i], case.src_pos[i], case.rec_pos[i])
+        assert rel_l2(got[i], r64) < 1e-2
+    d = [case.rng.standard_normal((len(r), case.scheme.nts)).astype(np.float32) for r in case.rec_pos]
+    ga = ctx(case, stepper="blocked", wavefield="bf16").born_adjoint(shots(case, d))
+    r64 = sum(orc.born_adj(case.scheme, v64, d[i], case.sig[i], case.src_pos[i], case.rec_pos[i])
+              for i in range(len(d)))
+    assert rel_l2(ga, r64) < 1e-2
