@@ -20,6 +20,7 @@
 #include "aio_b200.h"
 #include "aio_kernels.cuh"
 #include "aio_tb.cuh"
+#include "aio_tile.cuh"
 
 namespace aio {
 
@@ -193,8 +194,8 @@ struct Context {
         require(p.nExt >= 1 && (p.nExt % 2) == 1, "nExt must be a positive odd number");
         require(p.wavefieldPrecision == AIO_WFLD_FP32 || p.wavefieldPrecision == AIO_WFLD_BF16,
                 "stored wavefield precision must be AIO_WFLD_FP32 or AIO_WFLD_BF16");
-        require(p.stepper >= AIO_STEPPER_AUTO && p.stepper <= AIO_STEPPER_BLOCKED, "unknown stepper");
-        require(p.stepper != AIO_STEPPER_BLOCKED || p.sub == 4, "the interval-blocked stepper requires sub == 4");
+        require(p.stepper >= AIO_STEPPER_AUTO && p.stepper <= AIO_STEPPER_TILED, "unknown stepper");
+        require(p.stepper < AIO_STEPPER_BLOCKED || p.sub == 4, "the interval-blocked steppers require sub == 4");
         require(p.wavefieldPrecision == AIO_WFLD_FP32 || (p.stepper != AIO_STEPPER_FINE && p.sub == 4),
                 "compressed stored wavefields need the interval-blocked stepper (sub == 4)");
         g = make_geom(p.nz, p.nx, p.nts, p.sub, p.minPad, p.nExt);
@@ -769,7 +770,8 @@ struct Context {
     // images use interior slices; the stored wavefield is FP32 or BF16.
     DevMem tbState, tbPart, tbImg, tbW, tbEnt, tbStart, tbDesc;
     struct TBPlan {
-        int T = 4, HZ = 0, nStrips = 0, LX = 0, nChunks = 0, iters = 0, threads = 0;
+        int T = 4, HZ = 0, nStrips = 0, LX = 0, nChunks = 0, iters = 0, threads = 0, NQ = 0;
+        bool tile = false;
     };
 
     bool tb_enabled() const { return P.stepper != AIO_STEPPER_FINE && g.sub == 4; }
@@ -777,6 +779,21 @@ struct Context {
 
     TBPlan tb_plan() const {
         TBPlan pl;
+        if (P.stepper == AIO_STEPPER_TILED) {
+            // k_tile: strips of HZ (multiple of 4) output rows, NQ = HZ/4 + 10 row quads,
+            // 8 column pairs per quad, x-chunks marched in blocks of 16 columns.
+            pl.tile = true;
+            const int maxHZ = 4 * (KT_MAXQ - 10);
+            pl.nStrips = (g.nzi + maxHZ - 1) / maxHZ;
+            pl.HZ = round_up((g.nzi + pl.nStrips - 1) / pl.nStrips, 4);
+            pl.NQ = pl.HZ / 4 + 10;
+            pl.threads = round_up(8 * pl.NQ, 32);
+            int target = P.chunkColumns > 0 ? P.chunkColumns : 160;
+            pl.nChunks = std::max(1, (g.nxi + target / 2) / target);
+            pl.LX = (g.nxi + pl.nChunks - 1) / pl.nChunks;
+            pl.iters = (pl.LX + 10 * pl.T + KT_BX - 1) / KT_BX;
+            return pl;
+        }
         const int maxHZ = TB_MAXROWS - 10 * pl.T;
         pl.nStrips = (g.nzi + maxHZ - 1) / maxHZ;
         pl.HZ = (g.nzi + pl.nStrips - 1) / pl.nStrips;
@@ -904,7 +921,53 @@ struct Context {
     }
 
     template <int MODE, int WP>
+    void kt_launch_t(const TBPlan& pl, int nb, TBArgs& a, int v) {
+        KTArgs k2;
+        std::memset(&k2, 0, sizeof(k2));
+        k2.g = a.g;
+        k2.c = a.c;
+        k2.v2 = a.v2;
+        k2.taper = a.taper;
+        k2.dm = a.dm;
+        k2.shots = tbDesc.as<TBShot>() + (size_t)v * nb;
+        std::copy(a.h, a.h + 2 * (SUB_MAX + 1), k2.h);
+        k2.its = a.its;
+        k2.HZ = pl.HZ;
+        k2.LX = pl.LX;
+        k2.nStrips = pl.nStrips;
+        k2.nChunks = pl.nChunks;
+        k2.NQ = pl.NQ;
+        k2.iters = pl.iters;
+        k2.maxEnt = a.maxEnt;
+        k2.wStride = a.wStride;
+        const size_t smem = kt_smem_bytes(pl.NQ, pl.iters, a.maxEnt);
+        static int attrDev = -1;
+        if (attrDev != dev) {
+            AIO_CK(cudaFuncSetAttribute(k_tile<MODE, WP>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            attrDev = dev;
+        }
+        require(smem <= 200 * 1024, "tiled stepper: shared memory plan exceeds 200 KiB");
+        require(pl.threads <= KT_MAXT, "tiled stepper: too many threads per CTA");
+        const bool timed = profEvery > 0 && (launches % profEvery) == 0;
+        std::pair<cudaEvent_t, cudaEvent_t> ev{};
+        if (timed) {
+            ev = take_events();
+            AIO_CK(cudaEventRecord(ev.first, st));
+        }
+        k_tile<MODE, WP><<<dim3(pl.nStrips, pl.nChunks, nb), pl.threads, smem, st>>>(k2);
+        AIO_CK(cudaGetLastError());
+        if (timed) {
+            AIO_CK(cudaEventRecord(ev.second, st));
+            evBusy.push_back(ev);
+            evPoints.push_back((long long)nb * g.nzi * g.nxi * pl.T);
+        }
+        launches++;
+        kernels++;
+    }
+
+    template <int MODE, int WP>
     void tb_launch_t(const TBPlan& pl, int nb, TBArgs& a, int v) {
+        if (pl.tile) return kt_launch_t<MODE, WP>(pl, nb, a, v);
         const size_t smem = tb_smem_bytes(pl.T, MODE, a.maxEnt);
         static int attrDev = -1;
         if (attrDev != dev) {

@@ -65,10 +65,37 @@ __global__ void __launch_bounds__(TZ* TY) k_step(const StepArgs a) {
             s[r][lane < FAT ? lane : TZ + lane] = hv;
         }
     }
-    __syncthreads();
 
     const int zi = z0 + lane;
     const int xb = x0 + ty * PX;
+    const float* __restrict__ ssA = (INJ == 2) ? ssBase + a.ssOffA : nullptr;
+    const float* __restrict__ ssB = (INJ == 2) ? ssBase + a.ssOffB : nullptr;
+    float* __restrict__ accA = ACC ? accBase + a.accOffA : nullptr;
+    float* __restrict__ accB = ACC ? accBase + a.accOffB : nullptr;
+
+    // Point operands are loaded before the barrier so that their latency overlaps
+    // the tile load (each point is read and written by this thread only).
+    float ov[PX], pv[PX], sa[PX], sb[PX], aa[PX], ab[PX];
+#pragma unroll
+    for (int j = 0; j < PX; j++) {
+        const int xi = xb + j;
+        ov[j] = pv[j] = sa[j] = sb[j] = aa[j] = ab[j] = 0.f;
+        if (zi < g.nzi && xi < g.nxi) {
+            const long long hidx = (long long)(xi + FAT) * g.hp + ZOFF + zi;
+            const long long iidx = (long long)xi * g.ip + zi;
+            ov[j] = old[hidx];
+            pv[j] = ADJ ? cur[hidx] : __ldg(a.v2 + iidx);
+            if (INJ == 2) {
+                sa[j] = ssA[iidx];
+                sb[j] = ssB[iidx];
+            }
+            if (ACC) {
+                aa[j] = accA[iidx];
+                ab[j] = accB[iidx];
+            }
+        }
+    }
+    __syncthreads();
     float inj[PX];
 #pragma unroll
     for (int j = 0; j < PX; j++) inj[j] = 0.f;
@@ -88,11 +115,6 @@ __global__ void __launch_bounds__(TZ* TY) k_step(const StepArgs a) {
             }
         }
     }
-
-    const float* __restrict__ ssA = (INJ == 2) ? ssBase + a.ssOffA : nullptr;
-    const float* __restrict__ ssB = (INJ == 2) ? ssBase + a.ssOffB : nullptr;
-    float* __restrict__ accA = ACC ? accBase + a.accOffA : nullptr;
-    float* __restrict__ accB = ACC ? accBase + a.accOffB : nullptr;
 
     float w[PX + 2 * FAT];
 #pragma unroll
@@ -121,22 +143,22 @@ __global__ void __launch_bounds__(TZ* TY) k_step(const StepArgs a) {
             const long long iidx = (long long)xi * g.ip + zi;
             const int d = min(dzd, min(xi, g.nxi - 1 - xi));
             const float D = d < g.minPad ? __ldg(a.taper + d) : 1.f;
-            const float o = D * old[hidx];
+            const float o = D * ov[j];
             float n;
             if (ADJ) {
-                const float cr = cur[hidx];
+                const float cr = pv[j];
                 n = lap + cr + cr - o;
             } else {
-                n = __ldg(a.v2 + iidx) * lap + c + c - o;
+                n = pv[j] * lap + c + c - o;
             }
             if (INJ == 1) n = n + inj[j];
-            if (INJ == 2) n = n + (ssA[iidx] * a.hInjA + ssB[iidx] * a.hInjB);
+            if (INJ == 2) n = n + (sa[j] * a.hInjA + sb[j] * a.hInjB);
             const float sv = n * D;
             S[j] = sv;
             old[hidx] = sv;
             if (ACC) {
-                accA[iidx] += sv * a.hAccA;
-                accB[iidx] += sv * a.hAccB;
+                accA[iidx] = aa[j] + sv * a.hAccA;
+                accB[iidx] = ab[j] + sv * a.hAccB;
             }
         }
     }

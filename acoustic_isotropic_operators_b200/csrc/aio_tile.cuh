@@ -1,0 +1,462 @@
+// Tiled interval stepper: one launch advances every shot of a wave by one
+// coarse interval (T = sub = 4 fine steps), on 2-D register micro-tiles.
+//
+// Each CTA owns an interior z-strip of HZ output rows (recomputing 5*T halo
+// rows on each side: R = HZ + 10T rows, NQ = R/4 row quads) and an x-chunk of
+// LX output columns, and marches along x in blocks of BX = 16 columns. At
+// iteration k the input block starts at column B = xs + 16k and time level t
+// (t = 1..T) is computed on the columns [B - 5t, B - 5t + 16): the blocks of
+// consecutive levels are skewed by the stencil half-width, so level t only
+// needs level t-1 columns that are already in shared memory. Every time level
+// 0..T-1 lives in a shared ring of KT_CB = 32 columns; one barrier separates
+// the levels of an iteration.
+//
+// A thread owns a 4 (z) x 2 (x) micro-tile: row quad q (rows 4q..4q+3 of the
+// strip, one float4) in columns c0, c0+1. Per level it reads 5 quads of each of
+// its two columns (z-stencil and centre) and one quad of each of the 10
+// neighbouring columns (x-stencil) as float4 from the ring of level t-1.
+//
+// The scheme per fine step is the reference's (F/src/kernelsGpu.cu:202-219,
+// 513-552): S_t = D * (v2 * L(S_{t-1}) + 2 S_{t-1} - D * S_{t-2} + injection),
+// with the second damping of p_cur applied when the level is used as p_old,
+// D = taper[min(dist_z, dist_x)] = min(Dz, Dx) (monotone taper) and D = 0
+// outside the interior so the zero boundary stays zero. Adjoint passes use the
+// same recursion on U = v2 * S (stepAdjGpu, :574-610, multiplied by v2
+// point-wise).
+//
+// Per-interval products — the coarse source-wavefield sample, receiver data,
+// the imaging condition — are formed from the T levels of each output point
+// when level T is computed; level T itself is only written to global memory.
+// State slices use the interior layout (pitch ip = round_up(nzi, 32)).
+#pragma once
+#include <cuda_bf16.h>
+
+#include "aio_common.cuh"
+#include "aio_tb.cuh"
+
+namespace aio {
+
+constexpr int KT_T = 4;        // fine steps per launch (sub)
+constexpr int KT_BX = 16;      // block columns per iteration
+constexpr int KT_CB = 32;      // ring depth in columns (>= BX + 5T - 5 + 1 for the output reads)
+constexpr int KT_PADQ = 2;     // zero quads above and below every ring column
+constexpr int KT_MAXQ = 50;    // row quads per strip (R <= 200)
+constexpr int KT_MAXT = (8 * KT_MAXQ + 31) / 32 * 32;  // threads per CTA (8 column pairs per quad)
+static_assert(KT_CB >= KT_BX + 5 * KT_T - 5 + 1, "output stage reads level 1 5(T-1) columns behind its block");
+static_assert(KT_CB >= KT_BX + 10, "a level is read 10 columns behind its block");
+
+struct KTArgs {
+    Geom g;
+    Coefs c;
+    const float* v2;       // interior slice (pitch ip)
+    const float* taper;    // minPad entries
+    const float* dm;       // SCAT: scaled model perturbation (interior slice)
+    const TBShot* shots;
+    float h[2 * (SUB_MAX + 1)];
+    int its;               // coarse interval
+    int HZ, LX;            // strip rows (multiple of 4) / chunk columns
+    int nStrips, nChunks;
+    int NQ;                // row quads per strip (HZ/4 + 10)
+    int iters;             // iterations per CTA
+    int maxEnt;            // shared entry capacity
+    long long wStride;     // elements per stored coarse slice (= isz)
+};
+
+__host__ __device__ inline int kt_ring_stride(int NQ) { return (NQ + 2 * KT_PADQ) * 4; }
+inline size_t kt_smem_bytes(int NQ, int iters, int maxEnt) {
+    return ((size_t)KT_T * KT_CB * kt_ring_stride(NQ) + (size_t)iters * KT_BX + 64) * sizeof(float) +
+           (size_t)maxEnt * sizeof(TBEnt);
+}
+
+template <int WPREC>
+__device__ __forceinline__ float4 kt_wload4(const void* W, long long idx) {
+    if (WPREC == TBW_F32) return __ldg(reinterpret_cast<const float4*>((const float*)W + idx));
+    const uint2 r = __ldg(reinterpret_cast<const uint2*>((const __nv_bfloat16*)W + idx));
+    const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162*>(&r.x);
+    const __nv_bfloat162 b = *reinterpret_cast<const __nv_bfloat162*>(&r.y);
+    const float2 fa = __bfloat1622float2(a), fb = __bfloat1622float2(b);
+    return make_float4(fa.x, fa.y, fb.x, fb.y);
+}
+
+template <int WPREC>
+__device__ __forceinline__ void kt_wstore4(void* W, long long idx, const float v[4]) {
+    if (WPREC == TBW_F32) {
+        *reinterpret_cast<float4*>((float*)W + idx) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+        const __nv_bfloat162 a = __floats2bfloat162_rn(v[0], v[1]);
+        const __nv_bfloat162 b = __floats2bfloat162_rn(v[2], v[3]);
+        uint2 r;
+        r.x = *reinterpret_cast<const unsigned*>(&a);
+        r.y = *reinterpret_cast<const unsigned*>(&b);
+        *reinterpret_cast<uint2*>((__nv_bfloat16*)W + idx) = r;
+    }
+}
+
+__device__ __forceinline__ float4 kt_ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ void kt_st4(float* p, const float v[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ float kt_el(const float4& v, int i) {
+    return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
+}
+
+template <int MODE, int WPREC>
+__global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
+    constexpr int T = KT_T;
+    extern __shared__ float4 kt_smem4[];
+    const int NQ = a.NQ;
+    const int RS = kt_ring_stride(NQ);
+    float* ring = reinterpret_cast<float*>(kt_smem4);         // [T][KT_CB][RS]
+    float* dxt = ring + T * KT_CB * RS;                         // column damping, columns xs-32 ...
+    TBEnt* sEnt = reinterpret_cast<TBEnt*>(dxt + a.iters * KT_BX + 64);
+
+    const Geom& g = a.g;
+    const TBShot sh = a.shots[blockIdx.z];
+    float* __restrict__ pNcur = sh.ncur;
+    float* __restrict__ pNold = sh.nold;
+    const float* __restrict__ pPart = sh.part;
+    float* __restrict__ pPartOut = sh.partOut;
+    double* __restrict__ pImg = sh.img;
+    float* __restrict__ pRec = sh.recSig;
+    const float* __restrict__ pInj = sh.injSig;
+    const float* __restrict__ cur = sh.cur;
+    const float* __restrict__ old = sh.old;
+    const float* __restrict__ v2p = a.v2;
+    const float* __restrict__ dmp = a.dm;
+    const int injLd = sh.injLd, recLd = sh.recLd;
+    const int strip = blockIdx.x, chunk = blockIdx.y;
+    const int ip = g.ip, nxi = g.nxi, nzi = g.nzi, H = g.H, sub = g.sub, its = a.its;
+
+    const int tid = threadIdx.x;
+    const int cp = tid / NQ;              // column pair 0..7 (>= 8: idle thread)
+    const int q = tid - cp * NQ;          // row quad
+    const bool act = cp < KT_BX / 2;
+    const int z0 = strip * a.HZ;
+    const int zq = z0 - 5 * T + 4 * q;    // first row of the quad (multiple of 4)
+    const int x0 = chunk * a.LX;
+    const int x1 = min(x0 + a.LX, nxi);
+    const int xs = x0 - 5 * T;
+
+    // ---- shared set-up: zero rings, column damping table, sparse entries
+    const int nRing = T * KT_CB * RS;
+    for (int i = tid; i < nRing; i += blockDim.x) ring[i] = 0.f;
+    const int nDx = a.iters * KT_BX + 64;
+    for (int i = tid; i < nDx; i += blockDim.x) {
+        const int c = xs - 32 + i;
+        float d = 0.f;
+        if (c >= 0 && c < nxi) {
+            const int dd = min(c, nxi - 1 - c);
+            d = dd < g.minPad ? __ldg(a.taper + dd) : 1.f;
+        }
+        dxt[i] = d;
+    }
+    int nInj = 0, nRec = 0, recOff = 0;
+    if (sh.entStart) {
+        const int4 se = sh.entStart[strip * a.nChunks + chunk];
+        const int n = min(se.w - se.x, a.maxEnt);
+        for (int i = tid; i < n; i += blockDim.x) sEnt[i] = sh.ent[se.x + i];
+        nInj = se.y - se.x;
+        recOff = se.z - se.x;
+        nRec = se.w - se.z;
+    }
+    __syncthreads();
+    // does any injection / recording point fall in this thread's row quad?
+    bool qInj = false, qRec = false;
+    for (int e = 0; e < nInj; e++) qInj |= (unsigned)(sEnt[e].row - zq) < 4u;
+    for (int e = 0; e < nRec; e++) qRec |= (unsigned)(sEnt[recOff + e].row - zq) < 4u;
+    int injPtr[T];
+#pragma unroll
+    for (int t = 0; t < T; t++) injPtr[t] = 0;
+    int recPtr = 0;
+
+    // ---- per-thread constants
+    float Dz[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int z = zq + i;
+        float d = 0.f;
+        if (z >= 0 && z < nzi) {
+            const int dd = min(z, nzi - 1 - z);
+            d = dd < g.minPad ? __ldg(a.taper + dd) : 1.f;
+        }
+        Dz[i] = d;
+    }
+    const bool zLoad = act && zq >= 0 && zq < nzi;        // quad holds interior rows
+    const int zv = min(max(zq, 0), ip - 4);               // clamped quad for v2 / operand reads
+    const bool zOut = act && q >= 5 * T / 4 && q < 5 * T / 4 + a.HZ / 4 && zq < nzi;
+    float zc[6], xc[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) {
+        zc[i] = a.c.zc[i];
+        xc[i] = a.c.xc[i];
+    }
+    float* const ringQ = ring + (KT_PADQ + q) * 4;  // quad q of ring column 0, level 0
+
+    // ---- input staging: the block of iteration k+1 is loaded during iteration k
+    float4 nCur[2], nOld[2];
+    auto load_input = [&](int k) {
+        const int B = xs + KT_BX * k;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int c = B + 2 * cp + j;
+            nCur[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (zLoad && c >= 0 && c < nxi) nCur[j] = __ldg(reinterpret_cast<const float4*>(cur + (long long)c * ip + zq));
+            const int co = B - 5 + 2 * cp + j;  // level-1 centre columns of iteration k
+            nOld[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (zLoad && co >= 0 && co < nxi) nOld[j] = __ldg(reinterpret_cast<const float4*>(old + (long long)co * ip + zq));
+        }
+    };
+    auto store_input = [&](int k) {
+        const int B = xs + KT_BX * k;
+        if (act) {
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                const float v[4] = {nCur[j].x, nCur[j].y, nCur[j].z, nCur[j].w};
+                kt_st4(ringQ + ((B + 2 * cp + j) & (KT_CB - 1)) * RS, v);
+            }
+        }
+    };
+    load_input(0);
+    store_input(0);
+    float4 pOld[2] = {nOld[0], nOld[1]};
+    load_input(1);
+    __syncthreads();
+
+    for (int k = 0; k < a.iters; k++) {
+        const int B = xs + KT_BX * k;
+        // Output operands of this iteration's level-T columns (issued early).
+        float4 oPart[2], oW[2];
+        double oImg[2][4];
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            oPart[j] = oW[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+            for (int i = 0; i < 4; i++) oImg[j][i] = 0.0;
+            const int c = B - 5 * T + 2 * cp + j;
+            if ((MODE == TB_SRC || MODE == TB_ADJ) && zOut && c >= x0 && c < x1) {
+                const long long idx = (long long)c * ip + zq;
+                oPart[j] = __ldg(reinterpret_cast<const float4*>(pPart + idx));
+                if (MODE == TB_ADJ) {
+                    oW[j] = kt_wload4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, its + 1), idx);
+                    const double2 i0 = *reinterpret_cast<const double2*>(pImg + idx);
+                    const double2 i1 = *reinterpret_cast<const double2*>(pImg + idx + 2);
+                    oImg[j][0] = i0.x; oImg[j][1] = i0.y; oImg[j][2] = i1.x; oImg[j][3] = i1.y;
+                }
+            }
+        }
+
+        float lvT[2][T + 1][4];  // levels 1..T at the output columns (T-1 from the rings)
+#pragma unroll
+        for (int t = 1; t <= T; t++) {
+            const int c0 = B - 5 * t + 2 * cp;
+            // level t is valid on columns >= xs + 5t and needed up to x1 - 1 + 5(T - t)
+            const bool need = act && q >= (5 * t) / 4 && q < NQ - (5 * t) / 4 &&
+                              c0 + 1 >= xs + 5 * t && c0 <= x1 - 1 + 5 * (T - t);
+            float S[2][4];
+            if (t == 3) store_input(k + 1);  // level-0 slots of columns [B-16, B): last read by level 2
+            if (need) {
+                const float* L = ringQ + (t - 1) * KT_CB * RS;
+                float4 zq4[2][5];
+#pragma unroll
+                for (int j = 0; j < 2; j++)
+#pragma unroll
+                    for (int d = 0; d < 5; d++) zq4[j][d] = kt_ld4(L + ((c0 + j) & (KT_CB - 1)) * RS + 4 * (d - 2));
+                float4 xm[5], xp[5];  // columns c0-5..c0-1 and c0+2..c0+6
+#pragma unroll
+                for (int d = 0; d < 5; d++) {
+                    xm[d] = kt_ld4(L + ((c0 - 5 + d) & (KT_CB - 1)) * RS);
+                    xp[d] = kt_ld4(L + ((c0 + 2 + d) & (KT_CB - 1)) * RS);
+                }
+                float4 ol[2];
+                if (t == 1) {
+                    ol[0] = pOld[0];
+                    ol[1] = pOld[1];
+                } else {
+                    const float* Lo = ringQ + (t - 2) * KT_CB * RS;
+                    ol[0] = kt_ld4(Lo + (c0 & (KT_CB - 1)) * RS);
+                    ol[1] = kt_ld4(Lo + ((c0 + 1) & (KT_CB - 1)) * RS);
+                }
+                float4 vq[2];
+                float Dx[2];
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int c = c0 + j;
+                    vq[j] = __ldg(reinterpret_cast<const float4*>(v2p + (long long)min(max(c, 0), nxi - 1) * ip + zv));
+                    Dx[j] = dxt[c - xs + 32];
+                }
+                float4 sa[2], sb[2];
+                if (MODE == TB_SCAT) {
+#pragma unroll
+                    for (int j = 0; j < 2; j++) {
+                        const long long idx = (long long)min(max(c0 + j, 0), nxi - 1) * ip + zv;
+                        const float4 dmv = __ldg(reinterpret_cast<const float4*>(dmp + idx));
+                        const float4 wa = kt_wload4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, its), idx);
+                        const float4 wb = kt_wload4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, its + 1), idx);
+                        sa[j] = make_float4(dmv.x * wa.x, dmv.y * wa.y, dmv.z * wa.z, dmv.w * wa.w);
+                        sb[j] = make_float4(dmv.x * wb.x, dmv.y * wb.y, dmv.z * wb.z, dmv.w * wb.w);
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    // x-neighbour columns of column c0+j: offsets -5..5 map to xm / xp / the other column
+                    float4 xn[11];
+#pragma unroll
+                    for (int d = -5; d <= 5; d++) {
+                        const int o = j + d;  // offset from c0
+                        xn[d + 5] = o < 0 ? xm[o + 5] : (o == 0 ? zq4[0][2] : (o == 1 ? zq4[1][2] : xp[o - 2]));
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        float zz[11];  // rows i-5 .. i+5 of this column
+#pragma unroll
+                        for (int d = -5; d <= 5; d++) {
+                            const int r = i + d + 8;  // 0..18 over quads q-2..q+2
+                            zz[d + 5] = kt_el(zq4[j][r >> 2], r & 3);
+                        }
+                        const float ctr = zz[5];
+                        const float lz = zc[0] * ctr + zc[1] * (zz[4] + zz[6]) + zc[2] * (zz[3] + zz[7]) +
+                                         zc[3] * (zz[2] + zz[8]) + zc[4] * (zz[1] + zz[9]) + zc[5] * (zz[0] + zz[10]);
+                        const float lx = xc[0] * ctr + xc[1] * (kt_el(xn[6], i) + kt_el(xn[4], i)) +
+                                         xc[2] * (kt_el(xn[7], i) + kt_el(xn[3], i)) +
+                                         xc[3] * (kt_el(xn[8], i) + kt_el(xn[2], i)) +
+                                         xc[4] * (kt_el(xn[9], i) + kt_el(xn[1], i)) +
+                                         xc[5] * (kt_el(xn[10], i) + kt_el(xn[0], i));
+                        const float Dm = fminf(Dz[i], Dx[j]);
+                        float n = kt_el(vq[j], i) * (lz + lx) + ctr + ctr - Dm * kt_el(ol[j], i);
+                        if (MODE == TB_SCAT) n = n + (kt_el(sa[j], i) * a.h[t - 1] + kt_el(sb[j], i) * a.h[H + t - 1]);
+                        S[j][i] = n;  // damped below, after injection
+                    }
+                }
+                // sparse injection into this micro-tile (entries sorted by column)
+                if (MODE != TB_SCAT && qInj) {
+                    int p = injPtr[t - 1];
+                    while (p < nInj && sEnt[p].col < c0) p++;
+                    injPtr[t - 1] = p;
+                    for (int e = p; e < nInj && sEnt[e].col <= c0 + 1; e++) {
+                        const int rr = sEnt[e].row - zq;
+                        if (rr >= 0 && rr < 4) {
+                            const float* tr = pInj + (long long)sEnt[e].dev * injLd;
+                            const int j = sEnt[e].col - c0;
+                            float v;
+                            if (MODE == TB_ADJ) {
+                                const int it2 = sub - t;
+                                v = kt_el(j ? vq[1] : vq[0], rr) * (tr[its] * a.h[it2 + 1] + tr[its + 1] * a.h[H + it2 + 1]);
+                            } else {
+                                v = tr[its * sub + t - 1];
+                            }
+#pragma unroll
+                            for (int jj = 0; jj < 2; jj++)
+#pragma unroll
+                                for (int i = 0; i < 4; i++)
+                                    if (jj == j && i == rr) S[jj][i] = S[jj][i] + v;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < 2; j++)
+#pragma unroll
+                    for (int i = 0; i < 4; i++) S[j][i] = S[j][i] * fminf(Dz[i], Dx[j]);
+                if (t < T) {
+                    float* Lw = ringQ + t * KT_CB * RS;
+#pragma unroll
+                    for (int j = 0; j < 2; j++) kt_st4(Lw + ((c0 + j) & (KT_CB - 1)) * RS, S[j]);
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 2; j++)
+#pragma unroll
+                    for (int i = 0; i < 4; i++) S[j][i] = 0.f;
+            }
+            if (t == T) {
+#pragma unroll
+                for (int j = 0; j < 2; j++)
+#pragma unroll
+                    for (int i = 0; i < 4; i++) lvT[j][T][i] = S[j][i];
+            }
+            __syncthreads();
+        }
+
+        // ---- outputs at the level-T columns [B - 5T, B - 5T + 16)
+        {
+            const int c0 = B - 5 * T + 2 * cp;
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                const int c = c0 + j;
+#pragma unroll
+                for (int l = 1; l < T; l++) {
+                    const float4 v = kt_ld4(ringQ + (l * KT_CB + (c & (KT_CB - 1))) * RS);
+                    lvT[j][l][0] = v.x; lvT[j][l][1] = v.y; lvT[j][l][2] = v.z; lvT[j][l][3] = v.w;
+                }
+                if (!(zOut && c >= x0 && c < x1)) continue;
+                const long long idx = (long long)c * ip + zq;
+                kt_st4(pNcur + idx, lvT[j][T]);
+                kt_st4(pNold + idx, lvT[j][T - 1]);
+                if (MODE == TB_SRC) {
+                    float wa[4], wb[4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        wa[i] = kt_el(oPart[j], i);
+                        wb[i] = 0.f;
+#pragma unroll
+                        for (int l = 1; l <= T; l++) {
+                            wa[i] += lvT[j][l][i] * a.h[l];
+                            wb[i] += lvT[j][l][i] * a.h[H + l];
+                        }
+                    }
+                    kt_st4(pPartOut + idx, wb);
+                    kt_wstore4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, its), idx, wa);
+                    if (its == g.nts - 2) kt_wstore4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, its + 1), idx, wb);
+                } else if (MODE == TB_ADJ) {
+                    float ra[4], rb[4];
+                    double acc[4];
+                    float4 w0 = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (its == 0) w0 = kt_wload4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, 0), idx);
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        ra[i] = 0.f;
+                        rb[i] = kt_el(oPart[j], i);
+#pragma unroll
+                        for (int l = 1; l <= T; l++) {
+                            ra[i] += lvT[j][l][i] * a.h[sub - l];
+                            rb[i] += lvT[j][l][i] * a.h[H + sub - l];
+                        }
+                        acc[i] = oImg[j][i] + (double)(kt_el(oW[j], i) * rb[i]);
+                        if (its == 0) acc[i] += (double)(kt_el(w0, i) * ra[i]);
+                    }
+                    kt_st4(pPartOut + idx, ra);
+                    *reinterpret_cast<double2*>(pImg + idx) = make_double2(acc[0], acc[1]);
+                    *reinterpret_cast<double2*>(pImg + idx + 2) = make_double2(acc[2], acc[3]);
+                } else if (qRec) {
+                    int p = recPtr;
+                    while (p < nRec && sEnt[recOff + p].col < c) p++;
+                    recPtr = p;
+                    for (int e = p; e < nRec && sEnt[recOff + e].col == c; e++) {
+                        const int rr = sEnt[recOff + e].row - zq;
+                        if (rr >= 0 && rr < 4) {
+                            float ra = 0.f, rb = 0.f;
+#pragma unroll
+                            for (int l = 1; l <= T; l++) {
+#pragma unroll
+                                for (int i = 0; i < 4; i++) {
+                                    if (i == rr) {
+                                        ra += lvT[j][l][i] * a.h[l];
+                                        rb += lvT[j][l][i] * a.h[H + l];
+                                    }
+                                }
+                            }
+                            float* tr = pRec + (long long)sEnt[recOff + e].dev * recLd;
+                            tr[its] += ra;
+                            tr[its + 1] += rb;
+                        }
+                    }
+                }
+            }
+        }
+        pOld[0] = nOld[0];
+        pOld[1] = nOld[1];
+        if (k + 2 <= a.iters) load_input(k + 2);
+        __syncthreads();
+    }
+}
+
+}  // namespace aio

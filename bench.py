@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-nts", type=int, default=0, help="coarse samples of the CPU sample (0 = auto)")
-    ap.add_argument("--stepper", default="auto", choices=["auto", "fine", "blocked"])
+    ap.add_argument("--stepper", default="auto", choices=["auto", "fine", "blocked", "tiled"])
     ap.add_argument("--chunk", type=int, default=0, help="blocked-stepper chunk width (0 = automatic)")
     return ap.parse_args()
 

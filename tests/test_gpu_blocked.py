@@ -1,5 +1,6 @@
-"""Interval-blocked stepper (one launch per coarse interval, sub = 4) vs the CPU
-oracle and vs the per-fine-step stepper.
+"""Interval-blocked steppers (one launch per coarse interval, sub = 4) vs the CPU
+oracle and vs the per-fine-step stepper: "blocked" (one thread per row) and
+"tiled" (2-D micro-tiles).
 
 The grid is chosen so the blocked kernel runs several z-strips and x-chunks,
 with sources on strip / chunk boundaries (the recomputed halo regions must
@@ -54,8 +55,12 @@ def shots(case, data=None):
             for i in range(len(case.src_pos))]
 
 
-def test_nonlinear_forward_blocked(case):
-    got = ctx(case, stepper="blocked").nonlinear_forward(shots(case))
+STEPPERS = ["blocked", "tiled"]
+
+
+@pytest.mark.parametrize("stepper", STEPPERS)
+def test_nonlinear_forward_blocked(case, stepper):
+    got = ctx(case, stepper=stepper).nonlinear_forward(shots(case))
     fine = ctx(case, stepper="fine").nonlinear_forward(shots(case))
     for i in range(len(got)):
         r32 = orc.nl_fwd(case.scheme, case.vel, case.sig[i], case.src_pos[i], case.rec_pos[i], dtype=np.float32)
@@ -63,9 +68,10 @@ def test_nonlinear_forward_blocked(case):
         assert rel_l2(got[i], fine[i]) < 1e-5
 
 
-def test_born_forward_blocked(case):
+@pytest.mark.parametrize("stepper", STEPPERS)
+def test_born_forward_blocked(case, stepper):
     m = case.rng.standard_normal((case.nx, case.nz)).astype(np.float32) * interior_mask(case.nx, case.nz)
-    c = ctx(case, stepper="blocked")
+    c = ctx(case, stepper=stepper)
     got = c.born_forward(m, shots(case))
     assert c.last_launches == 2 * (case.scheme.nts - 1)
     for i in range(len(got)):
@@ -73,17 +79,19 @@ def test_born_forward_blocked(case):
         assert rel_l2(got[i], r32) < 1e-5
 
 
-def test_born_adjoint_blocked(case):
+@pytest.mark.parametrize("stepper", STEPPERS)
+def test_born_adjoint_blocked(case, stepper):
     d = [case.rng.standard_normal((len(r), case.scheme.nts)).astype(np.float32) for r in case.rec_pos]
-    got = ctx(case, stepper="blocked").born_adjoint(shots(case, d))
+    got = ctx(case, stepper=stepper).born_adjoint(shots(case, d))
     r32 = sum(orc.born_adj(case.scheme, case.vel, d[i], case.sig[i], case.src_pos[i], case.rec_pos[i],
                            dtype=np.float32) for i in range(len(d)))
     assert rel_l2(got, r32) < 1e-5
     assert np.all(got[~interior_mask(case.nx, case.nz)] == 0)
 
 
-def test_born_dot_blocked(case):
-    c = ctx(case, stepper="blocked")
+@pytest.mark.parametrize("stepper", STEPPERS)
+def test_born_dot_blocked(case, stepper):
+    c = ctx(case, stepper=stepper)
     m = case.rng.standard_normal((case.nx, case.nz)).astype(np.float32) * interior_mask(case.nx, case.nz)
     d = [case.rng.standard_normal((len(r), case.scheme.nts)).astype(np.float32) for r in case.rec_pos]
     fm = c.born_forward(m, shots(case))
@@ -93,15 +101,33 @@ def test_born_dot_blocked(case):
     assert abs(a - b) / abs(b) < 1e-5
 
 
-def test_born_bf16_error(case):
+@pytest.mark.parametrize("stepper", STEPPERS)
+def test_born_bf16_error(case, stepper):
     m = case.rng.standard_normal((case.nx, case.nz)).astype(np.float32) * interior_mask(case.nx, case.nz)
-    got = ctx(case, stepper="blocked", wavefield="bf16").born_forward(m, shots(case))
+    got = ctx(case, stepper=stepper, wavefield="bf16").born_forward(m, shots(case))
     v64 = case.vel.astype(np.float64)
     for i in range(len(got)):
         r64 = orc.born_fwd(case.scheme, v64, m, case.sig[i], case.src_pos[i], case.rec_pos[i])
         assert rel_l2(got[i], r64) < 1e-2
     d = [case.rng.standard_normal((len(r), case.scheme.nts)).astype(np.float32) for r in case.rec_pos]
-    ga = ctx(case, stepper="blocked", wavefield="bf16").born_adjoint(shots(case, d))
+    ga = ctx(case, stepper=stepper, wavefield="bf16").born_adjoint(shots(case, d))
     r64 = sum(orc.born_adj(case.scheme, v64, d[i], case.sig[i], case.src_pos[i], case.rec_pos[i])
               for i in range(len(d)))
     assert rel_l2(ga, r64) < 1e-2
+
+
+@pytest.mark.parametrize("stepper", STEPPERS)
+def test_ragged_grid(stepper):
+    """Interior extents that are not multiples of 4, 16 or 32 (last strip / chunk / quad partial)."""
+    c = blocked_case(seed=9, nzi=250, nxi=203, nts=24, nshots=1)
+    got = ctx(c, stepper=stepper).nonlinear_forward(shots(c))[0]
+    r32 = orc.nl_fwd(c.scheme, c.vel, c.sig[0], c.src_pos[0], c.rec_pos[0], dtype=np.float32)
+    assert rel_l2(got, r32) < 1e-5
+    m = c.rng.standard_normal((c.nx, c.nz)).astype(np.float32) * interior_mask(c.nx, c.nz)
+    d = [c.rng.standard_normal((len(c.rec_pos[0]), c.scheme.nts)).astype(np.float32)]
+    ga = ctx(c, stepper=stepper).born_adjoint(shots(c, d))
+    ra = orc.born_adj(c.scheme, c.vel, d[0], c.sig[0], c.src_pos[0], c.rec_pos[0], dtype=np.float32)
+    assert rel_l2(ga, ra) < 1e-5
+    gf = ctx(c, stepper=stepper).born_forward(m, shots(c))[0]
+    rf = orc.born_fwd(c.scheme, c.vel, m, c.sig[0], c.src_pos[0], c.rec_pos[0], dtype=np.float32)
+    assert rel_l2(gf, rf) < 1e-5
