@@ -940,7 +940,7 @@ struct Context {
         k2.iters = pl.iters;
         k2.maxEnt = a.maxEnt;
         k2.wStride = a.wStride;
-        const size_t smem = kt_smem_bytes(pl.NQ, pl.iters, a.maxEnt);
+        const size_t smem = kt_smem_bytes(pl.iters, a.maxEnt);
         static int attrDev = -1;
         if (attrDev != dev) {
             AIO_CK(cudaFuncSetAttribute(k_tile<MODE, WP>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -948,6 +948,7 @@ struct Context {
         }
         require(smem <= 200 * 1024, "tiled stepper: shared memory plan exceeds 200 KiB");
         require(pl.threads <= KT_MAXT, "tiled stepper: too many threads per CTA");
+        require(pl.NQ <= KT_MAXQ, "tiled stepper: strip taller than the ring");
         const bool timed = profEvery > 0 && (launches % profEvery) == 0;
         std::pair<cudaEvent_t, cudaEvent_t> ev{};
         if (timed) {

@@ -40,7 +40,8 @@ constexpr int KT_T = 4;        // fine steps per launch (sub)
 constexpr int KT_BX = 16;      // block columns per iteration
 constexpr int KT_CB = 32;      // ring depth in columns (>= BX + 5T - 5 + 1 for the output reads)
 constexpr int KT_PADQ = 2;     // zero quads above and below every ring column
-constexpr int KT_MAXQ = 50;    // row quads per strip (R <= 200)
+constexpr int KT_MAXQ = 42;    // row quads per strip (R <= 168, HZ <= 128)
+constexpr int KT_RS = (KT_MAXQ + 2 * KT_PADQ) * 4;  // floats per ring column (compile-time offsets)
 constexpr int KT_MAXT = (8 * KT_MAXQ + 31) / 32 * 32;  // threads per CTA (8 column pairs per quad)
 static_assert(KT_CB >= KT_BX + 5 * KT_T - 5 + 1, "output stage reads level 1 5(T-1) columns behind its block");
 static_assert(KT_CB >= KT_BX + 10, "a level is read 10 columns behind its block");
@@ -62,9 +63,9 @@ struct KTArgs {
     long long wStride;     // elements per stored coarse slice (= isz)
 };
 
-__host__ __device__ inline int kt_ring_stride(int NQ) { return (NQ + 2 * KT_PADQ) * 4; }
-inline size_t kt_smem_bytes(int NQ, int iters, int maxEnt) {
-    return ((size_t)KT_T * KT_CB * kt_ring_stride(NQ) + (size_t)iters * KT_BX + 64) * sizeof(float) +
+// rings, column damping table, per-launch injection values (T per entry), entries
+inline size_t kt_smem_bytes(int iters, int maxEnt) {
+    return ((size_t)KT_T * KT_CB * KT_RS + (size_t)iters * KT_BX + 64 + (size_t)maxEnt * KT_T) * sizeof(float) +
            (size_t)maxEnt * sizeof(TBEnt);
 }
 
@@ -105,10 +106,11 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
     constexpr int T = KT_T;
     extern __shared__ float4 kt_smem4[];
     const int NQ = a.NQ;
-    const int RS = kt_ring_stride(NQ);
+    constexpr int RS = KT_RS;
     float* ring = reinterpret_cast<float*>(kt_smem4);         // [T][KT_CB][RS]
     float* dxt = ring + T * KT_CB * RS;                         // column damping, columns xs-32 ...
-    TBEnt* sEnt = reinterpret_cast<TBEnt*>(dxt + a.iters * KT_BX + 64);
+    float* sInjV = dxt + a.iters * KT_BX + 64;                  // [maxEnt][T] injection value per level
+    TBEnt* sEnt = reinterpret_cast<TBEnt*>(sInjV + a.maxEnt * T);
 
     const Geom& g = a.g;
     const TBShot sh = a.shots[blockIdx.z];
@@ -160,6 +162,23 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
         nRec = se.w - se.z;
     }
     __syncthreads();
+    // Injected values of this interval, one per entry and fine step, read once here
+    // instead of inside the level loop (adjoint: the v2 factor is applied at use).
+    if (MODE != TB_SCAT) {
+        for (int i = tid; i < nInj * T; i += blockDim.x) {
+            const int e = i / T, t = i - e * T + 1;
+            const float* tr = pInj + (long long)sEnt[e].dev * injLd;
+            float v;
+            if (MODE == TB_ADJ) {
+                const int it2 = sub - t;
+                v = tr[its] * a.h[it2 + 1] + tr[its + 1] * a.h[H + it2 + 1];
+            } else {
+                v = tr[its * sub + t - 1];
+            }
+            sInjV[i] = v;
+        }
+    }
+    __syncthreads();
     // does any injection / recording point fall in this thread's row quad?
     bool qInj = false, qRec = false;
     for (int e = 0; e < nInj; e++) qInj |= (unsigned)(sEnt[e].row - zq) < 4u;
@@ -193,7 +212,7 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
     float* const ringQ = ring + (KT_PADQ + q) * 4;  // quad q of ring column 0, level 0
 
     // ---- input staging: the block of iteration k+1 is loaded during iteration k
-    float4 nCur[2], nOld[2];
+    float4 nCur[2], nOld[2], nV[2];
     auto load_input = [&](int k) {
         const int B = xs + KT_BX * k;
 #pragma unroll
@@ -204,6 +223,7 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
             const int co = B - 5 + 2 * cp + j;  // level-1 centre columns of iteration k
             nOld[j] = make_float4(0.f, 0.f, 0.f, 0.f);
             if (zLoad && co >= 0 && co < nxi) nOld[j] = __ldg(reinterpret_cast<const float4*>(old + (long long)co * ip + zq));
+            nV[j] = __ldg(reinterpret_cast<const float4*>(v2p + (long long)min(max(co, 0), nxi - 1) * ip + zv));
         }
     };
     auto store_input = [&](int k) {
@@ -219,6 +239,7 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
     load_input(0);
     store_input(0);
     float4 pOld[2] = {nOld[0], nOld[1]};
+    float4 pV[2] = {nV[0], nV[1]};
     load_input(1);
     __syncthreads();
 
@@ -281,9 +302,16 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
 #pragma unroll
                 for (int j = 0; j < 2; j++) {
                     const int c = c0 + j;
-                    vq[j] = __ldg(reinterpret_cast<const float4*>(v2p + (long long)min(max(c, 0), nxi - 1) * ip + zv));
+                    // level 1: prefetched with the input; later levels re-read the same lines from L1
+                    vq[j] = (t == 1) ? pV[j]
+                                     : __ldg(reinterpret_cast<const float4*>(v2p + (long long)min(max(c, 0), nxi - 1) * ip + zv));
                     Dx[j] = dxt[c - xs + 32];
                 }
+                float Dm[2][4];
+#pragma unroll
+                for (int j = 0; j < 2; j++)
+#pragma unroll
+                    for (int i = 0; i < 4; i++) Dm[j][i] = fminf(Dz[i], Dx[j]);
                 float4 sa[2], sb[2];
                 if (MODE == TB_SCAT) {
 #pragma unroll
@@ -321,8 +349,7 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                                          xc[3] * (kt_el(xn[8], i) + kt_el(xn[2], i)) +
                                          xc[4] * (kt_el(xn[9], i) + kt_el(xn[1], i)) +
                                          xc[5] * (kt_el(xn[10], i) + kt_el(xn[0], i));
-                        const float Dm = fminf(Dz[i], Dx[j]);
-                        float n = kt_el(vq[j], i) * (lz + lx) + ctr + ctr - Dm * kt_el(ol[j], i);
+                        float n = kt_el(vq[j], i) * (lz + lx) + ctr + ctr - Dm[j][i] * kt_el(ol[j], i);
                         if (MODE == TB_SCAT) n = n + (kt_el(sa[j], i) * a.h[t - 1] + kt_el(sb[j], i) * a.h[H + t - 1]);
                         S[j][i] = n;  // damped below, after injection
                     }
@@ -335,15 +362,9 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                     for (int e = p; e < nInj && sEnt[e].col <= c0 + 1; e++) {
                         const int rr = sEnt[e].row - zq;
                         if (rr >= 0 && rr < 4) {
-                            const float* tr = pInj + (long long)sEnt[e].dev * injLd;
                             const int j = sEnt[e].col - c0;
-                            float v;
-                            if (MODE == TB_ADJ) {
-                                const int it2 = sub - t;
-                                v = kt_el(j ? vq[1] : vq[0], rr) * (tr[its] * a.h[it2 + 1] + tr[its + 1] * a.h[H + it2 + 1]);
-                            } else {
-                                v = tr[its * sub + t - 1];
-                            }
+                            float v = sInjV[e * T + t - 1];
+                            if (MODE == TB_ADJ) v = kt_el(j ? vq[1] : vq[0], rr) * v;
 #pragma unroll
                             for (int jj = 0; jj < 2; jj++)
 #pragma unroll
@@ -355,7 +376,7 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
 #pragma unroll
                 for (int j = 0; j < 2; j++)
 #pragma unroll
-                    for (int i = 0; i < 4; i++) S[j][i] = S[j][i] * fminf(Dz[i], Dx[j]);
+                    for (int i = 0; i < 4; i++) S[j][i] = S[j][i] * Dm[j][i];
                 if (t < T) {
                     float* Lw = ringQ + t * KT_CB * RS;
 #pragma unroll
@@ -444,9 +465,10 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                                     }
                                 }
                             }
+                            // one thread owns each receiver: the atomics are plain read-free adds
                             float* tr = pRec + (long long)sEnt[recOff + e].dev * recLd;
-                            tr[its] += ra;
-                            tr[its + 1] += rb;
+                            atomicAdd(tr + its, ra);
+                            atomicAdd(tr + its + 1, rb);
                         }
                     }
                 }
@@ -454,6 +476,8 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
         }
         pOld[0] = nOld[0];
         pOld[1] = nOld[1];
+        pV[0] = nV[0];
+        pV[1] = nV[1];
         if (k + 2 <= a.iters) load_input(k + 2);
         __syncthreads();
     }
