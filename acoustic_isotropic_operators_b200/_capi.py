@@ -24,7 +24,7 @@ AIO_MEM_HOST = 0
 AIO_MEM_DEVICE = 1
 AIO_NONLINEAR, AIO_BORN, AIO_BORN_EXT, AIO_TOMO_EXT, AIO_WEMVA_EXT = range(5)
 AIO_WFLD_FP32, AIO_WFLD_BF16, AIO_WFLD_FP16 = range(3)
-AIO_STEPPER_AUTO, AIO_STEPPER_FINE, AIO_STEPPER_BLOCKED, AIO_STEPPER_TILED = range(4)
+AIO_STEPPER_AUTO, AIO_STEPPER_FINE, AIO_STEPPER_BLOCKED = range(3)
 
 EXPORTED = [
     "aio_last_error", "aio_context_create", "aio_context_destroy", "aio_context_set_velocity",

@@ -53,7 +53,7 @@ class Context:
         p = A.AioParams(nz, nx, nts, sub, minPad, nExt, dz, dx, dts, alphaCos, leg1, leg2, sloth,
                         _WFLD[wavefield], int(bool(image_fp64)), device, int(mem_budget_bytes),
                         {"auto": A.AIO_STEPPER_AUTO, "fine": A.AIO_STEPPER_FINE,
-                         "blocked": A.AIO_STEPPER_BLOCKED, "tiled": A.AIO_STEPPER_TILED}[stepper], int(chunk_columns))
+                         "blocked": A.AIO_STEPPER_BLOCKED}[stepper], int(chunk_columns))
         v2 = np.ascontiguousarray(vel2Dtw2, dtype=np.float32).reshape(-1)
         rs = None if reflectivity_scale is None else np.ascontiguousarray(reflectivity_scale,
                                                                           dtype=np.float32).reshape(-1)

@@ -19,7 +19,6 @@
 
 #include "aio_b200.h"
 #include "aio_kernels.cuh"
-#include "aio_tb.cuh"
 #include "aio_tile.cuh"
 
 namespace aio {
@@ -167,6 +166,7 @@ struct Context {
     Geom g;
     HostConsts k;
     int dev = 0;
+    int smCount = 148;  // streaming multiprocessors of `dev`
     cudaStream_t st = nullptr;
     DevMem v2, rs, taper;
     // per-wave buffers
@@ -194,7 +194,7 @@ struct Context {
         require(p.nExt >= 1 && (p.nExt % 2) == 1, "nExt must be a positive odd number");
         require(p.wavefieldPrecision == AIO_WFLD_FP32 || p.wavefieldPrecision == AIO_WFLD_BF16,
                 "stored wavefield precision must be AIO_WFLD_FP32 or AIO_WFLD_BF16");
-        require(p.stepper >= AIO_STEPPER_AUTO && p.stepper <= AIO_STEPPER_TILED, "unknown stepper");
+        require(p.stepper >= AIO_STEPPER_AUTO && p.stepper <= AIO_STEPPER_BLOCKED, "unknown stepper");
         require(p.stepper < AIO_STEPPER_BLOCKED || p.sub == 4, "the interval-blocked steppers require sub == 4");
         require(p.wavefieldPrecision == AIO_WFLD_FP32 || (p.stepper != AIO_STEPPER_FINE && p.sub == 4),
                 "compressed stored wavefields need the interval-blocked stepper (sub == 4)");
@@ -206,6 +206,7 @@ struct Context {
         dev = p.device;
         AIO_CK(cudaSetDevice(dev));
         AIO_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        AIO_CK(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, dev));
         v2.ensure(g.isz * 4);
         rs.ensure(g.isz * 4);
         taper.ensure(PAD_MAX * 4);
@@ -769,39 +770,50 @@ struct Context {
     // One launch per coarse interval (aio_tb.cuh). State, partial sums and
     // images use interior slices; the stored wavefield is FP32 or BF16.
     DevMem tbState, tbPart, tbImg, tbW, tbEnt, tbStart, tbDesc;
+    // k_tile plan: strips of HZ (multiple of 4) output rows, NQ = HZ/4 + 10 row quads,
+    // 8 column pairs per quad, x-chunks of LX columns marched in blocks of 16.
     struct TBPlan {
-        int T = 4, HZ = 0, nStrips = 0, LX = 0, nChunks = 0, iters = 0, threads = 0, NQ = 0;
-        bool tile = false;
+        int T = KT_T, HZ = 0, nStrips = 0, LX = 0, nChunks = 0, iters = 0, threads = 0, NQ = 0;
     };
 
-    bool tb_enabled() const { return P.stepper != AIO_STEPPER_FINE && g.sub == 4; }
+    bool tb_enabled() const { return P.stepper != AIO_STEPPER_FINE && g.sub == KT_T; }
     int wbytes() const { return P.wavefieldPrecision == AIO_WFLD_BF16 ? 2 : 4; }
 
-    TBPlan tb_plan() const {
+    // nb: shots of the wave (one CTA column per shot)
+    TBPlan tb_plan(int nb) const {
         TBPlan pl;
-        if (P.stepper == AIO_STEPPER_TILED) {
-            // k_tile: strips of HZ (multiple of 4) output rows, NQ = HZ/4 + 10 row quads,
-            // 8 column pairs per quad, x-chunks marched in blocks of 16 columns.
-            pl.tile = true;
-            const int maxHZ = 4 * (KT_MAXQ - 10);
-            pl.nStrips = (g.nzi + maxHZ - 1) / maxHZ;
-            pl.HZ = round_up((g.nzi + pl.nStrips - 1) / pl.nStrips, 4);
-            pl.NQ = pl.HZ / 4 + 10;
-            pl.threads = round_up(8 * pl.NQ, 32);
-            int target = P.chunkColumns > 0 ? P.chunkColumns : 160;
-            pl.nChunks = std::max(1, (g.nxi + target / 2) / target);
-            pl.LX = (g.nxi + pl.nChunks - 1) / pl.nChunks;
-            pl.iters = (pl.LX + 10 * pl.T + KT_BX - 1) / KT_BX;
-            return pl;
-        }
-        const int maxHZ = TB_MAXROWS - 10 * pl.T;
+        const int maxHZ = 4 * (KT_MAXQ - 10);
         pl.nStrips = (g.nzi + maxHZ - 1) / maxHZ;
-        pl.HZ = (g.nzi + pl.nStrips - 1) / pl.nStrips;
-        pl.threads = round_up(pl.HZ + 10 * pl.T, 32);
-        int target = P.chunkColumns > 0 ? P.chunkColumns : 128;
-        pl.nChunks = std::max(1, (g.nxi + target / 2) / target);
+        pl.HZ = round_up((g.nzi + pl.nStrips - 1) / pl.nStrips, 4);
+        pl.NQ = pl.HZ / 4 + 10;
+        pl.threads = round_up(8 * pl.NQ, 32);
+        if (P.chunkColumns > 0) {
+            pl.nChunks = std::max(1, (g.nxi + P.chunkColumns / 2) / P.chunkColumns);
+        } else {
+            // Chunk count minimising the modelled time: whole CTA waves over the SMs
+            // (one resident CTA per SM) times the iterations of one CTA (each chunk
+            // recomputes 10T warm-up columns). At least 4 waves are preferred so that
+            // CTAs of uneven cost (strips holding sources / receivers) balance out.
+            double best = 1e300, bestAny = 1e300;
+            int ncAny = 1;
+            pl.nChunks = 0;
+            for (int nc = 1; nc <= std::max(1, g.nxi / 48); nc++) {
+                const int lx = (g.nxi + nc - 1) / nc;
+                const long long ctas = (long long)pl.nStrips * nc * nb;
+                const double cost = (double)((ctas + smCount - 1) / smCount) * ((lx + 10 * pl.T + KT_BX - 1) / KT_BX);
+                if (cost < bestAny * 0.999) {
+                    bestAny = cost;
+                    ncAny = nc;
+                }
+                if (ctas >= 4LL * smCount && cost < best * 0.999) {
+                    best = cost;
+                    pl.nChunks = nc;
+                }
+            }
+            if (pl.nChunks == 0) pl.nChunks = ncAny;
+        }
         pl.LX = (g.nxi + pl.nChunks - 1) / pl.nChunks;
-        pl.iters = round_up(pl.LX + 10 * pl.T + TBD, TBQ);
+        pl.iters = (pl.LX + 10 * pl.T + KT_BX - 1) / KT_BX;
         return pl;
     }
 
@@ -901,8 +913,8 @@ struct Context {
         AIO_CK(cudaMemcpyAsync(tbDesc.p, d.data(), d.size() * sizeof(TBShot), cudaMemcpyHostToDevice, st));
     }
 
-    TBArgs tb_args(const TBPlan& pl, int maxEnt, const float* dm) const {
-        TBArgs a;
+    KTArgs tb_args(const TBPlan& pl, int maxEnt, const float* dm) const {
+        KTArgs a;
         std::memset(&a, 0, sizeof(a));
         a.g = g;
         a.c = k.c;
@@ -914,6 +926,7 @@ struct Context {
         a.LX = pl.LX;
         a.nStrips = pl.nStrips;
         a.nChunks = pl.nChunks;
+        a.NQ = pl.NQ;
         a.iters = pl.iters;
         a.maxEnt = maxEnt;
         a.wStride = g.isz;
@@ -921,61 +934,15 @@ struct Context {
     }
 
     template <int MODE, int WP>
-    void kt_launch_t(const TBPlan& pl, int nb, TBArgs& a, int v) {
-        KTArgs k2;
-        std::memset(&k2, 0, sizeof(k2));
-        k2.g = a.g;
-        k2.c = a.c;
-        k2.v2 = a.v2;
-        k2.taper = a.taper;
-        k2.dm = a.dm;
-        k2.shots = tbDesc.as<TBShot>() + (size_t)v * nb;
-        std::copy(a.h, a.h + 2 * (SUB_MAX + 1), k2.h);
-        k2.its = a.its;
-        k2.HZ = pl.HZ;
-        k2.LX = pl.LX;
-        k2.nStrips = pl.nStrips;
-        k2.nChunks = pl.nChunks;
-        k2.NQ = pl.NQ;
-        k2.iters = pl.iters;
-        k2.maxEnt = a.maxEnt;
-        k2.wStride = a.wStride;
+    void tb_launch_t(const TBPlan& pl, int nb, KTArgs& a, int v) {
         const size_t smem = kt_smem_bytes(pl.iters, a.maxEnt);
         static int attrDev = -1;
         if (attrDev != dev) {
             AIO_CK(cudaFuncSetAttribute(k_tile<MODE, WP>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
             attrDev = dev;
         }
-        require(smem <= 200 * 1024, "tiled stepper: shared memory plan exceeds 200 KiB");
-        require(pl.threads <= KT_MAXT, "tiled stepper: too many threads per CTA");
-        require(pl.NQ <= KT_MAXQ, "tiled stepper: strip taller than the ring");
-        const bool timed = profEvery > 0 && (launches % profEvery) == 0;
-        std::pair<cudaEvent_t, cudaEvent_t> ev{};
-        if (timed) {
-            ev = take_events();
-            AIO_CK(cudaEventRecord(ev.first, st));
-        }
-        k_tile<MODE, WP><<<dim3(pl.nStrips, pl.nChunks, nb), pl.threads, smem, st>>>(k2);
-        AIO_CK(cudaGetLastError());
-        if (timed) {
-            AIO_CK(cudaEventRecord(ev.second, st));
-            evBusy.push_back(ev);
-            evPoints.push_back((long long)nb * g.nzi * g.nxi * pl.T);
-        }
-        launches++;
-        kernels++;
-    }
-
-    template <int MODE, int WP>
-    void tb_launch_t(const TBPlan& pl, int nb, TBArgs& a, int v) {
-        if (pl.tile) return kt_launch_t<MODE, WP>(pl, nb, a, v);
-        const size_t smem = tb_smem_bytes(pl.T, MODE, a.maxEnt);
-        static int attrDev = -1;
-        if (attrDev != dev) {
-            AIO_CK(cudaFuncSetAttribute(k_interval<4, MODE, WP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)tb_smem_bytes(4, MODE, 4096)));
-            attrDev = dev;
-        }
+        require(smem <= 200 * 1024, "blocked stepper: shared memory plan exceeds 200 KiB (too many devices per tile)");
+        require(pl.threads <= KT_MAXT && pl.NQ <= KT_MAXQ, "blocked stepper: strip taller than the ring");
         a.shots = tbDesc.as<TBShot>() + (size_t)v * nb;
         const bool timed = profEvery > 0 && (launches % profEvery) == 0;
         std::pair<cudaEvent_t, cudaEvent_t> ev{};
@@ -983,7 +950,7 @@ struct Context {
             ev = take_events();
             AIO_CK(cudaEventRecord(ev.first, st));
         }
-        k_interval<4, MODE, WP><<<dim3(pl.nStrips, pl.nChunks, nb), pl.threads, smem, st>>>(a);
+        k_tile<MODE, WP><<<dim3(pl.nStrips, pl.nChunks, nb), pl.threads, smem, st>>>(a);
         AIO_CK(cudaGetLastError());
         if (timed) {
             AIO_CK(cudaEventRecord(ev.second, st));
@@ -994,7 +961,7 @@ struct Context {
         kernels++;
     }
     template <int MODE>
-    void tb_launch(const TBPlan& pl, int nb, TBArgs& a, int v) {
+    void tb_launch(const TBPlan& pl, int nb, KTArgs& a, int v) {
         if (P.wavefieldPrecision == AIO_WFLD_BF16) tb_launch_t<MODE, TBW_BF16>(pl, nb, a, v);
         else tb_launch_t<MODE, TBW_F32>(pl, nb, a, v);
     }
@@ -1008,11 +975,11 @@ struct Context {
     // Source pass storing W[nts] (F/src/BornShotsGpuFunctions.cu:297-321), or the
     // nonlinear forward when recordData (F/src/nonlinearShotsGpuFunctions.cu:269-295).
     void tb_src_pass(int nb, const aio_shot* shots, bool nonlinear) {
-        const TBPlan pl = tb_plan();
+        const TBPlan pl = tb_plan(nb);
         const int maxEnt = tb_lists(pl, nb, shots, 1, nonlinear);
         tb_zero(nb, false);
         tb_desc(pl, nb, true, false, nonlinear, nonlinear ? nullptr : tbW.p, false);
-        TBArgs a = tb_args(pl, maxEnt, nullptr);
+        KTArgs a = tb_args(pl, maxEnt, nullptr);
         for (int its = 0; its < g.nts - 1; its++) {
             a.its = its;
             if (nonlinear) tb_launch<TB_NL>(pl, nb, a, its & 1);
@@ -1022,11 +989,11 @@ struct Context {
 
     // Scattered pass with data recording (F/src/BornShotsGpuFunctions.cu:323-376).
     void tb_scat_pass(int nb, const aio_shot* shots, const float* dm) {
-        const TBPlan pl = tb_plan();
+        const TBPlan pl = tb_plan(nb);
         const int maxEnt = tb_lists(pl, nb, shots, 0, true);
         tb_zero(nb, false);
         tb_desc(pl, nb, false, false, true, tbW.p, false);
-        TBArgs a = tb_args(pl, maxEnt, dm);
+        KTArgs a = tb_args(pl, maxEnt, dm);
         for (int its = 0; its < g.nts - 1; its++) {
             a.its = its;
             tb_launch<TB_SCAT>(pl, nb, a, its & 1);
@@ -1037,11 +1004,11 @@ struct Context {
     // Launch L handles interval its = nts-2-L: it reads the partial R(its+1) written by
     // launch L-1 and writes R(its); state ping-pongs with L.
     void tb_adj_pass(int nb, const aio_shot* shots) {
-        const TBPlan pl = tb_plan();
+        const TBPlan pl = tb_plan(nb);
         const int maxEnt = tb_lists(pl, nb, shots, 2, false);
         tb_zero(nb, true);
         tb_desc(pl, nb, false, true, false, tbW.p, false);
-        TBArgs a = tb_args(pl, maxEnt, nullptr);
+        KTArgs a = tb_args(pl, maxEnt, nullptr);
         for (int L = 0; L < g.nts - 1; L++) {
             a.its = g.nts - 2 - L;
             tb_launch<TB_ADJ>(pl, nb, a, L & 1);

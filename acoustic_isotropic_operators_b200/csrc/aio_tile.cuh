@@ -100,6 +100,15 @@ __device__ __forceinline__ void kt_st4(float* p, const float v[4]) {
 __device__ __forceinline__ float kt_el(const float4& v, int i) {
     return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
 }
+// rows (2h, 2h+1) of a quad
+__device__ __forceinline__ float2 kt_half(const float4& v, int h) {
+    return h == 0 ? make_float2(v.x, v.y) : make_float2(v.z, v.w);
+}
+// rows (r, r+1), r in [-8, 10], of the 20-row window held as quads Z[0..4] (rows -8..11)
+__device__ __forceinline__ float2 kt_pair(const float4 (&Z)[5], int r) {
+    const int i = r + 8;
+    return make_float2(kt_el(Z[i >> 2], i & 3), kt_el(Z[(i + 1) >> 2], (i + 1) & 3));
+}
 
 template <int MODE, int WPREC>
 __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
@@ -203,11 +212,11 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
     const bool zLoad = act && zq >= 0 && zq < nzi;        // quad holds interior rows
     const int zv = min(max(zq, 0), ip - 4);               // clamped quad for v2 / operand reads
     const bool zOut = act && q >= 5 * T / 4 && q < 5 * T / 4 + a.HZ / 4 && zq < nzi;
-    float zc[6], xc[6];
+    float2 zc2[6], xc2[6];  // coefficients, duplicated for paired instructions
 #pragma unroll
     for (int i = 0; i < 6; i++) {
-        zc[i] = a.c.zc[i];
-        xc[i] = a.c.xc[i];
+        zc2[i] = make_float2(a.c.zc[i], a.c.zc[i]);
+        xc2[i] = make_float2(a.c.xc[i], a.c.xc[i]);
     }
     float* const ringQ = ring + (KT_PADQ + q) * 4;  // quad q of ring column 0, level 0
 
@@ -333,25 +342,29 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                         const int o = j + d;  // offset from c0
                         xn[d + 5] = o < 0 ? xm[o + 5] : (o == 0 ? zq4[0][2] : (o == 1 ? zq4[1][2] : xp[o - 2]));
                     }
+                    // Two rows per paired FP32 instruction (f32x2): rows (2P, 2P+1) of the quad.
+                    // z-neighbour pairs at even offsets are register pairs of the loaded quads;
+                    // odd offsets pair rows of two quads (kt_pair builds them).
 #pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        float zz[11];  // rows i-5 .. i+5 of this column
+                    for (int P = 0; P < 2; P++) {
+                        const int a0 = 2 * P;
+                        const float2 ctr = kt_pair(zq4[j], a0);
+                        float2 lz = __fmul2_rn(zc2[0], ctr);
 #pragma unroll
-                        for (int d = -5; d <= 5; d++) {
-                            const int r = i + d + 8;  // 0..18 over quads q-2..q+2
-                            zz[d + 5] = kt_el(zq4[j][r >> 2], r & 3);
-                        }
-                        const float ctr = zz[5];
-                        const float lz = zc[0] * ctr + zc[1] * (zz[4] + zz[6]) + zc[2] * (zz[3] + zz[7]) +
-                                         zc[3] * (zz[2] + zz[8]) + zc[4] * (zz[1] + zz[9]) + zc[5] * (zz[0] + zz[10]);
-                        const float lx = xc[0] * ctr + xc[1] * (kt_el(xn[6], i) + kt_el(xn[4], i)) +
-                                         xc[2] * (kt_el(xn[7], i) + kt_el(xn[3], i)) +
-                                         xc[3] * (kt_el(xn[8], i) + kt_el(xn[2], i)) +
-                                         xc[4] * (kt_el(xn[9], i) + kt_el(xn[1], i)) +
-                                         xc[5] * (kt_el(xn[10], i) + kt_el(xn[0], i));
-                        float n = kt_el(vq[j], i) * (lz + lx) + ctr + ctr - Dm[j][i] * kt_el(ol[j], i);
-                        if (MODE == TB_SCAT) n = n + (kt_el(sa[j], i) * a.h[t - 1] + kt_el(sb[j], i) * a.h[H + t - 1]);
-                        S[j][i] = n;  // damped below, after injection
+                        for (int kk = 1; kk <= 5; kk++)
+                            lz = __ffma2_rn(zc2[kk], __fadd2_rn(kt_pair(zq4[j], a0 + kk), kt_pair(zq4[j], a0 - kk)), lz);
+                        float2 lx = __fmul2_rn(xc2[0], ctr);
+#pragma unroll
+                        for (int kk = 1; kk <= 5; kk++)
+                            lx = __ffma2_rn(xc2[kk], __fadd2_rn(kt_half(xn[5 + kk], P), kt_half(xn[5 - kk], P)), lx);
+                        float2 n = __ffma2_rn(kt_half(vq[j], P), __fadd2_rn(lz, lx), ctr);
+                        n = __fadd2_rn(n, ctr);
+                        n = __ffma2_rn(make_float2(-Dm[j][a0], -Dm[j][a0 + 1]), kt_half(ol[j], P), n);
+                        if (MODE == TB_SCAT)
+                            n = __fadd2_rn(n, __ffma2_rn(kt_half(sb[j], P), make_float2(a.h[H + t - 1], a.h[H + t - 1]),
+                                                         __fmul2_rn(kt_half(sa[j], P), make_float2(a.h[t - 1], a.h[t - 1]))));
+                        S[j][a0] = n.x;  // damped below, after injection
+                        S[j][a0 + 1] = n.y;
                     }
                 }
                 // sparse injection into this micro-tile (entries sorted by column)

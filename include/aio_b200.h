@@ -71,8 +71,7 @@ typedef struct {
 
 #define AIO_STEPPER_AUTO 0      /* interval-blocked where available (sub == 4), else per fine step */
 #define AIO_STEPPER_FINE 1      /* one fused launch per fine step (the reference's schedule) */
-#define AIO_STEPPER_BLOCKED 2   /* one launch per coarse interval (requires sub == 4) */
-#define AIO_STEPPER_TILED 3     /* one launch per coarse interval on 2-D micro-tiles (requires sub == 4) */
+#define AIO_STEPPER_BLOCKED 2   /* one launch per coarse interval, 2-D register tiles (requires sub == 4) */
 
 typedef struct {
     const int* sourcesPositionReg;   /* host array, nSourcesReg */

@@ -1,6 +1,5 @@
-"""Interval-blocked steppers (one launch per coarse interval, sub = 4) vs the CPU
-oracle and vs the per-fine-step stepper: "blocked" (one thread per row) and
-"tiled" (2-D micro-tiles).
+"""Interval-blocked stepper (one launch per coarse interval, sub = 4, 2-D
+register tiles) vs the CPU oracle and vs the per-fine-step stepper.
 
 The grid is chosen so the blocked kernel runs several z-strips and x-chunks,
 with sources on strip / chunk boundaries (the recomputed halo regions must
@@ -55,7 +54,7 @@ def shots(case, data=None):
             for i in range(len(case.src_pos))]
 
 
-STEPPERS = ["blocked", "tiled"]
+STEPPERS = ["blocked"]
 
 
 @pytest.mark.parametrize("stepper", STEPPERS)
