@@ -1564,6 +1564,18 @@ AIO_API int aio_nonlinear_forward(aio_context* ctx, int nShots, const aio_shot* 
 AIO_API int aio_nonlinear_adjoint(aio_context* ctx, int nShots, const aio_shot* shots, int memSpace) {
     return guard([&] { ctx->c.nonlinear_adjoint(nShots, shots, memSpace, nullptr); });
 }
+AIO_API int aio_nonlinear_forward_wavefield(aio_context* ctx, const aio_shot* shot, int memSpace, float* wavefield) {
+    return guard([&] {
+        require(wavefield != nullptr, "wavefield output is NULL");
+        ctx->c.nonlinear_forward(1, shot, memSpace, wavefield);
+    });
+}
+AIO_API int aio_nonlinear_adjoint_wavefield(aio_context* ctx, const aio_shot* shot, int memSpace, float* wavefield) {
+    return guard([&] {
+        require(wavefield != nullptr, "wavefield output is NULL");
+        ctx->c.nonlinear_adjoint(1, shot, memSpace, wavefield);
+    });
+}
 AIO_API int aio_born_forward(aio_context* ctx, const float* model, int nShots, const aio_shot* shots, int memSpace) {
     return guard([&] { ctx->c.born_forward(model, nShots, shots, memSpace); });
 }

@@ -109,6 +109,11 @@ int aio_context_reset_stats(aio_context* ctx);
 /* Nonlinear: model = source traces (sourcesSignals), data per shot. */
 int aio_nonlinear_forward(aio_context* ctx, int nShots, const aio_shot* shots, int memSpace);
 int aio_nonlinear_adjoint(aio_context* ctx, int nShots, const aio_shot* shots, int memSpace);
+/* One shot with its coarse wavefield [nts][nx][nz] (host) written out: nonlinear forward
+ * (F/src/nonlinearShotsGpuFunctions.cu:310-395, propShotsFwdGpuWavefield) and adjoint
+ * (:653-739, propShotsAdjGpuWavefield; unscaled, the caller applies dtw^2 v^2). */
+int aio_nonlinear_forward_wavefield(aio_context* ctx, const aio_shot* shot, int memSpace, float* wavefield);
+int aio_nonlinear_adjoint_wavefield(aio_context* ctx, const aio_shot* shot, int memSpace, float* wavefield);
 /* Born: model nz*nx (shared by all shots). adjoint: add=0 overwrites, add=1 accumulates. */
 int aio_born_forward(aio_context* ctx, const float* model, int nShots, const aio_shot* shots, int memSpace);
 int aio_born_adjoint(aio_context* ctx, float* model, int add, int nShots, const aio_shot* shots, int memSpace);

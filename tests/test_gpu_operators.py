@@ -1,0 +1,132 @@
+"""Reference-named operator classes (pybind11 modules pyAcoustic_iso_float_*) on
+the GPU: results against the CPU oracle fed by the oracle's own host chain
+(spread to the grid, d2/dt2, dtw^2 v^2, fine-time interpolation), and the
+reference's dot-product test through Operator::dotTest for every family.
+
+Tolerances: relative L2 1e-5 against the FP32 oracle (the FP32 parity bar);
+dot tests at the reference's default maxError 1e-5.
+"""
+import numpy as np
+import pytest
+
+import orc
+from cases import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+NZI, NXI, NTS, DTS, SUB, PAD = 32, 48, 40, 0.004, 3, 8
+NZ, NX = NZI + 10, NXI + 10
+
+
+@pytest.fixture(scope="module")
+def api():
+    from acoustic_isotropic_operators_b200 import reference_api
+    return reference_api
+
+
+@pytest.fixture(scope="module")
+def setup(api):
+    rng = np.random.default_rng(5)
+    zz = np.linspace(0, 1, NZ)[None, :]
+    vel = (2000.0 + 400.0 * zz + 50.0 * rng.random((NX, NZ))).astype(np.float32)
+    par = api.params(nts=NTS, dts=DTS, sub=SUB, nz=NZ, nx=NX, zPadMinus=PAD, zPadPlus=PAD, xPadMinus=PAD,
+                     xPadPlus=PAD, dz=10.0, dx=10.0, fMax=20.0, blockSize=16, fat=5, nShot=2, iGpu=[0], nExt=5,
+                     leg1=1, leg2=1)
+    v = api.vector(vel, [(NZ, 0.0, 10.0), (NX, 0.0, 10.0)])
+    nl = api.pyAcoustic_iso_float_nl
+    srcs = [nl.deviceGpu([9], [15], v, NTS, 0, 0, 0), nl.deviceGpu([10], [40], v, NTS, 0, 0, 0)]
+    rec = nl.deviceGpu([8] * 40, list(range(8, 48)), v, NTS, 0, 0, 0)
+    t = np.arange(NTS) * DTS - 0.05
+    wav = ((1 - 2 * (np.pi * 15 * t) ** 2) * np.exp(-(np.pi * 15 * t) ** 2)).astype(np.float32)
+    sig = api.vector(wav[None, :], [(NTS, 0.0, DTS), (1, 0.0, 1.0)])
+    s = orc.Scheme(nz=NZ, nx=NX, nts=NTS, dts=DTS, sub=SUB, dz=10.0, dx=10.0, minPad=PAD, nExt=5)
+    return dict(vel=vel, v=v, par=par, srcs=srcs, rec=rec, wav=wav, sig=sig, scheme=s, rng=rng)
+
+
+def oracle_source(st, dev, d2):
+    """Regular fine source traces of a grid-point device via the oracle's host chain."""
+    pos = np.array(dev.getRegPosUnique(), np.int32)
+    reg = np.zeros((len(pos), NTS))
+    reg[0] = st["wav"]                    # corner 0 carries weight 1, the other corners 0
+    if d2:
+        reg = orc.second_deriv(NTS, DTS, reg, dtype=np.float32)
+    dtw = np.float32(DTS / SUB)
+    vflat = st["vel"].reshape(-1)
+    reg = (reg * (dtw * dtw * vflat[pos] * vflat[pos])[:, None]).astype(np.float32)
+    return pos, orc.time_interp_fwd(NTS, DTS, SUB, reg, dtype=np.float32)
+
+
+def rec_gather(st, dreg):
+    """Irregular receiver traces from regular ones: each receiver is corner 0 of its 4."""
+    pos = st["rec"].getRegPosUnique()
+    index = {p: i for i, p in enumerate(pos)}
+    return np.stack([dreg[index[(8 + r) * NZ + 8]] for r in range(40)])
+
+
+def data_vec(api, values=None):
+    return api.vector(values, [(NTS, 0.0, DTS), (40, 0.0, 1.0), (2, 0.0, 1.0)])
+
+
+def test_born_forward_matches_oracle(api, setup):
+    st = setup
+    rng = np.random.default_rng(1)
+    m = np.zeros((NX, NZ), np.float32)
+    m[5:-5, 5:-5] = rng.standard_normal((NXI, NZI))
+    op = api.pyAcoustic_iso_float_born.BornShotsGpu(st["v"], st["par"], st["srcs"], [st["sig"]], [st["rec"]])
+    model = api.vector(m, [(NZ, 0.0, 10.0), (NX, 0.0, 10.0)])
+    data = data_vec(api)
+    op.forward(False, model, data)
+    got = data.getNdArray().copy()
+    rpos = np.array(st["rec"].getRegPosUnique(), np.int32)
+    for i, src in enumerate(st["srcs"]):
+        spos, sig = oracle_source(st, src, True)
+        dreg = orc.born_fwd(st["scheme"], st["vel"], m, sig, spos, rpos, dtype=np.float32)
+        assert rel_l2(got[i], rec_gather(st, dreg)) < 1e-5
+    # add=True accumulates
+    op.forward(True, model, data)
+    assert rel_l2(data.getNdArray(), 2 * got) < 1e-6
+
+
+def test_nonlinear_forward_matches_oracle(api, setup):
+    st = setup
+    op = api.pyAcoustic_iso_float_nl.nonlinearPropShotsGpu(st["v"], st["par"], st["srcs"], [st["rec"]])
+    model = api.vector(st["wav"][None, None, :], [(NTS, 0.0, DTS), (1, 0.0, 1.0), (1, 0.0, 1.0)])
+    data = data_vec(api)
+    op.forward(False, model, data)
+    rpos = np.array(st["rec"].getRegPosUnique(), np.int32)
+    for i, src in enumerate(st["srcs"]):
+        spos, sig = oracle_source(st, src, False)
+        dreg = orc.nl_fwd(st["scheme"], st["vel"], sig, spos, rpos, dtype=np.float32)
+        assert rel_l2(data.getNdArray()[i], rec_gather(st, dreg)) < 1e-5
+
+
+@pytest.mark.parametrize("family", ["nl", "born", "born_ext", "tomo", "wemva"])
+def test_dot_product(api, setup, family):
+    st = setup
+    rng = np.random.default_rng(7)
+    img2 = [(NZ, 0.0, 10.0), (NX, 0.0, 10.0)]
+    ext3 = [(NZ, 0.0, 10.0), (NX, 0.0, 10.0), (5, -2 * DTS, DTS)]
+    if family == "nl":
+        op = api.pyAcoustic_iso_float_nl.nonlinearPropShotsGpu(st["v"], st["par"], st["srcs"], [st["rec"]])
+        m1 = api.vector(None, [(NTS, 0.0, DTS), (1, 0.0, 1.0), (2, 0.0, 1.0)])
+        d1 = data_vec(api)
+    elif family == "born":
+        op = api.pyAcoustic_iso_float_born.BornShotsGpu(st["v"], st["par"], st["srcs"], [st["sig"]], [st["rec"]])
+        m1, d1 = api.vector(None, img2), data_vec(api)
+    elif family == "born_ext":
+        op = api.pyAcoustic_iso_float_born_ext.BornExtShotsGpu(st["v"], st["par"], st["srcs"], [st["sig"]], [st["rec"]])
+        m1, d1 = api.vector(None, ext3), data_vec(api)
+    elif family == "tomo":
+        refl = np.zeros((5, NX, NZ), np.float32)
+        refl[:, 5:-5, 5:-5] = rng.standard_normal((5, NXI, NZI))
+        op = api.pyAcoustic_iso_float_tomo.tomoExtShotsGpu(st["v"], st["par"], st["srcs"], [st["sig"]], [st["rec"]],
+                                                            api.vector(refl, ext3))
+        m1, d1 = api.vector(None, img2), data_vec(api)
+    else:
+        rd = [api.vector(rng.standard_normal((40, NTS)).astype(np.float32) * 1e-2, [(NTS, 0.0, DTS), (40, 0.0, 1.0)])
+              for _ in range(2)]
+        op = api.pyAcoustic_iso_float_wemva.wemvaExtShotsGpu(st["v"], st["par"], st["srcs"], [st["sig"]], [st["rec"]],
+                                                              rd)
+        m1, d1 = api.vector(None, img2), api.vector(None, ext3)
+    op.setDomainRange(m1, d1)
+    assert op.dotTest(False, 1e-5)
