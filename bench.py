@@ -209,8 +209,9 @@ def main():
     from acoustic_isotropic_operators_b200.batch import Context
     from acoustic_isotropic_operators_b200 import synthetic as S
 
+    from acoustic_isotropic_operators_b200.multigpu import max_over_ranks, reduce_image, shard
     full = workload(args, args.shots * world)
-    mine = full.shots[rank::world]
+    mine = [full.shots[i] for i in shard(len(full.shots), rank, world)]
     w = full
     lib = _capi.lib()
     v2 = np.zeros(w.nz * w.nx, np.float32)
@@ -257,12 +258,8 @@ def main():
         barrier()
     ctx.profile(0)
     kernels, step_ms, n_timed, step_pts = ctx.stats()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.all_reduce(image_d)  # the image stack across ranks (one reduction per adjoint)
+    ms = max_over_ranks(e0.elapsed_time(e1), device=dev)
+    reduce_image(image_d)  # the images of all ranks' shots (the one collective of the path)
     ms_per_step = ms / args.steps
     pts_per_step = w.n_interior * w.fine_steps * PASSES * args.shots * world
     value = pts_per_step / (ms_per_step / 1e3) / 1e9
@@ -304,11 +301,7 @@ def main():
             ctx.born_forward(model_h, host_shots)
             img = ctx.born_adjoint(host_shots)
         barrier()
-        e_ms = (time.perf_counter() - t0) * 1e3 / max(1, args.steps)
-        if dist:
-            t = torch.tensor([e_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
+        e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / max(1, args.steps), device=dev)
         h2d = model_h.nbytes + 2 * sum(s.nbytes for s in sigs) + sum(len(a.rec_pos) * w.nts * 4 for a in mine)
         d2h = sum(len(a.rec_pos) * w.nts * 4 for a in mine) + img.nbytes
         e2e = {"value": pts_per_step / (e_ms / 1e3) / 1e9, "unit": UNIT, "ms_per_step": e_ms,
