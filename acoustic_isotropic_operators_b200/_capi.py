@@ -31,7 +31,7 @@ EXPORTED = [
     "aio_context_wave_capacity", "aio_context_last_launches", "aio_context_stream", "aio_context_profile",
     "aio_context_stats", "aio_context_reset_stats",
     "aio_nonlinear_forward", "aio_nonlinear_adjoint", "aio_nonlinear_forward_wavefield",
-    "aio_nonlinear_adjoint_wavefield", "aio_born_forward", "aio_born_adjoint",
+    "aio_nonlinear_adjoint_wavefield", "aio_born_forward", "aio_born_adjoint", "aio_born_adjoint_shots",
     "aio_born_ext_forward", "aio_born_ext_adjoint", "aio_tomo_ext_forward", "aio_tomo_ext_adjoint",
     "aio_wemva_ext_forward", "aio_wemva_ext_adjoint",
     "aio_getGpuInfo",

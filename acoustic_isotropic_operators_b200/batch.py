@@ -158,6 +158,14 @@ class Context:
         A.check(A.lib().aio_born_adjoint(self._h, A.fptr(out), int(add), len(shots), arr, A.AIO_MEM_HOST))
         return out
 
+    def born_adjoint_shots(self, shots: List[Shot]) -> List[np.ndarray]:
+        """Born adjoint with one image per shot (the shots still run in the same launches)."""
+        outs = [np.zeros((self.nx, self.nz), np.float32) for _ in shots]
+        ptrs = (C.c_void_p * len(shots))(*[o.ctypes.data for o in outs])
+        arr = self._shots(shots, data_out=False)
+        A.check(A.lib().aio_born_adjoint_shots(self._h, ptrs, len(shots), arr, A.AIO_MEM_HOST))
+        return outs
+
     def born_ext_forward(self, model, shots: List[Shot]) -> List[np.ndarray]:
         m = self._model(model, self.nExt)
         arr = self._shots(shots, data_out=True)

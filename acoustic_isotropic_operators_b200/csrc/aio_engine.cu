@@ -769,7 +769,7 @@ struct Context {
     // ============================================================ blocked stepper
     // One launch per coarse interval (aio_tb.cuh). State, partial sums and
     // images use interior slices; the stored wavefield is FP32 or BF16.
-    DevMem tbState, tbPart, tbImg, tbW, tbEnt, tbStart, tbDesc;
+    DevMem tbState, tbPart, tbImg, tbW, tbEnt, tbStart, tbDesc, shotImg;
     // k_tile plan: strips of HZ (multiple of 4) output rows, NQ = HZ/4 + 10 row quads,
     // 8 column pairs per quad, x-chunks of LX columns marched in blocks of 16.
     struct TBPlan {
@@ -1112,8 +1112,11 @@ struct Context {
         }
     }
 
-    void born_adjoint_tb(float* modelOut, int add, int nShots, const aio_shot* shots, int mem) {
-        float* out = stage_out(modelOut, 1, add, mem);
+    // perShot: if non-null, perShot[s] receives shot s's own image (overwritten) and
+    // modelOut may be null.
+    void born_adjoint_tb(float* modelOut, int add, int nShots, const aio_shot* shots, int mem,
+                         float* const* perShot = nullptr) {
+        float* out = modelOut ? stage_out(modelOut, 1, add, mem) : nullptr;
         Needs n;
         for (int s0 = 0; s0 < nShots;) {
             const int nb = tb_wave_size(nShots - s0, shots + s0, true, true);
@@ -1127,13 +1130,33 @@ struct Context {
             k_scale_d<<<ew_grid(nb, nI), 256, 0, st>>>(tbImg.as<double>(), nI, 1, v2.as<float>(), rs.as<float>(),
                                                        g.isz, 3);
             kcheck();
-            k_sum_shots<double><<<ew_grid(1, nI), 256, 0, st>>>(out, tbImg.as<double>(), nI, nb, nI, 1);
-            kcheck();
+            if (out) {
+                k_sum_shots<double><<<ew_grid(1, nI), 256, 0, st>>>(out, tbImg.as<double>(), nI, nb, nI, 1);
+                kcheck();
+            }
+            if (perShot) {
+                shotImg.ensure((size_t)g.isz * 4);
+                for (int s = 0; s < nb; s++) {
+                    k_sum_shots<double><<<ew_grid(1, nI), 256, 0, st>>>(shotImg.as<float>(), tbImg.as<double>() + s * nI,
+                                                                        nI, 1, nI, 0);
+                    kcheck();
+                    write_model(perShot[s0 + s], 1, 0, mem, shotImg.as<float>());
+                }
+            }
             sync();
             s0 += nb;
         }
-        write_model(modelOut, 1, add, mem, out);
+        if (out) write_model(modelOut, 1, add, mem, out);
         sync();
+    }
+
+    // Born adjoint with one image per shot. Blocked stepper: all shots in the same
+    // launches; per-fine-step stepper: one shot per call.
+    void born_adjoint_shots(float* const* images, int nShots, const aio_shot* shots, int mem) {
+        begin_call();
+        for (int s = 0; s < nShots; s++) require(images && images[s], "per-shot image output is NULL");
+        if (tb_enabled()) return born_adjoint_tb(nullptr, 0, nShots, shots, mem, images);
+        for (int s = 0; s < nShots; s++) born_adjoint(images[s], 0, 1, shots + s, mem);
     }
 
     void nonlinear_forward_tb(int nShots, const aio_shot* shots, int mem) {
@@ -1582,6 +1605,10 @@ AIO_API int aio_born_forward(aio_context* ctx, const float* model, int nShots, c
 AIO_API int aio_born_adjoint(aio_context* ctx, float* model, int add, int nShots, const aio_shot* shots,
                              int memSpace) {
     return guard([&] { ctx->c.born_adjoint(model, add, nShots, shots, memSpace); });
+}
+AIO_API int aio_born_adjoint_shots(aio_context* ctx, float* const* images, int nShots, const aio_shot* shots,
+                                   int memSpace) {
+    return guard([&] { ctx->c.born_adjoint_shots(images, nShots, shots, memSpace); });
 }
 AIO_API int aio_born_ext_forward(aio_context* ctx, const float* model, int nShots, const aio_shot* shots,
                                  int memSpace) {

@@ -1,0 +1,358 @@
+"""Serving loop with continuous batching for operator requests of mixed grids and lengths.
+
+A request is one shot of one operator call — nonlinear forward, Born forward or
+Born adjoint — on a given grid / time axis / velocity (and model, for Born
+forward). The server keeps a FIFO of waiting requests and a set of GPU workers
+(one engine context and one CUDA stream per worker and grid, so batches of
+different workers overlap on the device). Whenever a worker is idle it takes
+the oldest waiting request together with every other waiting request that can
+share its launches — same operator, grid, velocity and model — up to
+``max_batch`` shots, provided their device memory fits in what the running
+batches leave of the HBM budget. Requests that arrive while others are on the
+GPU therefore join the next batch that frees a slot (continuous batching).
+Order: the oldest waiting request always leads the next batch (no request is
+passed over while it is at the head); later compatible requests may ride in
+that batch.
+
+Each request's result does not depend on what it was batched with: every shot
+of a launch is computed independently (the Born adjoint returns each shot's own
+image through ``aio_born_adjoint_shots``).
+
+Latency = completion - arrival, reported as p50 / p99 with throughput in
+shots/s (``Server.report``).
+"""
+from __future__ import annotations
+
+import threading
+import time
+from collections import deque
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional, Tuple
+
+import numpy as np
+
+OPS = ("nonlinear_forward", "born_forward", "born_adjoint")
+
+
+@dataclass(frozen=True)
+class Grid:
+    nz: int
+    nx: int
+    nts: int
+    dts: float
+    sub: int
+    dz: float
+    dx: float
+    minPad: int
+
+    @property
+    def interior_points(self) -> int:
+        return (self.nz - 10) * (self.nx - 10)
+
+    @property
+    def ntw(self) -> int:
+        return (self.nts - 1) * self.sub + 1
+
+
+@dataclass
+class Request:
+    op: str
+    grid: Grid
+    velocity_id: str                 # identity of (vel2Dtw2, reflectivityScale); equal ids share a context
+    vel2dtw2: np.ndarray
+    refl_scale: Optional[np.ndarray]
+    shot: object                     # batch.Shot
+    model_id: str = ""               # Born forward: identity of the model (equal ids share a launch)
+    model: Optional[np.ndarray] = None
+    arrival: float = field(default_factory=time.perf_counter)
+    start: float = 0.0
+    done: float = 0.0
+    future: Future = field(default_factory=Future, repr=False)
+
+    def key(self) -> Tuple:
+        return (self.op, self.grid, self.velocity_id, self.model_id if self.op == "born_forward" else "")
+
+
+def shot_bytes(req: Request, wavefield_bytes: int = 4) -> int:
+    """Device memory one shot of `req` needs in a batch (state, partial sums, stored wavefield, image)."""
+    g = req.grid
+    isz = ((g.nz - 10 + 31) // 32 * 32) * (g.nx - 10)
+    b = 4 * isz * 4 + 2 * isz * 4                       # 4 state slices + 2 partial-sum slices
+    if req.op != "nonlinear_forward":
+        b += g.nts * isz * wavefield_bytes              # stored source wavefield
+    if req.op == "born_adjoint":
+        b += isz * 8                                    # FP64 image
+    b += (len(req.shot.src_pos) * g.ntw + 2 * len(req.shot.rec_pos) * g.nts) * 4
+    return b
+
+
+def _engine_batch(ctx_cache: Dict, worker: int, reqs: List[Request], device: int, wavefield: str):
+    """Run one batch on this worker's context for the batch's grid (created on first use)."""
+    from .batch import Context
+    r0 = reqs[0]
+    g = r0.grid
+    key = (worker, g, r0.velocity_id)
+    ctx = ctx_cache.get(key)
+    if ctx is None:
+        ctx = Context(g.nz, g.nx, g.nts, g.dts, g.sub, g.dz, g.dx, g.minPad, r0.vel2dtw2, r0.refl_scale,
+                      image_fp64=True, device=device, wavefield=wavefield)
+        ctx_cache[key] = ctx
+    shots = [r.shot for r in reqs]
+    if r0.op == "nonlinear_forward":
+        return ctx.nonlinear_forward(shots)
+    if r0.op == "born_forward":
+        return ctx.born_forward(r0.model, shots)
+    return ctx.born_adjoint_shots(shots)
+
+
+class Server:
+    """Continuous-batching request server over the engine (see module docstring).
+
+    run_batch(worker, requests) -> list of results may replace the engine (tests of the
+    scheduling logic on CPU)."""
+
+    def __init__(self, *, device: int = 0, workers: int = 2, max_batch: int = 16,
+                 mem_budget_bytes: Optional[int] = None, wavefield: str = "fp32",
+                 run_batch: Optional[Callable] = None):
+        self.workers = workers
+        self.max_batch = max_batch
+        self.wavefield = wavefield
+        self.wbytes = 2 if wavefield in ("bf16", "fp16") else 4
+        if mem_budget_bytes is None:
+            import torch
+            free, _ = torch.cuda.mem_get_info(device)
+            mem_budget_bytes = int(0.8 * free)
+        self.budget = int(mem_budget_bytes)
+        self.in_use = 0
+        self._ctx: Dict = {}
+        self._run = run_batch or (lambda w, reqs: _engine_batch(self._ctx, w, reqs, device, wavefield))
+        self._queue: deque = deque()
+        self._idle = list(range(workers))
+        self._lock = threading.Condition()
+        self._closing = False
+        self.finished: List[Request] = []
+        self.batches: List[Tuple[int, int]] = []   # (worker, batch size)
+        self._threads: List[threading.Thread] = []
+        self._sched = threading.Thread(target=self._schedule, daemon=True)
+        self._sched.start()
+
+    # ------------------------------------------------------------------ client side
+    def submit(self, req: Request) -> Future:
+        if req.op not in OPS:
+            raise ValueError(f"unknown operator {req.op!r}")
+        need = shot_bytes(req, self.wbytes)
+        if need > self.budget:
+            raise ValueError(f"request needs {need} bytes, above the budget of {self.budget}")
+        with self._lock:
+            req.arrival = time.perf_counter() if not req.arrival else req.arrival
+            self._queue.append(req)
+            self._lock.notify_all()
+        return req.future
+
+    def close(self, wait: bool = True):
+        with self._lock:
+            self._closing = True
+            self._lock.notify_all()
+        if wait:
+            self._sched.join()
+            for t in self._threads:
+                t.join()
+        for c in self._ctx.values():
+            c.close()
+        self._ctx.clear()
+
+    # ------------------------------------------------------------------ scheduling
+    def _take_batch(self) -> Optional[List[Request]]:
+        """Oldest waiting request plus compatible waiting ones that fit in free memory."""
+        head = self._queue[0]
+        need = shot_bytes(head, self.wbytes)
+        if self.in_use + need > self.budget:
+            return None                                   # wait for memory; no overtaking of the head
+        batch, used = [head], need
+        key = head.key()
+        for r in list(self._queue)[1:]:
+            if len(batch) >= self.max_batch:
+                break
+            if r.key() == key:
+                b = shot_bytes(r, self.wbytes)
+                if self.in_use + used + b <= self.budget:
+                    batch.append(r)
+                    used += b
+        for r in batch:
+            self._queue.remove(r)
+        self.in_use += used
+        return batch
+
+    def _schedule(self):
+        while True:
+            with self._lock:
+                while True:
+                    if self._queue and self._idle:
+                        batch = self._take_batch()
+                        if batch is not None:
+                            break
+                    if self._closing and not self._queue:
+                        return
+                    self._lock.wait(timeout=0.05)
+                w = self._idle.pop(0)
+            t = threading.Thread(target=self._work, args=(w, batch), daemon=True)
+            self._threads.append(t)
+            t.start()
+
+    def _work(self, w: int, batch: List[Request]):
+        t0 = time.perf_counter()
+        for r in batch:
+            r.start = t0
+        err = None
+        try:
+            results = self._run(w, batch)
+        except Exception as e:  # reported through every future of the batch
+            err, results = e, [None] * len(batch)
+        t1 = time.perf_counter()
+        with self._lock:
+            self.in_use -= sum(shot_bytes(r, self.wbytes) for r in batch)
+            self._idle.append(w)
+            self.batches.append((w, len(batch)))
+            for r, res in zip(batch, results):
+                r.done = t1
+                self.finished.append(r)
+            self._lock.notify_all()
+        for r, res in zip(batch, results):
+            if err is not None:
+                r.future.set_exception(err)
+            else:
+                r.future.set_result(res)
+
+    # ------------------------------------------------------------------ report
+    def report(self) -> dict:
+        lat = np.array([r.done - r.arrival for r in self.finished])
+        if lat.size == 0:
+            return {"requests": 0}
+        t0 = min(r.arrival for r in self.finished)
+        t1 = max(r.done for r in self.finished)
+        pts = sum(r.grid.interior_points * (r.grid.nts - 1) * r.grid.sub * (1 if r.op == "nonlinear_forward" else 2)
+                  for r in self.finished)
+        return {"requests": int(lat.size), "shots_per_s": lat.size / (t1 - t0), "p50_s": float(np.percentile(lat, 50)),
+                "p99_s": float(np.percentile(lat, 99)), "mean_batch": float(np.mean([b for _, b in self.batches])),
+                "gpts_per_s": pts / (t1 - t0) / 1e9, "makespan_s": t1 - t0}
+
+
+# ---------------------------------------------------------------------------- benchmark
+def _stream(n_requests: int, n_models: int, scale: float, seed: int):
+    """Seeded served stream: models with grids uniform in [200x400, 1000x3000] m at 10 m (times
+    `scale`), gradient + blob velocities, nts uniform in [1000, 4000] (times `scale`), operators
+    one third each; every request is one shot on one of the models."""
+    from . import synthetic as S
+    rng = np.random.default_rng(seed)
+    models = []
+    for k in range(n_models):
+        nzp = int(rng.uniform(200, 1000) * scale) // 16 * 16 + 16
+        nxp = int(rng.uniform(400, 3000) * scale) // 16 * 16 + 16
+        nts = int(rng.uniform(1000, 4000) * scale)
+        d, dts = 10.0, 0.004
+        p = S.padding(nzp, nxp)
+        v = S.with_blobs(S.gradient(nzp, nxp), rng, d)
+        vel = S.pad_model(v.astype(np.float32), p)
+        sub = S.sub_for(float(v.max()), dts, d)
+        shots = [S.surface_acquisition(p, p.nz, int(x)) for x in np.linspace(0, nxp - 1, 8)]
+        g = Grid(p.nz, p.nx, nts, dts, sub, d, d, min(p.zPadMinus, p.zPadPlus, p.xPadMinus, p.xPadPlus))
+        models.append((g, vel, shots))
+    reqs = []
+    for i in range(n_requests):
+        k = int(rng.integers(n_models))
+        op = OPS[int(rng.integers(3))]
+        reqs.append((k, op, int(rng.integers(1 << 30))))
+    return models, reqs
+
+
+def main(argv=None):
+    import argparse
+    import ctypes as C
+    import json
+    from . import _capi
+    from .batch import Context, Shot
+    ap = argparse.ArgumentParser(description="served request stream vs one-shot-per-call plain path")
+    ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--models", type=int, default=4)
+    ap.add_argument("--scale", type=float, default=0.3, help="grid and nts scale of the served stream")
+    ap.add_argument("--plain", type=int, default=6, help="requests timed on the plain path")
+    ap.add_argument("--workers", type=int, default=2)
+    ap.add_argument("--max-batch", type=int, default=16)
+    ap.add_argument("--load", type=float, default=0.85, help="arrival rate as a fraction of measured capacity")
+    ap.add_argument("--seed", type=int, default=3)
+    a = ap.parse_args(argv)
+    lib = _capi.lib()
+    models, stream = _stream(a.requests, a.models, a.scale, a.seed)
+    prepared = []
+    for g, vel, shots in models:
+        v2 = np.zeros(g.nz * g.nx, np.float32)
+        rs = np.zeros_like(v2)
+        velf = np.ascontiguousarray(vel.reshape(-1), np.float32)
+        lib.aio_fd_precompute(g.nz, g.nx, C.c_float(g.dts), g.sub, velf.ctypes.data_as(C.c_void_p),
+                              v2.ctypes.data_as(C.c_void_p), rs.ctypes.data_as(C.c_void_p))
+        prepared.append((v2, rs))
+
+    def make(k, op, seed):
+        g, _, shots = models[k]
+        v2, rs = prepared[k]
+        rng = np.random.default_rng(seed)
+        a_ = shots[int(rng.integers(len(shots)))]
+        sig = (np.sin(np.arange(g.ntw) * 0.01 * (1 + rng.random()))[None, :] * 1e-2).astype(np.float32)
+        sig = np.repeat(sig, len(a_.src_pos), axis=0)
+        data = (rng.standard_normal((len(a_.rec_pos), g.nts)) * 1e-3).astype(np.float32) if op == "born_adjoint" else None
+        m = np.zeros((g.nx, g.nz), np.float32)
+        m[5:-5, 5:-5] = 0.01
+        return Request(op=op, grid=g, velocity_id=f"m{k}", vel2dtw2=v2, refl_scale=rs,
+                       shot=Shot(a_.src_pos, a_.rec_pos, sig, data), model_id=f"m{k}", model=m)
+
+    def run_alone(r, stepper):
+        ctx = Context(r.grid.nz, r.grid.nx, r.grid.nts, r.grid.dts, r.grid.sub, r.grid.dz, r.grid.dx, r.grid.minPad,
+                      r.vel2dtw2, r.refl_scale, image_fp64=True, stepper=stepper)
+        t0 = time.perf_counter()
+        if r.op == "nonlinear_forward":
+            ctx.nonlinear_forward([r.shot])
+        elif r.op == "born_forward":
+            ctx.born_forward(r.model, [r.shot])
+        else:
+            ctx.born_adjoint([r.shot])
+        dt = time.perf_counter() - t0
+        ctx.close()
+        return dt
+
+    # plain path: one shot per call, the reference's per-fine-step schedule, FP32
+    plain = [run_alone(make(*stream[i]), "fine") for i in range(min(a.plain, len(stream)))]
+    plain_rate = len(plain) / sum(plain)
+    # capacity probe: everything submitted at once
+    srv = Server(workers=a.workers, max_batch=a.max_batch)
+    for f in [srv.submit(make(*s)) for s in stream]:
+        f.result()
+    cap = srv.report()["shots_per_s"]
+    srv.close()
+    # served stream: Poisson arrivals at `load` x capacity
+    rate = a.load * cap
+    gaps = np.random.default_rng(a.seed + 1).exponential(1.0 / rate, len(stream))
+    srv = Server(workers=a.workers, max_batch=a.max_batch)
+    futs = []
+    t0 = time.perf_counter()
+    for gap, s in zip(gaps, stream):
+        t0 += gap
+        time.sleep(max(0.0, t0 - time.perf_counter()))
+        r = make(*s)
+        r.arrival = time.perf_counter()
+        futs.append(srv.submit(r))
+    for f in futs:
+        f.result()
+    rep = srv.report()
+    srv.close()
+    print(json.dumps({"metric": "served shots/s (one-shot requests, mixed grids and operators)",
+                      "value": rep["shots_per_s"], "unit": "shots/s", "p50_s": rep["p50_s"], "p99_s": rep["p99_s"],
+                      "mean_batch": rep["mean_batch"], "capacity_shots_per_s": cap, "arrival_rate": rate,
+                      "plain_shots_per_s": plain_rate, "vs_plain": rep["shots_per_s"] / plain_rate,
+                      "capacity_vs_plain": cap / plain_rate, "requests": len(stream), "models": a.models,
+                      "scale": a.scale, "workers": a.workers,
+                      "grids": [[g.nz, g.nx, g.nts, g.sub] for g, _, _ in models]}))
+
+
+if __name__ == "__main__":
+    main()

@@ -117,6 +117,9 @@ int aio_nonlinear_adjoint_wavefield(aio_context* ctx, const aio_shot* shot, int 
 /* Born: model nz*nx (shared by all shots). adjoint: add=0 overwrites, add=1 accumulates. */
 int aio_born_forward(aio_context* ctx, const float* model, int nShots, const aio_shot* shots, int memSpace);
 int aio_born_adjoint(aio_context* ctx, float* model, int add, int nShots, const aio_shot* shots, int memSpace);
+/* Born adjoint returning each shot's own image: images[s] (nz*nx, overwritten, host or device
+ * per memSpace). The shots still run together; used to batch independent requests. */
+int aio_born_adjoint_shots(aio_context* ctx, float* const* images, int nShots, const aio_shot* shots, int memSpace);
 /* Extended (time-lag) Born: model nExt*nz*nx. */
 int aio_born_ext_forward(aio_context* ctx, const float* model, int nShots, const aio_shot* shots, int memSpace);
 int aio_born_ext_adjoint(aio_context* ctx, float* model, int add, int nShots, const aio_shot* shots, int memSpace);
