@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--cpu-nts", type=int, default=0, help="coarse samples of the CPU sample (0 = auto)")
     ap.add_argument("--stepper", default="auto", choices=["auto", "fine", "blocked"])
     ap.add_argument("--chunk", type=int, default=0, help="blocked-stepper chunk width (0 = automatic)")
+    ap.add_argument("--plain", type=int, default=0,
+                    help="instead of the batched step: time N shots one per call on the per-fine-step "
+                         "stepper (the reference's schedule), FP32, and print that line")
     return ap.parse_args()
 
 
@@ -189,10 +192,45 @@ def config_dict(args, w):
             "parallelism": f"dp{args.gpus} (shots)", "l2": "inputs larger than L2 (5.4 GB wavefield per shot)"}
 
 
+def run_plain(args):
+    """One shot per call, per-fine-step stepper, FP32 wavefield: the plain GPU path."""
+    import torch
+    from acoustic_isotropic_operators_b200 import _capi
+    from acoustic_isotropic_operators_b200.batch import Context, Shot
+    w = workload(args, args.plain)
+    lib = _capi.lib()
+    v2 = np.zeros(w.nz * w.nx, np.float32)
+    rs = np.zeros_like(v2)
+    velf = np.ascontiguousarray(w.vel.reshape(-1), np.float32)
+    lib.aio_fd_precompute(w.nz, w.nx, C.c_float(w.dts), w.sub, velf.ctypes.data_as(C.c_void_p),
+                          v2.ctypes.data_as(C.c_void_p), rs.ctypes.data_as(C.c_void_p))
+    sigs = prepare_signals(w, lib)
+    model = np.ascontiguousarray(w.model, np.float32)
+    times = []
+    for i, (a, sg) in enumerate(zip(w.shots, sigs)):
+        ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs, image_fp64=True,
+                      stepper="fine")
+        shot = Shot(a.src_pos, a.rec_pos, sg)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.born_forward(model, [shot])
+        ctx.born_adjoint([shot])
+        times.append(time.perf_counter() - t0)
+        ctx.close()
+    t = statistics.mean(times[1:] if len(times) > 1 else times)
+    pts = w.n_interior * w.fine_steps * PASSES
+    print(json.dumps({"impl": "plain (this engine, one shot per call, per-fine-step stepper, FP32 W)",
+                      "metric": METRIC, "value": pts / t / 1e9, "unit": UNIT, "seconds_per_shot": t,
+                      "shots_per_s": 1.0 / t, "shots": len(times), "config": config_dict(args, w)}))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.plain:
+        return run_plain(args)
 
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -1,0 +1,51 @@
+"""Times the reference's own GPU drivers (oracle/_ref: the reference's FP32
+BornShotsGpuFunctions.cu compiled unmodified for sm_100a) on one shot of the
+Born benchmark workload (512x1312 interior, nts=2000, sub=4): Born forward then
+Born adjoint through its free functions, one shot per call as the reference's
+shot loop does. Prints one JSON line (Gpts/s over the 4 propagation passes and
+shots/s). Run on a GPU machine with oracle/_ref built:
+
+    python tests/measure_reference_gpu.py [--nts 2000] [--repeats 2]
+"""
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--nts", type=int, default=2000)
+    ap.add_argument("--repeats", type=int, default=2)
+    a = ap.parse_args()
+    import orc
+    import refgpu
+    import bench
+    from acoustic_isotropic_operators_b200 import _capi, synthetic as S
+    w = S.born_workload(nshots=1, nts=a.nts)
+    sig = bench.prepare_signals(w, _capi.lib())[0]
+    sh = w.shots[0]
+    s = orc.Scheme(nz=w.nz, nx=w.nx, nts=w.nts, dts=w.dts, sub=w.sub, dz=w.dz, dx=w.dx, minPad=w.minPad)
+    times = []
+    for _ in range(a.repeats + 1):
+        t0 = time.perf_counter()
+        d = refgpu.born_fwd(s, w.vel, w.model, sig, sh.src_pos, sh.rec_pos)
+        refgpu.born_adj(s, w.vel, d, sig, sh.src_pos, sh.rec_pos)
+        times.append(time.perf_counter() - t0)
+    t = float(np.mean(times[1:]))
+    pts = w.n_interior * w.fine_steps * 4
+    print(json.dumps({"impl": "reference-gpu (own sm_100a build, one shot per call)",
+                      "workload": "Born forward+adjoint, 1 shot, 512x1312 interior, nts=%d" % w.nts,
+                      "seconds_per_shot": t, "gpts_per_s": pts / t / 1e9, "shots_per_s": 1.0 / t}))
+
+
+if __name__ == "__main__":
+    main()
