@@ -935,13 +935,16 @@ struct Context {
 
     template <int MODE, int WP>
     void tb_launch_t(const TBPlan& pl, int nb, KTArgs& a, int v) {
-        const size_t smem = kt_smem_bytes(pl.iters, a.maxEnt);
+        const size_t smem = kt_smem_bytes(MODE, pl.threads, pl.iters, a.maxEnt);
         static int attrDev = -1;
+        static int smemMax = 0;
         if (attrDev != dev) {
-            AIO_CK(cudaFuncSetAttribute(k_tile<MODE, WP>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            AIO_CK(cudaDeviceGetAttribute(&smemMax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+            AIO_CK(cudaFuncSetAttribute(k_tile<MODE, WP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smemMax));
             attrDev = dev;
         }
-        require(smem <= 200 * 1024, "blocked stepper: shared memory plan exceeds 200 KiB (too many devices per tile)");
+        require(smem <= (size_t)smemMax, "blocked stepper: shared memory plan of " + std::to_string(smem) +
+                                             " bytes exceeds the device limit (too many devices per tile)");
         require(pl.threads <= KT_MAXT && pl.NQ <= KT_MAXQ, "blocked stepper: strip taller than the ring");
         a.shots = tbDesc.as<TBShot>() + (size_t)v * nb;
         const bool timed = profEvery > 0 && (launches % profEvery) == 0;

@@ -38,7 +38,9 @@ namespace aio {
 
 constexpr int KT_T = 4;        // fine steps per launch (sub)
 constexpr int KT_BX = 16;      // block columns per iteration
-constexpr int KT_CB = 32;      // ring depth in columns (>= BX + 5T - 5 + 1 for the output reads)
+constexpr int KT_CB = 32;      // ring depth in columns of levels 1..T-1 (>= BX + 5T - 5 + 1 for the output reads)
+constexpr int KT_CB0 = 64;     // ring depth of level 0: the next input block lands while the current one is read
+constexpr int KT_RINGCOLS = KT_CB0 + (KT_T - 1) * KT_CB;
 constexpr int KT_PADQ = 2;     // zero quads above and below every ring column
 constexpr int KT_MAXQ = 42;    // row quads per strip (R <= 168, HZ <= 128)
 constexpr int KT_RS = (KT_MAXQ + 2 * KT_PADQ) * 4;  // floats per ring column (compile-time offsets)
@@ -63,10 +65,40 @@ struct KTArgs {
     long long wStride;     // elements per stored coarse slice (= isz)
 };
 
-// rings, column damping table, per-launch injection values (T per entry), entries
-inline size_t kt_smem_bytes(int iters, int maxEnt) {
-    return ((size_t)KT_T * KT_CB * KT_RS + (size_t)iters * KT_BX + 64 + (size_t)maxEnt * KT_T) * sizeof(float) +
-           (size_t)maxEnt * sizeof(TBEnt);
+// Per-thread staging slots (16 bytes each) filled by asynchronous copies: level-1 operands
+// of the next iteration (old level, v^2: slots 0-3) and the output operands of the current
+// iteration (partial sum: 4-5, stored wavefield: 6-7, FP64 image: 8-11).
+__host__ __device__ constexpr int kt_slots(int mode) { return mode == TB_ADJ ? 12 : (mode == TB_SRC ? 6 : 4); }
+// rings, staging, column damping table, per-launch injection values (T per entry), entries
+inline size_t kt_smem_bytes(int mode, int threads, int iters, int maxEnt) {
+    return (size_t)KT_RINGCOLS * KT_RS * sizeof(float) + (size_t)kt_slots(mode) * threads * 16 +
+           ((size_t)iters * KT_BX + 64 + (size_t)maxEnt * KT_T) * sizeof(float) + (size_t)maxEnt * sizeof(TBEnt);
+}
+
+// cp.async: 16 (or 8) bytes global -> shared, zero-filled when !ok (no bytes are read then).
+__device__ __forceinline__ void kt_cp16(void* s, const void* g, bool ok) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(g), "r"(ok ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void kt_cp16_l1(void* s, const void* g, bool ok) {  // also allocates in L1
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(g), "r"(ok ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void kt_cp8(void* s, const void* g, bool ok) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(g), "r"(ok ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void kt_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void kt_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+// four stored-wavefield samples from a staging slot (FP32: 16 bytes, BF16: the first 8)
+template <int WPREC>
+__device__ __forceinline__ float4 kt_wfrom(const float4& slot) {
+    if (WPREC == TBW_F32) return slot;
+    const uint2 r = *reinterpret_cast<const uint2*>(&slot);
+    const float2 fa = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&r.x));
+    const float2 fb = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&r.y));
+    return make_float4(fa.x, fa.y, fb.x, fb.y);
 }
 
 template <int WPREC>
@@ -116,8 +148,10 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
     extern __shared__ float4 kt_smem4[];
     const int NQ = a.NQ;
     constexpr int RS = KT_RS;
-    float* ring = reinterpret_cast<float*>(kt_smem4);         // [T][KT_CB][RS]
-    float* dxt = ring + T * KT_CB * RS;                         // column damping, columns xs-32 ...
+    constexpr int NS = kt_slots(MODE);
+    float* ring = reinterpret_cast<float*>(kt_smem4);         // level 0: [KT_CB0][RS], levels 1..T-1: [KT_CB][RS]
+    float4* stg = reinterpret_cast<float4*>(ring + KT_RINGCOLS * RS);  // [NS][blockDim.x]
+    float* dxt = reinterpret_cast<float*>(stg + NS * blockDim.x);      // column damping, columns xs-32 ...
     float* sInjV = dxt + a.iters * KT_BX + 64;                  // [maxEnt][T] injection value per level
     TBEnt* sEnt = reinterpret_cast<TBEnt*>(sInjV + a.maxEnt * T);
 
@@ -149,7 +183,7 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
     const int xs = x0 - 5 * T;
 
     // ---- shared set-up: zero rings, column damping table, sparse entries
-    const int nRing = T * KT_CB * RS;
+    const int nRing = KT_RINGCOLS * RS;
     for (int i = tid; i < nRing; i += blockDim.x) ring[i] = 0.f;
     const int nDx = a.iters * KT_BX + 64;
     for (int i = tid; i < nDx; i += blockDim.x) {
@@ -219,61 +253,57 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
         xc2[i] = make_float2(a.c.xc[i], a.c.xc[i]);
     }
     float* const ringQ = ring + (KT_PADQ + q) * 4;  // quad q of ring column 0, level 0
+    // quad q of column c of level t's ring
+    auto col = [&](int t, int c) -> float* {
+        return t == 0 ? ringQ + (c & (KT_CB0 - 1)) * RS : ringQ + (KT_CB0 + (t - 1) * KT_CB + (c & (KT_CB - 1))) * RS;
+    };
+    float4* const mySlot = stg + tid;  // slot i of this thread: mySlot[i * blockDim.x]
+    const int bd = blockDim.x;
 
-    // ---- input staging: the block of iteration k+1 is loaded during iteration k
-    float4 nCur[2], nOld[2], nV[2];
-    auto load_input = [&](int k) {
+    // Input of iteration k, issued one iteration ahead: the level-0 block [B, B+16) straight
+    // into its ring slots, and the level-1 operands of iteration k (old level and v^2 at the
+    // level-1 columns) into this thread's staging slots 0-3.
+    auto issue_input = [&](int k) {
+        if (!act) return;
         const int B = xs + KT_BX * k;
 #pragma unroll
         for (int j = 0; j < 2; j++) {
             const int c = B + 2 * cp + j;
-            nCur[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (zLoad && c >= 0 && c < nxi) nCur[j] = __ldg(reinterpret_cast<const float4*>(cur + (long long)c * ip + zq));
-            const int co = B - 5 + 2 * cp + j;  // level-1 centre columns of iteration k
-            nOld[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (zLoad && co >= 0 && co < nxi) nOld[j] = __ldg(reinterpret_cast<const float4*>(old + (long long)co * ip + zq));
-            nV[j] = __ldg(reinterpret_cast<const float4*>(v2p + (long long)min(max(co, 0), nxi - 1) * ip + zv));
+            const bool okc = zLoad && c >= 0 && c < nxi;
+            kt_cp16(col(0, c), okc ? cur + (long long)c * ip + zq : cur, okc);
+            const int co = B - 5 + 2 * cp + j;
+            const bool oko = zLoad && co >= 0 && co < nxi;
+            kt_cp16(mySlot + j * bd, oko ? old + (long long)co * ip + zq : old, oko);
+            kt_cp16_l1(mySlot + (2 + j) * bd, v2p + (long long)min(max(co, 0), nxi - 1) * ip + zv, true);
         }
     };
-    auto store_input = [&](int k) {
-        const int B = xs + KT_BX * k;
-        if (act) {
-#pragma unroll
-            for (int j = 0; j < 2; j++) {
-                const float v[4] = {nCur[j].x, nCur[j].y, nCur[j].z, nCur[j].w};
-                kt_st4(ringQ + ((B + 2 * cp + j) & (KT_CB - 1)) * RS, v);
-            }
-        }
-    };
-    load_input(0);
-    store_input(0);
-    float4 pOld[2] = {nOld[0], nOld[1]};
-    float4 pV[2] = {nV[0], nV[1]};
-    load_input(1);
+    issue_input(0);
+    kt_commit();
+    kt_wait<0>();
     __syncthreads();
 
     for (int k = 0; k < a.iters; k++) {
         const int B = xs + KT_BX * k;
-        // Output operands of this iteration's level-T columns (issued early).
-        float4 oPart[2], oW[2];
-        double oImg[2][4];
+        // Output operands of this iteration's level-T columns, copied asynchronously into
+        // this thread's staging slots (read at the output stage).
+        if (MODE == TB_SRC || MODE == TB_ADJ) {
 #pragma unroll
-        for (int j = 0; j < 2; j++) {
-            oPart[j] = oW[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-            for (int i = 0; i < 4; i++) oImg[j][i] = 0.0;
-            const int c = B - 5 * T + 2 * cp + j;
-            if ((MODE == TB_SRC || MODE == TB_ADJ) && zOut && c >= x0 && c < x1) {
-                const long long idx = (long long)c * ip + zq;
-                oPart[j] = __ldg(reinterpret_cast<const float4*>(pPart + idx));
-                if (MODE == TB_ADJ) {
-                    oW[j] = kt_wload4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, its + 1), idx);
-                    const double2 i0 = *reinterpret_cast<const double2*>(pImg + idx);
-                    const double2 i1 = *reinterpret_cast<const double2*>(pImg + idx + 2);
-                    oImg[j][0] = i0.x; oImg[j][1] = i0.y; oImg[j][2] = i1.x; oImg[j][3] = i1.y;
+            for (int j = 0; j < 2; j++) {
+                const int c = B - 5 * T + 2 * cp + j;
+                if (zOut && c >= x0 && c < x1) {
+                    const long long idx = (long long)c * ip + zq;
+                    kt_cp16(mySlot + (4 + j) * bd, pPart + idx, true);
+                    if (MODE == TB_ADJ) {
+                        const void* w = tb_wslice<WPREC>(sh.W, a.wStride, its + 1);
+                        if (WPREC == TBW_F32) kt_cp16(mySlot + (6 + j) * bd, (const float*)w + idx, true);
+                        else kt_cp8(mySlot + (6 + j) * bd, (const __nv_bfloat16*)w + idx, true);
+                        kt_cp16(mySlot + (8 + 2 * j) * bd, pImg + idx, true);
+                        kt_cp16(mySlot + (9 + 2 * j) * bd, pImg + idx + 2, true);
+                    }
                 }
             }
         }
+        kt_commit();
 
         float lvT[2][T + 1][4];  // levels 1..T at the output columns (T-1 from the rings)
 #pragma unroll
@@ -283,28 +313,25 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
             const bool need = act && q >= (5 * t) / 4 && q < NQ - (5 * t) / 4 &&
                               c0 + 1 >= xs + 5 * t && c0 <= x1 - 1 + 5 * (T - t);
             float S[2][4];
-            if (t == 3) store_input(k + 1);  // level-0 slots of columns [B-16, B): last read by level 2
             if (need) {
-                const float* L = ringQ + (t - 1) * KT_CB * RS;
                 float4 zq4[2][5];
 #pragma unroll
                 for (int j = 0; j < 2; j++)
 #pragma unroll
-                    for (int d = 0; d < 5; d++) zq4[j][d] = kt_ld4(L + ((c0 + j) & (KT_CB - 1)) * RS + 4 * (d - 2));
+                    for (int d = 0; d < 5; d++) zq4[j][d] = kt_ld4(col(t - 1, c0 + j) + 4 * (d - 2));
                 float4 xm[5], xp[5];  // columns c0-5..c0-1 and c0+2..c0+6
 #pragma unroll
                 for (int d = 0; d < 5; d++) {
-                    xm[d] = kt_ld4(L + ((c0 - 5 + d) & (KT_CB - 1)) * RS);
-                    xp[d] = kt_ld4(L + ((c0 + 2 + d) & (KT_CB - 1)) * RS);
+                    xm[d] = kt_ld4(col(t - 1, c0 - 5 + d));
+                    xp[d] = kt_ld4(col(t - 1, c0 + 2 + d));
                 }
                 float4 ol[2];
                 if (t == 1) {
-                    ol[0] = pOld[0];
-                    ol[1] = pOld[1];
+                    ol[0] = mySlot[0];
+                    ol[1] = mySlot[bd];
                 } else {
-                    const float* Lo = ringQ + (t - 2) * KT_CB * RS;
-                    ol[0] = kt_ld4(Lo + (c0 & (KT_CB - 1)) * RS);
-                    ol[1] = kt_ld4(Lo + ((c0 + 1) & (KT_CB - 1)) * RS);
+                    ol[0] = kt_ld4(col(t - 2, c0));
+                    ol[1] = kt_ld4(col(t - 2, c0 + 1));
                 }
                 float4 vq[2];
                 float Dx[2];
@@ -312,7 +339,7 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                 for (int j = 0; j < 2; j++) {
                     const int c = c0 + j;
                     // level 1: prefetched with the input; later levels re-read the same lines from L1
-                    vq[j] = (t == 1) ? pV[j]
+                    vq[j] = (t == 1) ? mySlot[(2 + j) * bd]
                                      : __ldg(reinterpret_cast<const float4*>(v2p + (long long)min(max(c, 0), nxi - 1) * ip + zv));
                     Dx[j] = dxt[c - xs + 32];
                 }
@@ -391,9 +418,8 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
 #pragma unroll
                     for (int i = 0; i < 4; i++) S[j][i] = S[j][i] * Dm[j][i];
                 if (t < T) {
-                    float* Lw = ringQ + t * KT_CB * RS;
 #pragma unroll
-                    for (int j = 0; j < 2; j++) kt_st4(Lw + ((c0 + j) & (KT_CB - 1)) * RS, S[j]);
+                    for (int j = 0; j < 2; j++) kt_st4(col(t, c0 + j), S[j]);
                 }
             } else {
 #pragma unroll
@@ -401,14 +427,21 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
 #pragma unroll
                     for (int i = 0; i < 4; i++) S[j][i] = 0.f;
             }
+            if (t == 1) {
+                // level-1 operands of this iteration are consumed: stage the next input
+                issue_input(k + 1);
+                kt_commit();
+            }
             if (t == T) {
 #pragma unroll
                 for (int j = 0; j < 2; j++)
 #pragma unroll
                     for (int i = 0; i < 4; i++) lvT[j][T][i] = S[j][i];
+            } else {
+                __syncthreads();  // level t complete before level t+1 (and the outputs) read it
             }
-            __syncthreads();
         }
+        kt_wait<1>();  // this iteration's output operands (the input group may still be in flight)
 
         // ---- outputs at the level-T columns [B - 5T, B - 5T + 16)
         {
@@ -418,7 +451,7 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                 const int c = c0 + j;
 #pragma unroll
                 for (int l = 1; l < T; l++) {
-                    const float4 v = kt_ld4(ringQ + (l * KT_CB + (c & (KT_CB - 1))) * RS);
+                    const float4 v = kt_ld4(col(l, c));
                     lvT[j][l][0] = v.x; lvT[j][l][1] = v.y; lvT[j][l][2] = v.z; lvT[j][l][3] = v.w;
                 }
                 if (!(zOut && c >= x0 && c < x1)) continue;
@@ -429,7 +462,7 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                     float wa[4], wb[4];
 #pragma unroll
                     for (int i = 0; i < 4; i++) {
-                        wa[i] = kt_el(oPart[j], i);
+                        wa[i] = kt_el(mySlot[(4 + j) * bd], i);
                         wb[i] = 0.f;
 #pragma unroll
                         for (int l = 1; l <= T; l++) {
@@ -443,18 +476,23 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                 } else if (MODE == TB_ADJ) {
                     float ra[4], rb[4];
                     double acc[4];
+                    const float4 oP = mySlot[(4 + j) * bd];
+                    const float4 oW = kt_wfrom<WPREC>(mySlot[(6 + j) * bd]);
+                    const double2* oI = reinterpret_cast<const double2*>(&mySlot[(8 + 2 * j) * bd]);
+                    const double2* oI2 = reinterpret_cast<const double2*>(&mySlot[(9 + 2 * j) * bd]);
+                    const double oImg[4] = {oI->x, oI->y, oI2->x, oI2->y};
                     float4 w0 = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (its == 0) w0 = kt_wload4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, 0), idx);
 #pragma unroll
                     for (int i = 0; i < 4; i++) {
                         ra[i] = 0.f;
-                        rb[i] = kt_el(oPart[j], i);
+                        rb[i] = kt_el(oP, i);
 #pragma unroll
                         for (int l = 1; l <= T; l++) {
                             ra[i] += lvT[j][l][i] * a.h[sub - l];
                             rb[i] += lvT[j][l][i] * a.h[H + sub - l];
                         }
-                        acc[i] = oImg[j][i] + (double)(kt_el(oW[j], i) * rb[i]);
+                        acc[i] = oImg[i] + (double)(kt_el(oW, i) * rb[i]);
                         if (its == 0) acc[i] += (double)(kt_el(w0, i) * ra[i]);
                     }
                     kt_st4(pPartOut + idx, ra);
@@ -487,12 +525,8 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                 }
             }
         }
-        pOld[0] = nOld[0];
-        pOld[1] = nOld[1];
-        pV[0] = nV[0];
-        pV[1] = nV[1];
-        if (k + 2 <= a.iters) load_input(k + 2);
-        __syncthreads();
+        kt_wait<0>();     // the next input block and level-1 operands have landed
+        __syncthreads();  // ... for every thread; outputs done before level 1 reuses ring slots
     }
 }
 
