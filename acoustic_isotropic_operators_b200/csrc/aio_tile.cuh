@@ -72,7 +72,7 @@ __host__ __device__ constexpr int kt_slots(int mode) { return mode == TB_ADJ ? 1
 // rings, staging, column damping table, per-launch injection values (T per entry), entries
 inline size_t kt_smem_bytes(int mode, int threads, int iters, int maxEnt) {
     return (size_t)KT_RINGCOLS * KT_RS * sizeof(float) + (size_t)kt_slots(mode) * threads * 16 +
-           ((size_t)iters * KT_BX + 64 + (size_t)maxEnt * KT_T) * sizeof(float) + (size_t)maxEnt * sizeof(TBEnt);
+           (3 * ((size_t)iters * KT_BX + 64) + (size_t)maxEnt * KT_T) * sizeof(float) + (size_t)maxEnt * sizeof(TBEnt);
 }
 
 // cp.async: 16 (or 8) bytes global -> shared, zero-filled when !ok (no bytes are read then).
@@ -152,7 +152,10 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
     float* ring = reinterpret_cast<float*>(kt_smem4);         // level 0: [KT_CB0][RS], levels 1..T-1: [KT_CB][RS]
     float4* stg = reinterpret_cast<float4*>(ring + KT_RINGCOLS * RS);  // [NS][blockDim.x]
     float* dxt = reinterpret_cast<float*>(stg + NS * blockDim.x);      // column damping, columns xs-32 ...
-    float* sInjV = dxt + a.iters * KT_BX + 64;                  // [maxEnt][T] injection value per level
+    const int nDx = a.iters * KT_BX + 64;                       // columns xs-32 .. of the tables below
+    int* injFirst = reinterpret_cast<int*>(dxt + nDx);          // first injection entry of a column, or -1
+    int* recFirst = injFirst + nDx;                             // first recording entry of a column, or -1
+    float* sInjV = reinterpret_cast<float*>(recFirst + nDx);    // [maxEnt][T] injection value per level
     TBEnt* sEnt = reinterpret_cast<TBEnt*>(sInjV + a.maxEnt * T);
 
     const Geom& g = a.g;
@@ -185,8 +188,9 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
     // ---- shared set-up: zero rings, column damping table, sparse entries
     const int nRing = KT_RINGCOLS * RS;
     for (int i = tid; i < nRing; i += blockDim.x) ring[i] = 0.f;
-    const int nDx = a.iters * KT_BX + 64;
     for (int i = tid; i < nDx; i += blockDim.x) {
+        injFirst[i] = -1;
+        recFirst[i] = -1;
         const int c = xs - 32 + i;
         float d = 0.f;
         if (c >= 0 && c < nxi) {
@@ -221,15 +225,16 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
             sInjV[i] = v;
         }
     }
+    // column -> first entry (entries are sorted by column; inside [xs - 32, xs - 32 + nDx))
+    for (int e = tid; e < nInj; e += blockDim.x)
+        if (e == 0 || sEnt[e - 1].col != sEnt[e].col) injFirst[sEnt[e].col - xs + 32] = e;
+    for (int e = tid; e < nRec; e += blockDim.x)
+        if (e == 0 || sEnt[recOff + e - 1].col != sEnt[recOff + e].col) recFirst[sEnt[recOff + e].col - xs + 32] = e;
     __syncthreads();
     // does any injection / recording point fall in this thread's row quad?
     bool qInj = false, qRec = false;
     for (int e = 0; e < nInj; e++) qInj |= (unsigned)(sEnt[e].row - zq) < 4u;
     for (int e = 0; e < nRec; e++) qRec |= (unsigned)(sEnt[recOff + e].row - zq) < 4u;
-    int injPtr[T];
-#pragma unroll
-    for (int t = 0; t < T; t++) injPtr[t] = 0;
-    int recPtr = 0;
 
     // ---- per-thread constants
     float Dz[4];
@@ -396,20 +401,17 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                 }
                 // sparse injection into this micro-tile (entries sorted by column)
                 if (MODE != TB_SCAT && qInj) {
-                    int p = injPtr[t - 1];
-                    while (p < nInj && sEnt[p].col < c0) p++;
-                    injPtr[t - 1] = p;
-                    for (int e = p; e < nInj && sEnt[e].col <= c0 + 1; e++) {
-                        const int rr = sEnt[e].row - zq;
-                        if (rr >= 0 && rr < 4) {
-                            const int j = sEnt[e].col - c0;
-                            float v = sInjV[e * T + t - 1];
-                            if (MODE == TB_ADJ) v = kt_el(j ? vq[1] : vq[0], rr) * v;
 #pragma unroll
-                            for (int jj = 0; jj < 2; jj++)
+                    for (int j = 0; j < 2; j++) {
+                        for (int e = injFirst[c0 + j - xs + 32]; e >= 0 && e < nInj && sEnt[e].col == c0 + j; e++) {
+                            const int rr = sEnt[e].row - zq;
+                            if (rr >= 0 && rr < 4) {
+                                float v = sInjV[e * T + t - 1];
+                                if (MODE == TB_ADJ) v = kt_el(vq[j], rr) * v;
 #pragma unroll
                                 for (int i = 0; i < 4; i++)
-                                    if (jj == j && i == rr) S[jj][i] = S[jj][i] + v;
+                                    if (i == rr) S[j][i] = S[j][i] + v;
+                            }
                         }
                     }
                 }
@@ -499,10 +501,7 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                     *reinterpret_cast<double2*>(pImg + idx) = make_double2(acc[0], acc[1]);
                     *reinterpret_cast<double2*>(pImg + idx + 2) = make_double2(acc[2], acc[3]);
                 } else if (qRec) {
-                    int p = recPtr;
-                    while (p < nRec && sEnt[recOff + p].col < c) p++;
-                    recPtr = p;
-                    for (int e = p; e < nRec && sEnt[recOff + e].col == c; e++) {
+                    for (int e = recFirst[c - xs + 32]; e >= 0 && e < nRec && sEnt[recOff + e].col == c; e++) {
                         const int rr = sEnt[recOff + e].row - zq;
                         if (rr >= 0 && rr < 4) {
                             float ra = 0.f, rb = 0.f;
