@@ -68,10 +68,15 @@ struct KTArgs {
 // Per-thread staging slots (16 bytes each) filled by asynchronous copies: level-1 operands
 // of the next iteration (old level, v^2: slots 0-3) and the output operands of the current
 // iteration (partial sum: 4-5, stored wavefield: 6-7, FP64 image: 8-11).
-__host__ __device__ constexpr int kt_slots(int mode) { return mode == TB_ADJ ? 12 : (mode == TB_SRC ? 6 : 4); }
+__host__ __device__ constexpr int kt_slots(int mode) {
+    return mode == TB_ADJ ? 12 : (mode == TB_SRC ? 6 : (mode == TB_SCAT ? 8 : 4));
+}
+// Ring columns: levels 0..T-1, plus (scattered pass) the secondary sources dm*W[its] and
+// dm*W[its+1] of the last 32 level-1 columns, formed once at level 1 and read by levels 2..T.
+__host__ __device__ constexpr int kt_ringcols(int mode) { return KT_RINGCOLS + (mode == TB_SCAT ? 2 * KT_CB : 0); }
 // rings, staging, column damping table, per-launch injection values (T per entry), entries
 inline size_t kt_smem_bytes(int mode, int threads, int iters, int maxEnt) {
-    return (size_t)KT_RINGCOLS * KT_RS * sizeof(float) + (size_t)kt_slots(mode) * threads * 16 +
+    return (size_t)kt_ringcols(mode) * KT_RS * sizeof(float) + (size_t)kt_slots(mode) * threads * 16 +
            (3 * ((size_t)iters * KT_BX + 64) + (size_t)maxEnt * KT_T) * sizeof(float) + (size_t)maxEnt * sizeof(TBEnt);
 }
 
@@ -150,7 +155,7 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
     constexpr int RS = KT_RS;
     constexpr int NS = kt_slots(MODE);
     float* ring = reinterpret_cast<float*>(kt_smem4);         // level 0: [KT_CB0][RS], levels 1..T-1: [KT_CB][RS]
-    float4* stg = reinterpret_cast<float4*>(ring + KT_RINGCOLS * RS);  // [NS][blockDim.x]
+    float4* stg = reinterpret_cast<float4*>(ring + kt_ringcols(MODE) * RS);  // [NS][blockDim.x]
     float* dxt = reinterpret_cast<float*>(stg + NS * blockDim.x);      // column damping, columns xs-32 ...
     const int nDx = a.iters * KT_BX + 64;                       // columns xs-32 .. of the tables below
     int* injFirst = reinterpret_cast<int*>(dxt + nDx);          // first injection entry of a column, or -1
@@ -186,7 +191,7 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
     const int xs = x0 - 5 * T;
 
     // ---- shared set-up: zero rings, column damping table, sparse entries
-    const int nRing = KT_RINGCOLS * RS;
+    const int nRing = kt_ringcols(MODE) * RS;
     for (int i = tid; i < nRing; i += blockDim.x) ring[i] = 0.f;
     for (int i = tid; i < nDx; i += blockDim.x) {
         injFirst[i] = -1;
@@ -262,6 +267,8 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
     auto col = [&](int t, int c) -> float* {
         return t == 0 ? ringQ + (c & (KT_CB0 - 1)) * RS : ringQ + (KT_CB0 + (t - 1) * KT_CB + (c & (KT_CB - 1))) * RS;
     };
+    // secondary-source rings of the scattered pass (s = 0: dm*W[its], 1: dm*W[its+1])
+    auto ssCol = [&](int sidx, int c) -> float* { return ringQ + (KT_RINGCOLS + sidx * KT_CB + (c & (KT_CB - 1))) * RS; };
     float4* const mySlot = stg + tid;  // slot i of this thread: mySlot[i * blockDim.x]
     const int bd = blockDim.x;
 
@@ -279,7 +286,19 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
             const int co = B - 5 + 2 * cp + j;
             const bool oko = zLoad && co >= 0 && co < nxi;
             kt_cp16(mySlot + j * bd, oko ? old + (long long)co * ip + zq : old, oko);
-            kt_cp16_l1(mySlot + (2 + j) * bd, v2p + (long long)min(max(co, 0), nxi - 1) * ip + zv, true);
+            const long long ic = (long long)min(max(co, 0), nxi - 1) * ip + zv;
+            kt_cp16_l1(mySlot + (2 + j) * bd, v2p + ic, true);
+            if (MODE == TB_SCAT) {  // stored wavefield at its and its+1 (slots 4-7)
+                const void* wa = tb_wslice<WPREC>(sh.W, a.wStride, its);
+                const void* wb = tb_wslice<WPREC>(sh.W, a.wStride, its + 1);
+                if (WPREC == TBW_F32) {
+                    kt_cp16(mySlot + (4 + j) * bd, (const float*)wa + ic, true);
+                    kt_cp16(mySlot + (6 + j) * bd, (const float*)wb + ic, true);
+                } else {
+                    kt_cp8(mySlot + (4 + j) * bd, (const __nv_bfloat16*)wa + ic, true);
+                    kt_cp8(mySlot + (6 + j) * bd, (const __nv_bfloat16*)wb + ic, true);
+                }
+            }
         }
     };
     issue_input(0);
@@ -357,12 +376,22 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                 if (MODE == TB_SCAT) {
 #pragma unroll
                     for (int j = 0; j < 2; j++) {
-                        const long long idx = (long long)min(max(c0 + j, 0), nxi - 1) * ip + zv;
-                        const float4 dmv = __ldg(reinterpret_cast<const float4*>(dmp + idx));
-                        const float4 wa = kt_wload4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, its), idx);
-                        const float4 wb = kt_wload4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, its + 1), idx);
-                        sa[j] = make_float4(dmv.x * wa.x, dmv.y * wa.y, dmv.z * wa.z, dmv.w * wa.w);
-                        sb[j] = make_float4(dmv.x * wb.x, dmv.y * wb.y, dmv.z * wb.z, dmv.w * wb.w);
+                        if (t == 1) {
+                            // imagingFwdGpu (F/src/kernelsGpu.cu:309-316): dm * W, kept for levels 2..T
+                            const long long idx = (long long)min(max(c0 + j, 0), nxi - 1) * ip + zv;
+                            const float4 dmv = __ldg(reinterpret_cast<const float4*>(dmp + idx));
+                            const float4 wa = kt_wfrom<WPREC>(mySlot[(4 + j) * bd]);
+                            const float4 wb = kt_wfrom<WPREC>(mySlot[(6 + j) * bd]);
+                            sa[j] = make_float4(dmv.x * wa.x, dmv.y * wa.y, dmv.z * wa.z, dmv.w * wa.w);
+                            sb[j] = make_float4(dmv.x * wb.x, dmv.y * wb.y, dmv.z * wb.z, dmv.w * wb.w);
+                            const float va[4] = {sa[j].x, sa[j].y, sa[j].z, sa[j].w};
+                            const float vb[4] = {sb[j].x, sb[j].y, sb[j].z, sb[j].w};
+                            kt_st4(ssCol(0, c0 + j), va);
+                            kt_st4(ssCol(1, c0 + j), vb);
+                        } else {
+                            sa[j] = kt_ld4(ssCol(0, c0 + j));
+                            sb[j] = kt_ld4(ssCol(1, c0 + j));
+                        }
                     }
                 }
 #pragma unroll
