@@ -192,8 +192,9 @@ struct Context {
         require(p.sub >= 1 && p.sub < SUB_MAX, "sub must be in [1, 100)");
         require(p.minPad >= 0 && p.minPad < PAD_MAX, "minPad must be in [0, 200)");
         require(p.nExt >= 1 && (p.nExt % 2) == 1, "nExt must be a positive odd number");
-        require(p.wavefieldPrecision == AIO_WFLD_FP32 || p.wavefieldPrecision == AIO_WFLD_BF16,
-                "stored wavefield precision must be AIO_WFLD_FP32 or AIO_WFLD_BF16");
+        require(p.wavefieldPrecision == AIO_WFLD_FP32 || p.wavefieldPrecision == AIO_WFLD_BF16 ||
+                    p.wavefieldPrecision == AIO_WFLD_FP16,
+                "stored wavefield precision must be AIO_WFLD_FP32, AIO_WFLD_BF16 or AIO_WFLD_FP16");
         require(p.stepper >= AIO_STEPPER_AUTO && p.stepper <= AIO_STEPPER_BLOCKED, "unknown stepper");
         require(p.stepper < AIO_STEPPER_BLOCKED || p.sub == 4, "the interval-blocked steppers require sub == 4");
         require(p.wavefieldPrecision == AIO_WFLD_FP32 || (p.stepper != AIO_STEPPER_FINE && p.sub == 4),
@@ -770,6 +771,7 @@ struct Context {
     // One launch per coarse interval (aio_tb.cuh). State, partial sums and
     // images use interior slices; the stored wavefield is FP32 or BF16.
     DevMem tbState, tbPart, tbImg, tbW, tbEnt, tbStart, tbDesc, shotImg;
+    DevMem tbWscale, tbWmax, tbWstage;  // FP16 stored wavefield: per-slice scales, max |W|, FP32 staging
     // k_tile plan: strips of HZ (multiple of 4) output rows, NQ = HZ/4 + 10 row quads,
     // 8 column pairs per quad, x-chunks of LX columns marched in blocks of 16.
     struct TBPlan {
@@ -777,7 +779,8 @@ struct Context {
     };
 
     bool tb_enabled() const { return P.stepper != AIO_STEPPER_FINE && g.sub == KT_T; }
-    int wbytes() const { return P.wavefieldPrecision == AIO_WFLD_BF16 ? 2 : 4; }
+    int wbytes() const { return P.wavefieldPrecision == AIO_WFLD_FP32 ? 4 : 2; }
+    bool f16() const { return P.wavefieldPrecision == AIO_WFLD_FP16; }
 
     // nb: shots of the wave (one CTA column per shot)
     TBPlan tb_plan(int nb) const {
@@ -881,6 +884,11 @@ struct Context {
         tbPart.ensure((size_t)nb * 2 * g.isz * 4);
         if (needImg) tbImg.ensure((size_t)nb * g.isz * 8);
         tbDesc.ensure((size_t)2 * nb * sizeof(TBShot));
+        if (f16()) {
+            tbWscale.ensure((size_t)nb * g.nts * 4);
+            tbWmax.ensure((size_t)nb * g.nts * 4);
+            tbWstage.ensure((size_t)nb * 2 * g.isz * 4);
+        }
     }
 
     // Descriptor pairs: version v reads state/part set v and writes set 1-v
@@ -909,6 +917,11 @@ struct Context {
                 t.ent = tbEnt.as<TBEnt>();
                 t.W = W ? (void*)((char*)W + (size_t)s * g.nts * g.isz * wbytes()) : nullptr;
                 t.img = tbImg.p ? tbImg.as<double>() + (size_t)s * g.isz : nullptr;
+                if (f16()) {
+                    t.wscale = tbWscale.as<float>() + (size_t)s * g.nts;
+                    t.wmax = tbWmax.as<unsigned>() + (size_t)s * g.nts;
+                    t.wstage = tbWstage.as<float>() + (size_t)s * 2 * g.isz;
+                }
             }
         AIO_CK(cudaMemcpyAsync(tbDesc.p, d.data(), d.size() * sizeof(TBShot), cudaMemcpyHostToDevice, st));
     }
@@ -966,6 +979,7 @@ struct Context {
     template <int MODE>
     void tb_launch(const TBPlan& pl, int nb, KTArgs& a, int v) {
         if (P.wavefieldPrecision == AIO_WFLD_BF16) tb_launch_t<MODE, TBW_BF16>(pl, nb, a, v);
+        else if (P.wavefieldPrecision == AIO_WFLD_FP16) tb_launch_t<MODE, TBW_F16>(pl, nb, a, v);
         else tb_launch_t<MODE, TBW_F32>(pl, nb, a, v);
     }
 
@@ -983,10 +997,16 @@ struct Context {
         tb_zero(nb, false);
         tb_desc(pl, nb, true, false, nonlinear, nonlinear ? nullptr : tbW.p, false);
         KTArgs a = tb_args(pl, maxEnt, nullptr);
+        if (!nonlinear && f16()) AIO_CK(cudaMemsetAsync(tbWmax.p, 0, (size_t)nb * g.nts * 4, st));
         for (int its = 0; its < g.nts - 1; its++) {
             a.its = its;
             if (nonlinear) tb_launch<TB_NL>(pl, nb, a, its & 1);
             else tb_launch<TB_SRC>(pl, nb, a, its & 1);
+        }
+        if (!nonlinear && f16()) {  // last two slices and the per-slice scales
+            k_f16_finish<<<dim3(std::max(1, smCount), nb), 256, 0, st>>>(tbDesc.as<TBShot>(), g.isz, g.ip, g.nzi,
+                                                                          g.nxi, g.nts);
+            kcheck();
         }
     }
 
@@ -1090,6 +1110,7 @@ struct Context {
             maxRec = std::max(maxRec, shots[s].nReceiversReg);
         }
         long long per = 6LL * g.isz * 4 + (wavefield ? (long long)g.nts * g.isz * wbytes() : 0) +
+                        (wavefield && f16() ? 2LL * g.isz * 4 + 8LL * g.nts : 0) +
                         (image ? g.isz * 8LL : 0) + (long long)maxSrc * g.ntw * 4 + 2LL * maxRec * g.nts * 4 +
                         2 * g.hsz * 4 + 2 * g.isz * 4 + (1 << 16);
         long long shared = 4LL * g.isz * 4 + (64LL << 20);

@@ -2,12 +2,15 @@
 // modes, stored-wavefield precision, the per-CTA sparse device entries and the
 // per-shot descriptor of one launch.
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace aio {
 
 enum TBMode { TB_SRC = 0, TB_NL = 1, TB_SCAT = 2, TB_ADJ = 3 };
-enum TBWfld { TBW_F32 = 0, TBW_BF16 = 1 };
+// Stored source wavefield: FP32, BF16, or FP16 scaled per coarse slice and shot (the scale
+// maps the slice's max |W| to 2^15, computed exactly from the finished FP32 slice).
+enum TBWfld { TBW_F32 = 0, TBW_BF16 = 1, TBW_F16 = 2 };
 
 struct TBEnt {   // sparse device entry of one CTA, sorted by column
     int col;     // interior x
@@ -30,6 +33,10 @@ struct TBShot {
     float* partOut;       // coarse partial sum carried out (SRC: W[its+1], ADJ: R(its))
     double* img;          // ADJ: image accumulator
     int injLd, recLd;
+    // FP16 stored wavefield only
+    float* wscale;        // [nts] value of one FP16 unit of slice t
+    float* wstage;        // [2][isz] FP32 slices its and its+1 being accumulated (SRC)
+    unsigned* wmax;       // [nts] max |W| of slice t as float bits (SRC)
 };
 
 // Coarse slice t of a stored wavefield of `stride` elements per slice.

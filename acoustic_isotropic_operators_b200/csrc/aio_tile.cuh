@@ -96,24 +96,33 @@ __device__ __forceinline__ void kt_cp8(void* s, const void* g, bool ok) {
 __device__ __forceinline__ void kt_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void kt_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-// four stored-wavefield samples from a staging slot (FP32: 16 bytes, BF16: the first 8)
+// four stored-wavefield samples from a staging slot (FP32: 16 bytes, BF16 / FP16: the first 8)
 template <int WPREC>
-__device__ __forceinline__ float4 kt_wfrom(const float4& slot) {
+__device__ __forceinline__ float4 kt_wfrom(const float4& slot, float sc) {
     if (WPREC == TBW_F32) return slot;
     const uint2 r = *reinterpret_cast<const uint2*>(&slot);
-    const float2 fa = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&r.x));
-    const float2 fb = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&r.y));
-    return make_float4(fa.x, fa.y, fb.x, fb.y);
+    if (WPREC == TBW_BF16) {
+        const float2 fa = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&r.x));
+        const float2 fb = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&r.y));
+        return make_float4(fa.x, fa.y, fb.x, fb.y);
+    }
+    const float2 fa = __half22float2(*reinterpret_cast<const __half2*>(&r.x));
+    const float2 fb = __half22float2(*reinterpret_cast<const __half2*>(&r.y));
+    return make_float4(fa.x * sc, fa.y * sc, fb.x * sc, fb.y * sc);
 }
 
 template <int WPREC>
-__device__ __forceinline__ float4 kt_wload4(const void* W, long long idx) {
+__device__ __forceinline__ float4 kt_wload4(const void* W, long long idx, float sc) {
     if (WPREC == TBW_F32) return __ldg(reinterpret_cast<const float4*>((const float*)W + idx));
-    const uint2 r = __ldg(reinterpret_cast<const uint2*>((const __nv_bfloat16*)W + idx));
-    const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162*>(&r.x);
-    const __nv_bfloat162 b = *reinterpret_cast<const __nv_bfloat162*>(&r.y);
-    const float2 fa = __bfloat1622float2(a), fb = __bfloat1622float2(b);
-    return make_float4(fa.x, fa.y, fb.x, fb.y);
+    const uint2 r = __ldg(reinterpret_cast<const uint2*>((const unsigned short*)W + idx));
+    if (WPREC == TBW_BF16) {
+        const float2 fa = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&r.x));
+        const float2 fb = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&r.y));
+        return make_float4(fa.x, fa.y, fb.x, fb.y);
+    }
+    const float2 fa = __half22float2(*reinterpret_cast<const __half2*>(&r.x));
+    const float2 fb = __half22float2(*reinterpret_cast<const __half2*>(&r.y));
+    return make_float4(fa.x * sc, fa.y * sc, fb.x * sc, fb.y * sc);
 }
 
 template <int WPREC>
@@ -128,6 +137,46 @@ __device__ __forceinline__ void kt_wstore4(void* W, long long idx, const float v
         r.y = *reinterpret_cast<const unsigned*>(&b);
         *reinterpret_cast<uint2*>((__nv_bfloat16*)W + idx) = r;
     }
+}
+
+// FP16 unit of a slice whose max |W| is m (0 for an all-zero slice): m / 2^15
+__device__ __forceinline__ float kt_f16_scale(unsigned maxBits) {
+    const float m = __uint_as_float(maxBits);
+    return m > 0.f ? m * (1.f / 32768.f) : 1.f;
+}
+// quantize four FP32 samples to FP16 units of `sc`
+__device__ __forceinline__ uint2 kt_f16_pack(const float4& v, float sc) {
+    const float inv = 1.f / sc;
+    const __half2 a = __floats2half2_rn(v.x * inv, v.y * inv);
+    const __half2 b = __floats2half2_rn(v.z * inv, v.w * inv);
+    uint2 r;
+    r.x = *reinterpret_cast<const unsigned*>(&a);
+    r.y = *reinterpret_cast<const unsigned*>(&b);
+    return r;
+}
+
+// FP16 stored wavefield: quantize the finished FP32 slice t (staging buffer) over the
+// region [z0, z1) x [x0, x1) (z0 multiple of 4) with its exact scale.
+__device__ __forceinline__ void kt_f16_quantize(const TBShot& sh, long long wStride, int ip, int t, int z0, int z1,
+                                                int x0, int x1, int tid, int nthr) {
+    const float sc = kt_f16_scale(sh.wmax[t]);
+    const float* src = sh.wstage + (long long)(t & 1) * wStride;
+    unsigned short* dst = (unsigned short*)sh.W + (long long)t * wStride;
+    const int nq = (z1 - z0 + 3) / 4, n = nq * (x1 - x0);
+    for (int i = tid; i < n; i += nthr) {
+        const int x = x0 + i / nq, z = z0 + 4 * (i % nq);
+        const long long idx = (long long)x * ip + z;
+        *reinterpret_cast<uint2*>(dst + idx) = kt_f16_pack(*reinterpret_cast<const float4*>(src + idx), sc);
+    }
+}
+
+// Finishes the last two slices (nts-2, nts-1) of an FP16 source pass and records the scales.
+__global__ void k_f16_finish(const TBShot* shots, long long wStride, int ip, int nzi, int nxi, int nts) {
+    const TBShot sh = shots[blockIdx.y];
+    const int nthr = gridDim.x * blockDim.x, tid = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int t = nts - 2; t < nts; t++) kt_f16_quantize(sh, wStride, ip, t, 0, nzi, 0, nxi, tid, nthr);
+    if (tid == 0)
+        for (int t = 0; t < nts; t++) sh.wscale[t] = kt_f16_scale(sh.wmax[t]);
 }
 
 __device__ __forceinline__ float4 kt_ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
@@ -180,6 +229,10 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
     const int strip = blockIdx.x, chunk = blockIdx.y;
     const int ip = g.ip, nxi = g.nxi, nzi = g.nzi, H = g.H, sub = g.sub, its = a.its;
 
+    // FP16 slice scales read by this launch (SCAT: its, its+1; ADJ: 0, its+1)
+    const float scA = (WPREC == TBW_F16 && MODE == TB_SCAT) ? sh.wscale[its] : 1.f;
+    const float scB = (WPREC == TBW_F16 && (MODE == TB_SCAT || MODE == TB_ADJ)) ? sh.wscale[its + 1] : 1.f;
+    const float sc0 = (WPREC == TBW_F16 && MODE == TB_ADJ) ? sh.wscale[0] : 1.f;
     const int tid = threadIdx.x;
     const int cp = tid / NQ;              // column pair 0..7 (>= 8: idle thread)
     const int q = tid - cp * NQ;          // row quad
@@ -301,6 +354,11 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
             }
         }
     };
+    if (WPREC == TBW_F16 && MODE == TB_SRC && its > 0) {
+        // slice its-1 is complete (previous launch): quantize this CTA's output region of it
+        kt_f16_quantize(sh, a.wStride, ip, its - 1, z0, min(z0 + a.HZ, nzi), x0, x1, tid, blockDim.x);
+        __syncthreads();  // the region's staging slots are rewritten below (slice its+1 at the end)
+    }
     issue_input(0);
     kt_commit();
     kt_wait<0>();
@@ -380,8 +438,8 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                             // imagingFwdGpu (F/src/kernelsGpu.cu:309-316): dm * W, kept for levels 2..T
                             const long long idx = (long long)min(max(c0 + j, 0), nxi - 1) * ip + zv;
                             const float4 dmv = __ldg(reinterpret_cast<const float4*>(dmp + idx));
-                            const float4 wa = kt_wfrom<WPREC>(mySlot[(4 + j) * bd]);
-                            const float4 wb = kt_wfrom<WPREC>(mySlot[(6 + j) * bd]);
+                            const float4 wa = kt_wfrom<WPREC>(mySlot[(4 + j) * bd], scA);
+                            const float4 wb = kt_wfrom<WPREC>(mySlot[(6 + j) * bd], scB);
                             sa[j] = make_float4(dmv.x * wa.x, dmv.y * wa.y, dmv.z * wa.z, dmv.w * wa.w);
                             sb[j] = make_float4(dmv.x * wb.x, dmv.y * wb.y, dmv.z * wb.z, dmv.w * wb.w);
                             const float va[4] = {sa[j].x, sa[j].y, sa[j].z, sa[j].w};
@@ -502,18 +560,31 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                         }
                     }
                     kt_st4(pPartOut + idx, wb);
-                    kt_wstore4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, its), idx, wa);
-                    if (its == g.nts - 2) kt_wstore4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, its + 1), idx, wb);
+                    if (WPREC == TBW_F16) {
+                        // FP32 slice its (and its+1 at the end) into the staging buffer; the
+                        // next launch (or k_f16_finish) quantizes it with the slice's exact max
+                        kt_st4(sh.wstage + (long long)(its & 1) * a.wStride + idx, wa);
+                        float m = fmaxf(fmaxf(fabsf(wa[0]), fabsf(wa[1])), fmaxf(fabsf(wa[2]), fabsf(wa[3])));
+                        if (m > 0.f) atomicMax(sh.wmax + its, __float_as_uint(m));
+                        if (its == g.nts - 2) {
+                            kt_st4(sh.wstage + (long long)((its + 1) & 1) * a.wStride + idx, wb);
+                            m = fmaxf(fmaxf(fabsf(wb[0]), fabsf(wb[1])), fmaxf(fabsf(wb[2]), fabsf(wb[3])));
+                            if (m > 0.f) atomicMax(sh.wmax + its + 1, __float_as_uint(m));
+                        }
+                    } else {
+                        kt_wstore4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, its), idx, wa);
+                        if (its == g.nts - 2) kt_wstore4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, its + 1), idx, wb);
+                    }
                 } else if (MODE == TB_ADJ) {
                     float ra[4], rb[4];
                     double acc[4];
                     const float4 oP = mySlot[(4 + j) * bd];
-                    const float4 oW = kt_wfrom<WPREC>(mySlot[(6 + j) * bd]);
+                    const float4 oW = kt_wfrom<WPREC>(mySlot[(6 + j) * bd], scB);
                     const double2* oI = reinterpret_cast<const double2*>(&mySlot[(8 + 2 * j) * bd]);
                     const double2* oI2 = reinterpret_cast<const double2*>(&mySlot[(9 + 2 * j) * bd]);
                     const double oImg[4] = {oI->x, oI->y, oI2->x, oI2->y};
                     float4 w0 = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (its == 0) w0 = kt_wload4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, 0), idx);
+                    if (its == 0) w0 = kt_wload4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, 0), idx, sc0);
 #pragma unroll
                     for (int i = 0; i < 4; i++) {
                         ra[i] = 0.f;

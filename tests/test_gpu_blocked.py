@@ -130,3 +130,21 @@ def test_ragged_grid(stepper):
     gf = ctx(c, stepper=stepper).born_forward(m, shots(c))[0]
     rf = orc.born_fwd(c.scheme, c.vel, m, c.sig[0], c.src_pos[0], c.rec_pos[0], dtype=np.float32)
     assert rel_l2(gf, rf) < 1e-5
+
+
+def test_born_fp16_dot_and_error(case):
+    """FP16 stored wavefield with per-slice scales: the operator stays linear in the model
+    (dot test at the FP32 bound) and close to the FP64 oracle."""
+    c = ctx(case, stepper="blocked", wavefield="fp16")
+    m = case.rng.standard_normal((case.nx, case.nz)).astype(np.float32) * interior_mask(case.nx, case.nz)
+    d = [case.rng.standard_normal((len(r), case.scheme.nts)).astype(np.float32) for r in case.rec_pos]
+    fm = c.born_forward(m, shots(case))
+    fm = [x.copy() for x in fm]
+    ad = c.born_adjoint(shots(case, d))
+    a = sum(float(np.sum(fm[i].astype(np.float64) * d[i])) for i in range(len(d)))
+    b = float(np.sum(m.astype(np.float64) * ad))
+    assert abs(a - b) / abs(b) < 1e-5
+    v64 = case.vel.astype(np.float64)
+    for i in range(len(fm)):
+        r64 = orc.born_fwd(case.scheme, v64, m, case.sig[i], case.src_pos[i], case.rec_pos[i])
+        assert rel_l2(fm[i], r64) < 1e-3
