@@ -29,7 +29,7 @@ AIO_STEPPER_AUTO, AIO_STEPPER_FINE, AIO_STEPPER_BLOCKED = range(3)
 EXPORTED = [
     "aio_last_error", "aio_context_create", "aio_context_destroy", "aio_context_set_velocity",
     "aio_context_wave_capacity", "aio_context_last_launches", "aio_context_stream", "aio_context_profile",
-    "aio_context_stats", "aio_context_reset_stats",
+    "aio_context_stats", "aio_context_reset_stats", "aio_context_blocked_plan",
     "aio_nonlinear_forward", "aio_nonlinear_adjoint", "aio_nonlinear_forward_wavefield",
     "aio_nonlinear_adjoint_wavefield", "aio_born_forward", "aio_born_adjoint", "aio_born_adjoint_shots",
     "aio_born_ext_forward", "aio_born_ext_adjoint", "aio_tomo_ext_forward", "aio_tomo_ext_adjoint",

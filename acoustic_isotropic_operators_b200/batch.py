@@ -94,6 +94,12 @@ class Context:
         A.check(A.lib().aio_context_stats(self._h, C.byref(k), C.byref(ms), C.byref(n), C.byref(pts)))
         return int(k.value), float(ms.value), int(n.value), float(pts.value)
 
+    def blocked_plan(self, n_shots: int) -> dict:
+        """Strip rows, strips, chunk columns and chunks the blocked stepper uses for n_shots."""
+        out = (C.c_int * 4)()
+        A.check(A.lib().aio_context_blocked_plan(self._h, int(n_shots), out))
+        return {"strip_rows": out[0], "strips": out[1], "chunk_columns": out[2], "chunks": out[3]}
+
     def reset_stats(self) -> None:
         A.check(A.lib().aio_context_reset_stats(self._h))
 

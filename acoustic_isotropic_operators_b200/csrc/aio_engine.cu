@@ -783,20 +783,29 @@ struct Context {
     bool f16() const { return P.wavefieldPrecision == AIO_WFLD_FP16; }
 
     // nb: shots of the wave (one CTA column per shot)
+    // Plan of a wave of nb shots: the autotuned plan when one was measured, else the model's.
     TBPlan tb_plan(int nb) const {
+        auto it = tbTuned.find(nb);
+        if (it != tbTuned.end()) return it->second;
+        return tb_model_plan(nb, 4 * (KT_MAXQ - 10), P.chunkColumns > 0 ? P.chunkColumns : 0);
+    }
+
+    // Strips of at most maxHZ rows; x-chunks of about chunkColumns columns, or (0) the chunk
+    // count minimising the modelled time: whole CTA waves over the SMs (one resident CTA per
+    // SM) times the iterations of one CTA (each chunk recomputes 10T warm-up columns), at
+    // least 4 waves preferred so that CTAs of uneven cost (strips holding sources or
+    // receivers) balance out.
+    TBPlan tb_model_plan(int nb, int maxHZ, int chunkColumns, int forceChunks = 0) const {
         TBPlan pl;
-        const int maxHZ = 4 * (KT_MAXQ - 10);
         pl.nStrips = (g.nzi + maxHZ - 1) / maxHZ;
         pl.HZ = round_up((g.nzi + pl.nStrips - 1) / pl.nStrips, 4);
         pl.NQ = pl.HZ / 4 + 10;
         pl.threads = round_up(8 * pl.NQ, 32);
-        if (P.chunkColumns > 0) {
-            pl.nChunks = std::max(1, (g.nxi + P.chunkColumns / 2) / P.chunkColumns);
+        if (forceChunks > 0) {
+            pl.nChunks = std::min(forceChunks, g.nxi);
+        } else if (chunkColumns > 0) {
+            pl.nChunks = std::max(1, (g.nxi + chunkColumns / 2) / chunkColumns);
         } else {
-            // Chunk count minimising the modelled time: whole CTA waves over the SMs
-            // (one resident CTA per SM) times the iterations of one CTA (each chunk
-            // recomputes 10T warm-up columns). At least 4 waves are preferred so that
-            // CTAs of uneven cost (strips holding sources / receivers) balance out.
             double best = 1e300, bestAny = 1e300;
             int ncAny = 1;
             pl.nChunks = 0;
@@ -818,6 +827,63 @@ struct Context {
         pl.LX = (g.nxi + pl.nChunks - 1) / pl.nChunks;
         pl.iters = (pl.LX + 10 * pl.T + KT_BX - 1) / KT_BX;
         return pl;
+    }
+
+    // Measured autotuning of the blocked stepper's plan for waves of nb shots (chunkColumns
+    // == 0): strip heights {128, 112, 96} rows x chunk counts around the model's choice are
+    // each timed on the source-pass launch of interval 0 (idempotent: it reads one state set
+    // and overwrites the other, the stored slice 0 and the partial sums), the fastest is
+    // cached for the context. The state is zeroed again afterwards.
+    std::map<int, TBPlan> tbTuned;
+    TBPlan tbLast;  // plan of the most recent blocked launch
+    void tb_autotune(int nb, const aio_shot* shots) {
+        if (P.chunkColumns != 0 || tbTuned.count(nb)) return;
+        std::vector<TBPlan> cand;
+        for (int maxHZ : {128, 112, 96}) {
+            const TBPlan m = tb_model_plan(nb, maxHZ, 0);
+            for (int d : {-2, -1, 0, 1, 2}) {
+                const int nc = m.nChunks + d;
+                if (nc < 1 || nc > std::max(1, g.nxi / 32)) continue;
+                TBPlan c = tb_model_plan(nb, maxHZ, 0, nc);
+                bool dup = false;
+                for (auto& o : cand) dup |= (o.HZ == c.HZ && o.nChunks == c.nChunks);
+                if (!dup && c.threads <= KT_MAXT && c.NQ <= KT_MAXQ) cand.push_back(c);
+            }
+        }
+        cudaEvent_t e0, e1;
+        AIO_CK(cudaEventCreate(&e0));
+        AIO_CK(cudaEventCreate(&e1));
+        float bestMs = 1e30f;
+        TBPlan best = cand.front();
+        const long long saveLaunches = launches, saveKernels = kernels;
+        const int saveProf = profEvery;
+        profEvery = 0;
+        for (const TBPlan& pl : cand) {
+            const int maxEnt = tb_lists(pl, nb, shots, 1, false);
+            tb_zero(nb, false);
+            tb_desc(pl, nb, true, false, false, tbW.p, false);
+            KTArgs a = tb_args(pl, maxEnt, nullptr);
+            a.its = 0;
+            if (f16()) AIO_CK(cudaMemsetAsync(tbWmax.p, 0, (size_t)nb * g.nts * 4, st));
+            tb_launch<TB_SRC>(pl, nb, a, 0);  // warm-up (smem carve-out, caches)
+            AIO_CK(cudaEventRecord(e0, st));
+            tb_launch<TB_SRC>(pl, nb, a, 0);
+            tb_launch<TB_SRC>(pl, nb, a, 0);
+            AIO_CK(cudaEventRecord(e1, st));
+            AIO_CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            AIO_CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < bestMs) {
+                bestMs = ms;
+                best = pl;
+            }
+        }
+        AIO_CK(cudaEventDestroy(e0));
+        AIO_CK(cudaEventDestroy(e1));
+        launches = saveLaunches;
+        kernels = saveKernels;
+        profEvery = saveProf;
+        tbTuned[nb] = best;
     }
 
     // Per-CTA sparse lists of every shot of a wave. inj: 0 none, 1 sources, 2 receivers
@@ -960,6 +1026,7 @@ struct Context {
                                              " bytes exceeds the device limit (too many devices per tile)");
         require(pl.threads <= KT_MAXT && pl.NQ <= KT_MAXQ, "blocked stepper: strip taller than the ring");
         a.shots = tbDesc.as<TBShot>() + (size_t)v * nb;
+        tbLast = pl;
         const bool timed = profEvery > 0 && (launches % profEvery) == 0;
         std::pair<cudaEvent_t, cudaEvent_t> ev{};
         if (timed) {
@@ -992,6 +1059,7 @@ struct Context {
     // Source pass storing W[nts] (F/src/BornShotsGpuFunctions.cu:297-321), or the
     // nonlinear forward when recordData (F/src/nonlinearShotsGpuFunctions.cu:269-295).
     void tb_src_pass(int nb, const aio_shot* shots, bool nonlinear) {
+        if (!nonlinear) tb_autotune(nb, shots);
         const TBPlan pl = tb_plan(nb);
         const int maxEnt = tb_lists(pl, nb, shots, 1, nonlinear);
         tb_zero(nb, false);
@@ -1629,6 +1697,16 @@ AIO_API int aio_born_forward(aio_context* ctx, const float* model, int nShots, c
 AIO_API int aio_born_adjoint(aio_context* ctx, float* model, int add, int nShots, const aio_shot* shots,
                              int memSpace) {
     return guard([&] { ctx->c.born_adjoint(model, add, nShots, shots, memSpace); });
+}
+AIO_API int aio_context_blocked_plan(aio_context* ctx, int nShots, int* plan) {
+    return guard([&] {
+        require(plan != nullptr, "plan output is NULL");
+        const auto pl = nShots >= 1 ? ctx->c.tb_plan(nShots) : ctx->c.tbLast;
+        plan[0] = pl.HZ;
+        plan[1] = pl.nStrips;
+        plan[2] = pl.LX;
+        plan[3] = pl.nChunks;
+    });
 }
 AIO_API int aio_born_adjoint_shots(aio_context* ctx, float* const* images, int nShots, const aio_shot* shots,
                                    int memSpace) {

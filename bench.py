@@ -353,11 +353,15 @@ def main():
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"1 shot, Born forward+adjoint, full grid, nts={nts_sample} ({dt:.1f} s)"}
 
+    try:
+        plan = ctx.blocked_plan(0) if kernel_name(args, w).startswith("k_tile") else None  # last launch's plan
+    except Exception:
+        plan = None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, BASELINE shapes)",
-                "config": config_dict(args, w),
+                "config": dict(config_dict(args, w), plan=plan),
                 "roofline": {"bound": "hbm", "kernel": kernel_name(args, w),
                              "achieved": achieved, "peak": hbm_peak, "peak_source": peak_src, "unit": "GB/s",
                              "frac": (achieved / hbm_peak) if achieved else None,

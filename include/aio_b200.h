@@ -66,7 +66,8 @@ typedef struct {
     int device;          /* CUDA device ordinal */
     long long memBudgetBytes; /* cap on device memory for shot buffers; 0 = 90% of free */
     int stepper;         /* AIO_STEPPER_*: how Born / nonlinear passes advance time */
-    int chunkColumns;    /* blocked stepper x-chunk width (0 = automatic) */
+    int chunkColumns;    /* blocked stepper x-chunk width: 0 = autotuned (measured once per wave size),
+                            > 0 = fixed width (strips of at most 128 rows) */
 } aio_params;
 
 #define AIO_STEPPER_AUTO 0      /* interval-blocked where available (sub == 4), else per fine step */
@@ -98,6 +99,10 @@ long long aio_context_last_launches(aio_context* ctx);
 const char* aio_last_error(void);
 /* The CUDA stream (cudaStream_t) every kernel of this context runs on. */
 void* aio_context_stream(aio_context* ctx);
+/* Blocked-stepper plan for a wave of nShots shots (nShots <= 0: the plan of the most recent
+ * blocked launch): plan[0..3] = strip rows, strips, chunk columns, chunks (the autotuned plan
+ * once a Born source pass of that wave size has run). */
+int aio_context_blocked_plan(aio_context* ctx, int nShots, int* plan);
 /* Live stepper timing: bracket every sampleEvery-th stepper launch with CUDA events (0 = off). */
 int aio_context_profile(aio_context* ctx, int sampleEvery);
 /* Kernels launched, and timed-stepper totals (milliseconds, launches, interior
