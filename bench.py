@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--cpu-nts", type=int, default=0, help="coarse samples of the CPU sample (0 = auto)")
     ap.add_argument("--stepper", default="auto", choices=["auto", "fine", "blocked"])
     ap.add_argument("--chunk", type=int, default=0, help="blocked-stepper chunk width (0 = automatic)")
+    ap.add_argument("--ext", type=int, default=0,
+                    help="instead of the Born step: time the extended (time-lag, nExt=31) Born adjoint of N "
+                         "shots on the 500x1500 grid and print that line")
     ap.add_argument("--plain", type=int, default=0,
                     help="instead of the batched step: time N shots one per call on the per-fine-step "
                          "stepper (the reference's schedule), FP32, and print that line")
@@ -225,12 +228,49 @@ def run_plain(args):
     return 0
 
 
+def run_ext(args):
+    """Extended (time-lag, nExt = 31) Born adjoint of N shots on the 500x1500 physical grid
+    (608x1600 interior), host buffers, one call after one warm-up call."""
+    import torch
+    from acoustic_isotropic_operators_b200 import _capi, synthetic as S
+    from acoustic_isotropic_operators_b200.batch import Context, Shot
+    n_ext = 31
+    w = S.born_workload(nz_phys=500, nx_phys=1500, nshots=args.ext, nts=args.nts)
+    lib = _capi.lib()
+    v2 = np.zeros(w.nz * w.nx, np.float32)
+    rs = np.zeros_like(v2)
+    velf = np.ascontiguousarray(w.vel.reshape(-1), np.float32)
+    lib.aio_fd_precompute(w.nz, w.nx, C.c_float(w.dts), w.sub, velf.ctypes.data_as(C.c_void_p),
+                          v2.ctypes.data_as(C.c_void_p), rs.ctypes.data_as(C.c_void_p))
+    sigs = prepare_signals(w, lib)
+    rng = np.random.default_rng(4)
+    shots = [Shot(a.src_pos, a.rec_pos, sg, (rng.standard_normal((len(a.rec_pos), w.nts)) * 1e-3).astype(np.float32))
+             for a, sg in zip(w.shots, sigs)]
+    ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs, nExt=n_ext, image_fp64=True)
+    ctx.born_ext_adjoint(shots)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.born_ext_adjoint(shots)
+    t = time.perf_counter() - t0
+    n, steps, T = w.n_interior, w.fine_steps, w.nts - 1
+    pts = n * steps * 2 * len(shots)
+    algo = len(shots) * n * (2 * 16 * steps + 4 * w.nts + (4 + 4) * T + 8 * n_ext)
+    print(json.dumps({"impl": "this engine, extended Born adjoint (per-fine-step stepper, FP32 W)",
+                      "metric": "Gpts/s, extended (time-lag) Born adjoint", "value": pts / t / 1e9, "unit": UNIT,
+                      "seconds": t, "shots": len(shots), "nExt": n_ext, "interior": [w.nz - 10, w.nx - 10],
+                      "nts": w.nts, "algorithmic_GBps": algo / t / 1e9, "data": "synthetic (seeded)"}))
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.plain:
         return run_plain(args)
+    if args.ext:
+        return run_ext(args)
 
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
