@@ -772,6 +772,7 @@ struct Context {
     // images use interior slices; the stored wavefield is FP32 or BF16.
     DevMem tbState, tbPart, tbImg, tbW, tbEnt, tbStart, tbDesc, shotImg;
     DevMem tbWscale, tbWmax, tbWstage;  // FP16 stored wavefield: per-slice scales, max |W|, FP32 staging
+    DevMem tbR;                         // extended adjoint: coarse receiver samples [shot][2][isz]
     // k_tile plan: strips of HZ (multiple of 4) output rows, NQ = HZ/4 + 10 row quads,
     // 8 column pairs per quad, x-chunks of LX columns marched in blocks of 16.
     struct TBPlan {
@@ -983,6 +984,7 @@ struct Context {
                 t.ent = tbEnt.as<TBEnt>();
                 t.W = W ? (void*)((char*)W + (size_t)s * g.nts * g.isz * wbytes()) : nullptr;
                 t.img = tbImg.p ? tbImg.as<double>() + (size_t)s * g.isz : nullptr;
+                t.rcoarse = tbR.p ? tbR.as<float>() + (size_t)s * 2 * g.isz : nullptr;
                 if (f16()) {
                     t.wscale = tbWscale.as<float>() + (size_t)s * g.nts;
                     t.wmax = tbWmax.as<unsigned>() + (size_t)s * g.nts;
@@ -1104,6 +1106,66 @@ struct Context {
             a.its = g.nts - 2 - L;
             tb_launch<TB_ADJ>(pl, nb, a, L & 1);
         }
+    }
+
+    // Receiver pass of the extended (time-lag) adjoint (F/src/BornExtShotsGpuFunctions.cu:1525-1675)
+    // on the blocked stepper: launch L (interval its = nts-2-L) finishes the coarse receiver sample
+    // R(its+1) (and R(0) at its == 0); image[e] += R(t) * W[t - 2(e-h)] follows per sample
+    // (imagingTimeAdjGpu, F/src/kernelsGpu.cu:352-364).
+    void tb_adjx_pass(int nb, const aio_shot* shots) {
+        const TBPlan pl = tb_plan(nb);
+        const int maxEnt = tb_lists(pl, nb, shots, 2, false);
+        tb_zero(nb, false);
+        tb_desc(pl, nb, false, true, false, tbW.p, false);
+        KTArgs a = tb_args(pl, maxEnt, nullptr);
+        const long long mSt = (long long)g.nExt * g.isz;
+        auto image = [&](int t, long long rOff) {
+            int e0, e1;
+            bounds_src(t, e0, e1);
+            if (P.imageFp64)
+                k_img_time_adj<double><<<ew_grid(nb, g.isz), 256, 0, st>>>(
+                    img.as<double>(), mSt, tbR.as<float>() + rOff, 2 * g.isz, tbW.as<float>(), wfSt(), g.isz, t, e0, e1,
+                    g.hExt, +1, 0);
+            else
+                k_img_time_adj<float><<<ew_grid(nb, g.isz), 256, 0, st>>>(
+                    img.as<float>(), mSt, tbR.as<float>() + rOff, 2 * g.isz, tbW.as<float>(), wfSt(), g.isz, t, e0, e1,
+                    g.hExt, +1, 0);
+            kcheck();
+        };
+        for (int L = 0; L < g.nts - 1; L++) {
+            a.its = g.nts - 2 - L;
+            tb_launch<TB_ADJR>(pl, nb, a, L & 1);
+            image(a.its + 1, 0);
+            if (a.its == 0) image(0, g.isz);
+        }
+    }
+
+    void born_ext_adjoint_tb(float* modelOut, int add, int nShots, const aio_shot* shots, int mem) {
+        require(P.wavefieldPrecision == AIO_WFLD_FP32,
+                "the extended operators keep the stored wavefield in FP32 (wavefieldPrecision)");
+        Needs n;
+        n.nImg = g.nExt;
+        float* out = stage_out(modelOut, g.nExt, add, mem);
+        for (int s0 = 0; s0 < nShots;) {
+            int nb = tb_wave_size(nShots - s0, shots + s0, true, false);
+            // extended images: nExt slices per shot
+            const long long perImg = (long long)g.nExt * g.isz * (P.imageFp64 ? 8 : 4) + 2LL * g.isz * 4;
+            nb = std::max(1, std::min<int>(nb, (int)std::max<long long>(1, (budget / 2) / perImg)));
+            setup_wave(n, nb, shots + s0, mem, true, false);
+            tb_alloc(nb, false);
+            tbW.ensure((size_t)nb * g.nts * g.isz * 4);
+            tbR.ensure((size_t)nb * 2 * g.isz * 4);
+            tb_src_pass(nb, shots + s0, false);
+            zero_images(nb, g.nExt);
+            tb_adjx_pass(nb, shots + s0);
+            // images of U = v2 * receiver wavefield: the reference's rs*v2 scaling reduces to rs,
+            // the sloth scaling -(m*v2) to a sign change
+            reduce_images(nb, g.nExt, P.sloth ? 4 : 3, out, true);
+            sync();
+            s0 += nb;
+        }
+        write_model(modelOut, g.nExt, add, mem, out);
+        sync();
     }
 
     // ============================================================ operators
@@ -1349,6 +1411,8 @@ struct Context {
     // Extended (time-lag) Born adjoint (F/src/BornExtShotsGpuFunctions.cu:1525-1675).
     void born_ext_adjoint(float* modelOut, int add, int nShots, const aio_shot* shots, int mem) {
         begin_call();
+        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32)
+            return born_ext_adjoint_tb(modelOut, add, nShots, shots, mem);
         Needs n;
         n.nWavefields = 1;
         n.nImg = g.nExt;

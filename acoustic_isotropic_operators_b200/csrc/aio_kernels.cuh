@@ -250,7 +250,8 @@ __global__ void k_img_time_adj(Acc* m, long long mSt, float* r, long long rSt, c
 }
 
 // Scalings (F/src/kernelsGpu.cu:246-252, 278-303). mode 0: m *= v2*rs;
-// mode 1: m *= rs*v2 (extended); mode 2: m = -(m*v2) (sloth).
+// mode 1: m *= rs*v2 (extended); mode 2: m = -(m*v2) (sloth); on images of v2-weighted
+// (adjoint U-form) wavefields: mode 3: m *= rs, mode 4: m = -m.
 __global__ void k_scale(float* m, long long mSt, int nSlices, const float* v2, const float* rs, long long isz,
                         int mode) {
     const int b = blockIdx.y;
@@ -261,6 +262,8 @@ __global__ void k_scale(float* m, long long mSt, int nSlices, const float* v2, c
         const float v = v2[i], r = rs[i];
         if (mode == 0) m[k] *= v * r;
         else if (mode == 1) m[k] *= r * v;
+        else if (mode == 3) m[k] *= r;   // images of v2-weighted (adjoint U-form) wavefields
+        else if (mode == 4) m[k] = -m[k];
         else m[k] = -(m[k] * v);
     }
 }
@@ -304,6 +307,7 @@ __global__ void k_scale_d(double* m, long long mSt, int nSlices, const float* v2
         if (mode == 0) m[k] *= (double)(float)(v * r);
         else if (mode == 1) m[k] *= (double)(float)(r * v);
         else if (mode == 3) m[k] *= r;   // images of v2-weighted (adjoint U-form) wavefields
+        else if (mode == 4) m[k] = -m[k];  // sloth images of U-form wavefields
         else m[k] = -(m[k] * v);
     }
 }

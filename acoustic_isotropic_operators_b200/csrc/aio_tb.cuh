@@ -7,7 +7,10 @@
 
 namespace aio {
 
-enum TBMode { TB_SRC = 0, TB_NL = 1, TB_SCAT = 2, TB_ADJ = 3 };
+// TB_ADJR: the adjoint recursion of TB_ADJ writing the finished coarse receiver sample
+// R(its+1) (and R(0) at its == 0) instead of forming the Born image (extended imaging
+// is done on those samples by the coarse kernels).
+enum TBMode { TB_SRC = 0, TB_NL = 1, TB_SCAT = 2, TB_ADJ = 3, TB_ADJR = 4 };
 // Stored source wavefield: FP32, BF16, or FP16 scaled per coarse slice and shot (the scale
 // maps the slice's max |W| to 2^15, computed exactly from the finished FP32 slice).
 enum TBWfld { TBW_F32 = 0, TBW_BF16 = 1, TBW_F16 = 2 };
@@ -37,6 +40,7 @@ struct TBShot {
     float* wscale;        // [nts] value of one FP16 unit of slice t
     float* wstage;        // [2][isz] FP32 slices its and its+1 being accumulated (SRC)
     unsigned* wmax;       // [nts] max |W| of slice t as float bits (SRC)
+    float* rcoarse;       // ADJR: [2][isz] coarse receiver samples R(its+1), R(0)
 };
 
 // Coarse slice t of a stored wavefield of `stride` elements per slice.

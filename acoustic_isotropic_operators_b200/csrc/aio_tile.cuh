@@ -69,7 +69,7 @@ struct KTArgs {
 // of the next iteration (old level, v^2: slots 0-3) and the output operands of the current
 // iteration (partial sum: 4-5, stored wavefield: 6-7, FP64 image: 8-11).
 __host__ __device__ constexpr int kt_slots(int mode) {
-    return mode == TB_ADJ ? 12 : (mode == TB_SRC ? 6 : (mode == TB_SCAT ? 8 : 4));
+    return mode == TB_ADJ ? 12 : ((mode == TB_SRC || mode == TB_ADJR) ? 6 : (mode == TB_SCAT ? 8 : 4));
 }
 // Ring columns: levels 0..T-1, plus (scattered pass) the secondary sources dm*W[its] and
 // dm*W[its+1] of the last 32 level-1 columns, formed once at level 1 and read by levels 2..T.
@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
             const int e = i / T, t = i - e * T + 1;
             const float* tr = pInj + (long long)sEnt[e].dev * injLd;
             float v;
-            if (MODE == TB_ADJ) {
+            if (MODE == TB_ADJ || MODE == TB_ADJR) {
                 const int it2 = sub - t;
                 v = tr[its] * a.h[it2 + 1] + tr[its + 1] * a.h[H + it2 + 1];
             } else {
@@ -368,7 +368,7 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
         const int B = xs + KT_BX * k;
         // Output operands of this iteration's level-T columns, copied asynchronously into
         // this thread's staging slots (read at the output stage).
-        if (MODE == TB_SRC || MODE == TB_ADJ) {
+        if (MODE == TB_SRC || MODE == TB_ADJ || MODE == TB_ADJR) {
 #pragma unroll
             for (int j = 0; j < 2; j++) {
                 const int c = B - 5 * T + 2 * cp + j;
@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                             const int rr = sEnt[e].row - zq;
                             if (rr >= 0 && rr < 4) {
                                 float v = sInjV[e * T + t - 1];
-                                if (MODE == TB_ADJ) v = kt_el(vq[j], rr) * v;
+                                if (MODE == TB_ADJ || MODE == TB_ADJR) v = kt_el(vq[j], rr) * v;
 #pragma unroll
                                 for (int i = 0; i < 4; i++)
                                     if (i == rr) S[j][i] = S[j][i] + v;
@@ -600,6 +600,22 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                     kt_st4(pPartOut + idx, ra);
                     *reinterpret_cast<double2*>(pImg + idx) = make_double2(acc[0], acc[1]);
                     *reinterpret_cast<double2*>(pImg + idx + 2) = make_double2(acc[2], acc[3]);
+                } else if (MODE == TB_ADJR) {
+                    float ra[4], rb[4];
+                    const float4 oP = mySlot[(4 + j) * bd];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        ra[i] = 0.f;
+                        rb[i] = kt_el(oP, i);
+#pragma unroll
+                        for (int l = 1; l <= T; l++) {
+                            ra[i] += lvT[j][l][i] * a.h[sub - l];
+                            rb[i] += lvT[j][l][i] * a.h[H + sub - l];
+                        }
+                    }
+                    kt_st4(pPartOut + idx, ra);
+                    kt_st4(sh.rcoarse + idx, rb);                             // R(its+1)
+                    if (its == 0) kt_st4(sh.rcoarse + a.wStride + idx, ra);    // R(0)
                 } else if (qRec) {
                     for (int e = recFirst[c - xs + 32]; e >= 0 && e < nRec && sEnt[recOff + e].col == c; e++) {
                         const int rr = sEnt[recOff + e].row - zq;

@@ -148,3 +148,26 @@ def test_born_fp16_dot_and_error(case):
     for i in range(len(fm)):
         r64 = orc.born_fwd(case.scheme, v64, m, case.sig[i], case.src_pos[i], case.rec_pos[i])
         assert rel_l2(fm[i], r64) < 1e-3
+
+
+@pytest.mark.parametrize("sloth", [0, 1])
+def test_born_ext_adjoint_blocked(case, sloth):
+    """Extended (time-lag) Born adjoint with the receiver pass on the blocked stepper: vs the
+    FP32 oracle, and the dot test against the extended forward (per-fine-step stepper)."""
+    import dataclasses
+    s5 = dataclasses.replace(case.scheme, nExt=5)
+    from acoustic_isotropic_operators_b200.batch import Context
+    k = orc.constants(s5, case.vel, dtype=np.float32)
+    c = Context(s5.nz, s5.nx, s5.nts, s5.dts, s5.sub, s5.dz, s5.dx, s5.minPad, k["v2"], k["rs"], nExt=5,
+                sloth=sloth, chunk_columns=64)
+    d = [case.rng.standard_normal((len(r), s5.nts)).astype(np.float32) for r in case.rec_pos]
+    got = c.born_ext_adjoint(shots(case, d))
+    assert c.last_launches == 2 * (s5.nts - 1)          # both passes on the blocked stepper
+    ref = sum(orc.bornext_adj(s5, case.vel, d[i], case.sig[i], case.src_pos[i], case.rec_pos[i],
+                              dtype=np.float32, sloth=sloth) for i in range(len(d)))
+    assert rel_l2(got, ref) < 1e-5
+    m = case.rng.standard_normal((5, case.nx, case.nz)).astype(np.float32) * interior_mask(case.nx, case.nz)
+    fm = c.born_ext_forward(m, shots(case))
+    a = sum(float(np.sum(fm[i].astype(np.float64) * d[i])) for i in range(len(d)))
+    b = float(np.sum(m.astype(np.float64) * got))
+    assert abs(a - b) / abs(b) < 1e-5
