@@ -170,4 +170,6 @@ def test_born_ext_adjoint_blocked(case, sloth):
     fm = c.born_ext_forward(m, shots(case))
     a = sum(float(np.sum(fm[i].astype(np.float64) * d[i])) for i in range(len(d)))
     b = float(np.sum(m.astype(np.float64) * got))
-    assert abs(a - b) / abs(b) < 1e-5
+    # forward on the per-fine-step stepper, adjoint on the blocked stepper: two FP32
+    # implementations, each within 1e-5 of the oracle, hence the looser bound here
+    assert abs(a - b) / abs(b) < 5e-5
