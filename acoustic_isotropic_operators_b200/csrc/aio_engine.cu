@@ -984,7 +984,7 @@ struct Context {
                 t.ent = tbEnt.as<TBEnt>();
                 t.W = W ? (void*)((char*)W + (size_t)s * g.nts * g.isz * wbytes()) : nullptr;
                 t.img = tbImg.p ? tbImg.as<double>() + (size_t)s * g.isz : nullptr;
-                t.rcoarse = tbR.p ? tbR.as<float>() + (size_t)s * 2 * g.isz : nullptr;
+                t.rcoarse = tbR.p ? tbR.as<float>() + (size_t)s * LAG_K * g.isz : nullptr;
                 if (f16()) {
                     t.wscale = tbWscale.as<float>() + (size_t)s * g.nts;
                     t.wmax = tbWmax.as<unsigned>() + (size_t)s * g.nts;
@@ -1109,9 +1109,10 @@ struct Context {
     }
 
     // Receiver pass of the extended (time-lag) adjoint (F/src/BornExtShotsGpuFunctions.cu:1525-1675)
-    // on the blocked stepper: launch L (interval its = nts-2-L) finishes the coarse receiver sample
-    // R(its+1) (and R(0) at its == 0); image[e] += R(t) * W[t - 2(e-h)] follows per sample
-    // (imagingTimeAdjGpu, F/src/kernelsGpu.cu:352-364).
+    // on the blocked stepper: launch L (interval its = nts-2-L) finishes the coarse receiver
+    // sample R(its+1) (and R(0) at its == 0) into a ring of LAG_K slices; each time the lowest
+    // sample of a block [bK, bK+K) has arrived, k_img_lag_block correlates the block with the
+    // stored wavefield (imagingTimeAdjGpu, F/src/kernelsGpu.cu:352-364, for every t of it).
     void tb_adjx_pass(int nb, const aio_shot* shots) {
         const TBPlan pl = tb_plan(nb);
         const int maxEnt = tb_lists(pl, nb, shots, 2, false);
@@ -1119,24 +1120,35 @@ struct Context {
         tb_desc(pl, nb, false, true, false, tbW.p, false);
         KTArgs a = tb_args(pl, maxEnt, nullptr);
         const long long mSt = (long long)g.nExt * g.isz;
-        auto image = [&](int t, long long rOff) {
-            int e0, e1;
-            bounds_src(t, e0, e1);
+        const int nP = 128;
+        const size_t lagSmem = (size_t)(LAG_K + 4 * g.hExt) * nP * 4;
+        static int lagAttr = -1;
+        if (lagAttr != dev) {
+            AIO_CK(cudaFuncSetAttribute(k_img_lag_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            AIO_CK(cudaFuncSetAttribute(k_img_lag_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            lagAttr = dev;
+        }
+        require(lagSmem <= 200 * 1024, "extension too long for the blocked lag imaging");
+        auto image = [&](int tlo, int thi) {
+            const dim3 grid((unsigned)((g.isz + nP - 1) / nP), nb);
             if (P.imageFp64)
-                k_img_time_adj<double><<<ew_grid(nb, g.isz), 256, 0, st>>>(
-                    img.as<double>(), mSt, tbR.as<float>() + rOff, 2 * g.isz, tbW.as<float>(), wfSt(), g.isz, t, e0, e1,
-                    g.hExt, +1, 0);
+                k_img_lag_block<double><<<grid, nP, lagSmem, st>>>(img.as<double>(), mSt, tbR.as<float>(),
+                                                                    (long long)LAG_K * g.isz, tbW.as<float>(), wfSt(),
+                                                                    g.isz, tlo, thi, g.nts, g.hExt, g.nExt);
             else
-                k_img_time_adj<float><<<ew_grid(nb, g.isz), 256, 0, st>>>(
-                    img.as<float>(), mSt, tbR.as<float>() + rOff, 2 * g.isz, tbW.as<float>(), wfSt(), g.isz, t, e0, e1,
-                    g.hExt, +1, 0);
+                k_img_lag_block<float><<<grid, nP, lagSmem, st>>>(img.as<float>(), mSt, tbR.as<float>(),
+                                                                   (long long)LAG_K * g.isz, tbW.as<float>(), wfSt(),
+                                                                   g.isz, tlo, thi, g.nts, g.hExt, g.nExt);
             kcheck();
         };
         for (int L = 0; L < g.nts - 1; L++) {
             a.its = g.nts - 2 - L;
+            const int t = a.its + 1;
+            a.rSlot = t % LAG_K;
+            a.rSlot0 = 0;
             tb_launch<TB_ADJR>(pl, nb, a, L & 1);
-            image(a.its + 1, 0);
-            if (a.its == 0) image(0, g.isz);
+            if (a.its == 0) image(0, std::min(LAG_K - 1, g.nts - 1));
+            else if (t % LAG_K == 0) image(t, std::min(t + LAG_K - 1, g.nts - 1));
         }
     }
 
@@ -1149,12 +1161,12 @@ struct Context {
         for (int s0 = 0; s0 < nShots;) {
             int nb = tb_wave_size(nShots - s0, shots + s0, true, false);
             // extended images: nExt slices per shot
-            const long long perImg = (long long)g.nExt * g.isz * (P.imageFp64 ? 8 : 4) + 2LL * g.isz * 4;
+            const long long perImg = (long long)g.nExt * g.isz * (P.imageFp64 ? 8 : 4) + (long long)LAG_K * g.isz * 4;
             nb = std::max(1, std::min<int>(nb, (int)std::max<long long>(1, (budget / 2) / perImg)));
             setup_wave(n, nb, shots + s0, mem, true, false);
             tb_alloc(nb, false);
             tbW.ensure((size_t)nb * g.nts * g.isz * 4);
-            tbR.ensure((size_t)nb * 2 * g.isz * 4);
+            tbR.ensure((size_t)nb * LAG_K * g.isz * 4);
             tb_src_pass(nb, shots + s0, false);
             zero_images(nb, g.nExt);
             tb_adjx_pass(nb, shots + s0);

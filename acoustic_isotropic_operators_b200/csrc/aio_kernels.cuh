@@ -249,6 +249,42 @@ __global__ void k_img_time_adj(Acc* m, long long mSt, float* r, long long rSt, c
     }
 }
 
+// Time-lag imaging of a block of coarse receiver samples (imagingTimeAdjGpu,
+// F/src/kernelsGpu.cu:352-364, applied at every t of the block):
+//   img[e] += sum_{t = tlo..thi} R(t) * W[t - 2(e-h)]   over 0 <= t - 2(e-h) < nts,
+// the same (t, e) pairs as the reference's truncating-division lag bounds. R(t) lives in a
+// ring of LAG_K slices (slot t % LAG_K). Each thread owns one point: its R samples are held in
+// registers and the W slices t-2h .. t+2h of the block in shared memory (own column only,
+// no barrier), so W is read once per block instead of once per lag, and the image once per
+// block instead of once per sample.
+constexpr int LAG_K = 16;
+template <typename Acc>
+__global__ void k_img_lag_block(Acc* img, long long mSt, const float* R, long long rSt, const float* W, long long WSt,
+                                long long isz, int tlo, int thi, int nts, int hExt, int nExt) {
+    extern __shared__ float lag_smem[];
+    const int b = blockIdx.y, tid = threadIdx.x, nP = blockDim.x;
+    const long long p = (long long)blockIdx.x * nP + tid;
+    if (p >= isz) return;
+    R += b * rSt;
+    W += b * WSt;
+    img += b * mSt;
+    const int taulo = max(tlo - 2 * hExt, 0), tauhi = min(thi + 2 * hExt, nts - 1);
+    float* Ws = lag_smem;
+    for (int k = 0; k <= tauhi - taulo; k++) Ws[k * nP + tid] = W[(long long)(taulo + k) * isz + p];
+    float r[LAG_K];
+#pragma unroll
+    for (int k = 0; k < LAG_K; k++) r[k] = (tlo + k <= thi) ? R[(long long)((tlo + k) % LAG_K) * isz + p] : 0.f;
+    for (int e = 0; e < nExt; e++) {
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 0; k < LAG_K; k++) {
+            const int tau = tlo + k - 2 * (e - hExt);
+            if (tlo + k <= thi && tau >= 0 && tau < nts) acc += r[k] * Ws[(tau - taulo) * nP + tid];
+        }
+        img[(long long)e * isz + p] += (Acc)acc;
+    }
+}
+
 // Scalings (F/src/kernelsGpu.cu:246-252, 278-303). mode 0: m *= v2*rs;
 // mode 1: m *= rs*v2 (extended); mode 2: m = -(m*v2) (sloth); on images of v2-weighted
 // (adjoint U-form) wavefields: mode 3: m *= rs, mode 4: m = -m.

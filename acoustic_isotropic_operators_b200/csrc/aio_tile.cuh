@@ -63,6 +63,7 @@ struct KTArgs {
     int iters;             // iterations per CTA
     int maxEnt;            // shared entry capacity
     long long wStride;     // elements per stored coarse slice (= isz)
+    int rSlot, rSlot0;     // ADJR: ring slots of R(its+1) and (its == 0) R(0)
 };
 
 // Per-thread staging slots (16 bytes each) filled by asynchronous copies: level-1 operands
@@ -614,8 +615,8 @@ __global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
                         }
                     }
                     kt_st4(pPartOut + idx, ra);
-                    kt_st4(sh.rcoarse + idx, rb);                             // R(its+1)
-                    if (its == 0) kt_st4(sh.rcoarse + a.wStride + idx, ra);    // R(0)
+                    kt_st4(sh.rcoarse + (long long)a.rSlot * a.wStride + idx, rb);                  // R(its+1)
+                    if (its == 0) kt_st4(sh.rcoarse + (long long)a.rSlot0 * a.wStride + idx, ra);  // R(0)
                 } else if (qRec) {
                     for (int e = recFirst[c - xs + 32]; e >= 0 && e < nRec && sEnt[recOff + e].col == c; e++) {
                         const int rr = sEnt[recOff + e].row - zq;

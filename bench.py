@@ -255,7 +255,7 @@ def run_ext(args):
     n, steps, T = w.n_interior, w.fine_steps, w.nts - 1
     pts = n * steps * 2 * len(shots)
     algo = len(shots) * n * (2 * 16 * steps + 4 * w.nts + (4 + 4) * T + 8 * n_ext)
-    print(json.dumps({"impl": "this engine, extended Born adjoint (blocked stepper, per-sample lag imaging, FP32 W)",
+    print(json.dumps({"impl": "this engine, extended Born adjoint (blocked stepper, blocked lag imaging, FP32 W)",
                       "metric": "Gpts/s, extended (time-lag) Born adjoint", "value": pts / t / 1e9, "unit": UNIT,
                       "seconds": t, "shots": len(shots), "nExt": n_ext, "interior": [w.nz - 10, w.nx - 10],
                       "nts": w.nts, "algorithmic_GBps": algo / t / 1e9, "data": "synthetic (seeded)"}))
