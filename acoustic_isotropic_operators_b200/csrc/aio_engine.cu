@@ -831,7 +831,7 @@ struct Context {
     }
 
     // Measured autotuning of the blocked stepper's plan for waves of nb shots (chunkColumns
-    // == 0): strip heights {128, 112, 96} rows x chunk counts around the model's choice are
+    // == 0): strip heights {128, 112, 96, 64} rows x chunk counts around the model's choice are
     // each timed on the source-pass launch of interval 0 (idempotent: it reads one state set
     // and overwrites the other, the stored slice 0 and the partial sums), the fastest is
     // cached for the context. The state is zeroed again afterwards.
@@ -840,7 +840,7 @@ struct Context {
     void tb_autotune(int nb, const aio_shot* shots) {
         if (P.chunkColumns != 0 || tbTuned.count(nb)) return;
         std::vector<TBPlan> cand;
-        for (int maxHZ : {128, 112, 96}) {
+        for (int maxHZ : {128, 112, 96, 64}) {
             const TBPlan m = tb_model_plan(nb, maxHZ, 0);
             for (int d : {-2, -1, 0, 1, 2}) {
                 const int nc = m.nChunks + d;
@@ -1014,19 +1014,19 @@ struct Context {
         return a;
     }
 
-    template <int MODE, int WP>
-    void tb_launch_t(const TBPlan& pl, int nb, KTArgs& a, int v) {
-        const size_t smem = kt_smem_bytes(MODE, pl.threads, pl.iters, a.maxEnt);
+    template <int MODE, int WP, int MAXQ>
+    void tb_launch_q(const TBPlan& pl, int nb, KTArgs& a, int v) {
+        const size_t smem = kt_smem_bytes(MODE, pl.threads, pl.iters, a.maxEnt, kt_rs(MAXQ));
         static int attrDev = -1;
         static int smemMax = 0;
         if (attrDev != dev) {
             AIO_CK(cudaDeviceGetAttribute(&smemMax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-            AIO_CK(cudaFuncSetAttribute(k_tile<MODE, WP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smemMax));
+            AIO_CK(cudaFuncSetAttribute(k_tile<MODE, WP, MAXQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, smemMax));
             attrDev = dev;
         }
         require(smem <= (size_t)smemMax, "blocked stepper: shared memory plan of " + std::to_string(smem) +
                                              " bytes exceeds the device limit (too many devices per tile)");
-        require(pl.threads <= KT_MAXT && pl.NQ <= KT_MAXQ, "blocked stepper: strip taller than the ring");
+        require(pl.NQ <= MAXQ && pl.threads <= (8 * MAXQ + 31) / 32 * 32, "blocked stepper: strip taller than the ring");
         a.shots = tbDesc.as<TBShot>() + (size_t)v * nb;
         tbLast = pl;
         const bool timed = profEvery > 0 && (launches % profEvery) == 0;
@@ -1035,7 +1035,7 @@ struct Context {
             ev = take_events();
             AIO_CK(cudaEventRecord(ev.first, st));
         }
-        k_tile<MODE, WP><<<dim3(pl.nStrips, pl.nChunks, nb), pl.threads, smem, st>>>(a);
+        k_tile<MODE, WP, MAXQ><<<dim3(pl.nStrips, pl.nChunks, nb), pl.threads, smem, st>>>(a);
         AIO_CK(cudaGetLastError());
         if (timed) {
             AIO_CK(cudaEventRecord(ev.second, st));
@@ -1044,6 +1044,12 @@ struct Context {
         }
         launches++;
         kernels++;
+    }
+    // Short strips (<= 64 rows) use the variant with a narrower ring (two CTAs per SM).
+    template <int MODE, int WP>
+    void tb_launch_t(const TBPlan& pl, int nb, KTArgs& a, int v) {
+        if (pl.NQ <= KT_MAXQ_S) tb_launch_q<MODE, WP, KT_MAXQ_S>(pl, nb, a, v);
+        else tb_launch_q<MODE, WP, KT_MAXQ>(pl, nb, a, v);
     }
     template <int MODE>
     void tb_launch(const TBPlan& pl, int nb, KTArgs& a, int v) {

@@ -43,7 +43,10 @@ constexpr int KT_CB0 = 64;     // ring depth of level 0: the next input block la
 constexpr int KT_RINGCOLS = KT_CB0 + (KT_T - 1) * KT_CB;
 constexpr int KT_PADQ = 2;     // zero quads above and below every ring column
 constexpr int KT_MAXQ = 42;    // row quads per strip (R <= 168, HZ <= 128)
-constexpr int KT_RS = (KT_MAXQ + 2 * KT_PADQ) * 4;  // floats per ring column (compile-time offsets)
+constexpr int KT_MAXQ_S = 26;  // short-strip variant (R <= 104, HZ <= 64): two CTAs per SM fit
+// floats per ring column (compile-time offsets) of a variant holding up to maxq row quads
+__host__ __device__ constexpr int kt_rs(int maxq) { return (maxq + 2 * KT_PADQ) * 4; }
+constexpr int KT_RS = kt_rs(KT_MAXQ);
 constexpr int KT_MAXT = (8 * KT_MAXQ + 31) / 32 * 32;  // threads per CTA (8 column pairs per quad)
 static_assert(KT_CB >= KT_BX + 5 * KT_T - 5 + 1, "output stage reads level 1 5(T-1) columns behind its block");
 static_assert(KT_CB >= KT_BX + 10, "a level is read 10 columns behind its block");
@@ -76,8 +79,8 @@ __host__ __device__ constexpr int kt_slots(int mode) {
 // dm*W[its+1] of the last 32 level-1 columns, formed once at level 1 and read by levels 2..T.
 __host__ __device__ constexpr int kt_ringcols(int mode) { return KT_RINGCOLS + (mode == TB_SCAT ? 2 * KT_CB : 0); }
 // rings, staging, column damping table, per-launch injection values (T per entry), entries
-inline size_t kt_smem_bytes(int mode, int threads, int iters, int maxEnt) {
-    return (size_t)kt_ringcols(mode) * KT_RS * sizeof(float) + (size_t)kt_slots(mode) * threads * 16 +
+inline size_t kt_smem_bytes(int mode, int threads, int iters, int maxEnt, int rs = KT_RS) {
+    return (size_t)kt_ringcols(mode) * rs * sizeof(float) + (size_t)kt_slots(mode) * threads * 16 +
            (3 * ((size_t)iters * KT_BX + 64) + (size_t)maxEnt * KT_T) * sizeof(float) + (size_t)maxEnt * sizeof(TBEnt);
 }
 
@@ -197,12 +200,12 @@ __device__ __forceinline__ float2 kt_pair(const float4 (&Z)[5], int r) {
     return make_float2(kt_el(Z[i >> 2], i & 3), kt_el(Z[(i + 1) >> 2], (i + 1) & 3));
 }
 
-template <int MODE, int WPREC>
-__global__ void __launch_bounds__(KT_MAXT, 1) k_tile(const KTArgs a) {
+template <int MODE, int WPREC, int MAXQ = KT_MAXQ>
+__global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ? 2 : 1) k_tile(const KTArgs a) {
     constexpr int T = KT_T;
     extern __shared__ float4 kt_smem4[];
     const int NQ = a.NQ;
-    constexpr int RS = KT_RS;
+    constexpr int RS = kt_rs(MAXQ);
     constexpr int NS = kt_slots(MODE);
     float* ring = reinterpret_cast<float*>(kt_smem4);         // level 0: [KT_CB0][RS], levels 1..T-1: [KT_CB][RS]
     float4* stg = reinterpret_cast<float4*>(ring + kt_ringcols(MODE) * RS);  // [NS][blockDim.x]

@@ -173,3 +173,21 @@ def test_born_ext_adjoint_blocked(case, sloth):
     # forward on the per-fine-step stepper, adjoint on the blocked stepper: two FP32
     # implementations, each within 1e-5 of the oracle, hence the looser bound here
     assert abs(a - b) / abs(b) < 5e-5
+
+
+def test_short_strip_variant():
+    """Interiors of at most 64 rows run the short-strip kernel variant (narrower rings, two CTAs
+    per SM): nonlinear forward and Born forward / adjoint against the FP32 oracle."""
+    c = blocked_case(seed=12, nzi=56, nxi=150, nts=26, nshots=1)
+    c.src_pos[0] = np.array([(5 + 40) * c.nz + 5 + 20, (5 + 90) * c.nz + 5 + 50], np.int32)
+    c.sig[0] = (c.rng.standard_normal((2, c.scheme.ntw)) * 1e-2).astype(np.float32)
+    c.rec_pos[0] = np.array([ix * c.nz + 5 + 9 for ix in range(5, c.nx - 5)], np.int32)
+    got = ctx(c, stepper="blocked").nonlinear_forward(shots(c))[0]
+    r32 = orc.nl_fwd(c.scheme, c.vel, c.sig[0], c.src_pos[0], c.rec_pos[0], dtype=np.float32)
+    assert rel_l2(got, r32) < 1e-5
+    m = c.rng.standard_normal((c.nx, c.nz)).astype(np.float32) * interior_mask(c.nx, c.nz)
+    gf = ctx(c, stepper="blocked").born_forward(m, shots(c))[0]
+    assert rel_l2(gf, orc.born_fwd(c.scheme, c.vel, m, c.sig[0], c.src_pos[0], c.rec_pos[0], dtype=np.float32)) < 1e-5
+    d = [c.rng.standard_normal((len(c.rec_pos[0]), c.scheme.nts)).astype(np.float32)]
+    ga = ctx(c, stepper="blocked").born_adjoint(shots(c, d))
+    assert rel_l2(ga, orc.born_adj(c.scheme, c.vel, d[0], c.sig[0], c.src_pos[0], c.rec_pos[0], dtype=np.float32)) < 1e-5
