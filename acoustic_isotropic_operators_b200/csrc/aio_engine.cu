@@ -772,7 +772,8 @@ struct Context {
     // images use interior slices; the stored wavefield is FP32 or BF16.
     DevMem tbState, tbPart, tbImg, tbW, tbEnt, tbStart, tbDesc, shotImg;
     DevMem tbWscale, tbWmax, tbWstage;  // FP16 stored wavefield: per-slice scales, max |W|, FP32 staging
-    DevMem tbR;                         // extended adjoint: coarse receiver samples [shot][2][isz]
+    DevMem tbR;                         // extended adjoint: coarse receiver samples [shot][LAG_K][isz]
+    DevMem tbSS;                        // extended forward: secondary sources [shot][2 LAG_K][isz]
     // k_tile plan: strips of HZ (multiple of 4) output rows, NQ = HZ/4 + 10 row quads,
     // 8 column pairs per quad, x-chunks of LX columns marched in blocks of 16.
     struct TBPlan {
@@ -960,7 +961,10 @@ struct Context {
 
     // Descriptor pairs: version v reads state/part set v and writes set 1-v
     // (partSwap=true: the ADJ part ordering, see tb_adj_pass).
-    void tb_desc(const TBPlan& pl, int nb, bool injSources, bool injData, bool recData, void* W, bool partFlip) {
+    // wSlices: coarse slices per shot in W (the stored wavefield: nts; a secondary-source ring: its length)
+    void tb_desc(const TBPlan& pl, int nb, bool injSources, bool injData, bool recData, void* W, bool partFlip,
+                 int wSlices = 0) {
+        if (wSlices <= 0) wSlices = g.nts;
         std::vector<TBShot> d(2 * (size_t)nb);
         const int nCTA = pl.nStrips * pl.nChunks;
         for (int v = 0; v < 2; v++)
@@ -982,7 +986,7 @@ struct Context {
                 t.recLd = g.nts;
                 t.entStart = tbStart.as<int4>() + (size_t)s * nCTA;
                 t.ent = tbEnt.as<TBEnt>();
-                t.W = W ? (void*)((char*)W + (size_t)s * g.nts * g.isz * wbytes()) : nullptr;
+                t.W = W ? (void*)((char*)W + (size_t)s * wSlices * g.isz * wbytes()) : nullptr;
                 t.img = tbImg.p ? tbImg.as<double>() + (size_t)s * g.isz : nullptr;
                 t.rcoarse = tbR.p ? tbR.as<float>() + (size_t)s * LAG_K * g.isz : nullptr;
                 if (f16()) {
@@ -1155,6 +1159,60 @@ struct Context {
             tb_launch<TB_ADJR>(pl, nb, a, L & 1);
             if (a.its == 0) image(0, std::min(LAG_K - 1, g.nts - 1));
             else if (t % LAG_K == 0) image(t, std::min(t + LAG_K - 1, g.nts - 1));
+        }
+    }
+
+    // Scattered pass of the extended (time-lag) forward (F/src/BornExtShotsGpuFunctions.cu:269-419)
+    // on the blocked stepper: the secondary sources ss(t) = sum_e ext[e] W[t - 2(e-h)] are formed
+    // for blocks of LAG_K coarse steps ahead of use (k_ss_lag_block) into a ring of 2 LAG_K slices,
+    // read by TB_SCATX at slots its and its+1.
+    void tb_scatx_pass(int nb, const aio_shot* shots, const float* ext) {
+        const int ring = 2 * LAG_K;
+        const TBPlan pl = tb_plan(nb);
+        const int maxEnt = tb_lists(pl, nb, shots, 0, true);
+        tb_zero(nb, false);
+        tb_desc(pl, nb, false, false, true, tbSS.p, false, ring);
+        KTArgs a = tb_args(pl, maxEnt, nullptr);
+        const int nP = 128;
+        const size_t lagSmem = (size_t)(LAG_K + 4 * g.hExt) * nP * 4;
+        static int ssAttr = -1;
+        if (ssAttr != dev) {
+            AIO_CK(cudaFuncSetAttribute(k_ss_lag_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            ssAttr = dev;
+        }
+        require(lagSmem <= 200 * 1024, "extension too long for the blocked lag imaging");
+        auto sources = [&](int tlo) {
+            const int thi = std::min(tlo + LAG_K - 1, g.nts - 1);
+            const dim3 grid((unsigned)((g.isz + nP - 1) / nP), nb);
+            k_ss_lag_block<<<grid, nP, lagSmem, st>>>(tbSS.as<float>(), (long long)ring * g.isz, ring, ext,
+                                                      tbW.as<float>(), wfSt(), g.isz, tlo, thi, g.nts, g.hExt, g.nExt);
+            kcheck();
+        };
+        for (int its = 0; its < g.nts - 1; its++) {
+            if (its == 0) sources(0);
+            if ((its + 1) % LAG_K == 0) sources(its + 1);  // next block, before ss(its+1) is read
+            a.its = its;
+            a.rSlot = its % ring;
+            a.rSlot0 = (its + 1) % ring;
+            tb_launch<TB_SCATX>(pl, nb, a, its & 1);
+        }
+    }
+
+    void born_ext_forward_tb(const float* model, int nShots, const aio_shot* shots, int mem) {
+        float* ext = stage_model(model, g.nExt, mem, this->model);
+        scale_shared(ext, g.nExt, P.sloth ? 2 : 1);
+        Needs n;
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = tb_wave_size(nShots - s0, shots + s0, true, false);
+            setup_wave(n, nb, shots + s0, mem, false, false);
+            tb_alloc(nb, false);
+            tbW.ensure((size_t)nb * g.nts * g.isz * 4);
+            tbSS.ensure((size_t)nb * 2 * LAG_K * g.isz * 4);
+            tb_src_pass(nb, shots + s0, false);
+            tb_scatx_pass(nb, shots + s0, ext);
+            download_data(nb, shots + s0, mem);
+            sync();
+            s0 += nb;
         }
     }
 
@@ -1407,6 +1465,7 @@ struct Context {
     // Extended (time-lag) Born forward (F/src/BornExtShotsGpuFunctions.cu:269-419).
     void born_ext_forward(const float* model, int nShots, const aio_shot* shots, int mem) {
         begin_call();
+        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32) return born_ext_forward_tb(model, nShots, shots, mem);
         Needs n;
         n.nWavefields = 1;
         n.ss = true;

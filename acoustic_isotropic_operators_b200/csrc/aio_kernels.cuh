@@ -285,6 +285,32 @@ __global__ void k_img_lag_block(Acc* img, long long mSt, const float* R, long lo
     }
 }
 
+// Secondary sources of a block of coarse steps of the time-lag extended forward
+// (imagingTimeFwdGpu, F/src/kernelsGpu.cu:337-350, at every t of the block):
+//   ss(t) = sum_e ext[e] * W[t - 2(e-h)]   over 0 <= t - 2(e-h) < nts,
+// written to a ring of ring slices (slot t % ring). One thread per point; the W slices of
+// the block live in shared memory (own column only), so W is read once per block.
+__global__ void k_ss_lag_block(float* ss, long long ssSt, int ring, const float* ext, const float* W, long long WSt,
+                               long long isz, int tlo, int thi, int nts, int hExt, int nExt) {
+    extern __shared__ float lag_smem[];
+    const int b = blockIdx.y, tid = threadIdx.x, nP = blockDim.x;
+    const long long p = (long long)blockIdx.x * nP + tid;
+    if (p >= isz) return;
+    ss += b * ssSt;
+    W += b * WSt;
+    const int taulo = max(tlo - 2 * hExt, 0), tauhi = min(thi + 2 * hExt, nts - 1);
+    float* Ws = lag_smem;
+    for (int k = 0; k <= tauhi - taulo; k++) Ws[k * nP + tid] = W[(long long)(taulo + k) * isz + p];
+    for (int t = tlo; t <= thi; t++) {
+        float acc = 0.f;
+        for (int e = 0; e < nExt; e++) {
+            const int tau = t - 2 * (e - hExt);
+            if (tau >= 0 && tau < nts) acc += ext[(long long)e * isz + p] * Ws[(tau - taulo) * nP + tid];
+        }
+        ss[(long long)(t % ring) * isz + p] = acc;
+    }
+}
+
 // Scalings (F/src/kernelsGpu.cu:246-252, 278-303). mode 0: m *= v2*rs;
 // mode 1: m *= rs*v2 (extended); mode 2: m = -(m*v2) (sloth); on images of v2-weighted
 // (adjoint U-form) wavefields: mode 3: m *= rs, mode 4: m = -m.

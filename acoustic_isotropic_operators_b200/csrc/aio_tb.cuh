@@ -10,7 +10,10 @@ namespace aio {
 // TB_ADJR: the adjoint recursion of TB_ADJ writing the finished coarse receiver sample
 // R(its+1) (and R(0) at its == 0) instead of forming the Born image (extended imaging
 // is done on those samples by the coarse kernels).
-enum TBMode { TB_SRC = 0, TB_NL = 1, TB_SCAT = 2, TB_ADJ = 3, TB_ADJR = 4 };
+// TB_SCATX: the scattered pass of TB_SCAT with precomputed secondary-source slices (time-lag
+// extended forward: ss(t) = sum_e ext[e] W[t - 2(e-h)]) in ring slots rSlot / rSlot0 of W.
+enum TBMode { TB_SRC = 0, TB_NL = 1, TB_SCAT = 2, TB_ADJ = 3, TB_ADJR = 4, TB_SCATX = 5 };
+__host__ __device__ constexpr bool tb_scatlike(int mode) { return mode == TB_SCAT || mode == TB_SCATX; }
 // Stored source wavefield: FP32, BF16, or FP16 scaled per coarse slice and shot (the scale
 // maps the slice's max |W| to 2^15, computed exactly from the finished FP32 slice).
 enum TBWfld { TBW_F32 = 0, TBW_BF16 = 1, TBW_F16 = 2 };

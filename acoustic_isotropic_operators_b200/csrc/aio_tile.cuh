@@ -73,11 +73,11 @@ struct KTArgs {
 // of the next iteration (old level, v^2: slots 0-3) and the output operands of the current
 // iteration (partial sum: 4-5, stored wavefield: 6-7, FP64 image: 8-11).
 __host__ __device__ constexpr int kt_slots(int mode) {
-    return mode == TB_ADJ ? 12 : ((mode == TB_SRC || mode == TB_ADJR) ? 6 : (mode == TB_SCAT ? 8 : 4));
+    return mode == TB_ADJ ? 12 : ((mode == TB_SRC || mode == TB_ADJR) ? 6 : (tb_scatlike(mode) ? 8 : 4));
 }
 // Ring columns: levels 0..T-1, plus (scattered pass) the secondary sources dm*W[its] and
 // dm*W[its+1] of the last 32 level-1 columns, formed once at level 1 and read by levels 2..T.
-__host__ __device__ constexpr int kt_ringcols(int mode) { return KT_RINGCOLS + (mode == TB_SCAT ? 2 * KT_CB : 0); }
+__host__ __device__ constexpr int kt_ringcols(int mode) { return KT_RINGCOLS + (tb_scatlike(mode) ? 2 * KT_CB : 0); }
 // rings, staging, column damping table, per-launch injection values (T per entry), entries
 inline size_t kt_smem_bytes(int mode, int threads, int iters, int maxEnt, int rs = KT_RS) {
     return (size_t)kt_ringcols(mode) * rs * sizeof(float) + (size_t)kt_slots(mode) * threads * 16 +
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
     __syncthreads();
     // Injected values of this interval, one per entry and fine step, read once here
     // instead of inside the level loop (adjoint: the v2 factor is applied at use).
-    if (MODE != TB_SCAT) {
+    if (!tb_scatlike(MODE)) {
         for (int i = tid; i < nInj * T; i += blockDim.x) {
             const int e = i / T, t = i - e * T + 1;
             const float* tr = pInj + (long long)sEnt[e].dev * injLd;
@@ -345,9 +345,9 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
             kt_cp16(mySlot + j * bd, oko ? old + (long long)co * ip + zq : old, oko);
             const long long ic = (long long)min(max(co, 0), nxi - 1) * ip + zv;
             kt_cp16_l1(mySlot + (2 + j) * bd, v2p + ic, true);
-            if (MODE == TB_SCAT) {  // stored wavefield at its and its+1 (slots 4-7)
-                const void* wa = tb_wslice<WPREC>(sh.W, a.wStride, its);
-                const void* wb = tb_wslice<WPREC>(sh.W, a.wStride, its + 1);
+            if (tb_scatlike(MODE)) {  // stored wavefield (SCATX: secondary sources) at its, its+1 (slots 4-7)
+                const void* wa = tb_wslice<WPREC>(sh.W, a.wStride, MODE == TB_SCATX ? a.rSlot : its);
+                const void* wb = tb_wslice<WPREC>(sh.W, a.wStride, MODE == TB_SCATX ? a.rSlot0 : its + 1);
                 if (WPREC == TBW_F32) {
                     kt_cp16(mySlot + (4 + j) * bd, (const float*)wa + ic, true);
                     kt_cp16(mySlot + (6 + j) * bd, (const float*)wb + ic, true);
@@ -435,17 +435,23 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
 #pragma unroll
                     for (int i = 0; i < 4; i++) Dm[j][i] = fminf(Dz[i], Dx[j]);
                 float4 sa[2], sb[2];
-                if (MODE == TB_SCAT) {
+                if (tb_scatlike(MODE)) {
 #pragma unroll
                     for (int j = 0; j < 2; j++) {
                         if (t == 1) {
                             // imagingFwdGpu (F/src/kernelsGpu.cu:309-316): dm * W, kept for levels 2..T
-                            const long long idx = (long long)min(max(c0 + j, 0), nxi - 1) * ip + zv;
-                            const float4 dmv = __ldg(reinterpret_cast<const float4*>(dmp + idx));
+                            // (SCATX: the secondary sources are staged as they are)
                             const float4 wa = kt_wfrom<WPREC>(mySlot[(4 + j) * bd], scA);
                             const float4 wb = kt_wfrom<WPREC>(mySlot[(6 + j) * bd], scB);
-                            sa[j] = make_float4(dmv.x * wa.x, dmv.y * wa.y, dmv.z * wa.z, dmv.w * wa.w);
-                            sb[j] = make_float4(dmv.x * wb.x, dmv.y * wb.y, dmv.z * wb.z, dmv.w * wb.w);
+                            if (MODE == TB_SCATX) {
+                                sa[j] = wa;
+                                sb[j] = wb;
+                            } else {
+                                const long long idx = (long long)min(max(c0 + j, 0), nxi - 1) * ip + zv;
+                                const float4 dmv = __ldg(reinterpret_cast<const float4*>(dmp + idx));
+                                sa[j] = make_float4(dmv.x * wa.x, dmv.y * wa.y, dmv.z * wa.z, dmv.w * wa.w);
+                                sb[j] = make_float4(dmv.x * wb.x, dmv.y * wb.y, dmv.z * wb.z, dmv.w * wb.w);
+                            }
                             const float va[4] = {sa[j].x, sa[j].y, sa[j].z, sa[j].w};
                             const float vb[4] = {sb[j].x, sb[j].y, sb[j].z, sb[j].w};
                             kt_st4(ssCol(0, c0 + j), va);
@@ -483,7 +489,7 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
                         float2 n = __ffma2_rn(kt_half(vq[j], P), __fadd2_rn(lz, lx), ctr);
                         n = __fadd2_rn(n, ctr);
                         n = __ffma2_rn(make_float2(-Dm[j][a0], -Dm[j][a0 + 1]), kt_half(ol[j], P), n);
-                        if (MODE == TB_SCAT)
+                        if (tb_scatlike(MODE))
                             n = __fadd2_rn(n, __ffma2_rn(kt_half(sb[j], P), make_float2(a.h[H + t - 1], a.h[H + t - 1]),
                                                          __fmul2_rn(kt_half(sa[j], P), make_float2(a.h[t - 1], a.h[t - 1]))));
                         S[j][a0] = n.x;  // damped below, after injection
@@ -491,7 +497,7 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
                     }
                 }
                 // sparse injection into this micro-tile (entries sorted by column)
-                if (MODE != TB_SCAT && qInj) {
+                if (!tb_scatlike(MODE) && qInj) {
 #pragma unroll
                     for (int j = 0; j < 2; j++) {
                         for (int e = injFirst[c0 + j - xs + 32]; e >= 0 && e < nInj && sEnt[e].col == c0 + j; e++) {
