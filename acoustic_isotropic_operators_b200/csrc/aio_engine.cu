@@ -774,6 +774,7 @@ struct Context {
     DevMem tbWscale, tbWmax, tbWstage;  // FP16 stored wavefield: per-slice scales, max |W|, FP32 staging
     DevMem tbR;                         // extended adjoint: coarse receiver samples [shot][LAG_K][isz]
     DevMem tbSS;                        // extended forward: secondary sources [shot][2 LAG_K][isz]
+    DevMem tbF2;                        // tomo / WEMVA: second full coarse field [shot][nts][isz]
     // k_tile plan: strips of HZ (multiple of 4) output rows, NQ = HZ/4 + 10 row quads,
     // 8 column pairs per quad, x-chunks of LX columns marched in blocks of 16.
     struct TBPlan {
@@ -962,9 +963,15 @@ struct Context {
     // Descriptor pairs: version v reads state/part set v and writes set 1-v
     // (partSwap=true: the ADJ part ordering, see tb_adj_pass).
     // wSlices: coarse slices per shot in W (the stored wavefield: nts; a secondary-source ring: its length)
+    // out / outSlices: per-shot slices written by ADJR / SCATW / ADJX (default: the LAG_K ring tbR)
+    // dataIn: traces injected when injData (default: the wave's data)
     void tb_desc(const TBPlan& pl, int nb, bool injSources, bool injData, bool recData, void* W, bool partFlip,
-                 int wSlices = 0) {
+                 int wSlices = 0, float* out = nullptr, int outSlices = 0, const float* const* dataIn = nullptr) {
         if (wSlices <= 0) wSlices = g.nts;
+        if (!out && tbR.p) {
+            out = tbR.as<float>();
+            outSlices = LAG_K;
+        }
         std::vector<TBShot> d(2 * (size_t)nb);
         const int nCTA = pl.nStrips * pl.nChunks;
         for (int v = 0; v < 2; v++)
@@ -980,7 +987,7 @@ struct Context {
                 const int vin = partFlip ? (v ^ 1) : v;
                 t.part = pb + (size_t)vin * g.isz;
                 t.partOut = pb + (size_t)(1 - vin) * g.isz;
-                t.injSig = injSources ? srcSig[s] : (injData ? dataPtr[s] : nullptr);
+                t.injSig = injSources ? srcSig[s] : (injData ? (dataIn ? dataIn[s] : dataPtr[s]) : nullptr);
                 t.injLd = injSources ? g.ntw : g.nts;
                 t.recSig = recData ? dataPtr[s] : nullptr;
                 t.recLd = g.nts;
@@ -988,7 +995,7 @@ struct Context {
                 t.ent = tbEnt.as<TBEnt>();
                 t.W = W ? (void*)((char*)W + (size_t)s * wSlices * g.isz * wbytes()) : nullptr;
                 t.img = tbImg.p ? tbImg.as<double>() + (size_t)s * g.isz : nullptr;
-                t.rcoarse = tbR.p ? tbR.as<float>() + (size_t)s * LAG_K * g.isz : nullptr;
+                t.rcoarse = out ? out + (size_t)s * outSlices * g.isz : nullptr;
                 if (f16()) {
                     t.wscale = tbWscale.as<float>() + (size_t)s * g.nts;
                     t.wmax = tbWmax.as<unsigned>() + (size_t)s * g.nts;
@@ -1090,12 +1097,13 @@ struct Context {
         }
     }
 
-    // Scattered pass with data recording (F/src/BornShotsGpuFunctions.cu:323-376).
-    void tb_scat_pass(int nb, const aio_shot* shots, const float* dm) {
+    // Scattered pass with data recording (F/src/BornShotsGpuFunctions.cu:323-376); W: the stored
+    // field the secondary sources dm * W come from (default: the source wavefield tbW).
+    void tb_scat_pass(int nb, const aio_shot* shots, const float* dm, const float* W = nullptr) {
         const TBPlan pl = tb_plan(nb);
         const int maxEnt = tb_lists(pl, nb, shots, 0, true);
         tb_zero(nb, false);
-        tb_desc(pl, nb, false, false, true, tbW.p, false);
+        tb_desc(pl, nb, false, false, true, W ? (void*)W : tbW.p, false);
         KTArgs a = tb_args(pl, maxEnt, dm);
         for (int its = 0; its < g.nts - 1; its++) {
             a.its = its;
@@ -1143,12 +1151,12 @@ struct Context {
             const dim3 grid((unsigned)((g.isz + nP - 1) / nP), nb);
             if (P.imageFp64)
                 k_img_lag_block<double><<<grid, nP, lagSmem, st>>>(img.as<double>(), mSt, tbR.as<float>(),
-                                                                    (long long)LAG_K * g.isz, tbW.as<float>(), wfSt(),
-                                                                    g.isz, tlo, thi, g.nts, g.hExt, g.nExt);
+                                                                    (long long)LAG_K * g.isz, LAG_K, tbW.as<float>(),
+                                                                    wfSt(), g.isz, tlo, thi, g.nts, g.hExt, g.nExt, 1);
             else
                 k_img_lag_block<float><<<grid, nP, lagSmem, st>>>(img.as<float>(), mSt, tbR.as<float>(),
-                                                                   (long long)LAG_K * g.isz, tbW.as<float>(), wfSt(),
-                                                                   g.isz, tlo, thi, g.nts, g.hExt, g.nExt);
+                                                                   (long long)LAG_K * g.isz, LAG_K, tbW.as<float>(),
+                                                                   wfSt(), g.isz, tlo, thi, g.nts, g.hExt, g.nExt, 1);
             kcheck();
         };
         for (int L = 0; L < g.nts - 1; L++) {
@@ -1166,7 +1174,7 @@ struct Context {
     // on the blocked stepper: the secondary sources ss(t) = sum_e ext[e] W[t - 2(e-h)] are formed
     // for blocks of LAG_K coarse steps ahead of use (k_ss_lag_block) into a ring of 2 LAG_K slices,
     // read by TB_SCATX at slots its and its+1.
-    void tb_scatx_pass(int nb, const aio_shot* shots, const float* ext) {
+    void tb_scatx_pass(int nb, const aio_shot* shots, const float* ext, const float* F = nullptr) {
         const int ring = 2 * LAG_K;
         const TBPlan pl = tb_plan(nb);
         const int maxEnt = tb_lists(pl, nb, shots, 0, true);
@@ -1185,7 +1193,8 @@ struct Context {
             const int thi = std::min(tlo + LAG_K - 1, g.nts - 1);
             const dim3 grid((unsigned)((g.isz + nP - 1) / nP), nb);
             k_ss_lag_block<<<grid, nP, lagSmem, st>>>(tbSS.as<float>(), (long long)ring * g.isz, ring, ext,
-                                                      tbW.as<float>(), wfSt(), g.isz, tlo, thi, g.nts, g.hExt, g.nExt);
+                                                      F ? F : tbW.as<float>(), wfSt(), g.isz, tlo, thi, g.nts, g.hExt,
+                                                      g.nExt, 1);
             kcheck();
         };
         for (int its = 0; its < g.nts - 1; its++) {
@@ -1242,6 +1251,277 @@ struct Context {
         }
         write_model(modelOut, g.nExt, add, mem, out);
         sync();
+    }
+
+    // ------------------------------------------- tomo / WEMVA on the blocked stepper
+    // Every leg is one blocked pass. Receiver-side fields are kept in U-form (U = v2 * S, the
+    // adjoint recursion of TB_ADJR / TB_ADJX), so secondary sources built from them already
+    // carry the v2 of U-form injection and every image term (one source-side factor, one
+    // receiver-side factor) carries v2 once: reduce_images divides it out (scaling mode 5).
+    static constexpr int TB_RING = 2 * LAG_K;  // source and sample rings: two blocks of LAG_K
+
+    struct TBSrc {                // dense secondary sources of a pass
+        const float* F = nullptr;   // full coarse field [shot][nts][isz]
+        const float* ext = nullptr; // lag sources ss(t) = sum_e ext[e] F[t - sign 2(e-h)]; null: F (times dm)
+        const float* dm = nullptr;  // zero-lag sources: dm * F(t) (null: F(t))
+        int sign = 1;
+    };
+    struct TBOut {                // what a pass does with its coarse samples
+        float* full = nullptr;      // store all of them [shot][nts][isz]
+        const float* imgF = nullptr;// else image them against this full field (ring of TB_RING samples)
+        bool lag = false;           // time-lag image (nExt slices) or zero-lag (one slice)
+        int sign = 1;
+    };
+
+    void tb_lag_attr() {
+        static int lagDev = -1;
+        if (lagDev == dev) return;
+        AIO_CK(cudaFuncSetAttribute(k_img_lag_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        AIO_CK(cudaFuncSetAttribute(k_img_lag_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        AIO_CK(cudaFuncSetAttribute(k_ss_lag_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        lagDev = dev;
+    }
+    size_t tb_lag_smem(int hExt) const {
+        const size_t b = (size_t)(LAG_K + 4 * hExt) * 128 * 4;
+        require(b <= 200 * 1024, "extension too long for the blocked lag imaging");
+        return b;
+    }
+    // secondary sources of the coarse steps [tlo, thi] into the ring tbSS
+    void tb_ss_block(int nb, const TBSrc& src, int tlo, int thi) {
+        tb_lag_attr();
+        const int nP = 128;
+        const dim3 grid((unsigned)((g.isz + nP - 1) / nP), nb);
+        k_ss_lag_block<<<grid, nP, tb_lag_smem(g.hExt), st>>>(tbSS.as<float>(), (long long)TB_RING * g.isz, TB_RING,
+                                                                src.ext, src.F, wfSt(), g.isz, tlo, thi, g.nts, g.hExt,
+                                                                g.nExt, src.sign);
+        kcheck();
+    }
+    // image the samples [tlo, thi] of the ring tbR against out.imgF
+    void tb_img_block(int nb, const TBOut& out, int tlo, int thi) {
+        tb_lag_attr();
+        const int nP = 128, nE = out.lag ? g.nExt : 1, hE = out.lag ? g.hExt : 0;
+        const dim3 grid((unsigned)((g.isz + nP - 1) / nP), nb);
+        const long long mSt = (long long)nE * g.isz, rSt = (long long)TB_RING * g.isz;
+        const size_t sm = tb_lag_smem(hE);
+        if (P.imageFp64)
+            k_img_lag_block<double><<<grid, nP, sm, st>>>(img.as<double>(), mSt, tbR.as<float>(), rSt, TB_RING,
+                                                          out.imgF, wfSt(), g.isz, tlo, thi, g.nts, hE, nE, out.sign);
+        else
+            k_img_lag_block<float><<<grid, nP, sm, st>>>(img.as<float>(), mSt, tbR.as<float>(), rSt, TB_RING,
+                                                         out.imgF, wfSt(), g.isz, tlo, thi, g.nts, hE, nE, out.sign);
+        kcheck();
+    }
+
+    // Forward-time dense pass (fwd_dense_pass on the blocked stepper, TB_SCATW):
+    // F/src/tomoExtShotsGpuFunctions.cu:1554-1656,2442-2527, F/src/wemvaExtShotsGpuFunctions.cu:961-1037.
+    // Lag sources are formed a block of LAG_K steps ahead; sample rings are imaged per block.
+    void tb_dense_fwd(int nb, const aio_shot* shots, const TBSrc& src, const TBOut& out) {
+        const TBPlan pl = tb_plan(nb);
+        const int maxEnt = tb_lists(pl, nb, shots, 0, false);
+        tb_zero(nb, false);
+        const bool lagSrc = src.ext != nullptr;
+        tb_desc(pl, nb, false, false, false, lagSrc ? tbSS.p : (void*)src.F, false, lagSrc ? TB_RING : g.nts,
+                out.full ? out.full : tbR.as<float>(), out.full ? g.nts : TB_RING);
+        KTArgs a = tb_args(pl, maxEnt, lagSrc ? nullptr : src.dm);
+        int lo = 0;  // lowest sample not yet imaged
+        for (int its = 0; its < g.nts - 1; its++) {
+            if (lagSrc) {
+                if (its == 0) tb_ss_block(nb, src, 0, std::min(LAG_K - 1, g.nts - 1));
+                if ((its + 1) % LAG_K == 0) tb_ss_block(nb, src, its + 1, std::min(its + LAG_K, g.nts - 1));
+                a.rSlot = its % TB_RING;
+                a.rSlot0 = (its + 1) % TB_RING;
+            } else {
+                a.rSlot = its;
+                a.rSlot0 = its + 1;
+            }
+            a.oA = out.full ? its : its % TB_RING;
+            a.oB = out.full ? its + 1 : (its + 1) % TB_RING;
+            a.its = its;
+            tb_launch_t<TB_SCATW, TBW_F32>(pl, nb, a, its & 1);
+            if (!out.full) {
+                if ((its + 1) % LAG_K == 0) {
+                    tb_img_block(nb, out, lo, its);
+                    lo = its + 1;
+                }
+                if (its == g.nts - 2) tb_img_block(nb, out, lo, g.nts - 1);
+            }
+        }
+    }
+
+    // Adjoint-time dense pass (adj_dense_pass on the blocked stepper, TB_ADJX) on U-form sources:
+    // F/src/tomoExtShotsGpuFunctions.cu:2619-2700, F/src/wemvaExtShotsGpuFunctions.cu:1038-1121.
+    void tb_dense_adj(int nb, const aio_shot* shots, const TBSrc& src, const TBOut& out) {
+        const TBPlan pl = tb_plan(nb);
+        const int maxEnt = tb_lists(pl, nb, shots, 0, false);
+        tb_zero(nb, false);
+        const bool lagSrc = src.ext != nullptr;
+        tb_desc(pl, nb, false, false, false, lagSrc ? tbSS.p : (void*)src.F, false, lagSrc ? TB_RING : g.nts,
+                out.full ? out.full : tbR.as<float>(), out.full ? g.nts : TB_RING);
+        KTArgs a = tb_args(pl, maxEnt, lagSrc ? nullptr : src.dm);
+        int srcLo = g.nts;   // lowest source sample in the ring
+        int hi = g.nts - 1;  // highest sample not yet imaged
+        for (int L = 0; L < g.nts - 1; L++) {
+            const int its = g.nts - 2 - L;
+            if (lagSrc) {
+                while (srcLo > its) {  // the blocks holding ss(its) and ss(its+1)
+                    const int b = (srcLo - 1) / LAG_K * LAG_K;
+                    tb_ss_block(nb, src, b, srcLo - 1);
+                    srcLo = b;
+                }
+                a.rSlot = its % TB_RING;
+                a.rSlot0 = (its + 1) % TB_RING;
+            } else {
+                a.rSlot = its;
+                a.rSlot0 = its + 1;
+            }
+            a.oA = 0;
+            a.oB = out.full ? its + 1 : (its + 1) % TB_RING;
+            a.its = its;
+            tb_launch_t<TB_ADJX, TBW_F32>(pl, nb, a, L & 1);
+            if (!out.full) {
+                const int t = its + 1;
+                if (t % LAG_K == 0) {
+                    tb_img_block(nb, out, t, hi);
+                    hi = t - 1;
+                }
+                if (its == 0) tb_img_block(nb, out, 0, hi);
+            }
+        }
+    }
+
+    // Receiver wavefield in U-form, every coarse sample stored (computeTomoRecWfld,
+    // F/src/tomoExtShotsGpuFunctions.cu:1481-1515, on TB_ADJR).
+    void tb_rec_full(int nb, const aio_shot* shots, const float* const* data, float* R) {
+        const TBPlan pl = tb_plan(nb);
+        const int maxEnt = tb_lists(pl, nb, shots, 2, false);
+        tb_zero(nb, false);
+        tb_desc(pl, nb, false, true, false, nullptr, false, 0, R, g.nts, data);
+        KTArgs a = tb_args(pl, maxEnt, nullptr);
+        for (int L = 0; L < g.nts - 1; L++) {
+            a.its = g.nts - 2 - L;
+            a.rSlot = a.its + 1;
+            a.rSlot0 = 0;
+            tb_launch_t<TB_ADJR, TBW_F32>(pl, nb, a, L & 1);
+        }
+    }
+
+    // Source wavefield and its second time derivative (computeTomoSrcWfldDt2,
+    // F/src/tomoExtShotsGpuFunctions.cu:1251-1361) into tbW.
+    void tb_src_dt2(int nb, const aio_shot* shots) {
+        tb_src_pass(nb, shots, false);
+        k_dt2<<<ew_grid(nb, g.isz), 256, 0, st>>>(tbW.as<float>(), wfSt(), g.isz, g.nts, k.cSide, k.cCenter);
+        kcheck();
+    }
+
+    // Shots per wave with two full coarse fields, the rings and imgSlices image slices per shot.
+    int tb_fields_wave(int nShots, const aio_shot* shots, int imgSlices) {
+        int maxSrc = 1, maxRec = 1;
+        for (int s = 0; s < nShots; s++) {
+            maxSrc = std::max(maxSrc, shots[s].nSourcesReg);
+            maxRec = std::max(maxRec, shots[s].nReceiversReg);
+        }
+        const long long per = 6LL * g.isz * 4 + 2LL * g.nts * g.isz * 4 + 2LL * TB_RING * g.isz * 4 +
+                              (long long)imgSlices * g.isz * (P.imageFp64 ? 8 : 4) + (long long)maxSrc * g.ntw * 4 +
+                              2LL * maxRec * g.nts * 4 + 2 * g.hsz * 4 + 2 * g.isz * 4 + (1 << 16);
+        const long long shared = (4LL + 2 * g.nExt) * g.isz * 4 + (64LL << 20);
+        const long long cap = (budget - shared) / per;
+        require(cap >= 1, "device memory budget cannot hold one shot for this operator");
+        return (int)std::min<long long>(cap, nShots);
+    }
+    void tb_fields_alloc(int nb) {
+        tb_alloc(nb, false);
+        tbW.ensure((size_t)nb * g.nts * g.isz * 4);
+        tbF2.ensure((size_t)nb * g.nts * g.isz * 4);
+        tbSS.ensure((size_t)nb * TB_RING * g.isz * 4);
+        tbR.ensure((size_t)nb * TB_RING * g.isz * 4);
+    }
+
+    // Extended tomo forward (F/src/tomoExtShotsGpuFunctions.cu:355-465, legs :1554-1881).
+    void tomo_forward_tb(const float* dm, const float* ex, int nShots, const aio_shot* shots, int mem) {
+        Needs n;
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = tb_fields_wave(nShots - s0, shots + s0, 0);
+            setup_wave(n, nb, shots + s0, mem, false, false);
+            tb_fields_alloc(nb);
+            tb_src_dt2(nb, shots + s0);
+            const float* W2 = tbW.as<float>();
+            float* W1 = tbF2.as<float>();
+            if (P.leg1) {
+                tb_dense_fwd(nb, shots + s0, TBSrc{W2, ex, nullptr, 1}, TBOut{W1});
+                tb_scat_pass(nb, shots + s0, dm, W1);
+            }
+            if (P.leg2) {
+                tb_dense_fwd(nb, shots + s0, TBSrc{W2, nullptr, dm, 1}, TBOut{W1});
+                tb_scatx_pass(nb, shots + s0, ex, W1);
+            }
+            download_data(nb, shots + s0, mem);
+            sync();
+            s0 += nb;
+        }
+    }
+
+    // Extended tomo adjoint (F/src/tomoExtShotsGpuFunctions.cu:797-910, legs :2442-2701).
+    void tomo_adjoint_tb(float* out, const float* ex, int nShots, const aio_shot* shots, int mem) {
+        Needs n;
+        n.nImg = 1;
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = tb_fields_wave(nShots - s0, shots + s0, 1);
+            setup_wave(n, nb, shots + s0, mem, true, false);
+            tb_fields_alloc(nb);
+            tb_src_dt2(nb, shots + s0);
+            const float* W2 = tbW.as<float>();
+            float* R = tbF2.as<float>();
+            std::vector<const float*> din(dataPtr.begin(), dataPtr.end());
+            tb_rec_full(nb, shots + s0, din.data(), R);
+            zero_images(nb, 1);
+            if (P.leg1) tb_dense_fwd(nb, shots + s0, TBSrc{W2, ex, nullptr, 1}, TBOut{nullptr, R, false, 1});
+            if (P.leg2) tb_dense_adj(nb, shots + s0, TBSrc{R, ex, nullptr, -1}, TBOut{nullptr, W2, false, 1});
+            reduce_images(nb, 1, 5, out, true);
+            sync();
+            s0 += nb;
+        }
+    }
+
+    // Extended WEMVA forward (F/src/wemvaExtShotsGpuFunctions.cu:344-456, legs :961-1122).
+    void wemva_forward_tb(const float* dm, float* out, int nShots, const aio_shot* shots, int mem) {
+        Needs n;
+        n.nImg = g.nExt;
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = tb_fields_wave(nShots - s0, shots + s0, g.nExt);
+            setup_wave(n, nb, shots + s0, mem, false, true);
+            tb_fields_alloc(nb);
+            tb_src_dt2(nb, shots + s0);
+            const float* W2 = tbW.as<float>();
+            float* R = tbF2.as<float>();
+            tb_rec_full(nb, shots + s0, wdataPtr.data(), R);
+            zero_images(nb, g.nExt);
+            if (P.leg1) tb_dense_fwd(nb, shots + s0, TBSrc{W2, nullptr, dm, 1}, TBOut{nullptr, R, true, -1});
+            if (P.leg2) tb_dense_adj(nb, shots + s0, TBSrc{R, nullptr, dm, 1}, TBOut{nullptr, W2, true, 1});
+            reduce_images(nb, g.nExt, 5, out, true);
+            sync();
+            s0 += nb;
+        }
+    }
+
+    // Extended WEMVA adjoint (F/src/wemvaExtShotsGpuFunctions.cu:575-688, legs :1270-1426).
+    void wemva_adjoint_tb(float* out, const float* im, int nShots, const aio_shot* shots, int mem) {
+        Needs n;
+        n.nImg = 1;
+        for (int s0 = 0; s0 < nShots;) {
+            const int nb = tb_fields_wave(nShots - s0, shots + s0, 1);
+            setup_wave(n, nb, shots + s0, mem, false, true);
+            tb_fields_alloc(nb);
+            tb_src_dt2(nb, shots + s0);
+            const float* W2 = tbW.as<float>();
+            float* R = tbF2.as<float>();
+            tb_rec_full(nb, shots + s0, wdataPtr.data(), R);
+            zero_images(nb, 1);
+            if (P.leg1) tb_dense_adj(nb, shots + s0, TBSrc{R, im, nullptr, -1}, TBOut{nullptr, W2, false, 1});
+            if (P.leg2) tb_dense_fwd(nb, shots + s0, TBSrc{W2, im, nullptr, 1}, TBOut{nullptr, R, false, 1});
+            reduce_images(nb, 1, 5, out, true);
+            sync();
+            s0 += nb;
+        }
     }
 
     // ============================================================ operators
@@ -1533,6 +1813,7 @@ struct Context {
         scale_shared(dm, 1, 0);
         float* ex = stage_model(extRefl, g.nExt, mem, this->ext);
         scale_shared(ex, g.nExt, P.sloth ? 2 : 1);
+        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32) return tomo_forward_tb(dm, ex, nShots, shots, mem);
         for (int s0 = 0; s0 < nShots;) {
             const int nb = wave_size(n, nShots - s0, shots + s0);
             setup_wave(n, nb, shots + s0, mem, false, false);
@@ -1572,6 +1853,12 @@ struct Context {
         float* ex = stage_model(extRefl, g.nExt, mem, this->ext);
         scale_shared(ex, g.nExt, P.sloth ? 2 : 1);
         float* out = stage_out(modelOut, 1, add, mem);
+        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32) {
+            tomo_adjoint_tb(out, ex, nShots, shots, mem);
+            write_model(modelOut, 1, add, mem, out);
+            sync();
+            return;
+        }
         for (int s0 = 0; s0 < nShots;) {
             const int nb = wave_size(n, nShots - s0, shots + s0);
             setup_wave(n, nb, shots + s0, mem, true, false);
@@ -1607,6 +1894,12 @@ struct Context {
         float* dm = stage_model(model, 1, mem, this->model);
         scale_shared(dm, 1, 0);
         float* out = stage_out(imageOut, g.nExt, add, mem);
+        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32) {
+            wemva_forward_tb(dm, out, nShots, shots, mem);
+            write_model(imageOut, g.nExt, add, mem, out);
+            sync();
+            return;
+        }
         for (int s0 = 0; s0 < nShots;) {
             const int nb = wave_size(n, nShots - s0, shots + s0);
             setup_wave(n, nb, shots + s0, mem, false, true);
@@ -1641,6 +1934,12 @@ struct Context {
         float* im = stage_model(image, g.nExt, mem, this->ext);
         scale_shared(im, g.nExt, 1);
         float* out = stage_out(modelOut, 1, add, mem);
+        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32) {
+            wemva_adjoint_tb(out, im, nShots, shots, mem);
+            write_model(modelOut, 1, add, mem, out);
+            sync();
+            return;
+        }
         for (int s0 = 0; s0 < nShots;) {
             const int nb = wave_size(n, nShots - s0, shots + s0);
             setup_wave(n, nb, shots + s0, mem, false, true);

@@ -249,18 +249,20 @@ __global__ void k_img_time_adj(Acc* m, long long mSt, float* r, long long rSt, c
     }
 }
 
-// Time-lag imaging of a block of coarse receiver samples (imagingTimeAdjGpu,
-// F/src/kernelsGpu.cu:352-364, applied at every t of the block):
-//   img[e] += sum_{t = tlo..thi} R(t) * W[t - 2(e-h)]   over 0 <= t - 2(e-h) < nts,
-// the same (t, e) pairs as the reference's truncating-division lag bounds. R(t) lives in a
-// ring of LAG_K slices (slot t % LAG_K). Each thread owns one point: its R samples are held in
-// registers and the W slices t-2h .. t+2h of the block in shared memory (own column only,
-// no barrier), so W is read once per block instead of once per lag, and the image once per
-// block instead of once per sample.
+// Time-lag imaging of a block of at most LAG_K coarse samples (imagingTimeAdjGpu,
+// F/src/kernelsGpu.cu:352-364, applied at every t of the block; sign = -1 gives
+// imagingWemvaTimeAdjGpu, :366-378):
+//   img[e] += sum_{t = tlo..thi} R(t) * W[t - sign 2(e-h)]   over 0 <= t - sign 2(e-h) < nts,
+// the same (t, e) pairs as the reference's truncating-division lag bounds (nExt = 1, hExt = 0:
+// the zero-lag imagingAdjGpu, :318-325). R(t) lives in a ring of rRing slices (slot t % rRing).
+// Each thread owns one point: its R samples are held in registers and the W slices t-2h .. t+2h
+// of the block in shared memory (own column only, no barrier), so W is read once per block
+// instead of once per lag, and the image once per block instead of once per sample.
 constexpr int LAG_K = 16;
 template <typename Acc>
-__global__ void k_img_lag_block(Acc* img, long long mSt, const float* R, long long rSt, const float* W, long long WSt,
-                                long long isz, int tlo, int thi, int nts, int hExt, int nExt) {
+__global__ void k_img_lag_block(Acc* img, long long mSt, const float* R, long long rSt, int rRing, const float* W,
+                                long long WSt, long long isz, int tlo, int thi, int nts, int hExt, int nExt,
+                                int sign) {
     extern __shared__ float lag_smem[];
     const int b = blockIdx.y, tid = threadIdx.x, nP = blockDim.x;
     const long long p = (long long)blockIdx.x * nP + tid;
@@ -273,12 +275,12 @@ __global__ void k_img_lag_block(Acc* img, long long mSt, const float* R, long lo
     for (int k = 0; k <= tauhi - taulo; k++) Ws[k * nP + tid] = W[(long long)(taulo + k) * isz + p];
     float r[LAG_K];
 #pragma unroll
-    for (int k = 0; k < LAG_K; k++) r[k] = (tlo + k <= thi) ? R[(long long)((tlo + k) % LAG_K) * isz + p] : 0.f;
+    for (int k = 0; k < LAG_K; k++) r[k] = (tlo + k <= thi) ? R[(long long)((tlo + k) % rRing) * isz + p] : 0.f;
     for (int e = 0; e < nExt; e++) {
         float acc = 0.f;
 #pragma unroll
         for (int k = 0; k < LAG_K; k++) {
-            const int tau = tlo + k - 2 * (e - hExt);
+            const int tau = tlo + k - sign * 2 * (e - hExt);
             if (tlo + k <= thi && tau >= 0 && tau < nts) acc += r[k] * Ws[(tau - taulo) * nP + tid];
         }
         img[(long long)e * isz + p] += (Acc)acc;
@@ -286,12 +288,13 @@ __global__ void k_img_lag_block(Acc* img, long long mSt, const float* R, long lo
 }
 
 // Secondary sources of a block of coarse steps of the time-lag extended forward
-// (imagingTimeFwdGpu, F/src/kernelsGpu.cu:337-350, at every t of the block):
-//   ss(t) = sum_e ext[e] * W[t - 2(e-h)]   over 0 <= t - 2(e-h) < nts,
+// (imagingTimeFwdGpu, F/src/kernelsGpu.cu:337-350, at every t of the block; sign = -1 gives
+// imagingTimeTomoAdjGpu, :445-458):
+//   ss(t) = sum_e ext[e] * W[t - sign 2(e-h)]   over 0 <= t - sign 2(e-h) < nts,
 // written to a ring of ring slices (slot t % ring). One thread per point; the W slices of
 // the block live in shared memory (own column only), so W is read once per block.
 __global__ void k_ss_lag_block(float* ss, long long ssSt, int ring, const float* ext, const float* W, long long WSt,
-                               long long isz, int tlo, int thi, int nts, int hExt, int nExt) {
+                               long long isz, int tlo, int thi, int nts, int hExt, int nExt, int sign) {
     extern __shared__ float lag_smem[];
     const int b = blockIdx.y, tid = threadIdx.x, nP = blockDim.x;
     const long long p = (long long)blockIdx.x * nP + tid;
@@ -304,7 +307,7 @@ __global__ void k_ss_lag_block(float* ss, long long ssSt, int ring, const float*
     for (int t = tlo; t <= thi; t++) {
         float acc = 0.f;
         for (int e = 0; e < nExt; e++) {
-            const int tau = t - 2 * (e - hExt);
+            const int tau = t - sign * 2 * (e - hExt);
             if (tau >= 0 && tau < nts) acc += ext[(long long)e * isz + p] * Ws[(tau - taulo) * nP + tid];
         }
         ss[(long long)(t % ring) * isz + p] = acc;
@@ -313,7 +316,8 @@ __global__ void k_ss_lag_block(float* ss, long long ssSt, int ring, const float*
 
 // Scalings (F/src/kernelsGpu.cu:246-252, 278-303). mode 0: m *= v2*rs;
 // mode 1: m *= rs*v2 (extended); mode 2: m = -(m*v2) (sloth); on images of v2-weighted
-// (adjoint U-form) wavefields: mode 3: m *= rs, mode 4: m = -m.
+// (adjoint U-form) wavefields: mode 3: m *= rs, mode 4: m = -m, mode 5: m *= (v2*rs) / v2
+// (zero where v2 is zero: padding lanes).
 __global__ void k_scale(float* m, long long mSt, int nSlices, const float* v2, const float* rs, long long isz,
                         int mode) {
     const int b = blockIdx.y;
@@ -326,6 +330,7 @@ __global__ void k_scale(float* m, long long mSt, int nSlices, const float* v2, c
         else if (mode == 1) m[k] *= r * v;
         else if (mode == 3) m[k] *= r;   // images of v2-weighted (adjoint U-form) wavefields
         else if (mode == 4) m[k] = -m[k];
+        else if (mode == 5) m[k] = v != 0.f ? m[k] / v * (v * r) : 0.f;
         else m[k] = -(m[k] * v);
     }
 }
@@ -370,6 +375,7 @@ __global__ void k_scale_d(double* m, long long mSt, int nSlices, const float* v2
         else if (mode == 1) m[k] *= (double)(float)(r * v);
         else if (mode == 3) m[k] *= r;   // images of v2-weighted (adjoint U-form) wavefields
         else if (mode == 4) m[k] = -m[k];  // sloth images of U-form wavefields
+        else if (mode == 5) m[k] = v != 0.0 ? m[k] / v * (double)(float)(v * r) : 0.0;  // U-form, v2*rs scaling
         else m[k] = -(m[k] * v);
     }
 }

@@ -12,8 +12,19 @@ namespace aio {
 // is done on those samples by the coarse kernels).
 // TB_SCATX: the scattered pass of TB_SCAT with precomputed secondary-source slices (time-lag
 // extended forward: ss(t) = sum_e ext[e] W[t - 2(e-h)]) in ring slots rSlot / rSlot0 of W.
-enum TBMode { TB_SRC = 0, TB_NL = 1, TB_SCAT = 2, TB_ADJ = 3, TB_ADJR = 4, TB_SCATX = 5 };
-__host__ __device__ constexpr bool tb_scatlike(int mode) { return mode == TB_SCAT || mode == TB_SCATX; }
+// TB_SCATW: forward pass driven by dense secondary sources read from slices rSlot / rSlot0 of W
+// (times dm when the launch has one), storing its finished coarse samples (tomo / WEMVA legs):
+// sample its to slice oA of rcoarse, and at its == nts-2 sample its+1 to slice oB.
+// TB_ADJX: the adjoint recursion (U = v2 * S) driven by dense secondary sources from slices
+// rSlot / rSlot0 of W (times dm when given) built from a U-form receiver wavefield, so no v2
+// factor is applied at injection; stores R(its+1) to slice oB and, at its == 0, R(0) to oA.
+enum TBMode { TB_SRC = 0, TB_NL = 1, TB_SCAT = 2, TB_ADJ = 3, TB_ADJR = 4, TB_SCATX = 5, TB_SCATW = 6, TB_ADJX = 7 };
+// modes whose injection is a dense secondary source staged from W (no sparse injection)
+__host__ __device__ constexpr bool tb_scatlike(int mode) {
+    return mode == TB_SCAT || mode == TB_SCATX || mode == TB_SCATW || mode == TB_ADJX;
+}
+// dense-source modes that also store coarse samples of the propagated field
+__host__ __device__ constexpr bool tb_dense_out(int mode) { return mode == TB_SCATW || mode == TB_ADJX; }
 // Stored source wavefield: FP32, BF16, or FP16 scaled per coarse slice and shot (the scale
 // maps the slice's max |W| to 2^15, computed exactly from the finished FP32 slice).
 enum TBWfld { TBW_F32 = 0, TBW_BF16 = 1, TBW_F16 = 2 };
@@ -43,7 +54,7 @@ struct TBShot {
     float* wscale;        // [nts] value of one FP16 unit of slice t
     float* wstage;        // [2][isz] FP32 slices its and its+1 being accumulated (SRC)
     unsigned* wmax;       // [nts] max |W| of slice t as float bits (SRC)
-    float* rcoarse;       // ADJR: [2][isz] coarse receiver samples R(its+1), R(0)
+    float* rcoarse;       // ADJR / SCATW / ADJX: slices of coarse samples written by the launch
 };
 
 // Coarse slice t of a stored wavefield of `stride` elements per slice.

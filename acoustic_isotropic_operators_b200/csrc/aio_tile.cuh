@@ -56,7 +56,7 @@ struct KTArgs {
     Coefs c;
     const float* v2;       // interior slice (pitch ip)
     const float* taper;    // minPad entries
-    const float* dm;       // SCAT: scaled model perturbation (interior slice)
+    const float* dm;       // SCAT (and SCATW / ADJX when set): scaled model perturbation (interior slice)
     const TBShot* shots;
     float h[2 * (SUB_MAX + 1)];
     int its;               // coarse interval
@@ -66,7 +66,9 @@ struct KTArgs {
     int iters;             // iterations per CTA
     int maxEnt;            // shared entry capacity
     long long wStride;     // elements per stored coarse slice (= isz)
-    int rSlot, rSlot0;     // ADJR: ring slots of R(its+1) and (its == 0) R(0)
+    int rSlot, rSlot0;     // ADJR: ring slots of R(its+1) and (its == 0) R(0);
+                           // SCATX / SCATW / ADJX: slices of W holding the sources at its, its+1
+    int oA, oB;            // SCATW / ADJX: slices of rcoarse receiving the samples its, its+1
 };
 
 // Per-thread staging slots (16 bytes each) filled by asynchronous copies: level-1 operands
@@ -345,9 +347,9 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
             kt_cp16(mySlot + j * bd, oko ? old + (long long)co * ip + zq : old, oko);
             const long long ic = (long long)min(max(co, 0), nxi - 1) * ip + zv;
             kt_cp16_l1(mySlot + (2 + j) * bd, v2p + ic, true);
-            if (tb_scatlike(MODE)) {  // stored wavefield (SCATX: secondary sources) at its, its+1 (slots 4-7)
-                const void* wa = tb_wslice<WPREC>(sh.W, a.wStride, MODE == TB_SCATX ? a.rSlot : its);
-                const void* wb = tb_wslice<WPREC>(sh.W, a.wStride, MODE == TB_SCATX ? a.rSlot0 : its + 1);
+            if (tb_scatlike(MODE)) {  // stored wavefield (or secondary sources) at its, its+1 (slots 4-7)
+                const void* wa = tb_wslice<WPREC>(sh.W, a.wStride, MODE == TB_SCAT ? its : a.rSlot);
+                const void* wb = tb_wslice<WPREC>(sh.W, a.wStride, MODE == TB_SCAT ? its + 1 : a.rSlot0);
                 if (WPREC == TBW_F32) {
                     kt_cp16(mySlot + (4 + j) * bd, (const float*)wa + ic, true);
                     kt_cp16(mySlot + (6 + j) * bd, (const float*)wb + ic, true);
@@ -440,10 +442,10 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
                     for (int j = 0; j < 2; j++) {
                         if (t == 1) {
                             // imagingFwdGpu (F/src/kernelsGpu.cu:309-316): dm * W, kept for levels 2..T
-                            // (SCATX: the secondary sources are staged as they are)
+                            // (SCATX, and SCATW / ADJX without dm: the sources are staged as they are)
                             const float4 wa = kt_wfrom<WPREC>(mySlot[(4 + j) * bd], scA);
                             const float4 wb = kt_wfrom<WPREC>(mySlot[(6 + j) * bd], scB);
-                            if (MODE == TB_SCATX) {
+                            if (MODE == TB_SCATX || (tb_dense_out(MODE) && dmp == nullptr)) {
                                 sa[j] = wa;
                                 sb[j] = wb;
                             } else {
@@ -489,9 +491,14 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
                         float2 n = __ffma2_rn(kt_half(vq[j], P), __fadd2_rn(lz, lx), ctr);
                         n = __fadd2_rn(n, ctr);
                         n = __ffma2_rn(make_float2(-Dm[j][a0], -Dm[j][a0 + 1]), kt_half(ol[j], P), n);
-                        if (tb_scatlike(MODE))
-                            n = __fadd2_rn(n, __ffma2_rn(kt_half(sb[j], P), make_float2(a.h[H + t - 1], a.h[H + t - 1]),
-                                                         __fmul2_rn(kt_half(sa[j], P), make_float2(a.h[t - 1], a.h[t - 1]))));
+                        if (tb_scatlike(MODE)) {
+                            // injectSecondarySource (F/src/kernelsGpu.cu:102-107): forward fine step it2 = t
+                            // weighs ss(its), ss(its+1) by h[it2-1], h[H+it2-1]; adjoint step it2 = T-t by
+                            // h[it2+1], h[H+it2+1]
+                            const int hi = MODE == TB_ADJX ? T - t + 1 : t - 1;
+                            n = __fadd2_rn(n, __ffma2_rn(kt_half(sb[j], P), make_float2(a.h[H + hi], a.h[H + hi]),
+                                                         __fmul2_rn(kt_half(sa[j], P), make_float2(a.h[hi], a.h[hi]))));
+                        }
                         S[j][a0] = n.x;  // damped below, after injection
                         S[j][a0 + 1] = n.y;
                     }
@@ -610,9 +617,28 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
                     kt_st4(pPartOut + idx, ra);
                     *reinterpret_cast<double2*>(pImg + idx) = make_double2(acc[0], acc[1]);
                     *reinterpret_cast<double2*>(pImg + idx + 2) = make_double2(acc[2], acc[3]);
-                } else if (MODE == TB_ADJR) {
+                } else if (MODE == TB_SCATW) {
+                    // interpFineToCoarseSlice on the scattered field (F/src/kernelsGpu.cu:166-182); the
+                    // partial sum is read directly (staging slots 4-7 hold the sources)
+                    const float4 oP = __ldg(reinterpret_cast<const float4*>(pPart + idx));
+                    float wa[4], wb[4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        wa[i] = kt_el(oP, i);
+                        wb[i] = 0.f;
+#pragma unroll
+                        for (int l = 1; l <= T; l++) {
+                            wa[i] += lvT[j][l][i] * a.h[l];
+                            wb[i] += lvT[j][l][i] * a.h[H + l];
+                        }
+                    }
+                    kt_st4(pPartOut + idx, wb);
+                    kt_st4(sh.rcoarse + (long long)a.oA * a.wStride + idx, wa);                          // its
+                    if (its == g.nts - 2) kt_st4(sh.rcoarse + (long long)a.oB * a.wStride + idx, wb);   // its+1
+                } else if (MODE == TB_ADJR || MODE == TB_ADJX) {
                     float ra[4], rb[4];
-                    const float4 oP = mySlot[(4 + j) * bd];
+                    const float4 oP = MODE == TB_ADJX ? __ldg(reinterpret_cast<const float4*>(pPart + idx))
+                                                      : mySlot[(4 + j) * bd];
 #pragma unroll
                     for (int i = 0; i < 4; i++) {
                         ra[i] = 0.f;
@@ -624,8 +650,9 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
                         }
                     }
                     kt_st4(pPartOut + idx, ra);
-                    kt_st4(sh.rcoarse + (long long)a.rSlot * a.wStride + idx, rb);                  // R(its+1)
-                    if (its == 0) kt_st4(sh.rcoarse + (long long)a.rSlot0 * a.wStride + idx, ra);  // R(0)
+                    const int sB = MODE == TB_ADJX ? a.oB : a.rSlot, sA = MODE == TB_ADJX ? a.oA : a.rSlot0;
+                    kt_st4(sh.rcoarse + (long long)sB * a.wStride + idx, rb);                  // R(its+1)
+                    if (its == 0) kt_st4(sh.rcoarse + (long long)sA * a.wStride + idx, ra);  // R(0)
                 } else if (qRec) {
                     for (int e = recFirst[c - xs + 32]; e >= 0 && e < nRec && sEnt[recOff + e].col == c; e++) {
                         const int rr = sEnt[recOff + e].row - zq;

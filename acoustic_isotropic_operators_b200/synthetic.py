@@ -230,6 +230,32 @@ def born_workload(nz_phys=400, nx_phys=1200, nshots=32, nts=2000, dts=0.004, see
     return Workload("born", p, nts, dts, sub, d, d, vel, ricker(nts, dts), shots, model=refl)
 
 
+def tomo_workload(nz_phys=800, nx_phys=3000, nshots=96, nts=3000, n_ext=41, dts=0.004, seed=5, d=10.0) -> Workload:
+    """Extended tomo / WEMVA configuration (800x3000, nExt = 41, 96 shots, nts = 3000): smoothed
+    gradient background; model = Gaussian velocity anomalies (sigma 300 m, +-5 %); extended image
+    (extra["ext"], (nExt, nx, nz)) = 20 interfaces times a Gaussian lag profile (sigma 3 lags)."""
+    w = born_workload(nz_phys, nx_phys, nshots, nts, dts, seed, d)
+    rng = np.random.default_rng(seed + 100)
+    v0 = gaussian_smooth(gradient(nz_phys, nx_phys), 100.0 / d)
+    z = np.arange(nz_phys)[None, :] * d
+    x = np.arange(nx_phys)[:, None] * d
+    dv = np.zeros((nx_phys, nz_phys))
+    for _ in range(8):
+        cz, cx = rng.uniform(0, nz_phys * d), rng.uniform(0, nx_phys * d)
+        dv += rng.choice([-1.0, 1.0]) * np.exp(-((z - cz) ** 2 + (x - cx) ** 2) / (2 * 300.0 ** 2))
+    dv = 0.05 * v0 * dv / max(1.0, float(np.abs(dv).max()))
+    model = pad_model(dv.astype(np.float32), w.pad)
+    model[:FAT + w.pad.xPadMinus] = 0; model[FAT + w.pad.xPadMinus + nx_phys:] = 0
+    model[:, :FAT + w.pad.zPadMinus] = 0; model[:, FAT + w.pad.zPadMinus + nz_phys:] = 0
+    h = (n_ext - 1) // 2
+    prof = np.exp(-(np.arange(n_ext) - h) ** 2 / (2 * 3.0 ** 2)).astype(np.float32)
+    w.extra["ext"] = prof[:, None, None] * w.model[None]
+    w.model = model
+    w.nExt = n_ext
+    w.name = "tomo"
+    return w
+
+
 def nonlinear_workload(nz_phys=200, nx_phys=400, nts=1000, dts=0.004, seed=1, d=10.0) -> Workload:
     """Plain nonlinear forward configuration (200x400 + blobs, one shot at x=2000 m)."""
     rng = np.random.default_rng(seed)

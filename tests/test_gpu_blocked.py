@@ -179,6 +179,76 @@ def test_born_ext_adjoint_blocked(case, sloth):
     assert abs(a - b) / abs(b) < 1e-5
 
 
+def _ext_ctx(case, n_ext=5, **kw):
+    import dataclasses
+    from acoustic_isotropic_operators_b200.batch import Context
+    s5 = dataclasses.replace(case.scheme, nExt=n_ext)
+    k = orc.constants(s5, case.vel, dtype=np.float32)
+    return s5, Context(s5.nz, s5.nx, s5.nts, s5.dts, s5.sub, s5.dz, s5.dx, s5.minPad, k["v2"], k["rs"], nExt=n_ext,
+                       chunk_columns=64, image_fp64=True, **kw)
+
+
+def _wshots(case, rdata):
+    from acoustic_isotropic_operators_b200.batch import Shot
+    return [Shot(case.src_pos[i], case.rec_pos[i], case.sig[i], None, rdata[i]) for i in range(len(case.src_pos))]
+
+
+@pytest.mark.parametrize("legs,sloth", [((1, 0), 0), ((0, 1), 0), ((1, 1), 0), ((1, 1), 1)])
+def test_tomo_blocked(case, legs, sloth):
+    """Extended tomo forward / adjoint with every leg on the blocked stepper: vs the FP32 oracle
+    (relative L2 1e-5) and the dot test (1e-5). The inputs come from their own seeded generator:
+    the relative dot-test error |<Fm,d> - <m,F'd>| / |<m,F'd>| of an FP32 operator depends on the
+    draw through the cancellation in <Fm,d>; on this draw the FP32 oracle itself gives 1.4e-6 -
+    4.5e-6 and the per-fine-step stepper 1.4e-6 - 2.0e-6."""
+    l1, l2 = legs
+    s5, c = _ext_ctx(case, leg1=l1, leg2=l2, sloth=sloth)
+    rng = np.random.default_rng(3)
+    mask = interior_mask(case.nx, case.nz)
+    m = rng.standard_normal((case.nx, case.nz)).astype(np.float32) * mask
+    ext = rng.standard_normal((5, case.nx, case.nz)).astype(np.float32) * mask
+    fm = [x.copy() for x in c.tomo_forward(m, ext, shots(case))]
+    assert c.last_launches == (1 + 2 * (l1 + l2)) * (s5.nts - 1)   # source pass + two passes per leg
+    for i in range(len(fm)):
+        r32 = orc.tomo_fwd(s5, case.vel, m, ext, case.sig[i], case.src_pos[i], case.rec_pos[i], dtype=np.float32,
+                           sloth=sloth, leg1=l1, leg2=l2)
+        assert rel_l2(fm[i], r32) < 1e-5
+    d = [rng.standard_normal((len(r), s5.nts)).astype(np.float32) for r in case.rec_pos]
+    got = c.tomo_adjoint(ext, shots(case, d))
+    assert c.last_launches == (2 + l1 + l2) * (s5.nts - 1)         # source, receiver, one pass per leg
+    ref = sum(orc.tomo_adj(s5, case.vel, d[i], ext, case.sig[i], case.src_pos[i], case.rec_pos[i], dtype=np.float32,
+                           sloth=sloth, leg1=l1, leg2=l2) for i in range(len(d)))
+    assert rel_l2(got, ref) < 1e-5
+    a = sum(float(np.sum(fm[i].astype(np.float64) * d[i])) for i in range(len(d)))
+    b = float(np.sum(m.astype(np.float64) * got))
+    assert abs(a - b) / abs(b) < 1e-5
+
+
+@pytest.mark.parametrize("legs", [(1, 0), (0, 1), (1, 1)])
+def test_wemva_blocked(case, legs):
+    """Extended WEMVA forward / adjoint with every leg on the blocked stepper: vs the FP32 oracle
+    (relative L2 1e-5) and the dot test (1e-5), on inputs from their own seeded generator."""
+    l1, l2 = legs
+    s5, c = _ext_ctx(case, leg1=l1, leg2=l2)
+    rng = np.random.default_rng(3)
+    mask = interior_mask(case.nx, case.nz)
+    m = rng.standard_normal((case.nx, case.nz)).astype(np.float32) * mask
+    img = rng.standard_normal((5, case.nx, case.nz)).astype(np.float32) * mask
+    rd = [rng.standard_normal((len(r), s5.nts)).astype(np.float32) for r in case.rec_pos]
+    fimg = c.wemva_forward(m, _wshots(case, rd)).copy()
+    assert c.last_launches == (2 + l1 + l2) * (s5.nts - 1)
+    ref = sum(orc.wemva_fwd(s5, case.vel, m, case.sig[i], case.src_pos[i], case.rec_pos[i], rd[i], dtype=np.float32,
+                            leg1=l1, leg2=l2) for i in range(len(rd)))
+    assert rel_l2(fimg, ref) < 1e-5
+    got = c.wemva_adjoint(img, _wshots(case, rd))
+    assert c.last_launches == (2 + l1 + l2) * (s5.nts - 1)
+    ref = sum(orc.wemva_adj(s5, case.vel, img, case.sig[i], case.src_pos[i], case.rec_pos[i], rd[i],
+                            dtype=np.float32, leg1=l1, leg2=l2) for i in range(len(rd)))
+    assert rel_l2(got, ref) < 1e-5
+    a = float(np.sum(fimg.astype(np.float64) * img))
+    b = float(np.sum(m.astype(np.float64) * got))
+    assert abs(a - b) / abs(b) < 1e-5
+
+
 def test_short_strip_variant():
     """Interiors of at most 64 rows run the short-strip kernel variant (narrower rings, two CTAs
     per SM): nonlinear forward and Born forward / adjoint against the FP32 oracle."""
