@@ -787,8 +787,11 @@ struct Context {
 
     // nb: shots of the wave (one CTA column per shot)
     // Plan of a wave of nb shots: the autotuned plan when one was measured, else the model's.
-    TBPlan tb_plan(int nb) const {
-        auto it = tbTuned.find(nb);
+    // Plans are tuned per wave size and kernel class: light modes (SRC, NL, ADJR: at most 6
+    // staging slots, no secondary-source rings) and heavy modes (SCAT, SCATX, SCATW, ADJX, ADJ),
+    // whose larger shared-memory footprint changes how many CTAs an SM holds.
+    TBPlan tb_plan(int nb, bool heavy = false) const {
+        auto it = tbTuned.find(2 * nb + (heavy ? 1 : 0));
         if (it != tbTuned.end()) return it->second;
         return tb_model_plan(nb, 4 * (KT_MAXQ - 10), P.chunkColumns > 0 ? P.chunkColumns : 0);
     }
@@ -798,7 +801,8 @@ struct Context {
     // SM) times the iterations of one CTA (each chunk recomputes 10T warm-up columns), at
     // least 4 waves preferred so that CTAs of uneven cost (strips holding sources or
     // receivers) balance out.
-    TBPlan tb_model_plan(int nb, int maxHZ, int chunkColumns, int forceChunks = 0) const {
+    // minWaves: smallest number of CTA waves (of one CTA per SM) the chunk count is chosen from
+    TBPlan tb_model_plan(int nb, int maxHZ, int chunkColumns, int forceChunks = 0, int minWaves = 4) const {
         TBPlan pl;
         pl.nStrips = (g.nzi + maxHZ - 1) / maxHZ;
         pl.HZ = round_up((g.nzi + pl.nStrips - 1) / pl.nStrips, 4);
@@ -820,7 +824,7 @@ struct Context {
                     bestAny = cost;
                     ncAny = nc;
                 }
-                if (ctas >= 4LL * smCount && cost < best * 0.999) {
+                if (ctas >= (long long)minWaves * smCount && cost < best * 0.999) {
                     best = cost;
                     pl.nChunks = nc;
                 }
@@ -833,31 +837,88 @@ struct Context {
     }
 
     // Measured autotuning of the blocked stepper's plan for waves of nb shots (chunkColumns
-    // == 0): strip heights {128, 112, 96, 64} rows x chunk counts around the model's choice are
-    // each timed on the source-pass launch of interval 0 (idempotent: it reads one state set
-    // and overwrites the other, the stored slice 0 and the partial sums), the fastest is
-    // cached for the context. The state is zeroed again afterwards.
+    // == 0): strip heights {128, 112, 96, 64} rows x chunk counts around the model's choices
+    // (at least 4 waves of CTAs, and the cheapest count for any number of waves) are each timed
+    // on the source-pass launch of interval 0 (idempotent: it reads one state set and
+    // overwrites the other, the stored slice 0 and the partial sums), the fastest is cached
+    // for the context. The state is zeroed again afterwards.
     std::map<int, TBPlan> tbTuned;
     TBPlan tbLast;  // plan of the most recent blocked launch
-    void tb_autotune(int nb, const aio_shot* shots) {
-        if (P.chunkColumns != 0 || tbTuned.count(nb)) return;
-        std::vector<TBPlan> cand;
-        for (int maxHZ : {128, 112, 96, 64}) {
-            const TBPlan m = tb_model_plan(nb, maxHZ, 0);
-            for (int d : {-2, -1, 0, 1, 2}) {
-                const int nc = m.nChunks + d;
-                if (nc < 1 || nc > std::max(1, g.nxi / 32)) continue;
-                TBPlan c = tb_model_plan(nb, maxHZ, 0, nc);
-                bool dup = false;
-                for (auto& o : cand) dup |= (o.HZ == c.HZ && o.nChunks == c.nChunks);
-                if (!dup && c.threads <= KT_MAXT && c.NQ <= KT_MAXQ) cand.push_back(c);
+
+    // Largest sparse-entry counts one CTA of plan pl holds, per kind of pass: sources injected
+    // over the halo region plus receivers recorded in the output region (SRC, NL), receivers
+    // recorded (SCAT, SCATX), receivers injected over the halo region plus sources recorded
+    // (ADJ, ADJR).
+    struct TBEntries {
+        int fwd = 1, scat = 1, adj = 1;
+    };
+    TBEntries tb_max_entries(const TBPlan& pl, int nb, const aio_shot* shots) const {
+        const int h = 5 * (pl.T - 1);
+        const size_t nCTA = (size_t)pl.nStrips * pl.nChunks;
+        std::vector<int> srcHalo(nCTA), srcOut(nCTA), recHalo(nCTA), recOut(nCTA);
+        TBEntries m;
+        for (int s = 0; s < nb; s++) {
+            for (auto* v : {&srcHalo, &srcOut, &recHalo, &recOut}) std::fill(v->begin(), v->end(), 0);
+            auto add = [&](const int* pos, int n, std::vector<int>& halo, std::vector<int>& out) {
+                for (int k2 = 0; k2 < n; k2++) {
+                    const int iz = (int)(pos[k2] % g.nz) - FAT, ix = (int)(pos[k2] / g.nz) - FAT;
+                    for (int st2 = std::max(0, (iz - h) / pl.HZ - 1); st2 <= std::min(pl.nStrips - 1, (iz + h) / pl.HZ + 1); st2++) {
+                        const int z0 = st2 * pl.HZ, z1 = std::min(z0 + pl.HZ, g.nzi);
+                        if (iz < z0 - h || iz >= z1 + h) continue;
+                        for (int ch = std::max(0, (ix - h) / pl.LX - 1); ch <= std::min(pl.nChunks - 1, (ix + h) / pl.LX + 1); ch++) {
+                            const int x0 = ch * pl.LX, x1 = std::min(x0 + pl.LX, g.nxi);
+                            if (ix < x0 - h || ix >= x1 + h) continue;
+                            const size_t c = (size_t)st2 * pl.nChunks + ch;
+                            halo[c]++;
+                            if (ix >= x0 && ix < x1 && iz >= z0 && iz < z1) out[c]++;
+                        }
+                    }
+                }
+            };
+            add(shots[s].sourcesPositionReg, shots[s].nSourcesReg, srcHalo, srcOut);
+            add(shots[s].receiversPositionReg, shots[s].nReceiversReg, recHalo, recOut);
+            for (size_t c = 0; c < nCTA; c++) {
+                m.fwd = std::max(m.fwd, srcHalo[c] + recOut[c]);
+                m.scat = std::max(m.scat, recOut[c]);
+                m.adj = std::max(m.adj, recHalo[c] + srcOut[c]);
             }
         }
+        return m;
+    }
+    // plan pl fits in shared memory in every mode
+    bool tb_plan_fits(const TBPlan& pl, const TBEntries& e) const {
+        int smemMax = 0;
+        if (cudaDeviceGetAttribute(&smemMax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
+        const int rs = kt_rs(pl.NQ <= KT_MAXQ_S ? KT_MAXQ_S : KT_MAXQ);
+        const std::pair<int, int> need[] = {{TB_SRC, e.fwd}, {TB_SCAT, e.scat}, {TB_ADJ, e.adj}, {TB_SCATW, 1}};
+        for (const auto& mn : need)
+            if (kt_smem_bytes(mn.first, pl.threads, pl.iters, mn.second, rs) > (size_t)smemMax) return false;
+        return true;
+    }
+
+    void tb_autotune(int nb, const aio_shot* shots) {
+        if (P.chunkColumns != 0 || tbTuned.count(2 * nb)) return;
+        std::vector<TBPlan> cand;
+        for (int maxHZ : {128, 112, 96, 64})
+            for (int minWaves : {4, 1}) {
+                const TBPlan m = tb_model_plan(nb, maxHZ, 0, 0, minWaves);
+                for (int d : {-2, -1, 0, 1, 2}) {
+                    const int nc = m.nChunks + d;
+                    if (nc < 1 || nc > std::max(1, g.nxi / 32)) continue;
+                    TBPlan c = tb_model_plan(nb, maxHZ, 0, nc);
+                    bool dup = false;
+                    for (auto& o : cand) dup |= (o.HZ == c.HZ && o.nChunks == c.nChunks);
+                    if (!dup && c.threads <= KT_MAXT && c.NQ <= KT_MAXQ &&
+                        tb_plan_fits(c, tb_max_entries(c, nb, shots)))
+                        cand.push_back(c);
+                }
+            }
+        if (cand.empty()) return;  // the model's plan (tb_plan) then stands
         cudaEvent_t e0, e1;
         AIO_CK(cudaEventCreate(&e0));
         AIO_CK(cudaEventCreate(&e1));
-        float bestMs = 1e30f;
-        TBPlan best = cand.front();
+        float bestMs = 1e30f, bestHeavyMs = 1e30f;
+        TBPlan best = cand.front(), bestHeavy = cand.front();
         const long long saveLaunches = launches, saveKernels = kernels;
         const int saveProf = profEvery;
         profEvery = 0;
@@ -880,13 +941,33 @@ struct Context {
                 bestMs = ms;
                 best = pl;
             }
+            // heavy class: the time-lag scattered pass (reads W slices 0, 1 as its sources;
+            // writes only the other state set)
+            const int maxEntH = tb_lists(pl, nb, shots, 0, false);  // before tb_desc: it may move the lists
+            tb_desc(pl, nb, false, false, false, tbW.p, false);
+            a = tb_args(pl, maxEntH, nullptr);
+            a.its = 0;
+            a.rSlot = 0;
+            a.rSlot0 = 1;
+            tb_launch<TB_SCATX>(pl, nb, a, 0);
+            AIO_CK(cudaEventRecord(e0, st));
+            tb_launch<TB_SCATX>(pl, nb, a, 0);
+            tb_launch<TB_SCATX>(pl, nb, a, 0);
+            AIO_CK(cudaEventRecord(e1, st));
+            AIO_CK(cudaEventSynchronize(e1));
+            AIO_CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < bestHeavyMs) {
+                bestHeavyMs = ms;
+                bestHeavy = pl;
+            }
         }
         AIO_CK(cudaEventDestroy(e0));
         AIO_CK(cudaEventDestroy(e1));
         launches = saveLaunches;
         kernels = saveKernels;
         profEvery = saveProf;
-        tbTuned[nb] = best;
+        tbTuned[2 * nb] = best;
+        tbTuned[2 * nb + 1] = bestHeavy;
     }
 
     // Per-CTA sparse lists of every shot of a wave. inj: 0 none, 1 sources, 2 receivers
@@ -1100,7 +1181,7 @@ struct Context {
     // Scattered pass with data recording (F/src/BornShotsGpuFunctions.cu:323-376); W: the stored
     // field the secondary sources dm * W come from (default: the source wavefield tbW).
     void tb_scat_pass(int nb, const aio_shot* shots, const float* dm, const float* W = nullptr) {
-        const TBPlan pl = tb_plan(nb);
+        const TBPlan pl = tb_plan(nb, true);
         const int maxEnt = tb_lists(pl, nb, shots, 0, true);
         tb_zero(nb, false);
         tb_desc(pl, nb, false, false, true, W ? (void*)W : tbW.p, false);
@@ -1115,7 +1196,7 @@ struct Context {
     // Launch L handles interval its = nts-2-L: it reads the partial R(its+1) written by
     // launch L-1 and writes R(its); state ping-pongs with L.
     void tb_adj_pass(int nb, const aio_shot* shots) {
-        const TBPlan pl = tb_plan(nb);
+        const TBPlan pl = tb_plan(nb, true);
         const int maxEnt = tb_lists(pl, nb, shots, 2, false);
         tb_zero(nb, true);
         tb_desc(pl, nb, false, true, false, tbW.p, false);
@@ -1138,8 +1219,8 @@ struct Context {
         tb_desc(pl, nb, false, true, false, tbW.p, false);
         KTArgs a = tb_args(pl, maxEnt, nullptr);
         const long long mSt = (long long)g.nExt * g.isz;
-        const int nP = 128;
-        const size_t lagSmem = (size_t)(LAG_K + 4 * g.hExt) * nP * 4;
+        const int nP = LAG_NP;
+        const size_t lagSmem = (size_t)lag_window_len(g.hExt) * nP * 4;
         static int lagAttr = -1;
         if (lagAttr != dev) {
             AIO_CK(cudaFuncSetAttribute(k_img_lag_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -1176,13 +1257,13 @@ struct Context {
     // read by TB_SCATX at slots its and its+1.
     void tb_scatx_pass(int nb, const aio_shot* shots, const float* ext, const float* F = nullptr) {
         const int ring = 2 * LAG_K;
-        const TBPlan pl = tb_plan(nb);
+        const TBPlan pl = tb_plan(nb, true);
         const int maxEnt = tb_lists(pl, nb, shots, 0, true);
         tb_zero(nb, false);
         tb_desc(pl, nb, false, false, true, tbSS.p, false, ring);
         KTArgs a = tb_args(pl, maxEnt, nullptr);
-        const int nP = 128;
-        const size_t lagSmem = (size_t)(LAG_K + 4 * g.hExt) * nP * 4;
+        const int nP = LAG_NP;
+        const size_t lagSmem = (size_t)lag_window_len(g.hExt) * nP * 4;
         static int ssAttr = -1;
         if (ssAttr != dev) {
             AIO_CK(cudaFuncSetAttribute(k_ss_lag_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -1282,14 +1363,14 @@ struct Context {
         lagDev = dev;
     }
     size_t tb_lag_smem(int hExt) const {
-        const size_t b = (size_t)(LAG_K + 4 * hExt) * 128 * 4;
+        const size_t b = (size_t)lag_window_len(hExt) * LAG_NP * 4;
         require(b <= 200 * 1024, "extension too long for the blocked lag imaging");
         return b;
     }
     // secondary sources of the coarse steps [tlo, thi] into the ring tbSS
     void tb_ss_block(int nb, const TBSrc& src, int tlo, int thi) {
         tb_lag_attr();
-        const int nP = 128;
+        const int nP = LAG_NP;
         const dim3 grid((unsigned)((g.isz + nP - 1) / nP), nb);
         k_ss_lag_block<<<grid, nP, tb_lag_smem(g.hExt), st>>>(tbSS.as<float>(), (long long)TB_RING * g.isz, TB_RING,
                                                                 src.ext, src.F, wfSt(), g.isz, tlo, thi, g.nts, g.hExt,
@@ -1299,7 +1380,7 @@ struct Context {
     // image the samples [tlo, thi] of the ring tbR against out.imgF
     void tb_img_block(int nb, const TBOut& out, int tlo, int thi) {
         tb_lag_attr();
-        const int nP = 128, nE = out.lag ? g.nExt : 1, hE = out.lag ? g.hExt : 0;
+        const int nP = LAG_NP, nE = out.lag ? g.nExt : 1, hE = out.lag ? g.hExt : 0;
         const dim3 grid((unsigned)((g.isz + nP - 1) / nP), nb);
         const long long mSt = (long long)nE * g.isz, rSt = (long long)TB_RING * g.isz;
         const size_t sm = tb_lag_smem(hE);
@@ -1316,7 +1397,7 @@ struct Context {
     // F/src/tomoExtShotsGpuFunctions.cu:1554-1656,2442-2527, F/src/wemvaExtShotsGpuFunctions.cu:961-1037.
     // Lag sources are formed a block of LAG_K steps ahead; sample rings are imaged per block.
     void tb_dense_fwd(int nb, const aio_shot* shots, const TBSrc& src, const TBOut& out) {
-        const TBPlan pl = tb_plan(nb);
+        const TBPlan pl = tb_plan(nb, true);
         const int maxEnt = tb_lists(pl, nb, shots, 0, false);
         tb_zero(nb, false);
         const bool lagSrc = src.ext != nullptr;
@@ -1351,7 +1432,7 @@ struct Context {
     // Adjoint-time dense pass (adj_dense_pass on the blocked stepper, TB_ADJX) on U-form sources:
     // F/src/tomoExtShotsGpuFunctions.cu:2619-2700, F/src/wemvaExtShotsGpuFunctions.cu:1038-1121.
     void tb_dense_adj(int nb, const aio_shot* shots, const TBSrc& src, const TBOut& out) {
-        const TBPlan pl = tb_plan(nb);
+        const TBPlan pl = tb_plan(nb, true);
         const int maxEnt = tb_lists(pl, nb, shots, 0, false);
         tb_zero(nb, false);
         const bool lagSrc = src.ext != nullptr;

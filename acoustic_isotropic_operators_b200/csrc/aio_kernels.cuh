@@ -255,35 +255,67 @@ __global__ void k_img_time_adj(Acc* m, long long mSt, float* r, long long rSt, c
 //   img[e] += sum_{t = tlo..thi} R(t) * W[t - sign 2(e-h)]   over 0 <= t - sign 2(e-h) < nts,
 // the same (t, e) pairs as the reference's truncating-division lag bounds (nExt = 1, hExt = 0:
 // the zero-lag imagingAdjGpu, :318-325). R(t) lives in a ring of rRing slices (slot t % rRing).
-// Each thread owns one point: its R samples are held in registers and the W slices t-2h .. t+2h
-// of the block in shared memory (own column only, no barrier), so W is read once per block
-// instead of once per lag, and the image once per block instead of once per sample.
-constexpr int LAG_K = 16;
+// Each thread owns one point: its R samples are held in registers and the W slices
+// tlo-2h .. tlo+LAG_K-1+2h of the block in shared memory (own column only, no barrier; zero
+// outside [0, nts), so every (t, e) term is formed without bounds tests and the terms outside
+// the reference's bounds add exact zeros), so W is read once per block instead of once per lag,
+// and the image once per block instead of once per sample. Global loads are issued in batches:
+// the kernels are latency bound otherwise.
+constexpr int LAG_K = 32;
+constexpr int LAG_B = 8;
+constexpr int LAG_NP = 128;  // threads per block (points), a compile-time shared-memory stride
+__host__ __device__ constexpr int lag_window_len(int hExt) { return LAG_K + 4 * hExt; }
+// W slices tlo-2h .. of point p into this thread's shared column, zero outside [0, nts)
+__device__ __forceinline__ void lag_window(float* Ws, const float* __restrict__ W, long long isz, long long p, int tlo,
+                                           int hExt, int nts) {
+    const int n = lag_window_len(hExt), t0 = tlo - 2 * hExt;
+    for (int k0 = 0; k0 < n; k0 += 2 * LAG_B) {
+        float v[2 * LAG_B];
+#pragma unroll
+        for (int j = 0; j < 2 * LAG_B; j++) {
+            const int tau = t0 + k0 + j;
+            v[j] = (k0 + j < n && tau >= 0 && tau < nts) ? __ldg(W + (long long)tau * isz + p) : 0.f;
+        }
+#pragma unroll
+        for (int j = 0; j < 2 * LAG_B; j++)
+            if (k0 + j < n) Ws[(k0 + j) * LAG_NP] = v[j];
+    }
+}
 template <typename Acc>
-__global__ void k_img_lag_block(Acc* img, long long mSt, const float* R, long long rSt, int rRing, const float* W,
-                                long long WSt, long long isz, int tlo, int thi, int nts, int hExt, int nExt,
-                                int sign) {
+__global__ void __launch_bounds__(LAG_NP) k_img_lag_block(Acc* __restrict__ img, long long mSt, const float* __restrict__ R,
+                                                          long long rSt, int rRing, const float* __restrict__ W,
+                                                          long long WSt, long long isz, int tlo, int thi, int nts,
+                                                          int hExt, int nExt, int sign) {
     extern __shared__ float lag_smem[];
-    const int b = blockIdx.y, tid = threadIdx.x, nP = blockDim.x;
-    const long long p = (long long)blockIdx.x * nP + tid;
+    const int b = blockIdx.y, tid = threadIdx.x;
+    const long long p = (long long)blockIdx.x * LAG_NP + tid;
     if (p >= isz) return;
     R += b * rSt;
     W += b * WSt;
     img += b * mSt;
-    const int taulo = max(tlo - 2 * hExt, 0), tauhi = min(thi + 2 * hExt, nts - 1);
-    float* Ws = lag_smem;
-    for (int k = 0; k <= tauhi - taulo; k++) Ws[k * nP + tid] = W[(long long)(taulo + k) * isz + p];
+    float* Ws = lag_smem + tid;
+    lag_window(Ws, W, isz, p, tlo, hExt, nts);
     float r[LAG_K];
 #pragma unroll
-    for (int k = 0; k < LAG_K; k++) r[k] = (tlo + k <= thi) ? R[(long long)((tlo + k) % rRing) * isz + p] : 0.f;
-    for (int e = 0; e < nExt; e++) {
-        float acc = 0.f;
+    for (int k = 0; k < LAG_K; k++) r[k] = (tlo + k <= thi) ? __ldg(R + (long long)((tlo + k) % rRing) * isz + p) : 0.f;
+    for (int e0 = 0; e0 < nExt; e0 += LAG_B) {
+        float acc[LAG_B];
 #pragma unroll
-        for (int k = 0; k < LAG_K; k++) {
-            const int tau = tlo + k - sign * 2 * (e - hExt);
-            if (tlo + k <= thi && tau >= 0 && tau < nts) acc += r[k] * Ws[(tau - taulo) * nP + tid];
+        for (int j = 0; j < LAG_B; j++) {
+            // W index of sample k at lag e: tlo + k - sign 2(e-h), window offset 2h - sign 2(e-h)
+            const int e = min(e0 + j, nExt - 1);
+            const float* w = Ws + (2 * hExt - sign * 2 * (e - hExt)) * LAG_NP;
+            float sum = 0.f;
+#pragma unroll
+            for (int k = 0; k < LAG_K; k++) sum += r[k] * w[k * LAG_NP];
+            acc[j] = sum;
         }
-        img[(long long)e * isz + p] += (Acc)acc;
+        Acc old[LAG_B];
+#pragma unroll
+        for (int j = 0; j < LAG_B; j++) old[j] = e0 + j < nExt ? img[(long long)(e0 + j) * isz + p] : (Acc)0;
+#pragma unroll
+        for (int j = 0; j < LAG_B; j++)
+            if (e0 + j < nExt) img[(long long)(e0 + j) * isz + p] = old[j] + (Acc)acc[j];
     }
 }
 
@@ -292,26 +324,41 @@ __global__ void k_img_lag_block(Acc* img, long long mSt, const float* R, long lo
 // imagingTimeTomoAdjGpu, :445-458):
 //   ss(t) = sum_e ext[e] * W[t - sign 2(e-h)]   over 0 <= t - sign 2(e-h) < nts,
 // written to a ring of ring slices (slot t % ring). One thread per point; the W slices of
-// the block live in shared memory (own column only), so W is read once per block.
-__global__ void k_ss_lag_block(float* ss, long long ssSt, int ring, const float* ext, const float* W, long long WSt,
-                               long long isz, int tlo, int thi, int nts, int hExt, int nExt, int sign) {
+// the block live in shared memory (own column only, zero outside [0, nts)), so W is read once
+// per block, and ext once per block (lags outer, the block's samples accumulated in registers,
+// in lag order).
+__global__ void __launch_bounds__(LAG_NP) k_ss_lag_block(float* __restrict__ ss, long long ssSt, int ring,
+                                                         const float* __restrict__ ext, const float* __restrict__ W,
+                                                         long long WSt, long long isz, int tlo, int thi, int nts,
+                                                         int hExt, int nExt, int sign) {
     extern __shared__ float lag_smem[];
-    const int b = blockIdx.y, tid = threadIdx.x, nP = blockDim.x;
-    const long long p = (long long)blockIdx.x * nP + tid;
+    const int b = blockIdx.y, tid = threadIdx.x;
+    const long long p = (long long)blockIdx.x * LAG_NP + tid;
     if (p >= isz) return;
     ss += b * ssSt;
     W += b * WSt;
-    const int taulo = max(tlo - 2 * hExt, 0), tauhi = min(thi + 2 * hExt, nts - 1);
-    float* Ws = lag_smem;
-    for (int k = 0; k <= tauhi - taulo; k++) Ws[k * nP + tid] = W[(long long)(taulo + k) * isz + p];
-    for (int t = tlo; t <= thi; t++) {
-        float acc = 0.f;
-        for (int e = 0; e < nExt; e++) {
-            const int tau = t - sign * 2 * (e - hExt);
-            if (tau >= 0 && tau < nts) acc += ext[(long long)e * isz + p] * Ws[(tau - taulo) * nP + tid];
+    float* Ws = lag_smem + tid;
+    lag_window(Ws, W, isz, p, tlo, hExt, nts);
+    float acc[LAG_K];
+#pragma unroll
+    for (int k = 0; k < LAG_K; k++) acc[k] = 0.f;
+    for (int e0 = 0; e0 < nExt; e0 += LAG_B) {
+        float x[LAG_B];
+#pragma unroll
+        for (int j = 0; j < LAG_B; j++) x[j] = e0 + j < nExt ? __ldg(ext + (long long)(e0 + j) * isz + p) : 0.f;
+#pragma unroll
+        for (int j = 0; j < LAG_B; j++) {
+            if (e0 + j < nExt) {
+                const int e = e0 + j;
+                const float* w = Ws + (2 * hExt - sign * 2 * (e - hExt)) * LAG_NP;
+#pragma unroll
+                for (int k = 0; k < LAG_K; k++) acc[k] += x[j] * w[k * LAG_NP];
+            }
         }
-        ss[(long long)(t % ring) * isz + p] = acc;
     }
+#pragma unroll
+    for (int k = 0; k < LAG_K; k++)
+        if (tlo + k <= thi) ss[(long long)((tlo + k) % ring) * isz + p] = acc[k];
 }
 
 // Scalings (F/src/kernelsGpu.cu:246-252, 278-303). mode 0: m *= v2*rs;
