@@ -47,6 +47,10 @@ EXPORTED = [
     "aio_tomoTimeShotsFwdGpu", "aio_tomoTimeShotsAdjGpu",
     "aio_initWemvaExtGpu", "aio_allocateWemvaExtShotsGpu", "aio_deallocateWemvaExtShotsGpu",
     "aio_wemvaTimeShotsFwdGpu", "aio_wemvaTimeShotsAdjGpu",
+    "aio_propShotsFwdFsGpu", "aio_propShotsFwdFsGpuWavefield", "aio_propShotsAdjFsGpu",
+    "aio_propShotsAdjFsGpuWavefield", "aio_BornShotsFwdFsGpu", "aio_BornShotsAdjFsGpu",
+    "aio_BornTimeShotsFwdFsGpu", "aio_BornTimeShotsAdjFsGpu", "aio_tomoTimeShotsFwdFsGpu",
+    "aio_tomoTimeShotsAdjFsGpu",
 ]
 
 
@@ -55,7 +59,8 @@ class AioParams(C.Structure):
                 ("nExt", C.c_int), ("dz", C.c_float), ("dx", C.c_float), ("dts", C.c_float),
                 ("alphaCos", C.c_float), ("leg1", C.c_int), ("leg2", C.c_int), ("sloth", C.c_int),
                 ("wavefieldPrecision", C.c_int), ("imageFp64", C.c_int), ("device", C.c_int),
-                ("memBudgetBytes", C.c_longlong), ("stepper", C.c_int), ("chunkColumns", C.c_int)]
+                ("memBudgetBytes", C.c_longlong), ("stepper", C.c_int), ("chunkColumns", C.c_int),
+                ("freeSurface", C.c_int)]
 
 
 class AioShot(C.Structure):

@@ -205,7 +205,6 @@ class fdParam {
         _oz = vel->getHyper()->getAxis(1).o;
         if ((_zPadMinus == 0 && _freeSurface != 1) || (_zPadMinus > 0 && _freeSurface == 1))
             aio_ops::fail("[fdParam]: zPadMinus and freeSurface flag are inconsistent");
-        if (_freeSurface == 1) aio_ops::fail("[fdParam]: free-surface propagation is not available in this build");
         if (_nz != vel->getHyper()->getAxis(1).n) aio_ops::fail("[fdParam]: nz from vel tag not consistent with nz from parfile");
         _nx = par->getInt("nx");
         _xPadPlus = par->getInt("xPadPlus");
@@ -293,6 +292,7 @@ class fdParam {
         p.memBudgetBytes = 0;
         p.stepper = AIO_STEPPER_AUTO;
         p.chunkColumns = 0;
+        p.freeSurface = _freeSurface;
         return p;
     }
 
@@ -334,6 +334,7 @@ class ShotLoop {
         _saveWavefield = par->getInt("saveWavefield", 0);
         _wavefieldShotNumber = par->getInt("wavefieldShotNumber", 0);
         _leg1 = par->getInt("leg1", 1);
+        _sloth = par->getInt("sloth", 0);  // F/src/BornExtGpu.cpp:14, F/src/tomoExtGpu.cpp:15
         _leg2 = par->getInt("leg2", 1);
     }
     virtual ~ShotLoop() { release(); }
@@ -368,6 +369,9 @@ class ShotLoop {
         if (!_ctx[iGpu]) {
             const fdParam& f = fd();
             aio_params p = f.engineParams(_gpuList[iGpu], _leg1, _leg2);
+            if (!_freeSurfaceDrivers) p.freeSurface = 0;
+            // the free-surface drivers take no sloth flag (e.g. F/include/BornExtShotsGpuFunctions.h:27)
+            p.sloth = p.freeSurface ? 0 : _sloth;
             ck(aio_context_create(&p, f._vel2Dtw2.data(), f._reflectivityScale.data(), &_ctx[iGpu]));
         }
         return _ctx[iGpu];
@@ -466,7 +470,10 @@ class ShotLoop {
     std::shared_ptr<SEP::float2DReg> _vel;
     std::shared_ptr<paramObj> _par;
     int _family, _nShot = 0, _nGpu = 0, _info = 0, _deviceNumberInfo = 0, _saveWavefield = 0, _wavefieldShotNumber = 0;
-    int _leg1 = 1, _leg2 = 1;
+    int _leg1 = 1, _leg2 = 1, _sloth = 0;
+    // the family has free-surface drivers (the reference's WEMVA runs its plain drivers whatever
+    // freeSurface says: F/src/wemvaExtGpu.cpp has no free-surface branch)
+    bool _freeSurfaceDrivers = true;
     bool _recFirst = false;
     std::vector<int> _gpuList;
     mutable std::shared_ptr<fdParam> _fd;
@@ -795,6 +802,7 @@ class wemvaExtShotsGpu : public Operator<SEP::float2DReg, SEP::float3DReg>, publ
                      std::vector<std::shared_ptr<SEP::float2DReg>> receiversSignalsVector)
         : BornFamily(vel, par, AIO_WEMVA_EXT, sourcesVector, sourcesSignalsVector, receiversVector) {
         _receiversSignalsVector = receiversSignalsVector;
+        _freeSurfaceDrivers = false;
     }
 
     void forward(const bool add, const std::shared_ptr<SEP::float2DReg> model,

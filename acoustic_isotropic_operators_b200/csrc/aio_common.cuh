@@ -97,6 +97,7 @@ struct StepArgs {
     float recCA, recCB;
     long long accOffA, accOffB;  // accumulation slices (offsets into acc)
     float hAccA, hAccB;
+    int fs;                      // free surface at the top interior row
 };
 
 }  // namespace aio

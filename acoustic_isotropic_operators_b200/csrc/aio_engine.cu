@@ -197,6 +197,9 @@ struct Context {
                 "stored wavefield precision must be AIO_WFLD_FP32, AIO_WFLD_BF16 or AIO_WFLD_FP16");
         require(p.stepper >= AIO_STEPPER_AUTO && p.stepper <= AIO_STEPPER_BLOCKED, "unknown stepper");
         require(p.stepper < AIO_STEPPER_BLOCKED || p.sub == 4, "the interval-blocked steppers require sub == 4");
+        require(p.freeSurface == 0 || p.freeSurface == 1, "freeSurface must be 0 or 1");
+        require(!(p.freeSurface && p.stepper == AIO_STEPPER_BLOCKED),
+                "the free surface runs on the per-fine-step stepper (stepper AUTO or FINE)");
         require(p.wavefieldPrecision == AIO_WFLD_FP32 || (p.stepper != AIO_STEPPER_FINE && p.sub == 4),
                 "compressed stored wavefields need the interval-blocked stepper (sub == 4)");
         g = make_geom(p.nz, p.nx, p.nts, p.sub, p.minPad, p.nExt);
@@ -408,6 +411,7 @@ struct Context {
         a.shots = desc.as<ShotDesc>();
         a.injTB = -1;
         a.recTB = -1;
+        a.fs = P.freeSurface ? 1 : 0;
         return a;
     }
 
@@ -781,7 +785,7 @@ struct Context {
         int T = KT_T, HZ = 0, nStrips = 0, LX = 0, nChunks = 0, iters = 0, threads = 0, NQ = 0;
     };
 
-    bool tb_enabled() const { return P.stepper != AIO_STEPPER_FINE && g.sub == KT_T; }
+    bool tb_enabled() const { return P.stepper != AIO_STEPPER_FINE && g.sub == KT_T && !P.freeSurface; }
     int wbytes() const { return P.wavefieldPrecision == AIO_WFLD_FP32 ? 4 : 2; }
     bool f16() const { return P.wavefieldPrecision == AIO_WFLD_FP16; }
 
@@ -2419,6 +2423,119 @@ AIO_API int aio_tomoTimeShotsAdjGpu(float* model, float* dataRegDts, float* extR
         c.P.sloth = sloth;
         aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
         c.tomo_adjoint(model, 0, extReflectivity, 1, &s, AIO_MEM_HOST);
+    });
+}
+
+// Free-surface seam calls (the reference's *FsGpu drivers): the slot's context runs the call
+// with the free surface on and, as those drivers take no sloth flag, without sloth.
+struct SeamFs {
+    Context& c;
+    int fs, sloth;
+    explicit SeamFs(Context& cc) : c(cc), fs(cc.P.freeSurface), sloth(cc.P.sloth) {
+        c.P.freeSurface = 1;
+        c.P.sloth = 0;
+    }
+    ~SeamFs() {
+        c.P.freeSurface = fs;
+        c.P.sloth = sloth;
+    }
+};
+AIO_API int aio_propShotsFwdFsGpu(float* modelRegDtw, float* dataRegDts, int* sp, int ns, int* rp, int nr,
+                                  float* wavefieldDts, int iGpu, int iGpuId) {
+    (void)wavefieldDts; (void)iGpuId;
+    return guard([&] {
+        SeamFs fs(seam_ctx(AIO_NONLINEAR, iGpu));
+        aio_shot s = one_shot(modelRegDtw, sp, ns, rp, nr, dataRegDts);
+        fs.c.nonlinear_forward(1, &s, AIO_MEM_HOST, nullptr);
+    });
+}
+AIO_API int aio_propShotsFwdFsGpuWavefield(float* modelRegDtw, float* dataRegDts, int* sp, int ns, int* rp, int nr,
+                                           float* wavefieldDts, int iGpu, int iGpuId) {
+    (void)iGpuId;
+    return guard([&] {
+        SeamFs fs(seam_ctx(AIO_NONLINEAR, iGpu));
+        aio_shot s = one_shot(modelRegDtw, sp, ns, rp, nr, dataRegDts);
+        fs.c.nonlinear_forward(1, &s, AIO_MEM_HOST, wavefieldDts);
+    });
+}
+AIO_API int aio_propShotsAdjFsGpu(float* modelRegDtw, float* dataRegDts, int* sp, int ns, int* rp, int nr,
+                                  float* wavefieldDts, int iGpu, int iGpuId) {
+    (void)wavefieldDts; (void)iGpuId;
+    return guard([&] {
+        SeamFs fs(seam_ctx(AIO_NONLINEAR, iGpu));
+        aio_shot s = one_shot(nullptr, sp, ns, rp, nr, dataRegDts);
+        s.sourcesOut = modelRegDtw;
+        fs.c.nonlinear_adjoint(1, &s, AIO_MEM_HOST, nullptr);
+    });
+}
+AIO_API int aio_propShotsAdjFsGpuWavefield(float* modelRegDtw, float* dataRegDts, int* sp, int ns, int* rp, int nr,
+                                           float* wavefieldDts, int iGpu, int iGpuId) {
+    (void)iGpuId;
+    return guard([&] {
+        SeamFs fs(seam_ctx(AIO_NONLINEAR, iGpu));
+        aio_shot s = one_shot(nullptr, sp, ns, rp, nr, dataRegDts);
+        s.sourcesOut = modelRegDtw;
+        fs.c.nonlinear_adjoint(1, &s, AIO_MEM_HOST, wavefieldDts);
+    });
+}
+AIO_API int aio_BornShotsFwdFsGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sp, int ns, int* rp,
+                                  int nr, float* srcWavefield, float* scatWavefield, int iGpu, int iGpuId) {
+    (void)srcWavefield; (void)scatWavefield; (void)iGpuId;
+    return guard([&] {
+        SeamFs fs(seam_ctx(AIO_BORN, iGpu));
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
+        fs.c.born_forward(model, 1, &s, AIO_MEM_HOST);
+    });
+}
+AIO_API int aio_BornShotsAdjFsGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sp, int ns, int* rp,
+                                  int nr, float* srcWavefield, float* recWavefield, int iGpu, int iGpuId) {
+    (void)srcWavefield; (void)recWavefield; (void)iGpuId;
+    return guard([&] {
+        SeamFs fs(seam_ctx(AIO_BORN, iGpu));
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
+        fs.c.born_adjoint(model, 0, 1, &s, AIO_MEM_HOST);
+    });
+}
+AIO_API int aio_BornTimeShotsFwdFsGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sp, int ns,
+                                      int* rp, int nr, float* srcWavefield, float* scatWavefield, int iGpu,
+                                      int iGpuId) {
+    (void)srcWavefield; (void)scatWavefield; (void)iGpuId;
+    return guard([&] {
+        SeamFs fs(seam_ctx(AIO_BORN_EXT, iGpu));
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
+        fs.c.born_ext_forward(model, 1, &s, AIO_MEM_HOST);
+    });
+}
+AIO_API int aio_BornTimeShotsAdjFsGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sp, int ns,
+                                      int* rp, int nr, float* srcWavefield, float* recWavefield, int iGpu,
+                                      int iGpuId) {
+    (void)srcWavefield; (void)recWavefield; (void)iGpuId;
+    return guard([&] {
+        SeamFs fs(seam_ctx(AIO_BORN_EXT, iGpu));
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
+        fs.c.born_ext_adjoint(model, 0, 1, &s, AIO_MEM_HOST);
+    });
+}
+AIO_API int aio_tomoTimeShotsFwdFsGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
+                                      int* sp, int ns, int* rp, int nr, float* w0, float* w1, float* w2, int iGpu,
+                                      int iGpuId, int saveWavefield) {
+    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    return guard([&] {
+        require(saveWavefield == 0, "saveWavefield=1 is not available for tomo in this build");
+        SeamFs fs(seam_ctx(AIO_TOMO_EXT, iGpu));
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
+        fs.c.tomo_forward(model, extReflectivity, 1, &s, AIO_MEM_HOST);
+    });
+}
+AIO_API int aio_tomoTimeShotsAdjFsGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
+                                      int* sp, int ns, int* rp, int nr, float* w0, float* w1, float* w2, int iGpu,
+                                      int iGpuId, int saveWavefield) {
+    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    return guard([&] {
+        require(saveWavefield == 0, "saveWavefield=1 is not available for tomo in this build");
+        SeamFs fs(seam_ctx(AIO_TOMO_EXT, iGpu));
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
+        fs.c.tomo_adjoint(model, 0, extReflectivity, 1, &s, AIO_MEM_HOST);
     });
 }
 

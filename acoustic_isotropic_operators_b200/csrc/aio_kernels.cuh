@@ -26,6 +26,11 @@ __device__ __forceinline__ float v2_scaled(float v, const float* __restrict__ v2
 // ADJ=false: n = v2*L(c) + 2c - D*o    (stepFwdGpu,  F/src/kernelsGpu.cu:513-552)
 // ADJ=true : n = L(v2*c) + 2c - D*o    (stepAdjGpu,  F/src/kernelsGpu.cu:574-610)
 // then      S = D * (n + injection), written over o.
+// Free surface (a.fs): forward steps see the current level with its top interior row zeroed
+// and the rows above it mirrored with opposite sign (setFsConditionFwdGpu, :555-567, which
+// the reference applies to the slice in memory before every step, so the old level's top row
+// is zero too); adjoint steps leave the top row at the old value and drop the mirror terms
+// from rows 1-4 (stepAdjFsGpu, :613-740); the taper ignores the top edge (dampCosineEdgeFs).
 // INJ: 0 none, 1 sparse traces (injectSource / interpInjectData, :88-99),
 //      2 dense secondary source ssA*hA + ssB*hB (injectSecondarySource, :102-107).
 // REC: sparse recording of S (recordInterpData / recordSource, :113-127).
@@ -52,16 +57,19 @@ __global__ void __launch_bounds__(TZ* TY) k_step(const StepArgs a) {
     float* __restrict__ old = a.parity ? p0 : p1;
 
     // Stage the current level (times v^2 dtw^2 for the adjoint) with its halo.
+    const bool fsFwd = !ADJ && a.fs && z0 == 0;
     for (int r = ty; r < TX + 2 * FAT; r += TY) {
         const int x = x0 - FAT + r;
         const float* col = cur + (long long)(x + FAT) * g.hp + ZOFF;
         float v = col[z0 + lane];
         if (ADJ) v = v2_scaled(v, a.v2, g, z0 + lane, x);
+        if (fsFwd && lane == 0) v = 0.f;
         s[r][FAT + lane] = v;
         if (lane < 2 * FAT) {
             const int zz = lane < FAT ? z0 - FAT + lane : z0 + TZ + (lane - FAT);
             float hv = col[zz];
             if (ADJ) hv = v2_scaled(hv, a.v2, g, zz, x);
+            if (fsFwd && zz < 0) hv = -col[-zz];
             s[r][lane < FAT ? lane : TZ + lane] = hv;
         }
     }
@@ -83,7 +91,7 @@ __global__ void __launch_bounds__(TZ* TY) k_step(const StepArgs a) {
         if (zi < g.nzi && xi < g.nxi) {
             const long long hidx = (long long)(xi + FAT) * g.hp + ZOFF + zi;
             const long long iidx = (long long)xi * g.ip + zi;
-            ov[j] = old[hidx];
+            ov[j] = (fsFwd && zi == 0) ? 0.f : old[hidx];
             pv[j] = ADJ ? cur[hidx] : __ldg(a.v2 + iidx);
             if (INJ == 2) {
                 sa[j] = ssA[iidx];
@@ -120,18 +128,23 @@ __global__ void __launch_bounds__(TZ* TY) k_step(const StepArgs a) {
 #pragma unroll
     for (int k = 0; k < PX + 2 * FAT; k++) w[k] = s[ty * PX + k][FAT + lane];
 
-    const int dzd = min(zi, g.nzi - 1 - zi);
+    const int dzd = a.fs ? g.nzi - 1 - zi : min(zi, g.nzi - 1 - zi);
     float S[PX];
 #pragma unroll
     for (int j = 0; j < PX; j++) {
         const int xi = xb + j;
         const float* row = s[FAT + ty * PX + j];
         const float c = w[FAT + j];
-        const float lap = a.c.zc[0] * c + a.c.zc[1] * (row[FAT + lane - 1] + row[FAT + lane + 1]) +
-                          a.c.zc[2] * (row[FAT + lane - 2] + row[FAT + lane + 2]) +
-                          a.c.zc[3] * (row[FAT + lane - 3] + row[FAT + lane + 3]) +
-                          a.c.zc[4] * (row[FAT + lane - 4] + row[FAT + lane + 4]) +
-                          a.c.zc[5] * (row[FAT + lane - 5] + row[FAT + lane + 5]) + a.c.xc[0] * c +
+        float lap = a.c.zc[0] * c + a.c.zc[1] * (row[FAT + lane - 1] + row[FAT + lane + 1]) +
+                    a.c.zc[2] * (row[FAT + lane - 2] + row[FAT + lane + 2]) +
+                    a.c.zc[3] * (row[FAT + lane - 3] + row[FAT + lane + 3]) +
+                    a.c.zc[4] * (row[FAT + lane - 4] + row[FAT + lane + 4]) +
+                    a.c.zc[5] * (row[FAT + lane - 5] + row[FAT + lane + 5]);
+        if (ADJ && a.fs && zi >= 1 && zi < FAT) {
+            // rows 1-4: minus zc[k] * (row k - zi) for k = zi+1 .. 5
+            for (int k = zi + 1; k <= 5; k++) lap = lap - a.c.zc[k] * row[FAT + lane + k - 2 * zi];
+        }
+        lap = lap + a.c.xc[0] * c +
                           a.c.xc[1] * (w[FAT + j + 1] + w[FAT + j - 1]) +
                           a.c.xc[2] * (w[FAT + j + 2] + w[FAT + j - 2]) +
                           a.c.xc[3] * (w[FAT + j + 3] + w[FAT + j - 3]) +
@@ -147,7 +160,7 @@ __global__ void __launch_bounds__(TZ* TY) k_step(const StepArgs a) {
             float n;
             if (ADJ) {
                 const float cr = pv[j];
-                n = lap + cr + cr - o;
+                n = (a.fs && zi == 0) ? o : lap + cr + cr - o;
             } else {
                 n = pv[j] * lap + c + c - o;
             }

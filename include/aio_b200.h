@@ -68,6 +68,8 @@ typedef struct {
     int stepper;         /* AIO_STEPPER_*: how Born / nonlinear passes advance time */
     int chunkColumns;    /* blocked stepper x-chunk width: 0 = autotuned (measured once per wave size),
                             > 0 = fixed width (strips of at most 128 rows) */
+    int freeSurface;     /* 1: free surface at the top interior row (reference par freeSurface;
+                            the *FsGpu drivers); runs on the per-fine-step stepper */
 } aio_params;
 
 #define AIO_STEPPER_AUTO 0      /* interval-blocked where available (sub == 4), else per fine step */
@@ -218,6 +220,48 @@ int aio_tomoTimeShotsAdjGpu(float* model, float* dataRegDts, float* extReflectiv
                             int* sourcesPositionReg, int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
                             float* tomoSrcWavefieldDt2, float* tomoSecWavefield1, float* tomoSecWavefield2,
                             int sloth, int iGpu, int iGpuId, int saveWavefield);
+/* Free-surface drivers (reference freeSurface == 1): same arguments as the plain calls of the family;
+ * they run on the per-fine-step stepper with the top interior row as a pressure-free surface. */
+/* F/include/nonlinearShotsGpuFunctions.h:15 */
+int aio_propShotsFwdFsGpu(float* modelRegDtw, float* dataRegDts, int* sourcesPositionReg, int nSourcesReg,
+                          int* receiversPositionReg, int nReceiversReg, float* wavefieldDts, int iGpu, int iGpuId);
+/* F/include/nonlinearShotsGpuFunctions.h:16 */
+int aio_propShotsFwdFsGpuWavefield(float* modelRegDtw, float* dataRegDts, int* sourcesPositionReg, int nSourcesReg,
+                                   int* receiversPositionReg, int nReceiversReg, float* wavefieldDts, int iGpu,
+                                   int iGpuId);
+/* F/include/nonlinearShotsGpuFunctions.h:23 */
+int aio_propShotsAdjFsGpu(float* modelRegDtw, float* dataRegDts, int* sourcesPositionReg, int nSourcesReg,
+                          int* receiversPositionReg, int nReceiversReg, float* wavefieldDts, int iGpu, int iGpuId);
+/* F/include/nonlinearShotsGpuFunctions.h:24 */
+int aio_propShotsAdjFsGpuWavefield(float* modelRegDtw, float* dataRegDts, int* sourcesPositionReg, int nSourcesReg,
+                                   int* receiversPositionReg, int nReceiversReg, float* wavefieldDts, int iGpu,
+                                   int iGpuId);
+/* F/include/BornShotsGpuFunctions.h:20 */
+int aio_BornShotsFwdFsGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                          int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
+                          float* scatWavefield, int iGpu, int iGpuId);
+/* F/include/BornShotsGpuFunctions.h:32 */
+int aio_BornShotsAdjFsGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                          int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
+                          float* recWavefield, int iGpu, int iGpuId);
+/* F/include/BornExtShotsGpuFunctions.h:27 */
+int aio_BornTimeShotsFwdFsGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                              int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
+                              float* scatWavefield, int iGpu, int iGpuId);
+/* F/include/BornExtShotsGpuFunctions.h:49 */
+int aio_BornTimeShotsAdjFsGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                              int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
+                              float* recWavefield, int iGpu, int iGpuId);
+/* F/include/tomoExtShotsGpuFunctions.h:20 */
+int aio_tomoTimeShotsFwdFsGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
+                              int* sourcesPositionReg, int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
+                              float* tomoSrcWavefieldDt2, float* tomoSecWavefield1, float* tomoSecWavefield2,
+                              int iGpu, int iGpuId, int saveWavefield);
+/* F/include/tomoExtShotsGpuFunctions.h:32 */
+int aio_tomoTimeShotsAdjFsGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
+                              int* sourcesPositionReg, int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
+                              float* tomoSrcWavefieldDt2, float* tomoSecWavefield1, float* tomoSecWavefield2,
+                              int iGpu, int iGpuId, int saveWavefield);
 /* F/include/wemvaExtShotsGpuFunctions.h:6-17 (time-lag extension) */
 int aio_initWemvaExtGpu(float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad, int blockSize,
                         float alphaCos, int nExt, int leg1, int leg2, int nGpu, int iGpuId, int iGpuAlloc);

@@ -40,6 +40,7 @@ constexpr int PAD_MAX = 200;  // F/include/varDeclare.h:11
 template <class T>
 struct Grid {
     int nz, nx, nts, sub, ntw, minPad, H, nExt, hExt;
+    int fs = 0;  // free surface at the top interior row (the reference's freeSurface == 1)
     T zc[6], xc[6];
     T h[2 * (SUB_MAX + 1)];
     T taper[PAD_MAX];
@@ -97,10 +98,26 @@ static void make_grid(Grid<T>& g, int nz, int nx, int nts, T dts, int sub, int m
 // iz in [FAT, nz-FAT), ix in [FAT, nx-FAT).
 // ----------------------------------------------------------------------------
 
-// stepFwdGpu, F/src/kernelsGpu.cu:513-552: n = v2*L(c) + 2c - o (n may alias o).
+// setFsConditionFwdGpu, F/src/kernelsGpu.cu:555-567: on every interior column the top
+// interior row of the current slice is set to zero and the FAT rows above it to the negative
+// mirror of the rows below it (applied to the slice in memory before each forward step).
 template <class T>
-static void step_fwd(const Grid<T>& g, T* o, const T* c) {
+static void set_fs_fwd(const Grid<T>& g, T* c) {
     const int nz = g.nz;
+    for (int ix = FAT; ix < g.nx - FAT; ix++) {
+        T* col = c + (size_t)ix * nz;
+        col[FAT] = 0;
+        for (int m = 1; m <= FAT; m++) col[FAT - m] = -col[FAT + m];
+    }
+}
+
+// stepFwdGpu, F/src/kernelsGpu.cu:513-552: n = v2*L(c) + 2c - o (n may alias o); with a free
+// surface the current slice first gets setFsConditionFwdGpu (the reference's drivers launch it
+// before every forward step, e.g. F/src/nonlinearShotsGpuFunctions.cu:446-450).
+template <class T>
+static void step_fwd(const Grid<T>& g, T* o, T* c) {
+    const int nz = g.nz;
+    if (g.fs) set_fs_fwd(g, c);
 #pragma omp parallel for schedule(static)
     for (int ix = FAT; ix < g.nx - FAT; ix++) {
         for (int iz = FAT; iz < nz - FAT; iz++) {
@@ -117,6 +134,8 @@ static void step_fwd(const Grid<T>& g, T* o, const T* c) {
 }
 
 // stepAdjGpu, F/src/kernelsGpu.cu:574-610: o = L(v2*c) + 2c - n (o may alias n).
+// Free surface: stepAdjFsGpu, :613-740 — the top interior row is not updated (it keeps n) and
+// the z-stencil of the next four rows loses the terms the forward mirror condition adds.
 template <class T>
 static void step_adj(const Grid<T>& g, T* o, const T* c, std::vector<T>& tmp) {
     const int nz = g.nz;
@@ -132,9 +151,16 @@ static void step_adj(const Grid<T>& g, T* o, const T* c, std::vector<T>& tmp) {
     for (int ix = FAT; ix < g.nx - FAT; ix++) {
         for (int iz = FAT; iz < nz - FAT; iz++) {
             size_t i = (size_t)ix * nz + iz;
+            if (g.fs && iz == FAT) continue;
             T lap = g.zc[0] * s[i] + g.zc[1] * (s[i - 1] + s[i + 1]) + g.zc[2] * (s[i - 2] + s[i + 2]) +
                     g.zc[3] * (s[i - 3] + s[i + 3]) + g.zc[4] * (s[i - 4] + s[i + 4]) +
-                    g.zc[5] * (s[i - 5] + s[i + 5]) + g.xc[0] * s[i] +
+                    g.zc[5] * (s[i - 5] + s[i + 5]);
+            if (g.fs && iz < 2 * FAT) {
+                // row r = iz - FAT (1..4): minus zc[k] * s[row k - r] for k = r+1 .. 5
+                const int r = iz - FAT;
+                for (int k = r + 1; k <= 5; k++) lap = lap - g.zc[k] * s[i + (k - 2 * r)];
+            }
+            lap = lap + g.xc[0] * s[i] +
                     g.xc[1] * (s[i + nz] + s[i - nz]) + g.xc[2] * (s[i + 2 * nz] + s[i - 2 * nz]) +
                     g.xc[3] * (s[i + 3 * nz] + s[i - 3 * nz]) + g.xc[4] * (s[i + 4 * nz] + s[i - 4 * nz]) +
                     g.xc[5] * (s[i + 5 * nz] + s[i - 5 * nz]);
@@ -143,14 +169,16 @@ static void step_adj(const Grid<T>& g, T* o, const T* c, std::vector<T>& tmp) {
     }
 }
 
-// dampCosineEdge, F/src/kernelsGpu.cu:202-219: both slices scaled within minPad of the interior edge.
+// dampCosineEdge, F/src/kernelsGpu.cu:202-219: both slices scaled within minPad of the interior edge
+// (free surface: dampCosineEdgeFs, :221-239, without the top edge).
 template <class T>
 static void damp(const Grid<T>& g, T* a, T* b) {
     const int nz = g.nz, nx = g.nx;
 #pragma omp parallel for schedule(static)
     for (int ix = FAT; ix < nx - FAT; ix++)
         for (int iz = FAT; iz < nz - FAT; iz++) {
-            int d = std::min(std::min(iz - FAT, ix - FAT), std::min(nz - iz - 1 - FAT, nx - ix - 1 - FAT));
+            int d = std::min(ix - FAT, std::min(nz - iz - 1 - FAT, nx - ix - 1 - FAT));
+            if (!g.fs) d = std::min(d, iz - FAT);
             if (d < g.minPad) {
                 size_t i = (size_t)ix * nz + iz;
                 a[i] *= g.taper[d];
@@ -786,6 +814,7 @@ using namespace orc;
 struct OrcParams {
     int nz, nx, nts, sub, minPad, nExt;
     double dz, dx, dts, alphaCos;
+    int freeSurface;
 };
 
 template <class T>
@@ -793,6 +822,7 @@ static Grid<T> grid_from(const OrcParams* p, const T* vel) {
     Grid<T> g;
     make_grid<T>(g, p->nz, p->nx, p->nts, (T)p->dts, p->sub, p->minPad, (T)p->alphaCos, (T)p->dz, (T)p->dx,
                  p->nExt, vel);
+    g.fs = p->freeSurface;
     return g;
 }
 

@@ -26,7 +26,7 @@ _lib = None
 class OrcParams(C.Structure):
     _fields_ = [("nz", C.c_int), ("nx", C.c_int), ("nts", C.c_int), ("sub", C.c_int),
                 ("minPad", C.c_int), ("nExt", C.c_int), ("dz", C.c_double), ("dx", C.c_double),
-                ("dts", C.c_double), ("alphaCos", C.c_double)]
+                ("dts", C.c_double), ("alphaCos", C.c_double), ("freeSurface", C.c_int)]
 
 
 def build() -> str:
@@ -57,6 +57,7 @@ class Scheme:
     minPad: int
     alphaCos: float = 0.99
     nExt: int = 1
+    freeSurface: int = 0
 
     @property
     def ntw(self) -> int:
@@ -64,7 +65,7 @@ class Scheme:
 
     def c(self) -> OrcParams:
         return OrcParams(self.nz, self.nx, self.nts, self.sub, self.minPad, self.nExt,
-                         self.dz, self.dx, self.dts, self.alphaCos)
+                         self.dz, self.dx, self.dts, self.alphaCos, self.freeSurface)
 
 
 def _suf(dtype) -> str:

@@ -54,6 +54,13 @@ REF_EXPORT int ref_nl_adj(R* modelDtw, R* data, int* sp, int ns, int* rp, int nr
     if (W) { GUARD(propShotsAdjGpuWavefield(modelDtw, data, sp, ns, rp, nr, W, 0, dev)) }
     GUARD(propShotsAdjGpu(modelDtw, data, sp, ns, rp, nr, W, 0, dev))
 }
+// free-surface drivers (F/include/nonlinearShotsGpuFunctions.h:15,23)
+REF_EXPORT int ref_nl_fwd_fs(R* modelDtw, R* data, int* sp, int ns, int* rp, int nr, R* W, int dev) {
+    GUARD(propShotsFwdFsGpu(modelDtw, data, sp, ns, rp, nr, W, 0, dev))
+}
+REF_EXPORT int ref_nl_adj_fs(R* modelDtw, R* data, int* sp, int ns, int* rp, int nr, R* W, int dev) {
+    GUARD(propShotsAdjFsGpu(modelDtw, data, sp, ns, rp, nr, W, 0, dev))
+}
 #elif defined(REF_FAMILY_BORN)
 // F/include/BornShotsGpuFunctions.h:7-33
 REF_EXPORT int ref_init(R dz, R dx, int nz, int nx, int nts, R dts, int sub, int minPad, R alphaCos, int nExt,
@@ -68,6 +75,13 @@ REF_EXPORT int ref_born_fwd(R* model, R* data, R* sig, int* sp, int ns, int* rp,
 }
 REF_EXPORT int ref_born_adj(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
     GUARD(BornShotsAdjGpu(model, data, sig, sp, ns, rp, nr, nullptr, nullptr, 0, dev))
+}
+// free-surface drivers (F/include/BornShotsGpuFunctions.h:20,32)
+REF_EXPORT int ref_born_fwd_fs(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
+    GUARD(BornShotsFwdFsGpu(model, data, sig, sp, ns, rp, nr, nullptr, nullptr, 0, dev))
+}
+REF_EXPORT int ref_born_adj_fs(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
+    GUARD(BornShotsAdjFsGpu(model, data, sig, sp, ns, rp, nr, nullptr, nullptr, 0, dev))
 }
 #elif defined(REF_FAMILY_BORNEXT)
 // F/include/BornExtShotsGpuFunctions.h:6-54
@@ -84,6 +98,13 @@ REF_EXPORT int ref_bornext_fwd(R* model, R* data, R* sig, int* sp, int ns, int* 
 REF_EXPORT int ref_bornext_adj(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, int sloth, int dev) {
     GUARD(BornTimeShotsAdjGpu(model, data, sig, sp, ns, rp, nr, nullptr, nullptr, sloth, 0, dev))
 }
+// free-surface drivers (F/include/BornExtShotsGpuFunctions.h:27,49; no sloth flag)
+REF_EXPORT int ref_bornext_fwd_fs(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
+    GUARD(BornTimeShotsFwdFsGpu(model, data, sig, sp, ns, rp, nr, nullptr, nullptr, 0, dev))
+}
+REF_EXPORT int ref_bornext_adj_fs(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
+    GUARD(BornTimeShotsAdjFsGpu(model, data, sig, sp, ns, rp, nr, nullptr, nullptr, 0, dev))
+}
 #elif defined(REF_FAMILY_TOMO)
 // F/include/tomoExtShotsGpuFunctions.h:6-33
 REF_EXPORT int ref_init(R dz, R dx, int nz, int nx, int nts, R dts, int sub, int minPad, R alphaCos, int nExt,
@@ -99,6 +120,13 @@ REF_EXPORT int ref_tomo_fwd(R* model, R* data, R* ext, R* sig, int* sp, int ns, 
 REF_EXPORT int ref_tomo_adj(R* model, R* data, R* ext, R* sig, int* sp, int ns, int* rp, int nr, int sloth,
                             int dev) {
     GUARD(tomoTimeShotsAdjGpu(model, data, ext, sig, sp, ns, rp, nr, nullptr, nullptr, nullptr, sloth, 0, dev, 0))
+}
+// free-surface drivers (F/include/tomoExtShotsGpuFunctions.h:20,32; no sloth flag)
+REF_EXPORT int ref_tomo_fwd_fs(R* model, R* data, R* ext, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
+    GUARD(tomoTimeShotsFwdFsGpu(model, data, ext, sig, sp, ns, rp, nr, nullptr, nullptr, nullptr, 0, dev, 0))
+}
+REF_EXPORT int ref_tomo_adj_fs(R* model, R* data, R* ext, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
+    GUARD(tomoTimeShotsAdjFsGpu(model, data, ext, sig, sp, ns, rp, nr, nullptr, nullptr, nullptr, 0, dev, 0))
 }
 #elif defined(REF_FAMILY_WEMVA)
 // F/include/wemvaExtShotsGpuFunctions.h:6-17

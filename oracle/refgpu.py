@@ -4,7 +4,8 @@ sm_100a (built by ``make -C oracle ref`` from the reference sources).
 TEST INFRASTRUCTURE ONLY (parity checker). Each operator family is a separate
 shared library because the reference keeps its state in per-translation-unit
 globals. Every call here runs one shot through the reference's own free
-functions: init -> allocate -> fwd/adj -> deallocate.
+functions: init -> allocate -> fwd/adj -> deallocate. A scheme with freeSurface = 1 runs the
+reference's free-surface drivers (*FsGpu; the time-lag ones take no sloth flag).
 """
 from __future__ import annotations
 
@@ -58,6 +59,10 @@ def _run(family, s, vel, dtype, call, nExt=1, leg1=1, leg2=1, device=0):
     return out
 
 
+def _fs(s):
+    return bool(getattr(s, "freeSurface", 0))
+
+
 def _i(a):
     return np.ascontiguousarray(a, np.int32)
 
@@ -70,7 +75,8 @@ def nl_fwd(s, vel, model_dtw, sp, rp, dtype=np.float32):
     sp, rp = _i(sp), _i(rp)
     m = _a(model_dtw, dtype)
     d = np.zeros((len(rp), s.nts), dtype)
-    _run("nl", s, vel, dtype, lambda L: L.ref_nl_fwd(_p(m), _p(d), _p(sp), len(sp), _p(rp), len(rp), None, 0))
+    _run("nl", s, vel, dtype, lambda L: (L.ref_nl_fwd_fs if _fs(s) else L.ref_nl_fwd)(
+        _p(m), _p(d), _p(sp), len(sp), _p(rp), len(rp), None, 0))
     return d
 
 
@@ -78,7 +84,8 @@ def nl_adj(s, vel, data, sp, rp, dtype=np.float32):
     sp, rp = _i(sp), _i(rp)
     d = _a(data, dtype)
     m = np.zeros((len(sp), s.ntw), dtype)
-    _run("nl", s, vel, dtype, lambda L: L.ref_nl_adj(_p(m), _p(d), _p(sp), len(sp), _p(rp), len(rp), None, 0))
+    _run("nl", s, vel, dtype, lambda L: (L.ref_nl_adj_fs if _fs(s) else L.ref_nl_adj)(
+        _p(m), _p(d), _p(sp), len(sp), _p(rp), len(rp), None, 0))
     return m
 
 
@@ -86,7 +93,8 @@ def born_fwd(s, vel, model, sig, sp, rp, dtype=np.float32):
     sp, rp = _i(sp), _i(rp)
     m, g = _a(model, dtype), _a(sig, dtype)
     d = np.zeros((len(rp), s.nts), dtype)
-    _run("born", s, vel, dtype, lambda L: L.ref_born_fwd(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0))
+    _run("born", s, vel, dtype, lambda L: (L.ref_born_fwd_fs if _fs(s) else L.ref_born_fwd)(
+        _p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0))
     return d
 
 
@@ -94,7 +102,8 @@ def born_adj(s, vel, data, sig, sp, rp, dtype=np.float32):
     sp, rp = _i(sp), _i(rp)
     d, g = _a(data, dtype), _a(sig, dtype)
     m = np.zeros((s.nx, s.nz), dtype)
-    _run("born", s, vel, dtype, lambda L: L.ref_born_adj(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0))
+    _run("born", s, vel, dtype, lambda L: (L.ref_born_adj_fs if _fs(s) else L.ref_born_adj)(
+        _p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0))
     return m
 
 
@@ -103,7 +112,8 @@ def bornext_fwd(s, vel, model, sig, sp, rp, sloth=0, dtype=np.float32):
     m, g = _a(model, dtype), _a(sig, dtype)
     d = np.zeros((len(rp), s.nts), dtype)
     _run("bornext", s, vel, dtype,
-         lambda L: L.ref_bornext_fwd(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), sloth, 0), nExt=s.nExt)
+         lambda L: L.ref_bornext_fwd_fs(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0) if _fs(s) else
+         L.ref_bornext_fwd(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), sloth, 0), nExt=s.nExt)
     return d
 
 
@@ -112,7 +122,8 @@ def bornext_adj(s, vel, data, sig, sp, rp, sloth=0, dtype=np.float32):
     d, g = _a(data, dtype), _a(sig, dtype)
     m = np.zeros((s.nExt, s.nx, s.nz), dtype)
     _run("bornext", s, vel, dtype,
-         lambda L: L.ref_bornext_adj(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), sloth, 0), nExt=s.nExt)
+         lambda L: L.ref_bornext_adj_fs(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0) if _fs(s) else
+         L.ref_bornext_adj(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), sloth, 0), nExt=s.nExt)
     return m
 
 
@@ -121,7 +132,8 @@ def tomo_fwd(s, vel, model, ext, sig, sp, rp, sloth=0, leg1=1, leg2=1, dtype=np.
     m, e, g = _a(model, dtype), _a(ext, dtype), _a(sig, dtype)
     d = np.zeros((len(rp), s.nts), dtype)
     _run("tomo", s, vel, dtype,
-         lambda L: L.ref_tomo_fwd(_p(m), _p(d), _p(e), _p(g), _p(sp), len(sp), _p(rp), len(rp), sloth, 0),
+         lambda L: L.ref_tomo_fwd_fs(_p(m), _p(d), _p(e), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0) if _fs(s) else
+         L.ref_tomo_fwd(_p(m), _p(d), _p(e), _p(g), _p(sp), len(sp), _p(rp), len(rp), sloth, 0),
          nExt=s.nExt, leg1=leg1, leg2=leg2)
     return d
 
@@ -131,7 +143,8 @@ def tomo_adj(s, vel, data, ext, sig, sp, rp, sloth=0, leg1=1, leg2=1, dtype=np.f
     d, e, g = _a(data, dtype), _a(ext, dtype), _a(sig, dtype)
     m = np.zeros((s.nx, s.nz), dtype)
     _run("tomo", s, vel, dtype,
-         lambda L: L.ref_tomo_adj(_p(m), _p(d), _p(e), _p(g), _p(sp), len(sp), _p(rp), len(rp), sloth, 0),
+         lambda L: L.ref_tomo_adj_fs(_p(m), _p(d), _p(e), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0) if _fs(s) else
+         L.ref_tomo_adj(_p(m), _p(d), _p(e), _p(g), _p(sp), len(sp), _p(rp), len(rp), sloth, 0),
          nExt=s.nExt, leg1=leg1, leg2=leg2)
     return m
 

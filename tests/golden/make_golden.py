@@ -11,6 +11,8 @@ test suite pin the CPU oracle against the reference without a GPU
 Run on a machine with a B200 and the oracle/_ref libraries built:
 
     python tests/golden/make_golden.py OUT.npz
+    python tests/golden/make_golden.py --fs OUT_FS.npz   # free-surface drivers (*FsGpu) ->
+                                                          # tests/golden/reference_small_fs.npz
 
 Every input is generated here from fixed seeds and stored in the file too, so
 the test does not depend on this script's random streams.
@@ -32,15 +34,18 @@ from cases import interior_mask, make_case  # noqa: E402
 CASE = dict(seed=11, nzi=32, nxi=48, nts=30, sub=3, nExt=5, minPad=8, nshots=1)
 
 
-def main(out):
+def main(out, fs=False):
     assert CASE["nzi"] % 16 == 0 and CASE["nxi"] % 16 == 0
     c = make_case(**CASE)
     s = c.scheme
+    if fs:
+        import dataclasses
+        s = dataclasses.replace(s, freeSurface=1)
     rng = np.random.default_rng(1234)
     mask = interior_mask(c.nx, c.nz)
     sp, rp, sig = c.src_pos[0], c.rec_pos[0], c.sig[0]
     f = dict(vel=c.vel, src_pos=sp, rec_pos=rp, sig=sig,
-             scheme=np.array([s.nz, s.nx, s.nts, s.sub, s.minPad, s.nExt], np.int64),
+             scheme=np.array([s.nz, s.nx, s.nts, s.sub, s.minPad, s.nExt, s.freeSurface], np.int64),
              scheme_f=np.array([s.dz, s.dx, s.dts, s.alphaCos], np.float64))
     f["data_in"] = (rng.standard_normal((len(rp), s.nts)) * 1e-3).astype(np.float32)
     f["dm"] = (rng.standard_normal((c.nx, c.nz)) * mask).astype(np.float32)
@@ -49,6 +54,19 @@ def main(out):
     f["rdata"] = (rng.standard_normal((len(rp), s.nts)) * 1e-3).astype(np.float32)
     for dt, tag in ((np.float32, "f32"), (np.float64, "f64")):
         v = c.vel.astype(dt)
+        if fs:  # the reference has free-surface drivers for these families (no sloth flag, no WEMVA)
+            f[f"nl_fwd_{tag}"] = refgpu.nl_fwd(s, v, sig, sp, rp, dtype=dt)
+            f[f"nl_adj_{tag}"] = refgpu.nl_adj(s, v, f["data_in"], sp, rp, dtype=dt)
+            f[f"born_fwd_{tag}"] = refgpu.born_fwd(s, v, f["dm"], sig, sp, rp, dtype=dt)
+            f[f"born_adj_{tag}"] = refgpu.born_adj(s, v, f["data_in"], sig, sp, rp, dtype=dt)
+            f[f"bornext_fwd_{tag}"] = refgpu.bornext_fwd(s, v, f["ext"], sig, sp, rp, dtype=dt)
+            f[f"bornext_adj_{tag}"] = refgpu.bornext_adj(s, v, f["data_in"], sig, sp, rp, dtype=dt)
+            for l1, l2 in ((1, 1), (1, 0), (0, 1)):
+                k = f"l{l1}{l2}_{tag}"
+                f["tomo_fwd_" + k] = refgpu.tomo_fwd(s, v, f["dm"], f["ext"], sig, sp, rp, leg1=l1, leg2=l2, dtype=dt)
+                f["tomo_adj_" + k] = refgpu.tomo_adj(s, v, f["data_in"], f["ext"], sig, sp, rp, leg1=l1, leg2=l2,
+                                                     dtype=dt)
+            continue
         f[f"nl_fwd_{tag}"] = refgpu.nl_fwd(s, v, sig, sp, rp, dtype=dt)
         f[f"nl_adj_{tag}"] = refgpu.nl_adj(s, v, f["data_in"], sp, rp, dtype=dt)
         f[f"born_fwd_{tag}"] = refgpu.born_fwd(s, v, f["dm"], sig, sp, rp, dtype=dt)
@@ -72,4 +90,6 @@ def main(out):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(HERE, "reference_small.npz"))
+    args = [a for a in sys.argv[1:] if a != "--fs"]
+    fs = "--fs" in sys.argv[1:]
+    main(args[0] if args else os.path.join(HERE, "reference_small_fs.npz" if fs else "reference_small.npz"), fs)

@@ -25,12 +25,17 @@ pytestmark = pytest.mark.skipif(not os.path.exists(GOLD), reason="golden fixture
 
 @pytest.fixture(scope="module")
 def g():
-    z = np.load(GOLD)
+    return _load(GOLD)
+
+
+def _load(path):
+    z = np.load(path)
     f = {k: z[k] for k in z.files}
-    nz, nx, nts, sub, minPad, nExt = (int(v) for v in f["scheme"])
+    nz, nx, nts, sub, minPad, nExt = (int(v) for v in f["scheme"][:6])
+    fs = int(f["scheme"][6]) if len(f["scheme"]) > 6 else 0
     dz, dx, dts, alpha = (float(v) for v in f["scheme_f"])
     f["s"] = orc.Scheme(nz=nz, nx=nx, nts=nts, dts=dts, sub=sub, dz=dz, dx=dx, minPad=minPad, nExt=nExt,
-                        alphaCos=alpha)
+                        alphaCos=alpha, freeSurface=fs)
     return f
 
 
@@ -96,3 +101,32 @@ def test_fixture_is_nontrivial(g):
     for k, a in g.items():
         if k.endswith(("_f32", "_f64")):
             assert np.abs(a).max() > 0, k
+
+
+GOLD_FS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_small_fs.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(GOLD_FS), reason="free-surface fixtures not generated")
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+def test_free_surface(tag):
+    """Oracle with freeSurface = 1 vs the reference's free-surface drivers (*FsGpu) run on a B200:
+    nonlinear, Born, extended Born and tomo (all legs), forward and adjoint."""
+    g = _load(GOLD_FS)
+    s, v, dt = g["s"], g["vel"].astype(DT[tag]), DT[tag]
+    assert s.freeSurface == 1
+    sp, rp, sig = g["src_pos"], g["rec_pos"], g["sig"]
+    checks = [
+        (orc.nl_fwd(s, v, sig, sp, rp, dtype=dt), "nl_fwd"),
+        (orc.nl_adj(s, v, g["data_in"], sp, rp, dtype=dt), "nl_adj"),
+        (orc.born_fwd(s, v, g["dm"], sig, sp, rp, dtype=dt), "born_fwd"),
+        (orc.born_adj(s, v, g["data_in"], sig, sp, rp, dtype=dt), "born_adj"),
+        (orc.bornext_fwd(s, v, g["ext"], sig, sp, rp, dtype=dt), "bornext_fwd"),
+        (orc.bornext_adj(s, v, g["data_in"], sig, sp, rp, dtype=dt), "bornext_adj"),
+    ]
+    for l1, l2 in ((1, 1), (1, 0), (0, 1)):
+        checks.append((orc.tomo_fwd(s, v, g["dm"], g["ext"], sig, sp, rp, dtype=dt, leg1=l1, leg2=l2),
+                       f"tomo_fwd_l{l1}{l2}"))
+        checks.append((orc.tomo_adj(s, v, g["data_in"], g["ext"], sig, sp, rp, dtype=dt, leg1=l1, leg2=l2),
+                       f"tomo_adj_l{l1}{l2}"))
+    for got, key in checks:
+        assert rel_l2(got, g[f"{key}_{tag}"]) < TOL[tag], key
