@@ -278,8 +278,11 @@ constexpr int LAG_K = 32;
 constexpr int LAG_B = 8;
 constexpr int LAG_NP = 128;  // threads per block (points), a compile-time shared-memory stride
 __host__ __device__ constexpr int lag_window_len(int hExt) { return LAG_K + 4 * hExt; }
-// W slices tlo-2h .. of point p into this thread's shared column, zero outside [0, nts)
-__device__ __forceinline__ void lag_window(float* Ws, const float* __restrict__ W, long long isz, long long p, int tlo,
+// W slices tlo-2h .. of point p into this thread's shared column, zero outside [0, nts). The
+// column holds consecutive samples in pairs (one float2 per pair): every lag offset 2h - 2(e-h)
+// is even, so sample pairs (k, k+1) of any lag are one aligned float2 and the inner products
+// run on paired FP32 instructions.
+__device__ __forceinline__ void lag_window(float2* W2, const float* __restrict__ W, long long isz, long long p, int tlo,
                                            int hExt, int nts) {
     const int n = lag_window_len(hExt), t0 = tlo - 2 * hExt;
     for (int k0 = 0; k0 < n; k0 += 2 * LAG_B) {
@@ -290,8 +293,8 @@ __device__ __forceinline__ void lag_window(float* Ws, const float* __restrict__ 
             v[j] = (k0 + j < n && tau >= 0 && tau < nts) ? __ldg(W + (long long)tau * isz + p) : 0.f;
         }
 #pragma unroll
-        for (int j = 0; j < 2 * LAG_B; j++)
-            if (k0 + j < n) Ws[(k0 + j) * LAG_NP] = v[j];
+        for (int j = 0; j < 2 * LAG_B; j += 2)
+            if (k0 + j < n) W2[((k0 + j) >> 1) * LAG_NP] = make_float2(v[j], v[j + 1]);
     }
 }
 template <typename Acc>
@@ -299,29 +302,36 @@ __global__ void __launch_bounds__(LAG_NP) k_img_lag_block(Acc* __restrict__ img,
                                                           long long rSt, int rRing, const float* __restrict__ W,
                                                           long long WSt, long long isz, int tlo, int thi, int nts,
                                                           int hExt, int nExt, int sign) {
-    extern __shared__ float lag_smem[];
+    extern __shared__ float2 lag_smem2[];
     const int b = blockIdx.y, tid = threadIdx.x;
     const long long p = (long long)blockIdx.x * LAG_NP + tid;
     if (p >= isz) return;
     R += b * rSt;
     W += b * WSt;
     img += b * mSt;
-    float* Ws = lag_smem + tid;
-    lag_window(Ws, W, isz, p, tlo, hExt, nts);
-    float r[LAG_K];
+    float2* W2 = lag_smem2 + tid;
+    lag_window(W2, W, isz, p, tlo, hExt, nts);
+    float2 r2[LAG_K / 2];
+    int slot = tlo % rRing;  // ring slot of sample tlo; the block's slots follow with one wrap at most
 #pragma unroll
-    for (int k = 0; k < LAG_K; k++) r[k] = (tlo + k <= thi) ? __ldg(R + (long long)((tlo + k) % rRing) * isz + p) : 0.f;
+    for (int k = 0; k < LAG_K; k += 2) {
+        const float ra = (tlo + k <= thi) ? __ldg(R + (long long)slot * isz + p) : 0.f;
+        slot = slot + 1 == rRing ? 0 : slot + 1;
+        const float rb = (tlo + k + 1 <= thi) ? __ldg(R + (long long)slot * isz + p) : 0.f;
+        slot = slot + 1 == rRing ? 0 : slot + 1;
+        r2[k >> 1] = make_float2(ra, rb);
+    }
     for (int e0 = 0; e0 < nExt; e0 += LAG_B) {
         float acc[LAG_B];
 #pragma unroll
         for (int j = 0; j < LAG_B; j++) {
             // W index of sample k at lag e: tlo + k - sign 2(e-h), window offset 2h - sign 2(e-h)
             const int e = min(e0 + j, nExt - 1);
-            const float* w = Ws + (2 * hExt - sign * 2 * (e - hExt)) * LAG_NP;
-            float sum = 0.f;
+            const float2* w = W2 + ((2 * hExt - sign * 2 * (e - hExt)) >> 1) * LAG_NP;
+            float2 sum = make_float2(0.f, 0.f);  // even and odd samples of the block
 #pragma unroll
-            for (int k = 0; k < LAG_K; k++) sum += r[k] * w[k * LAG_NP];
-            acc[j] = sum;
+            for (int kp = 0; kp < LAG_K / 2; kp++) sum = __ffma2_rn(r2[kp], w[kp * LAG_NP], sum);
+            acc[j] = sum.x + sum.y;
         }
         Acc old[LAG_B];
 #pragma unroll
@@ -339,22 +349,22 @@ __global__ void __launch_bounds__(LAG_NP) k_img_lag_block(Acc* __restrict__ img,
 // written to a ring of ring slices (slot t % ring). One thread per point; the W slices of
 // the block live in shared memory (own column only, zero outside [0, nts)), so W is read once
 // per block, and ext once per block (lags outer, the block's samples accumulated in registers,
-// in lag order).
+// in lag order, two samples per paired instruction).
 __global__ void __launch_bounds__(LAG_NP) k_ss_lag_block(float* __restrict__ ss, long long ssSt, int ring,
                                                          const float* __restrict__ ext, const float* __restrict__ W,
                                                          long long WSt, long long isz, int tlo, int thi, int nts,
                                                          int hExt, int nExt, int sign) {
-    extern __shared__ float lag_smem[];
+    extern __shared__ float2 lag_smem2[];
     const int b = blockIdx.y, tid = threadIdx.x;
     const long long p = (long long)blockIdx.x * LAG_NP + tid;
     if (p >= isz) return;
     ss += b * ssSt;
     W += b * WSt;
-    float* Ws = lag_smem + tid;
-    lag_window(Ws, W, isz, p, tlo, hExt, nts);
-    float acc[LAG_K];
+    float2* W2 = lag_smem2 + tid;
+    lag_window(W2, W, isz, p, tlo, hExt, nts);
+    float2 acc[LAG_K / 2];
 #pragma unroll
-    for (int k = 0; k < LAG_K; k++) acc[k] = 0.f;
+    for (int k = 0; k < LAG_K / 2; k++) acc[k] = make_float2(0.f, 0.f);
     for (int e0 = 0; e0 < nExt; e0 += LAG_B) {
         float x[LAG_B];
 #pragma unroll
@@ -363,15 +373,21 @@ __global__ void __launch_bounds__(LAG_NP) k_ss_lag_block(float* __restrict__ ss,
         for (int j = 0; j < LAG_B; j++) {
             if (e0 + j < nExt) {
                 const int e = e0 + j;
-                const float* w = Ws + (2 * hExt - sign * 2 * (e - hExt)) * LAG_NP;
+                const float2* w = W2 + ((2 * hExt - sign * 2 * (e - hExt)) >> 1) * LAG_NP;
+                const float2 xx = make_float2(x[j], x[j]);
 #pragma unroll
-                for (int k = 0; k < LAG_K; k++) acc[k] += x[j] * w[k * LAG_NP];
+                for (int kp = 0; kp < LAG_K / 2; kp++) acc[kp] = __ffma2_rn(xx, w[kp * LAG_NP], acc[kp]);
             }
         }
     }
+    int slot = tlo % ring;  // ring slot of sample tlo; the block's slots follow with one wrap at most
 #pragma unroll
-    for (int k = 0; k < LAG_K; k++)
-        if (tlo + k <= thi) ss[(long long)((tlo + k) % ring) * isz + p] = acc[k];
+    for (int k = 0; k < LAG_K; k += 2) {
+        if (tlo + k <= thi) ss[(long long)slot * isz + p] = acc[k >> 1].x;
+        slot = slot + 1 == ring ? 0 : slot + 1;
+        if (tlo + k + 1 <= thi) ss[(long long)slot * isz + p] = acc[k >> 1].y;
+        slot = slot + 1 == ring ? 0 : slot + 1;
+    }
 }
 
 // Scalings (F/src/kernelsGpu.cu:246-252, 278-303). mode 0: m *= v2*rs;
