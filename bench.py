@@ -70,6 +70,9 @@ def parse():
                     help="instead of the Born step: time the extended tomo and WEMVA operators (nExt=41) of N "
                          "shots on the 800x3000 grid (912x3104 interior) and print that line")
     ap.add_argument("--tomo-nts", type=int, default=3000)
+    ap.add_argument("--nl", action="store_true",
+                    help="instead of the Born step: time the nonlinear forward of one shot on the 200x400 grid "
+                         "(304x512 interior, nts=1000) per call and print that line")
     ap.add_argument("--plain", type=int, default=0,
                     help="instead of the batched step: time N shots one per call on the per-fine-step "
                          "stepper (the reference's schedule), FP32, and print that line")
@@ -319,6 +322,43 @@ def run_tomo(args):
     return 0
 
 
+def run_nl(args):
+    """Nonlinear forward of one shot on the 200x400 physical grid with Gaussian blobs (304x512
+    interior, nts = 1000, 400 receivers), one call per shot through the C ABI with host buffers:
+    the latency-bound single-shot case (its three state slices fit in L2)."""
+    import torch
+    from acoustic_isotropic_operators_b200 import _capi, synthetic as S
+    from acoustic_isotropic_operators_b200.batch import Context, Shot
+    w = S.nonlinear_workload()
+    lib = _capi.lib()
+    v2 = np.zeros(w.nz * w.nx, np.float32)
+    rs = np.zeros_like(v2)
+    velf = np.ascontiguousarray(w.vel.reshape(-1), np.float32)
+    lib.aio_fd_precompute(w.nz, w.nx, C.c_float(w.dts), w.sub, velf.ctypes.data_as(C.c_void_p),
+                          v2.ctypes.data_as(C.c_void_p), rs.ctypes.data_as(C.c_void_p))
+    sig = prepare_signals(w, lib)[0]
+    shot = Shot(w.shots[0].src_pos, w.shots[0].rec_pos, sig)
+    out = {}
+    for stepper in ("auto", "fine"):
+        ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs, stepper=stepper)
+        for _ in range(3):
+            ctx.nonlinear_forward([shot])
+        torch.cuda.synchronize()
+        reps = 10
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            ctx.nonlinear_forward([shot])
+        t = (time.perf_counter() - t0) / reps
+        out["blocked" if stepper == "auto" else "per_fine_step"] = {
+            "seconds_per_call": t, "Gpts_s": w.n_interior * w.fine_steps / t / 1e9}
+        ctx.close()
+    print(json.dumps({"impl": "this engine, nonlinear forward, one shot per call (host buffers)",
+                      "metric": "Gpts/s, nonlinear forward", "unit": UNIT, "value": out["blocked"]["Gpts_s"],
+                      "steppers": out, "interior": [w.nz - 10, w.nx - 10], "nts": w.nts, "sub": w.sub,
+                      "receivers": len(w.shots[0].rec_pos), "data": "synthetic (seeded)"}))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -329,6 +369,8 @@ def main():
         return run_ext(args)
     if args.tomo:
         return run_tomo(args)
+    if args.nl:
+        return run_nl(args)
 
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -6,6 +6,7 @@ shot loop does. Prints one JSON line (Gpts/s over the 4 propagation passes and
 shots/s). Run on a GPU machine with oracle/_ref built:
 
     python tests/measure_reference_gpu.py [--nts 2000] [--repeats 2]
+    python tests/measure_reference_gpu.py --nl     # nonlinear forward, 1 shot, 304x512 interior, nts=1000
 """
 import argparse
 import json
@@ -25,11 +26,42 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--nts", type=int, default=2000)
     ap.add_argument("--repeats", type=int, default=2)
+    ap.add_argument("--nl", action="store_true")
     a = ap.parse_args()
     import orc
     import refgpu
     import bench
     from acoustic_isotropic_operators_b200 import _capi, synthetic as S
+    if a.nl:
+        w = S.nonlinear_workload()
+        sig = bench.prepare_signals(w, _capi.lib())[0]
+        sh = w.shots[0]
+        s = orc.Scheme(nz=w.nz, nx=w.nx, nts=w.nts, dts=w.dts, sub=w.sub, dz=w.dz, dx=w.dx, minPad=w.minPad)
+        # init + allocate once (per operator, as the reference's shot loop does), then time the
+        # per-shot driver call, which allocates, copies and frees its own shot buffers
+        import ctypes as C
+        L = refgpu._lib("nl", np.float32)
+        k = orc.constants(s, w.vel, dtype=np.float32)
+        v2 = np.ascontiguousarray(k["v2"], np.float32)
+        assert L.ref_init(s.dz, s.dx, s.nz, s.nx, s.nts, s.dts, s.sub, s.minPad, s.alphaCos, 1, 1, 1, 0) == 0
+        assert L.ref_allocate(v2.ctypes.data_as(C.c_void_p), None, 0) == 0
+        sp = np.ascontiguousarray(sh.src_pos, np.int32)
+        rp = np.ascontiguousarray(sh.rec_pos, np.int32)
+        m = np.ascontiguousarray(sig, np.float32)
+        d = np.zeros((len(rp), s.nts), np.float32)
+        P = lambda x: x.ctypes.data_as(C.c_void_p)
+        times = []
+        for _ in range(a.repeats + 3):
+            t0 = time.perf_counter()
+            assert L.ref_nl_fwd(P(m), P(d), P(sp), len(sp), P(rp), len(rp), None, 0) == 0
+            times.append(time.perf_counter() - t0)
+        L.ref_deallocate(0)
+        t = float(np.mean(times[3:]))
+        print(json.dumps({"impl": "reference-gpu (own sm_100a build, one shot per call)",
+                          "workload": "nonlinear forward, 1 shot, %dx%d interior, nts=%d" % (w.nz - 10, w.nx - 10,
+                                                                                             w.nts),
+                          "seconds_per_shot": t, "gpts_per_s": w.n_interior * w.fine_steps / t / 1e9}))
+        return
     w = S.born_workload(nshots=1, nts=a.nts)
     sig = bench.prepare_signals(w, _capi.lib())[0]
     sh = w.shots[0]
