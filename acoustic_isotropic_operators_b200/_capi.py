@@ -51,6 +51,10 @@ EXPORTED = [
     "aio_propShotsAdjFsGpuWavefield", "aio_BornShotsFwdFsGpu", "aio_BornShotsAdjFsGpu",
     "aio_BornTimeShotsFwdFsGpu", "aio_BornTimeShotsAdjFsGpu", "aio_tomoTimeShotsFwdFsGpu",
     "aio_tomoTimeShotsAdjFsGpu",
+    "aio_BornOffsetShotsFwdGpu", "aio_BornOffsetShotsAdjGpu", "aio_BornOffsetShotsFwdFsGpu",
+    "aio_BornOffsetShotsAdjFsGpu", "aio_tomoOffsetShotsFwdGpu", "aio_tomoOffsetShotsAdjGpu",
+    "aio_tomoOffsetShotsFwdFsGpu", "aio_tomoOffsetShotsAdjFsGpu", "aio_wemvaOffsetShotsFwdGpu",
+    "aio_wemvaOffsetShotsAdjGpu",
 ]
 
 
@@ -60,7 +64,7 @@ class AioParams(C.Structure):
                 ("alphaCos", C.c_float), ("leg1", C.c_int), ("leg2", C.c_int), ("sloth", C.c_int),
                 ("wavefieldPrecision", C.c_int), ("imageFp64", C.c_int), ("device", C.c_int),
                 ("memBudgetBytes", C.c_longlong), ("stepper", C.c_int), ("chunkColumns", C.c_int),
-                ("freeSurface", C.c_int)]
+                ("freeSurface", C.c_int), ("extension", C.c_int)]
 
 
 class AioShot(C.Structure):

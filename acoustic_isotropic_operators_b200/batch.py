@@ -47,13 +47,14 @@ class Context:
 
     def __init__(self, nz, nx, nts, dts, sub, dz, dx, minPad, vel2Dtw2, reflectivity_scale=None, *, nExt=1,
                  alphaCos=0.99, leg1=1, leg2=1, sloth=0, wavefield="fp32", image_fp64=False, device=0,
-                 mem_budget_bytes=0, stepper="auto", chunk_columns=0, free_surface=0):
+                 mem_budget_bytes=0, stepper="auto", chunk_columns=0, free_surface=0, extension="time"):
         self.nz, self.nx, self.nts, self.sub, self.nExt = nz, nx, nts, sub, nExt
         self.ntw = (nts - 1) * sub + 1
         p = A.AioParams(nz, nx, nts, sub, minPad, nExt, dz, dx, dts, alphaCos, leg1, leg2, sloth,
                         _WFLD[wavefield], int(bool(image_fp64)), device, int(mem_budget_bytes),
                         {"auto": A.AIO_STEPPER_AUTO, "fine": A.AIO_STEPPER_FINE,
-                         "blocked": A.AIO_STEPPER_BLOCKED}[stepper], int(chunk_columns), int(free_surface))
+                         "blocked": A.AIO_STEPPER_BLOCKED}[stepper], int(chunk_columns), int(free_surface),
+                        {"time": 0, "offset": 1}[extension])
         v2 = np.ascontiguousarray(vel2Dtw2, dtype=np.float32).reshape(-1)
         rs = None if reflectivity_scale is None else np.ascontiguousarray(reflectivity_scale,
                                                                           dtype=np.float32).reshape(-1)

@@ -217,8 +217,6 @@ class fdParam {
         if (_nExt % 2 == 0) aio_ops::fail("Length of extended axis must be an uneven number");
         _hExt = (_nExt - 1) / 2;
         _extension = par->getString("extension", "none");
-        if (_nExt > 1 && _extension == "offset")
-            aio_ops::fail("subsurface-offset extension is not available in this build (time-lag extension is)");
         _fMax = par->getFloat("fMax", 1000.0f);
         _blockSize = par->getInt("blockSize");
         _fat = par->getInt("fat");
@@ -293,6 +291,9 @@ class fdParam {
         p.stepper = AIO_STEPPER_AUTO;
         p.chunkColumns = 0;
         p.freeSurface = _freeSurface;
+        // the extended classes run their time-lag drivers for "time" and the subsurface-offset ones
+        // otherwise (F/src/BornExtGpu.cpp:41-59, the same branch in tomoExtGpu.cpp and wemvaExtGpu.cpp)
+        p.extension = _extension == "time" ? AIO_EXT_TIME : AIO_EXT_OFFSET;
         return p;
     }
 

@@ -198,6 +198,10 @@ struct Context {
         require(p.stepper >= AIO_STEPPER_AUTO && p.stepper <= AIO_STEPPER_BLOCKED, "unknown stepper");
         require(p.stepper < AIO_STEPPER_BLOCKED || p.sub == 4, "the interval-blocked steppers require sub == 4");
         require(p.freeSurface == 0 || p.freeSurface == 1, "freeSurface must be 0 or 1");
+        require(p.extension == AIO_EXT_TIME || p.extension == AIO_EXT_OFFSET,
+                "extension must be AIO_EXT_TIME or AIO_EXT_OFFSET");
+        require(p.extension != AIO_EXT_OFFSET || 2 * ((p.nExt - 1) / 2) < p.nx - 2 * FAT,
+                "subsurface offsets longer than the interior width");
         require(!(p.freeSurface && p.stepper == AIO_STEPPER_BLOCKED),
                 "the free surface runs on the per-fine-step stepper (stepper AUTO or FINE)");
         require(p.wavefieldPrecision == AIO_WFLD_FP32 || (p.stepper != AIO_STEPPER_FINE && p.sub == 4),
@@ -715,6 +719,43 @@ struct Context {
             k_img_time_adj<float><<<ew_grid(nb, g.isz), 256, 0, st>>>(img.as<float>(), mSt, ring_ptr(slot), pairSt(),
                                                                       W, wfSt(), g.isz, t, e0, e1, g.hExt, sign, 1);
         kcheck();
+    }
+
+    // ---- subsurface offsets (interior-slice kernels in aio_kernels.cuh)
+    bool offsets() const { return P.extension == AIO_EXT_OFFSET; }
+    // ss[slot] = v2 * (ss[slot] + sum_s m_s(x-s) F_t(x-2s))  (imagingOffsetFwdGpu + scaleSecondarySourceFd)
+    void img_offset_fwd(int nb, long long slot, const float* m, const float* F, int t) {
+        k_img_offset_fwd<<<ew_grid(nb, g.isz), 256, 0, st>>>(ss_ptr(slot), pairSt(), m, 0, F + (long long)t * g.isz,
+                                                              wfSt(), v2.as<float>(), g.isz, g.ip, g.nxi, g.hExt);
+        kcheck();
+    }
+    // ss[slot] += sum_s m_s(x+s) R_t(x+2s) v2(x+2s)  (imagingOffsetTomoAdjGpu)
+    void img_offset_tomo_adj(int nb, long long slot, const float* m, const float* R, int t) {
+        k_img_offset_tomo_adj<<<ew_grid(nb, g.isz), 256, 0, st>>>(ss_ptr(slot), pairSt(), m, 0,
+                                                                   R + (long long)t * g.isz, wfSt(), v2.as<float>(),
+                                                                   nullptr, g.isz, g.ip, g.nxi, g.hExt);
+        kcheck();
+    }
+    // image_e(x) += A(x+s) B(x-s) on the ring slot (then zeroed): Born form, A = ring * v2, B = W_t
+    // (scaleSecondarySourceFd + imagingOffsetAdjGpu); WEMVA form, A = R_t * v2, B = ring
+    // (imagingOffsetWemvaScaleFwdGpu).
+    void img_offset_adj(int nb, long long slot, const float* F, int t, bool wemvaForm) {
+        const long long mSt = (long long)g.nExt * g.isz;
+        const float* ring = ring_ptr(slot);
+        const float* Ft = F + (long long)t * g.isz;
+        const float* A = wemvaForm ? Ft : ring;
+        const float* B = wemvaForm ? ring : Ft;
+        const long long ASt = wemvaForm ? wfSt() : pairSt(), BSt = wemvaForm ? pairSt() : wfSt();
+        if (P.imageFp64)
+            k_img_offset_adj<double><<<ew_grid(nb, mSt), 256, 0, st>>>(img.as<double>(), mSt, A, ASt, B, BSt,
+                                                                       v2.as<float>(), g.isz, g.ip, g.nxi, g.hExt,
+                                                                       g.nExt, wemvaForm ? 1 : 0);
+        else
+            k_img_offset_adj<float><<<ew_grid(nb, mSt), 256, 0, st>>>(img.as<float>(), mSt, A, ASt, B, BSt,
+                                                                      v2.as<float>(), g.isz, g.ip, g.nxi, g.hExt,
+                                                                      g.nExt, wemvaForm ? 1 : 0);
+        kcheck();
+        zero_slot(ringb, nb, slot);
     }
 
     void scale_shared(float* m, int nSlices, int mode) {
@@ -1830,20 +1871,27 @@ struct Context {
     // Extended (time-lag) Born forward (F/src/BornExtShotsGpuFunctions.cu:269-419).
     void born_ext_forward(const float* model, int nShots, const aio_shot* shots, int mem) {
         begin_call();
-        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32) return born_ext_forward_tb(model, nShots, shots, mem);
+        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32 && !offsets())
+            return born_ext_forward_tb(model, nShots, shots, mem);
         Needs n;
         n.nWavefields = 1;
         n.ss = true;
         float* dm = stage_model(model, g.nExt, mem, this->model);
-        scale_shared(dm, g.nExt, P.sloth ? 2 : 1);
+        // subsurface offsets (BornOffsetShotsFwdGpu, F/src/BornExtShotsGpuFunctions.cu:582-724): 2/v^3 only,
+        // v^2 dtw^2 applied to each secondary-source slice
+        scale_shared(dm, g.nExt, offsets() ? 3 : (P.sloth ? 2 : 1));
         for (int s0 = 0; s0 < nShots;) {
             const int nb = wave_size(n, nShots - s0, shots + s0);
             setup_wave(n, nb, shots + s0, mem, false, false);
             source_wavefield(nb, wf1);
             const float* W = wf1.as<float>();
             fwd_dense_pass(
-                nb, [&](int t, long long slot) { img_time_fwd(nb, slot, dm, W, t); }, true, true, ACC_NONE, nullptr,
-                [](int, long long) {});
+                nb,
+                [&](int t, long long slot) {
+                    if (offsets()) img_offset_fwd(nb, slot, dm, W, t);
+                    else img_time_fwd(nb, slot, dm, W, t);
+                },
+                true, true, ACC_NONE, nullptr, [](int, long long) {});
             download_data(nb, shots + s0, mem);
             sync();
             s0 += nb;
@@ -1853,7 +1901,7 @@ struct Context {
     // Extended (time-lag) Born adjoint (F/src/BornExtShotsGpuFunctions.cu:1525-1675).
     void born_ext_adjoint(float* modelOut, int add, int nShots, const aio_shot* shots, int mem) {
         begin_call();
-        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32)
+        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32 && !offsets())
             return born_ext_adjoint_tb(modelOut, add, nShots, shots, mem);
         Needs n;
         n.nWavefields = 1;
@@ -1866,9 +1914,12 @@ struct Context {
             zero_images(nb, g.nExt);
             const float* W = wf1.as<float>();
             std::vector<const float*> din(dataPtr.begin(), dataPtr.end());
-            adj_sparse_pass(nb, din, nullptr, ACC_RING, nullptr,
-                            [&](int t, long long slot) { img_time_adj(nb, slot, W, t, +1); });
-            reduce_images(nb, g.nExt, P.sloth ? 2 : 1, out, true);
+            // subsurface offsets: BornOffsetShotsAdjGpu, F/src/BornExtShotsGpuFunctions.cu:1848-1990
+            adj_sparse_pass(nb, din, nullptr, ACC_RING, nullptr, [&](int t, long long slot) {
+                if (offsets()) img_offset_adj(nb, slot, W, t, false);
+                else img_time_adj(nb, slot, W, t, +1);
+            });
+            reduce_images(nb, g.nExt, offsets() ? 3 : (P.sloth ? 2 : 1), out, true);
             sync();
             s0 += nb;
         }
@@ -1897,8 +1948,14 @@ struct Context {
         float* dm = stage_model(model, 1, mem, this->model);
         scale_shared(dm, 1, 0);
         float* ex = stage_model(extRefl, g.nExt, mem, this->ext);
-        scale_shared(ex, g.nExt, P.sloth ? 2 : 1);
-        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32) return tomo_forward_tb(dm, ex, nShots, shots, mem);
+        // subsurface offsets (tomoOffsetShotsFwdGpu, F/src/tomoExtShotsGpuFunctions.cu:467-575): 2/v^3 only
+        scale_shared(ex, g.nExt, offsets() ? 3 : (P.sloth ? 2 : 1));
+        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32 && !offsets())
+            return tomo_forward_tb(dm, ex, nShots, shots, mem);
+        auto ext_src = [&](int nb, long long slot, const float* F, int t) {
+            if (offsets()) img_offset_fwd(nb, slot, ex, F, t);
+            else img_time_fwd(nb, slot, ex, F, t);
+        };
         for (int s0 = 0; s0 < nShots;) {
             const int nb = wave_size(n, nShots - s0, shots + s0);
             setup_wave(n, nb, shots + s0, mem, false, false);
@@ -1908,8 +1965,7 @@ struct Context {
             auto nop = [](int, long long) {};
             if (P.leg1) {
                 fwd_dense_pass(
-                    nb, [&](int t, long long slot) { img_time_fwd(nb, slot, ex, W2, t); }, true, false, ACC_FULL, &wf1,
-                    nop);
+                    nb, [&](int t, long long slot) { ext_src(nb, slot, W2, t); }, true, false, ACC_FULL, &wf1, nop);
                 fwd_dense_pass(
                     nb, [&](int t, long long slot) { img_fwd(nb, slot, dm, 0, W1, t); }, false, true, ACC_NONE,
                     nullptr, nop);
@@ -1919,8 +1975,7 @@ struct Context {
                     nb, [&](int t, long long slot) { img_fwd(nb, slot, dm, 0, W2, t); }, false, false, ACC_FULL, &wf1,
                     nop);
                 fwd_dense_pass(
-                    nb, [&](int t, long long slot) { img_time_fwd(nb, slot, ex, W1, t); }, true, true, ACC_NONE,
-                    nullptr, nop);
+                    nb, [&](int t, long long slot) { ext_src(nb, slot, W1, t); }, true, true, ACC_NONE, nullptr, nop);
             }
             download_data(nb, shots + s0, mem);
             sync();
@@ -1936,9 +1991,10 @@ struct Context {
         n.ss = true;
         n.nImg = 1;
         float* ex = stage_model(extRefl, g.nExt, mem, this->ext);
-        scale_shared(ex, g.nExt, P.sloth ? 2 : 1);
+        // subsurface offsets (tomoOffsetShotsAdjGpu, F/src/tomoExtShotsGpuFunctions.cu:912-1023): 2/v^3 only
+        scale_shared(ex, g.nExt, offsets() ? 3 : (P.sloth ? 2 : 1));
         float* out = stage_out(modelOut, 1, add, mem);
-        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32) {
+        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32 && !offsets()) {
             tomo_adjoint_tb(out, ex, nShots, shots, mem);
             write_model(modelOut, 1, add, mem, out);
             sync();
@@ -1955,12 +2011,20 @@ struct Context {
             const float* R = wf1.as<float>();
             if (P.leg1)
                 fwd_dense_pass(
-                    nb, [&](int t, long long slot) { img_time_fwd(nb, slot, ex, W2, t); }, true, false, ACC_RING,
-                    nullptr, [&](int t, long long slot) { img_adj(nb, slot, R, t); });
+                    nb,
+                    [&](int t, long long slot) {
+                        if (offsets()) img_offset_fwd(nb, slot, ex, W2, t);
+                        else img_time_fwd(nb, slot, ex, W2, t);
+                    },
+                    true, false, ACC_RING, nullptr, [&](int t, long long slot) { img_adj(nb, slot, R, t); });
             if (P.leg2)
                 adj_dense_pass(
-                    nb, [&](int t, long long slot) { img_time_tomo_adj(nb, slot, ex, R, t); }, true,
-                    [&](int t, long long slot) { img_adj(nb, slot, W2, t); });
+                    nb,
+                    [&](int t, long long slot) {
+                        if (offsets()) img_offset_tomo_adj(nb, slot, ex, R, t);
+                        else img_time_tomo_adj(nb, slot, ex, R, t);
+                    },
+                    true, [&](int t, long long slot) { img_adj(nb, slot, W2, t); });
             reduce_images(nb, 1, 0, out, true);
             sync();
             s0 += nb;
@@ -1979,7 +2043,7 @@ struct Context {
         float* dm = stage_model(model, 1, mem, this->model);
         scale_shared(dm, 1, 0);
         float* out = stage_out(imageOut, g.nExt, add, mem);
-        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32) {
+        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32 && !offsets()) {
             wemva_forward_tb(dm, out, nShots, shots, mem);
             write_model(imageOut, g.nExt, add, mem, out);
             sync();
@@ -1993,15 +2057,22 @@ struct Context {
             zero_images(nb, g.nExt);
             const float* W2 = wf2.as<float>();
             const float* R = wf1.as<float>();
+            // subsurface offsets: wemvaOffsetShotsFwdGpu, F/src/wemvaExtShotsGpuFunctions.cu:458-574
             if (P.leg1)
                 fwd_dense_pass(
                     nb, [&](int t, long long slot) { img_fwd(nb, slot, dm, 0, W2, t); }, false, false, ACC_RING,
-                    nullptr, [&](int t, long long slot) { img_time_adj(nb, slot, R, t, -1); });
+                    nullptr, [&](int t, long long slot) {
+                        if (offsets()) img_offset_adj(nb, slot, R, t, true);
+                        else img_time_adj(nb, slot, R, t, -1);
+                    });
             if (P.leg2)
                 adj_dense_pass(
                     nb, [&](int t, long long slot) { img_fwd(nb, slot, dm, 0, R, t); }, false,
-                    [&](int t, long long slot) { img_time_adj(nb, slot, W2, t, +1); });
-            reduce_images(nb, g.nExt, 1, out, true);
+                    [&](int t, long long slot) {
+                        if (offsets()) img_offset_adj(nb, slot, W2, t, false);
+                        else img_time_adj(nb, slot, W2, t, +1);
+                    });
+            reduce_images(nb, g.nExt, offsets() ? 3 : 1, out, true);
             sync();
             s0 += nb;
         }
@@ -2017,9 +2088,10 @@ struct Context {
         n.ss = true;
         n.nImg = 1;
         float* im = stage_model(image, g.nExt, mem, this->ext);
-        scale_shared(im, g.nExt, 1);
+        // subsurface offsets (wemvaOffsetShotsAdjGpu, F/src/wemvaExtShotsGpuFunctions.cu:689-810): 2/v^3 only
+        scale_shared(im, g.nExt, offsets() ? 3 : 1);
         float* out = stage_out(modelOut, 1, add, mem);
-        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32) {
+        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32 && !offsets()) {
             wemva_adjoint_tb(out, im, nShots, shots, mem);
             write_model(modelOut, 1, add, mem, out);
             sync();
@@ -2035,12 +2107,20 @@ struct Context {
             const float* R = wf1.as<float>();
             if (P.leg1)
                 adj_dense_pass(
-                    nb, [&](int t, long long slot) { img_time_tomo_adj(nb, slot, im, R, t); }, true,
-                    [&](int t, long long slot) { img_adj(nb, slot, W2, t); });
+                    nb,
+                    [&](int t, long long slot) {
+                        if (offsets()) img_offset_tomo_adj(nb, slot, im, R, t);
+                        else img_time_tomo_adj(nb, slot, im, R, t);
+                    },
+                    true, [&](int t, long long slot) { img_adj(nb, slot, W2, t); });
             if (P.leg2)
                 fwd_dense_pass(
-                    nb, [&](int t, long long slot) { img_time_fwd(nb, slot, im, W2, t); }, true, false, ACC_RING,
-                    nullptr, [&](int t, long long slot) { img_adj(nb, slot, R, t); });
+                    nb,
+                    [&](int t, long long slot) {
+                        if (offsets()) img_offset_fwd(nb, slot, im, W2, t);
+                        else img_time_fwd(nb, slot, im, W2, t);
+                    },
+                    true, false, ACC_RING, nullptr, [&](int t, long long slot) { img_adj(nb, slot, R, t); });
             reduce_images(nb, 1, 0, out, true);
             sync();
             s0 += nb;
@@ -2539,6 +2619,96 @@ AIO_API int aio_tomoTimeShotsAdjFsGpu(float* model, float* dataRegDts, float* ex
     });
 }
 
+// Subsurface-offset seam calls (the reference's *OffsetShots* drivers, optionally free-surface):
+// the slot's context runs the call with the offset axis on.
+struct SeamExt {
+    Context& c;
+    int ext, fs;
+    SeamExt(Context& cc, bool freeSurface) : c(cc), ext(cc.P.extension), fs(cc.P.freeSurface) {
+        c.P.extension = AIO_EXT_OFFSET;
+        c.P.freeSurface = freeSurface ? 1 : 0;
+    }
+    ~SeamExt() {
+        c.P.extension = ext;
+        c.P.freeSurface = fs;
+    }
+};
+static void seam_born_offset(float* model, float* dataRegDts, float* sig, int* sp, int ns, int* rp, int nr, int iGpu,
+                             bool adjoint, bool fs) {
+    SeamExt x(seam_ctx(AIO_BORN_EXT, iGpu), fs);
+    aio_shot s = one_shot(sig, sp, ns, rp, nr, dataRegDts);
+    if (adjoint) x.c.born_ext_adjoint(model, 0, 1, &s, AIO_MEM_HOST);
+    else x.c.born_ext_forward(model, 1, &s, AIO_MEM_HOST);
+}
+AIO_API int aio_BornOffsetShotsFwdGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sp, int ns,
+                                      int* rp, int nr, float* srcWavefield, float* scatWavefield, int iGpu,
+                                      int iGpuId) {
+    (void)srcWavefield; (void)scatWavefield; (void)iGpuId;
+    return guard([&] { seam_born_offset(model, dataRegDts, sourcesSignals, sp, ns, rp, nr, iGpu, false, false); });
+}
+AIO_API int aio_BornOffsetShotsAdjGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sp, int ns,
+                                      int* rp, int nr, float* srcWavefield, float* recWavefield, int iGpu,
+                                      int iGpuId) {
+    (void)srcWavefield; (void)recWavefield; (void)iGpuId;
+    return guard([&] { seam_born_offset(model, dataRegDts, sourcesSignals, sp, ns, rp, nr, iGpu, true, false); });
+}
+AIO_API int aio_BornOffsetShotsFwdFsGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sp, int ns,
+                                        int* rp, int nr, float* srcWavefield, float* scatWavefield, int iGpu,
+                                        int iGpuId) {
+    (void)srcWavefield; (void)scatWavefield; (void)iGpuId;
+    return guard([&] { seam_born_offset(model, dataRegDts, sourcesSignals, sp, ns, rp, nr, iGpu, false, true); });
+}
+AIO_API int aio_BornOffsetShotsAdjFsGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sp, int ns,
+                                        int* rp, int nr, float* srcWavefield, float* recWavefield, int iGpu,
+                                        int iGpuId) {
+    (void)srcWavefield; (void)recWavefield; (void)iGpuId;
+    return guard([&] { seam_born_offset(model, dataRegDts, sourcesSignals, sp, ns, rp, nr, iGpu, true, true); });
+}
+static void seam_tomo_offset(float* model, float* dataRegDts, float* ext, float* sig, int* sp, int ns, int* rp, int nr,
+                             int iGpu, int saveWavefield, bool adjoint, bool fs) {
+    require(saveWavefield == 0, "saveWavefield=1 is not available for tomo in this build");
+    SeamExt x(seam_ctx(AIO_TOMO_EXT, iGpu), fs);
+    aio_shot s = one_shot(sig, sp, ns, rp, nr, dataRegDts);
+    if (adjoint) x.c.tomo_adjoint(model, 0, ext, 1, &s, AIO_MEM_HOST);
+    else x.c.tomo_forward(model, ext, 1, &s, AIO_MEM_HOST);
+}
+AIO_API int aio_tomoOffsetShotsFwdGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
+                                      int* sp, int ns, int* rp, int nr, float* w0, float* w1, float* w2, int iGpu,
+                                      int iGpuId, int saveWavefield) {
+    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    return guard([&] {
+        seam_tomo_offset(model, dataRegDts, extReflectivity, sourcesSignals, sp, ns, rp, nr, iGpu, saveWavefield,
+                         false, false);
+    });
+}
+AIO_API int aio_tomoOffsetShotsAdjGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
+                                      int* sp, int ns, int* rp, int nr, float* w0, float* w1, float* w2, int iGpu,
+                                      int iGpuId, int saveWavefield) {
+    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    return guard([&] {
+        seam_tomo_offset(model, dataRegDts, extReflectivity, sourcesSignals, sp, ns, rp, nr, iGpu, saveWavefield,
+                         true, false);
+    });
+}
+AIO_API int aio_tomoOffsetShotsFwdFsGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
+                                        int* sp, int ns, int* rp, int nr, float* w0, float* w1, float* w2, int iGpu,
+                                        int iGpuId, int saveWavefield) {
+    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    return guard([&] {
+        seam_tomo_offset(model, dataRegDts, extReflectivity, sourcesSignals, sp, ns, rp, nr, iGpu, saveWavefield,
+                         false, true);
+    });
+}
+AIO_API int aio_tomoOffsetShotsAdjFsGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
+                                        int* sp, int ns, int* rp, int nr, float* w0, float* w1, float* w2, int iGpu,
+                                        int iGpuId, int saveWavefield) {
+    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    return guard([&] {
+        seam_tomo_offset(model, dataRegDts, extReflectivity, sourcesSignals, sp, ns, rp, nr, iGpu, saveWavefield,
+                         true, true);
+    });
+}
+
 AIO_API int aio_initWemvaExtGpu(float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad,
                                 int blockSize, float alphaCos, int nExt, int leg1, int leg2, int nGpu, int iGpuId,
                                 int iGpuAlloc) {
@@ -2563,6 +2733,30 @@ AIO_API int aio_wemvaTimeShotsFwdGpu(float* model, float* wemvaExtImage, float* 
         aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, nullptr);
         s.wemvaData = wemvaDataRegDts;
         seam_ctx(AIO_WEMVA_EXT, iGpu).wemva_forward(model, wemvaExtImage, 0, 1, &s, AIO_MEM_HOST);
+    });
+}
+AIO_API int aio_wemvaOffsetShotsFwdGpu(float* model, float* wemvaExtImage, float* sourcesSignals, int* sp, int ns,
+                                       float* wemvaDataRegDts, int* rp, int nr, float* w0, float* w1, float* w2,
+                                       int iGpu, int iGpuId, int saveWavefield) {
+    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    return guard([&] {
+        require(saveWavefield == 0, "saveWavefield=1 is not available for WEMVA in this build");
+        SeamExt x(seam_ctx(AIO_WEMVA_EXT, iGpu), false);
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, nullptr);
+        s.wemvaData = wemvaDataRegDts;
+        x.c.wemva_forward(model, wemvaExtImage, 0, 1, &s, AIO_MEM_HOST);
+    });
+}
+AIO_API int aio_wemvaOffsetShotsAdjGpu(float* model, float* wemvaExtImage, float* sourcesSignals, int* sp, int ns,
+                                       float* wemvaDataRegDts, int* rp, int nr, float* w0, float* w1, float* w2,
+                                       int iGpu, int iGpuId, int saveWavefield) {
+    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    return guard([&] {
+        require(saveWavefield == 0, "saveWavefield=1 is not available for WEMVA in this build");
+        SeamExt x(seam_ctx(AIO_WEMVA_EXT, iGpu), false);
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, nullptr);
+        s.wemvaData = wemvaDataRegDts;
+        x.c.wemva_adjoint(model, 0, wemvaExtImage, 1, &s, AIO_MEM_HOST);
     });
 }
 AIO_API int aio_wemvaTimeShotsAdjGpu(float* model, float* wemvaExtImage, float* sourcesSignals, int* sp, int ns,

@@ -262,6 +262,73 @@ __global__ void k_img_time_adj(Acc* m, long long mSt, float* r, long long rSt, c
     }
 }
 
+// ---- subsurface (horizontal) offsets, interior-slice layout (x*ip + z), x in [0, nxi) ----
+// imagingOffsetFwdGpu + scaleSecondarySourceFd (F/src/kernelsGpu.cu:381-395, 269-276):
+//   ss(x) = v2(x) * (ss(x) + sum_s m_{s+h}(x-s) W(x-2s)) over the offsets whose model point x-s
+//   lies in [h, nxi-h), s ascending.
+__global__ void k_img_offset_fwd(float* ss, long long ssSt, const float* m, long long mSt, const float* W,
+                                 long long WSt, const float* v2, long long isz, int ip, int nxi, int hExt) {
+    const int b = blockIdx.y;
+    ss += b * ssSt; m += b * mSt; W += b * WSt;
+    AIO_GRID_STRIDE(i, isz) {
+        const int x = (int)(i / ip);
+        const int e0 = max(-hExt, x + 1 + hExt - nxi), e1 = min(x - hExt, hExt) + 1;
+        float acc = ss[i];
+        for (int s = e0; s < e1; s++) acc += m[(long long)(s + hExt) * isz + i - (long long)s * ip] * W[i - 2LL * s * ip];
+        ss[i] = acc * v2[i];
+    }
+}
+// imagingOffsetTomoAdjGpu (:460-476): ss(x) += sum_s m_{s+h}(x+s) R(x+2s) v2(x+2s) over the offsets
+// whose model point x+s lies in [h, nxi-h). With v2Out (U-form receiver wavefield, R = v2 R_ref
+// already, v2Rec = nullptr): ss(x) = v2(x) * (ss(x) + sum_s m_{s+h}(x+s) R(x+2s)).
+__global__ void k_img_offset_tomo_adj(float* ss, long long ssSt, const float* m, long long mSt, const float* R,
+                                      long long RSt, const float* v2Rec, const float* v2Out, long long isz, int ip,
+                                      int nxi, int hExt) {
+    const int b = blockIdx.y;
+    ss += b * ssSt; m += b * mSt; R += b * RSt;
+    AIO_GRID_STRIDE(i, isz) {
+        const int x = (int)(i / ip);
+        const int e0 = max(-hExt, hExt - x), e1 = min(nxi - 1 - x - hExt, hExt) + 1;
+        float acc = ss[i];
+        for (int s = e0; s < e1; s++) {
+            const long long j = i + 2LL * s * ip;
+            const float r = v2Rec ? R[j] * v2Rec[j] : R[j];
+            acc += m[(long long)(s + hExt) * isz + i + (long long)s * ip] * r;
+        }
+        ss[i] = v2Out ? acc * v2Out[i] : acc;
+    }
+}
+// imagingOffsetAdjGpu (:397-411): img_e(x) += A(x+s) B(x-s), s = e-h, x in [h, nxi-h).
+// wemvaForm = 0: (A(x+s) * scaleA(x+s)) * B(x-s) — the receiver sample scaled by
+//   scaleSecondarySourceFd (:269-276) before imagingOffsetAdjGpu;
+// wemvaForm = 1: (B(x-s) * A(x+s)) * scaleA(x+s) — imagingOffsetWemvaScaleFwdGpu (:429-443) with
+//   A the receiver wavefield and B the scattered sample.
+// scaleA may be null (factor 1).
+template <typename Acc>
+__global__ void k_img_offset_adj(Acc* img, long long mSt, const float* A, long long ASt, const float* B, long long BSt,
+                                 const float* scaleA, long long isz, int ip, int nxi, int hExt, int nExt,
+                                 int wemvaForm) {
+    const int b = blockIdx.y;
+    img += b * mSt; A += b * ASt; B += b * BSt;
+    const long long n = (long long)nExt * isz;
+    AIO_GRID_STRIDE(k, n) {
+        const int e = (int)(k / isz);
+        const long long i = k - (long long)e * isz;
+        const int x = (int)(i / ip), s = e - hExt;
+        if (x < hExt || x >= nxi - hExt) continue;
+        const long long ja = i + (long long)s * ip, jb = i - (long long)s * ip;
+        float v;
+        if (wemvaForm) {
+            v = B[jb] * A[ja];
+            if (scaleA) v = v * scaleA[ja];
+        } else {
+            const float a = scaleA ? A[ja] * scaleA[ja] : A[ja];
+            v = a * B[jb];
+        }
+        img[k] += (Acc)v;
+    }
+}
+
 // Time-lag imaging of a block of at most LAG_K coarse samples (imagingTimeAdjGpu,
 // F/src/kernelsGpu.cu:352-364, applied at every t of the block; sign = -1 gives
 // imagingWemvaTimeAdjGpu, :366-378):

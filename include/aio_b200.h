@@ -70,7 +70,12 @@ typedef struct {
                             > 0 = fixed width (strips of at most 128 rows) */
     int freeSurface;     /* 1: free surface at the top interior row (reference par freeSurface;
                             the *FsGpu drivers); runs on the per-fine-step stepper */
+    int extension;       /* AIO_EXT_*: extension axis of the extended Born / tomo / WEMVA operators
+                            (reference par extension "time" / "offset") */
 } aio_params;
+
+#define AIO_EXT_TIME 0      /* time lags (the *TimeShots* drivers) */
+#define AIO_EXT_OFFSET 1    /* horizontal subsurface offsets (the *OffsetShots* drivers; per-fine-step stepper) */
 
 #define AIO_STEPPER_AUTO 0      /* interval-blocked where available (sub == 4), else per fine step */
 #define AIO_STEPPER_FINE 1      /* one fused launch per fine step (the reference's schedule) */
@@ -262,6 +267,54 @@ int aio_tomoTimeShotsAdjFsGpu(float* model, float* dataRegDts, float* extReflect
                               int* sourcesPositionReg, int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
                               float* tomoSrcWavefieldDt2, float* tomoSecWavefield1, float* tomoSecWavefield2,
                               int iGpu, int iGpuId, int saveWavefield);
+/* Subsurface-offset drivers (reference extension "offset"): same arguments as the time-lag calls without
+ * sloth; they run on the per-fine-step stepper. */
+/* F/include/BornExtShotsGpuFunctions.h:22 */
+int aio_BornOffsetShotsFwdGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                              int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
+                              float* scatWavefield, int iGpu, int iGpuId);
+/* F/include/BornExtShotsGpuFunctions.h:44 */
+int aio_BornOffsetShotsAdjGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                              int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
+                              float* recWavefield, int iGpu, int iGpuId);
+/* F/include/BornExtShotsGpuFunctions.h:31 */
+int aio_BornOffsetShotsFwdFsGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                                int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
+                                float* scatWavefield, int iGpu, int iGpuId);
+/* F/include/BornExtShotsGpuFunctions.h:53 */
+int aio_BornOffsetShotsAdjFsGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                                int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
+                                float* recWavefield, int iGpu, int iGpuId);
+/* F/include/tomoExtShotsGpuFunctions.h:17 */
+int aio_tomoOffsetShotsFwdGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
+                              int* sourcesPositionReg, int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
+                              float* tomoSrcWavefieldDt2, float* tomoSecWavefield1, float* tomoSecWavefield2,
+                              int iGpu, int iGpuId, int saveWavefield);
+/* F/include/tomoExtShotsGpuFunctions.h:29 */
+int aio_tomoOffsetShotsAdjGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
+                              int* sourcesPositionReg, int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
+                              float* tomoSrcWavefieldDt2, float* tomoSecWavefield1, float* tomoSecWavefield2,
+                              int iGpu, int iGpuId, int saveWavefield);
+/* F/include/tomoExtShotsGpuFunctions.h:21 */
+int aio_tomoOffsetShotsFwdFsGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
+                                int* sourcesPositionReg, int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
+                                float* tomoSrcWavefieldDt2, float* tomoSecWavefield1, float* tomoSecWavefield2,
+                                int iGpu, int iGpuId, int saveWavefield);
+/* F/include/tomoExtShotsGpuFunctions.h:33 */
+int aio_tomoOffsetShotsAdjFsGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
+                                int* sourcesPositionReg, int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
+                                float* tomoSrcWavefieldDt2, float* tomoSecWavefield1, float* tomoSecWavefield2,
+                                int iGpu, int iGpuId, int saveWavefield);
+/* F/include/wemvaExtShotsGpuFunctions.h:13 */
+int aio_wemvaOffsetShotsFwdGpu(float* model, float* wemvaExtImage, float* sourcesSignals, int* sourcesPositionReg,
+                               int nSourcesReg, float* wemvaDataRegDts, int* receiversPositionReg, int nReceiversReg,
+                               float* wemvaSrcWavefieldDt2, float* wemvaSecWavefield1, float* wemvaSecWavefield2,
+                               int iGpu, int iGpuId, int saveWavefield);
+/* F/include/wemvaExtShotsGpuFunctions.h:17 */
+int aio_wemvaOffsetShotsAdjGpu(float* model, float* wemvaExtImage, float* sourcesSignals, int* sourcesPositionReg,
+                               int nSourcesReg, float* wemvaDataRegDts, int* receiversPositionReg, int nReceiversReg,
+                               float* wemvaSrcWavefieldDt2, float* wemvaSecWavefield1, float* wemvaSecWavefield2,
+                               int iGpu, int iGpuId, int saveWavefield);
 /* F/include/wemvaExtShotsGpuFunctions.h:6-17 (time-lag extension) */
 int aio_initWemvaExtGpu(float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad, int blockSize,
                         float alphaCos, int nExt, int leg1, int leg2, int nGpu, int iGpuId, int iGpuAlloc);

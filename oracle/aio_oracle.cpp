@@ -41,6 +41,7 @@ template <class T>
 struct Grid {
     int nz, nx, nts, sub, ntw, minPad, H, nExt, hExt;
     int fs = 0;  // free surface at the top interior row (the reference's freeSurface == 1)
+    int offset = 0;  // extension axis: 0 time lags, 1 subsurface (horizontal) offsets
     T zc[6], xc[6];
     T h[2 * (SUB_MAX + 1)];
     T taper[PAD_MAX];
@@ -306,6 +307,84 @@ static void imaging_time_tomo_adj(const Grid<T>& g, const T* Win, T* ss, const T
     });
 }
 
+// ---- subsurface-offset extension (F/src/kernelsGpu.cu:254-276, 381-441) ----
+// scaleReflectivityLinExt, :256-267: every offset slice times 2/v^3.
+template <class T>
+static void scale_refl_lin_ext(const Grid<T>& g, T* m) {
+    const size_t N = g.N();
+    for (int e = 0; e < g.nExt; e++) {
+        T* me = m + (size_t)e * N;
+        for_interior(g.nz, g.nx, [&](size_t i) { me[i] *= g.rs[i]; });
+    }
+}
+// scaleSecondarySourceFd, :270-276: a slice times v^2 dtw^2.
+template <class T>
+static void scale_ss_fd(const Grid<T>& g, T* ss) {
+    for_interior(g.nz, g.nx, [&](size_t i) { ss[i] *= g.v2[i]; });
+}
+// imagingOffsetFwdGpu, :381-395: ss(x) += sum_s m_s(x-s) W_its(x-2s) over the offsets whose model
+// point x-s lies in [FAT+h, nx-FAT-h).
+template <class T>
+static void imaging_offset_fwd(const Grid<T>& g, const T* m, T* ss, const T* W, int its) {
+    const int nz = g.nz, nx = g.nx, h = g.hExt;
+    const size_t N = g.N();
+    const T* w = W + (size_t)its * N;
+    for (int ix = FAT; ix < nx - FAT; ix++) {
+        const int e0 = std::max(-h, ix + 1 + FAT + h - nx), e1 = std::min(ix - h - FAT, h) + 1;
+        for (int iz = FAT; iz < nz - FAT; iz++) {
+            const size_t i = (size_t)ix * nz + iz;
+            for (int s = e0; s < e1; s++)
+                ss[i] += m[(size_t)(s + h) * N + (size_t)(ix - s) * nz + iz] * w[(size_t)(ix - 2 * s) * nz + iz];
+        }
+    }
+}
+// imagingOffsetAdjGpu, :397-411: m_e(x) += r(x+s) W_its(x-s), s = e-h, x in [FAT+h, nx-FAT-h).
+template <class T>
+static void imaging_offset_adj(const Grid<T>& g, T* m, const T* r, const T* W, int its) {
+    const int nz = g.nz, nx = g.nx, h = g.hExt;
+    const size_t N = g.N();
+    const T* w = W + (size_t)its * N;
+    for (int e = 0; e < g.nExt; e++) {
+        const int s = e - h;
+        for (int ix = FAT + h; ix < nx - FAT - h; ix++)
+            for (int iz = FAT; iz < nz - FAT; iz++)
+                m[(size_t)e * N + (size_t)ix * nz + iz] += r[(size_t)(ix + s) * nz + iz] * w[(size_t)(ix - s) * nz + iz];
+    }
+}
+// imagingOffsetWemvaScaleFwdGpu, :429-443: m_e(x) += c(x-s) R_its(x+s) v2(x+s).
+template <class T>
+static void imaging_offset_wemva_scale_fwd(const Grid<T>& g, T* m, const T* c, const T* R, int its) {
+    const int nz = g.nz, nx = g.nx, h = g.hExt;
+    const size_t N = g.N();
+    const T* r = R + (size_t)its * N;
+    for (int e = 0; e < g.nExt; e++) {
+        const int s = e - h;
+        for (int ix = FAT + h; ix < nx - FAT - h; ix++)
+            for (int iz = FAT; iz < nz - FAT; iz++) {
+                const size_t j = (size_t)(ix + s) * nz + iz;
+                m[(size_t)e * N + (size_t)ix * nz + iz] += c[(size_t)(ix - s) * nz + iz] * r[j] * g.v2[j];
+            }
+    }
+}
+// imagingOffsetTomoAdjGpu, :460-476: ss(x) += sum_s m_s(x+s) R_its(x+2s) v2(x+2s) over the offsets
+// whose model point x+s lies in [FAT+h, nx-FAT-h).
+template <class T>
+static void imaging_offset_tomo_adj(const Grid<T>& g, const T* R, T* ss, const T* m, int its) {
+    const int nz = g.nz, nx = g.nx, h = g.hExt;
+    const size_t N = g.N();
+    const T* r = R + (size_t)its * N;
+    for (int ix = FAT; ix < nx - FAT; ix++) {
+        const int e0 = std::max(-h, FAT + h - ix), e1 = std::min(nx - 1 - FAT - ix - h, h) + 1;
+        for (int iz = FAT; iz < nz - FAT; iz++) {
+            const size_t i = (size_t)ix * nz + iz;
+            for (int s = e0; s < e1; s++) {
+                const size_t j = (size_t)(ix + 2 * s) * nz + iz;
+                ss[i] += m[(size_t)(s + h) * N + (size_t)(ix + s) * nz + iz] * r[j] * g.v2[j];
+            }
+        }
+    }
+}
+
 // Lag bounds with C truncating division, as in F/src/BornExtShotsGpuFunctions.cu:366-383
 // ("source side": W index its-2*lag in [0,nts)) and
 // F/src/tomoExtShotsGpuFunctions.cu:2631-2650 ("receiver side": index its+2*lag).
@@ -556,11 +635,18 @@ static void bornext_fwd(const Grid<T>& g, const T* model, const T* sig, const in
     std::vector<T> W((size_t)g.nts * N);
     source_wavefield(g, w, sig, sp, ns, W.data());
     std::vector<T> dm(model, model + (size_t)g.nExt * N);
-    scale_refl_ext(g, dm.data(), sloth);
+    // subsurface offsets: BornOffsetShotsFwdGpu, F/src/BornExtShotsGpuFunctions.cu:582-724
+    if (g.offset) scale_refl_lin_ext(g, dm.data());
+    else scale_refl_ext(g, dm.data(), sloth);
     std::fill(data, data + (size_t)nr * g.nts, (T)0);
     scat_fwd_pass(
         g, w,
         [&](int t, T* ss) {
+            if (g.offset) {
+                imaging_offset_fwd(g, dm.data(), ss, W.data(), t);
+                scale_ss_fd(g, ss);
+                return;
+            }
             int e0, e1;
             lag_bounds_src(g, t, e0, e1);
             imaging_time_fwd(g, dm.data(), ss, W.data(), t, e0, e1);
@@ -591,10 +677,21 @@ static void bornext_adj(const Grid<T>& g, T* model, const T* sig, const int* sp,
             fine_to_coarse(g, pL, pR, P0, it2);
             std::swap(P0, P1);
         }
-        lag_bounds_src(g, its + 1, e0, e1);
-        imaging_time_adj(g, model, pR, W.data(), its + 1, e0, e1);
+        if (g.offset) {  // BornOffsetShotsAdjGpu, F/src/BornExtShotsGpuFunctions.cu:1848-1990
+            scale_ss_fd(g, pR);
+            imaging_offset_adj(g, model, pR, W.data(), its + 1);
+        } else {
+            lag_bounds_src(g, its + 1, e0, e1);
+            imaging_time_adj(g, model, pR, W.data(), its + 1, e0, e1);
+        }
         std::swap(pR, pL);
         std::fill(pL, pL + N, (T)0);
+    }
+    if (g.offset) {
+        scale_ss_fd(g, pR);
+        imaging_offset_adj(g, model, pR, W.data(), 0);
+        scale_refl_lin_ext(g, model);
+        return;
     }
     lag_bounds_src(g, 0, e0, e1);
     imaging_time_adj(g, model, pR, W.data(), 0, e0, e1);
@@ -613,10 +710,17 @@ static void tomo_fwd(const Grid<T>& g, const T* model, const T* extRefl, const T
     std::vector<T> dm(model, model + N);
     scale_refl(g, dm.data());
     std::vector<T> ext(extRefl, extRefl + (size_t)g.nExt * N);
-    scale_refl_ext(g, ext.data(), sloth);
+    // subsurface offsets: tomoOffsetShotsFwdGpu, F/src/tomoExtShotsGpuFunctions.cu:467-575, legs :2005-2105, :2227-2323
+    if (g.offset) scale_refl_lin_ext(g, ext.data());
+    else scale_refl_ext(g, ext.data(), sloth);
     std::fill(data, data + (size_t)nr * g.nts, (T)0);
     auto ext_src = [&](const T* Win) {
         return [&, Win](int t, T* ss) {
+            if (g.offset) {
+                imaging_offset_fwd(g, ext.data(), ss, Win, t);
+                scale_ss_fd(g, ss);
+                return;
+            }
             int e0, e1;
             lag_bounds_src(g, t, e0, e1);
             imaging_time_fwd(g, ext.data(), ss, Win, t, e0, e1);
@@ -650,12 +754,19 @@ static void tomo_adj(const Grid<T>& g, T* model, const T* extRefl, const T* sig,
     source_wavefield_dt2(g, w, sig, sp, ns, W2.data());
     receiver_wavefield(g, w, data, rp, nr, R.data());
     std::vector<T> ext(extRefl, extRefl + (size_t)g.nExt * N);
-    scale_refl_ext(g, ext.data(), sloth);
+    // subsurface offsets: tomoOffsetShotsAdjGpu, F/src/tomoExtShotsGpuFunctions.cu:912-1023, legs :2788-2866, :2949-3021
+    if (g.offset) scale_refl_lin_ext(g, ext.data());
+    else scale_refl_ext(g, ext.data(), sloth);
     std::fill(model, model + N, (T)0);
     if (leg1) {
         scat_fwd_pass(
             g, w,
             [&](int t, T* ss) {
+                if (g.offset) {
+                    imaging_offset_fwd(g, ext.data(), ss, W2.data(), t);
+                    scale_ss_fd(g, ss);
+                    return;
+                }
                 int e0, e1;
                 lag_bounds_src(g, t, e0, e1);
                 imaging_time_fwd(g, ext.data(), ss, W2.data(), t, e0, e1);
@@ -667,6 +778,10 @@ static void tomo_adj(const Grid<T>& g, T* model, const T* extRefl, const T* sig,
         scat_adj_pass(
             g, w,
             [&](int t, T* ss) {
+                if (g.offset) {
+                    imaging_offset_tomo_adj(g, R.data(), ss, ext.data(), t);
+                    return;
+                }
                 int e0, e1;
                 lag_bounds_rec(g, t, e0, e1);
                 imaging_time_tomo_adj(g, R.data(), ss, ext.data(), t, e0, e1);
@@ -694,6 +809,10 @@ static void wemva_fwd(const Grid<T>& g, const T* model, const T* sig, const int*
         scat_fwd_pass(
             g, w, [&](int t, T* ss) { imaging_fwd(g, dm.data(), ss, t, W2.data()); }, false,
             [](const T*, int, int) {}, true, [&](int t, T* C) {
+                if (g.offset) {  // wemvaOffsetShotsFwdGpu (:458-574) legs, F/src/wemvaExtShotsGpuFunctions.cu:1123-1269
+                    imaging_offset_wemva_scale_fwd(g, image, C, R.data(), t);
+                    return;
+                }
                 int e0, e1;
                 lag_bounds_rec(g, t, e0, e1);
                 imaging_wemva_time_adj(g, image, C, R.data(), t, e0, e1);
@@ -702,12 +821,18 @@ static void wemva_fwd(const Grid<T>& g, const T* model, const T* sig, const int*
     if (leg2) {
         scat_adj_pass(
             g, w, [&](int t, T* ss) { imaging_fwd(g, dm.data(), ss, t, R.data()); }, false, [&](int t, T* C) {
+                if (g.offset) {
+                    scale_ss_fd(g, C);
+                    imaging_offset_adj(g, image, C, W2.data(), t);
+                    return;
+                }
                 int e0, e1;
                 lag_bounds_src(g, t, e0, e1);
                 imaging_time_adj(g, image, C, W2.data(), t, e0, e1);
             });
     }
-    scale_refl_ext(g, image, 0);
+    if (g.offset) scale_refl_lin_ext(g, image);
+    else scale_refl_ext(g, image, 0);
 }
 
 // Extended WEMVA adjoint, F/src/wemvaExtShotsGpuFunctions.cu:575-688 with legs
@@ -721,12 +846,18 @@ static void wemva_adj(const Grid<T>& g, T* model, const T* sig, const int* sp, i
     source_wavefield_dt2(g, w, sig, sp, ns, W2.data());
     receiver_wavefield(g, w, rdata, rp, nr, R.data());
     std::vector<T> img(imageIn, imageIn + (size_t)g.nExt * N);
-    scale_refl_ext(g, img.data(), 0);
+    // subsurface offsets: wemvaOffsetShotsAdjGpu, F/src/wemvaExtShotsGpuFunctions.cu:689-810, legs :1428-1580
+    if (g.offset) scale_refl_lin_ext(g, img.data());
+    else scale_refl_ext(g, img.data(), 0);
     std::fill(model, model + N, (T)0);
     if (leg1) {
         scat_adj_pass(
             g, w,
             [&](int t, T* ss) {
+                if (g.offset) {
+                    imaging_offset_tomo_adj(g, R.data(), ss, img.data(), t);
+                    return;
+                }
                 int e0, e1;
                 lag_bounds_rec(g, t, e0, e1);
                 imaging_time_tomo_adj(g, R.data(), ss, img.data(), t, e0, e1);
@@ -737,6 +868,11 @@ static void wemva_adj(const Grid<T>& g, T* model, const T* sig, const int* sp, i
         scat_fwd_pass(
             g, w,
             [&](int t, T* ss) {
+                if (g.offset) {
+                    imaging_offset_fwd(g, img.data(), ss, W2.data(), t);
+                    scale_ss_fd(g, ss);
+                    return;
+                }
                 int e0, e1;
                 lag_bounds_src(g, t, e0, e1);
                 imaging_time_fwd(g, img.data(), ss, W2.data(), t, e0, e1);
@@ -815,6 +951,7 @@ struct OrcParams {
     int nz, nx, nts, sub, minPad, nExt;
     double dz, dx, dts, alphaCos;
     int freeSurface;
+    int extension;  // 0 time lags, 1 subsurface offsets
 };
 
 template <class T>
@@ -823,6 +960,7 @@ static Grid<T> grid_from(const OrcParams* p, const T* vel) {
     make_grid<T>(g, p->nz, p->nx, p->nts, (T)p->dts, p->sub, p->minPad, (T)p->alphaCos, (T)p->dz, (T)p->dx,
                  p->nExt, vel);
     g.fs = p->freeSurface;
+    g.offset = p->extension;
     return g;
 }
 

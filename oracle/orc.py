@@ -26,7 +26,7 @@ _lib = None
 class OrcParams(C.Structure):
     _fields_ = [("nz", C.c_int), ("nx", C.c_int), ("nts", C.c_int), ("sub", C.c_int),
                 ("minPad", C.c_int), ("nExt", C.c_int), ("dz", C.c_double), ("dx", C.c_double),
-                ("dts", C.c_double), ("alphaCos", C.c_double), ("freeSurface", C.c_int)]
+                ("dts", C.c_double), ("alphaCos", C.c_double), ("freeSurface", C.c_int), ("extension", C.c_int)]
 
 
 def build() -> str:
@@ -58,6 +58,7 @@ class Scheme:
     alphaCos: float = 0.99
     nExt: int = 1
     freeSurface: int = 0
+    extension: int = 0  # 0 time lags, 1 subsurface offsets
 
     @property
     def ntw(self) -> int:
@@ -65,7 +66,7 @@ class Scheme:
 
     def c(self) -> OrcParams:
         return OrcParams(self.nz, self.nx, self.nts, self.sub, self.minPad, self.nExt,
-                         self.dz, self.dx, self.dts, self.alphaCos, self.freeSurface)
+                         self.dz, self.dx, self.dts, self.alphaCos, self.freeSurface, self.extension)
 
 
 def _suf(dtype) -> str:

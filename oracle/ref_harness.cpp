@@ -98,6 +98,13 @@ REF_EXPORT int ref_bornext_fwd(R* model, R* data, R* sig, int* sp, int ns, int* 
 REF_EXPORT int ref_bornext_adj(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, int sloth, int dev) {
     GUARD(BornTimeShotsAdjGpu(model, data, sig, sp, ns, rp, nr, nullptr, nullptr, sloth, 0, dev))
 }
+// subsurface-offset drivers (F/include/BornExtShotsGpuFunctions.h:22,44)
+REF_EXPORT int ref_bornext_fwd_off(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
+    GUARD(BornOffsetShotsFwdGpu(model, data, sig, sp, ns, rp, nr, nullptr, nullptr, 0, dev))
+}
+REF_EXPORT int ref_bornext_adj_off(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
+    GUARD(BornOffsetShotsAdjGpu(model, data, sig, sp, ns, rp, nr, nullptr, nullptr, 0, dev))
+}
 // free-surface drivers (F/include/BornExtShotsGpuFunctions.h:27,49; no sloth flag)
 REF_EXPORT int ref_bornext_fwd_fs(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
     GUARD(BornTimeShotsFwdFsGpu(model, data, sig, sp, ns, rp, nr, nullptr, nullptr, 0, dev))
@@ -121,6 +128,13 @@ REF_EXPORT int ref_tomo_adj(R* model, R* data, R* ext, R* sig, int* sp, int ns, 
                             int dev) {
     GUARD(tomoTimeShotsAdjGpu(model, data, ext, sig, sp, ns, rp, nr, nullptr, nullptr, nullptr, sloth, 0, dev, 0))
 }
+// subsurface-offset drivers (F/include/tomoExtShotsGpuFunctions.h:17,29)
+REF_EXPORT int ref_tomo_fwd_off(R* model, R* data, R* ext, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
+    GUARD(tomoOffsetShotsFwdGpu(model, data, ext, sig, sp, ns, rp, nr, nullptr, nullptr, nullptr, 0, dev, 0))
+}
+REF_EXPORT int ref_tomo_adj_off(R* model, R* data, R* ext, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
+    GUARD(tomoOffsetShotsAdjGpu(model, data, ext, sig, sp, ns, rp, nr, nullptr, nullptr, nullptr, 0, dev, 0))
+}
 // free-surface drivers (F/include/tomoExtShotsGpuFunctions.h:20,32; no sloth flag)
 REF_EXPORT int ref_tomo_fwd_fs(R* model, R* data, R* ext, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
     GUARD(tomoTimeShotsFwdFsGpu(model, data, ext, sig, sp, ns, rp, nr, nullptr, nullptr, nullptr, 0, dev, 0))
@@ -141,5 +155,12 @@ REF_EXPORT int ref_wemva_fwd(R* model, R* image, R* sig, int* sp, int ns, R* rda
 }
 REF_EXPORT int ref_wemva_adj(R* model, R* image, R* sig, int* sp, int ns, R* rdata, int* rp, int nr, int dev) {
     GUARD(wemvaTimeShotsAdjGpu(model, image, sig, sp, ns, rdata, rp, nr, nullptr, nullptr, nullptr, 0, dev, 0))
+}
+// subsurface-offset drivers (F/include/wemvaExtShotsGpuFunctions.h:13,17)
+REF_EXPORT int ref_wemva_fwd_off(R* model, R* image, R* sig, int* sp, int ns, R* rdata, int* rp, int nr, int dev) {
+    GUARD(wemvaOffsetShotsFwdGpu(model, image, sig, sp, ns, rdata, rp, nr, nullptr, nullptr, nullptr, 0, dev, 0))
+}
+REF_EXPORT int ref_wemva_adj_off(R* model, R* image, R* sig, int* sp, int ns, R* rdata, int* rp, int nr, int dev) {
+    GUARD(wemvaOffsetShotsAdjGpu(model, image, sig, sp, ns, rdata, rp, nr, nullptr, nullptr, nullptr, 0, dev, 0))
 }
 #endif

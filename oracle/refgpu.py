@@ -5,7 +5,8 @@ TEST INFRASTRUCTURE ONLY (parity checker). Each operator family is a separate
 shared library because the reference keeps its state in per-translation-unit
 globals. Every call here runs one shot through the reference's own free
 functions: init -> allocate -> fwd/adj -> deallocate. A scheme with freeSurface = 1 runs the
-reference's free-surface drivers (*FsGpu; the time-lag ones take no sloth flag).
+reference's free-surface drivers (*FsGpu; the time-lag ones take no sloth flag); one with
+extension = 1 runs its subsurface-offset drivers (*OffsetShots*Gpu).
 """
 from __future__ import annotations
 
@@ -63,6 +64,10 @@ def _fs(s):
     return bool(getattr(s, "freeSurface", 0))
 
 
+def _off(s):
+    return bool(getattr(s, "extension", 0))
+
+
 def _i(a):
     return np.ascontiguousarray(a, np.int32)
 
@@ -112,7 +117,8 @@ def bornext_fwd(s, vel, model, sig, sp, rp, sloth=0, dtype=np.float32):
     m, g = _a(model, dtype), _a(sig, dtype)
     d = np.zeros((len(rp), s.nts), dtype)
     _run("bornext", s, vel, dtype,
-         lambda L: L.ref_bornext_fwd_fs(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0) if _fs(s) else
+         lambda L: L.ref_bornext_fwd_off(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0) if _off(s) else
+         L.ref_bornext_fwd_fs(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0) if _fs(s) else
          L.ref_bornext_fwd(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), sloth, 0), nExt=s.nExt)
     return d
 
@@ -122,7 +128,8 @@ def bornext_adj(s, vel, data, sig, sp, rp, sloth=0, dtype=np.float32):
     d, g = _a(data, dtype), _a(sig, dtype)
     m = np.zeros((s.nExt, s.nx, s.nz), dtype)
     _run("bornext", s, vel, dtype,
-         lambda L: L.ref_bornext_adj_fs(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0) if _fs(s) else
+         lambda L: L.ref_bornext_adj_off(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0) if _off(s) else
+         L.ref_bornext_adj_fs(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0) if _fs(s) else
          L.ref_bornext_adj(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), sloth, 0), nExt=s.nExt)
     return m
 
@@ -132,7 +139,8 @@ def tomo_fwd(s, vel, model, ext, sig, sp, rp, sloth=0, leg1=1, leg2=1, dtype=np.
     m, e, g = _a(model, dtype), _a(ext, dtype), _a(sig, dtype)
     d = np.zeros((len(rp), s.nts), dtype)
     _run("tomo", s, vel, dtype,
-         lambda L: L.ref_tomo_fwd_fs(_p(m), _p(d), _p(e), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0) if _fs(s) else
+         lambda L: L.ref_tomo_fwd_off(_p(m), _p(d), _p(e), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0) if _off(s) else
+         L.ref_tomo_fwd_fs(_p(m), _p(d), _p(e), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0) if _fs(s) else
          L.ref_tomo_fwd(_p(m), _p(d), _p(e), _p(g), _p(sp), len(sp), _p(rp), len(rp), sloth, 0),
          nExt=s.nExt, leg1=leg1, leg2=leg2)
     return d
@@ -143,7 +151,8 @@ def tomo_adj(s, vel, data, ext, sig, sp, rp, sloth=0, leg1=1, leg2=1, dtype=np.f
     d, e, g = _a(data, dtype), _a(ext, dtype), _a(sig, dtype)
     m = np.zeros((s.nx, s.nz), dtype)
     _run("tomo", s, vel, dtype,
-         lambda L: L.ref_tomo_adj_fs(_p(m), _p(d), _p(e), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0) if _fs(s) else
+         lambda L: L.ref_tomo_adj_off(_p(m), _p(d), _p(e), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0) if _off(s) else
+         L.ref_tomo_adj_fs(_p(m), _p(d), _p(e), _p(g), _p(sp), len(sp), _p(rp), len(rp), 0) if _fs(s) else
          L.ref_tomo_adj(_p(m), _p(d), _p(e), _p(g), _p(sp), len(sp), _p(rp), len(rp), sloth, 0),
          nExt=s.nExt, leg1=leg1, leg2=leg2)
     return m
@@ -154,7 +163,8 @@ def wemva_fwd(s, vel, model, sig, sp, rp, rdata, leg1=1, leg2=1, dtype=np.float3
     m, g, r = _a(model, dtype), _a(sig, dtype), _a(rdata, dtype)
     img = np.zeros((s.nExt, s.nx, s.nz), dtype)
     _run("wemva", s, vel, dtype,
-         lambda L: L.ref_wemva_fwd(_p(m), _p(img), _p(g), _p(sp), len(sp), _p(r), _p(rp), len(rp), 0),
+         lambda L: (L.ref_wemva_fwd_off if _off(s) else L.ref_wemva_fwd)(
+             _p(m), _p(img), _p(g), _p(sp), len(sp), _p(r), _p(rp), len(rp), 0),
          nExt=s.nExt, leg1=leg1, leg2=leg2)
     return img
 
@@ -164,6 +174,7 @@ def wemva_adj(s, vel, image, sig, sp, rp, rdata, leg1=1, leg2=1, dtype=np.float3
     img, g, r = _a(image, dtype), _a(sig, dtype), _a(rdata, dtype)
     m = np.zeros((s.nx, s.nz), dtype)
     _run("wemva", s, vel, dtype,
-         lambda L: L.ref_wemva_adj(_p(m), _p(img), _p(g), _p(sp), len(sp), _p(r), _p(rp), len(rp), 0),
+         lambda L: (L.ref_wemva_adj_off if _off(s) else L.ref_wemva_adj)(
+             _p(m), _p(img), _p(g), _p(sp), len(sp), _p(r), _p(rp), len(rp), 0),
          nExt=s.nExt, leg1=leg1, leg2=leg2)
     return m

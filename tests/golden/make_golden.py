@@ -13,6 +13,8 @@ Run on a machine with a B200 and the oracle/_ref libraries built:
     python tests/golden/make_golden.py OUT.npz
     python tests/golden/make_golden.py --fs OUT_FS.npz   # free-surface drivers (*FsGpu) ->
                                                           # tests/golden/reference_small_fs.npz
+    python tests/golden/make_golden.py --offset OUT.npz  # subsurface-offset drivers ->
+                                                          # tests/golden/reference_small_offset.npz
 
 Every input is generated here from fixed seeds and stored in the file too, so
 the test does not depend on this script's random streams.
@@ -34,18 +36,18 @@ from cases import interior_mask, make_case  # noqa: E402
 CASE = dict(seed=11, nzi=32, nxi=48, nts=30, sub=3, nExt=5, minPad=8, nshots=1)
 
 
-def main(out, fs=False):
+def main(out, fs=False, offset=False):
     assert CASE["nzi"] % 16 == 0 and CASE["nxi"] % 16 == 0
     c = make_case(**CASE)
     s = c.scheme
-    if fs:
+    if fs or offset:
         import dataclasses
-        s = dataclasses.replace(s, freeSurface=1)
+        s = dataclasses.replace(s, freeSurface=int(fs), extension=int(offset))
     rng = np.random.default_rng(1234)
     mask = interior_mask(c.nx, c.nz)
     sp, rp, sig = c.src_pos[0], c.rec_pos[0], c.sig[0]
     f = dict(vel=c.vel, src_pos=sp, rec_pos=rp, sig=sig,
-             scheme=np.array([s.nz, s.nx, s.nts, s.sub, s.minPad, s.nExt, s.freeSurface], np.int64),
+             scheme=np.array([s.nz, s.nx, s.nts, s.sub, s.minPad, s.nExt, s.freeSurface, s.extension], np.int64),
              scheme_f=np.array([s.dz, s.dx, s.dts, s.alphaCos], np.float64))
     f["data_in"] = (rng.standard_normal((len(rp), s.nts)) * 1e-3).astype(np.float32)
     f["dm"] = (rng.standard_normal((c.nx, c.nz)) * mask).astype(np.float32)
@@ -66,6 +68,19 @@ def main(out, fs=False):
                 f["tomo_fwd_" + k] = refgpu.tomo_fwd(s, v, f["dm"], f["ext"], sig, sp, rp, leg1=l1, leg2=l2, dtype=dt)
                 f["tomo_adj_" + k] = refgpu.tomo_adj(s, v, f["data_in"], f["ext"], sig, sp, rp, leg1=l1, leg2=l2,
                                                      dtype=dt)
+            continue
+        if offset:  # the offset drivers of the extended families (no sloth flag)
+            f[f"bornext_fwd_{tag}"] = refgpu.bornext_fwd(s, v, f["ext"], sig, sp, rp, dtype=dt)
+            f[f"bornext_adj_{tag}"] = refgpu.bornext_adj(s, v, f["data_in"], sig, sp, rp, dtype=dt)
+            for l1, l2 in ((1, 1), (1, 0), (0, 1)):
+                k = f"l{l1}{l2}_{tag}"
+                f["tomo_fwd_" + k] = refgpu.tomo_fwd(s, v, f["dm"], f["ext"], sig, sp, rp, leg1=l1, leg2=l2, dtype=dt)
+                f["tomo_adj_" + k] = refgpu.tomo_adj(s, v, f["data_in"], f["ext"], sig, sp, rp, leg1=l1, leg2=l2,
+                                                     dtype=dt)
+                f["wemva_fwd_" + k] = refgpu.wemva_fwd(s, v, f["dm"], sig, sp, rp, f["rdata"], leg1=l1, leg2=l2,
+                                                       dtype=dt)
+                f["wemva_adj_" + k] = refgpu.wemva_adj(s, v, f["image_in"], sig, sp, rp, f["rdata"], leg1=l1,
+                                                       leg2=l2, dtype=dt)
             continue
         f[f"nl_fwd_{tag}"] = refgpu.nl_fwd(s, v, sig, sp, rp, dtype=dt)
         f[f"nl_adj_{tag}"] = refgpu.nl_adj(s, v, f["data_in"], sp, rp, dtype=dt)
@@ -90,6 +105,7 @@ def main(out, fs=False):
 
 
 if __name__ == "__main__":
-    args = [a for a in sys.argv[1:] if a != "--fs"]
-    fs = "--fs" in sys.argv[1:]
-    main(args[0] if args else os.path.join(HERE, "reference_small_fs.npz" if fs else "reference_small.npz"), fs)
+    args = [a for a in sys.argv[1:] if a not in ("--fs", "--offset")]
+    fs, offset = "--fs" in sys.argv[1:], "--offset" in sys.argv[1:]
+    name = "reference_small_fs.npz" if fs else ("reference_small_offset.npz" if offset else "reference_small.npz")
+    main(args[0] if args else os.path.join(HERE, name), fs, offset)

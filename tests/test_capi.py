@@ -28,7 +28,7 @@ def test_error_without_gpu_is_reported():
     if torch.cuda.is_available():
         return
     from acoustic_isotropic_operators_b200 import _capi as A
-    p = A.AioParams(30, 30, 10, 2, 5, 1, 10.0, 10.0, 0.004, 0.99, 1, 1, 0, 0, 0, 0, 0, 0, 0, 0)
+    p = A.AioParams(30, 30, 10, 2, 5, 1, 10.0, 10.0, 0.004, 0.99, 1, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0)
     h = ctypes.c_void_p()
     import numpy as np
     v2 = np.ones(900, np.float32)

@@ -33,9 +33,10 @@ def _load(path):
     f = {k: z[k] for k in z.files}
     nz, nx, nts, sub, minPad, nExt = (int(v) for v in f["scheme"][:6])
     fs = int(f["scheme"][6]) if len(f["scheme"]) > 6 else 0
+    ext_axis = int(f["scheme"][7]) if len(f["scheme"]) > 7 else 0
     dz, dx, dts, alpha = (float(v) for v in f["scheme_f"])
     f["s"] = orc.Scheme(nz=nz, nx=nx, nts=nts, dts=dts, sub=sub, dz=dz, dx=dx, minPad=minPad, nExt=nExt,
-                        alphaCos=alpha, freeSurface=fs)
+                        alphaCos=alpha, freeSurface=fs, extension=ext_axis)
     return f
 
 
@@ -128,5 +129,32 @@ def test_free_surface(tag):
                        f"tomo_fwd_l{l1}{l2}"))
         checks.append((orc.tomo_adj(s, v, g["data_in"], g["ext"], sig, sp, rp, dtype=dt, leg1=l1, leg2=l2),
                        f"tomo_adj_l{l1}{l2}"))
+    for got, key in checks:
+        assert rel_l2(got, g[f"{key}_{tag}"]) < TOL[tag], key
+
+
+GOLD_OFF = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_small_offset.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(GOLD_OFF), reason="subsurface-offset fixtures not generated")
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+def test_subsurface_offset(tag):
+    """Oracle with extension = 1 vs the reference's subsurface-offset drivers run on a B200:
+    extended Born, tomo and WEMVA (all legs), forward and adjoint."""
+    g = _load(GOLD_OFF)
+    s, v, dt = g["s"], g["vel"].astype(DT[tag]), DT[tag]
+    assert s.extension == 1
+    sp, rp, sig = g["src_pos"], g["rec_pos"], g["sig"]
+    checks = [(orc.bornext_fwd(s, v, g["ext"], sig, sp, rp, dtype=dt), "bornext_fwd"),
+              (orc.bornext_adj(s, v, g["data_in"], sig, sp, rp, dtype=dt), "bornext_adj")]
+    for l1, l2 in ((1, 1), (1, 0), (0, 1)):
+        k = f"l{l1}{l2}"
+        checks += [(orc.tomo_fwd(s, v, g["dm"], g["ext"], sig, sp, rp, dtype=dt, leg1=l1, leg2=l2), "tomo_fwd_" + k),
+                   (orc.tomo_adj(s, v, g["data_in"], g["ext"], sig, sp, rp, dtype=dt, leg1=l1, leg2=l2),
+                    "tomo_adj_" + k),
+                   (orc.wemva_fwd(s, v, g["dm"], sig, sp, rp, g["rdata"], dtype=dt, leg1=l1, leg2=l2),
+                    "wemva_fwd_" + k),
+                   (orc.wemva_adj(s, v, g["image_in"], sig, sp, rp, g["rdata"], dtype=dt, leg1=l1, leg2=l2),
+                    "wemva_adj_" + k)]
     for got, key in checks:
         assert rel_l2(got, g[f"{key}_{tag}"]) < TOL[tag], key
