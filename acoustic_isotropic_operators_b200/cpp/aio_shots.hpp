@@ -291,9 +291,8 @@ class fdParam {
         p.stepper = AIO_STEPPER_AUTO;
         p.chunkColumns = 0;
         p.freeSurface = _freeSurface;
-        // the extended classes run their time-lag drivers for "time" and the subsurface-offset ones
-        // otherwise (F/src/BornExtGpu.cpp:41-59, the same branch in tomoExtGpu.cpp and wemvaExtGpu.cpp)
-        p.extension = _extension == "time" ? AIO_EXT_TIME : AIO_EXT_OFFSET;
+        // time-lag or subsurface-offset drivers of the extended classes (F/src/BornExtGpu.cpp:41-59)
+        p.extension = _extension == "offset" ? AIO_EXT_OFFSET : AIO_EXT_TIME;
         return p;
     }
 
@@ -619,6 +618,14 @@ class BornFamily : public ShotLoop {
                std::vector<std::shared_ptr<deviceGpu>> rec)
         : ShotLoop(vel, par, family), _sourcesVector(src), _sourcesSignalsVector(sig), _receiversVector(rec) {
         _recFirst = sig.size() != 1;
+        // The reference's extended classes call their time-lag drivers for "time" and their
+        // subsurface-offset ones for "offset"; any other value runs no driver in tomo, WEMVA and
+        // the extended Born adjoint (F/src/tomoExtGpu.cpp:48-60, wemvaExtGpu.cpp:131-154,
+        // BornExtGpu.cpp:95-124), so it is refused here.
+        if (family == AIO_BORN_EXT || family == AIO_TOMO_EXT || family == AIO_WEMVA_EXT) {
+            const std::string e = par->getString("extension", "none");
+            if (e != "time" && e != "offset") fail("extension must be \"time\" or \"offset\" for the extended operators");
+        }
     }
 
   protected:

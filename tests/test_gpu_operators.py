@@ -31,7 +31,7 @@ def setup(api):
     vel = (2000.0 + 400.0 * zz + 50.0 * rng.random((NX, NZ))).astype(np.float32)
     par = api.params(nts=NTS, dts=DTS, sub=SUB, nz=NZ, nx=NX, zPadMinus=PAD, zPadPlus=PAD, xPadMinus=PAD,
                      xPadPlus=PAD, dz=10.0, dx=10.0, fMax=20.0, blockSize=16, fat=5, nShot=2, iGpu=[0], nExt=5,
-                     leg1=1, leg2=1)
+                     leg1=1, leg2=1, extension="time")
     v = api.vector(vel, [(NZ, 0.0, 10.0), (NX, 0.0, 10.0)])
     nl = api.pyAcoustic_iso_float_nl
     srcs = [nl.deviceGpu([9], [15], v, NTS, 0, 0, 0), nl.deviceGpu([10], [40], v, NTS, 0, 0, 0)]
@@ -40,7 +40,10 @@ def setup(api):
     wav = ((1 - 2 * (np.pi * 15 * t) ** 2) * np.exp(-(np.pi * 15 * t) ** 2)).astype(np.float32)
     sig = api.vector(wav[None, :], [(NTS, 0.0, DTS), (1, 0.0, 1.0)])
     s = orc.Scheme(nz=NZ, nx=NX, nts=NTS, dts=DTS, sub=SUB, dz=10.0, dx=10.0, minPad=PAD, nExt=5)
-    return dict(vel=vel, v=v, par=par, srcs=srcs, rec=rec, wav=wav, sig=sig, scheme=s, rng=rng)
+    par_off = api.params(nts=NTS, dts=DTS, sub=SUB, nz=NZ, nx=NX, zPadMinus=PAD, zPadPlus=PAD, xPadMinus=PAD,
+                         xPadPlus=PAD, dz=10.0, dx=10.0, fMax=20.0, blockSize=16, fat=5, nShot=2, iGpu=[0], nExt=5,
+                         leg1=1, leg2=1, extension="offset")
+    return dict(vel=vel, v=v, par=par, par_off=par_off, srcs=srcs, rec=rec, wav=wav, sig=sig, scheme=s, rng=rng)
 
 
 def oracle_source(st, dev, d2):
@@ -100,9 +103,13 @@ def test_nonlinear_forward_matches_oracle(api, setup):
         assert rel_l2(data.getNdArray()[i], rec_gather(st, dreg)) < 1e-5
 
 
-@pytest.mark.parametrize("family", ["nl", "born", "born_ext", "tomo", "wemva"])
+@pytest.mark.parametrize("family", ["nl", "born", "born_ext", "tomo", "wemva", "born_ext_offset", "tomo_offset",
+                                    "wemva_offset"])
 def test_dot_product(api, setup, family):
-    st = setup
+    st = dict(setup)
+    if family.endswith("_offset"):  # the same classes with extension = "offset"
+        st["par"] = st["par_off"]
+        family = family[:-len("_offset")]
     rng = np.random.default_rng(7)
     img2 = [(NZ, 0.0, 10.0), (NX, 0.0, 10.0)]
     ext3 = [(NZ, 0.0, 10.0), (NX, 0.0, 10.0), (5, -2 * DTS, DTS)]
@@ -130,3 +137,13 @@ def test_dot_product(api, setup, family):
         m1, d1 = api.vector(None, img2), api.vector(None, ext3)
     op.setDomainRange(m1, d1)
     assert op.dotTest(False, 1e-5)
+
+
+def test_extension_must_be_named(api, setup):
+    """The extended classes refuse an extension other than "time" / "offset" (the reference runs no
+    driver for it in tomo, WEMVA and the extended Born adjoint)."""
+    st = setup
+    par = api.params(nts=NTS, dts=DTS, sub=SUB, nz=NZ, nx=NX, zPadMinus=PAD, zPadPlus=PAD, xPadMinus=PAD,
+                     xPadPlus=PAD, dz=10.0, dx=10.0, fMax=20.0, blockSize=16, fat=5, nShot=2, iGpu=[0], nExt=5)
+    with pytest.raises(Exception):
+        api.pyAcoustic_iso_float_born_ext.BornExtShotsGpu(st["v"], par, st["srcs"], [st["sig"]], [st["rec"]])
