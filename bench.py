@@ -466,6 +466,11 @@ def main():
         except Exception:
             traffic = None
 
+    try:  # plan of the timed region's last launch (a receiver pass of the last wave)
+        plan = ctx.blocked_plan(0) if kernel_name(args, w).startswith("k_tile") else None
+    except Exception:
+        plan = None
+
     # ------------------------------------------------ e2e through the C ABI (host buffers)
     e2e = None
     if not args.no_e2e:
@@ -493,10 +498,6 @@ def main():
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"1 shot, Born forward+adjoint, full grid, nts={nts_sample} ({dt:.1f} s)"}
 
-    try:
-        plan = ctx.blocked_plan(0) if kernel_name(args, w).startswith("k_tile") else None  # last launch's plan
-    except Exception:
-        plan = None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
