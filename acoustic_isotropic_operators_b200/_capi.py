@@ -54,7 +54,8 @@ EXPORTED = [
     "aio_BornOffsetShotsFwdGpu", "aio_BornOffsetShotsAdjGpu", "aio_BornOffsetShotsFwdFsGpu",
     "aio_BornOffsetShotsAdjFsGpu", "aio_tomoOffsetShotsFwdGpu", "aio_tomoOffsetShotsAdjGpu",
     "aio_tomoOffsetShotsFwdFsGpu", "aio_tomoOffsetShotsAdjFsGpu", "aio_wemvaOffsetShotsFwdGpu",
-    "aio_wemvaOffsetShotsAdjGpu",
+    "aio_wemvaOffsetShotsAdjGpu", "aio_born_forward_wavefield", "aio_born_adjoint_wavefield",
+    "aio_BornShotsFwdGpuWavefield", "aio_BornShotsAdjGpuWavefield",
 ]
 
 

@@ -656,6 +656,25 @@ class BornFamily : public ShotLoop {
             body(g, s0, s1, ps, shots);
         });
     }
+    // Prepare shot i alone (sources, receivers, optional input data) for a one-shot call.
+    aio_shot prepareOne(int i, const std::shared_ptr<SEP::float3DReg>* dataIn, PreparedShot& s) const {
+        const fdParam& f = fd();
+        prepareSource(*_sourcesVector[i], _sourcesSignalsVector[sigIndex(_sourcesSignalsVector.size(), i)]->getVals(),
+                      true, s);
+        prepareReceivers(*_receiversVector[recIndex(_receiversVector, i)], s);
+        if (dataIn) {
+            const int nRecIrreg = (*dataIn)->getHyper()->getAxis(2).n;
+            spreadData(const_cast<std::vector<std::shared_ptr<deviceGpu>>&>(_receiversVector), i,
+                       (*dataIn)->getVals() + (size_t)i * nRecIrreg * f._nts, s.dataReg);
+        }
+        return toShot(s);
+    }
+    // A coarse wavefield container [nts][nx][nz] (zeros), as the reference's setAllWavefields(1).
+    std::shared_ptr<SEP::float3DReg> coarseWavefield() const {
+        const fdParam& f = fd();
+        return std::make_shared<SEP::float3DReg>(SEP::axis(f._nz, f._oz, f._dz), SEP::axis(f._nx, f._ox, f._dx),
+                                                 SEP::axis(f._nts, f._ots, f._dts));
+    }
     // out (+)= sum over GPUs of per-GPU partial images
     void sumImages(std::vector<std::vector<float>>& parts, float* out, size_t n, bool add) const {
         if (!add) std::fill(out, out + n, 0.f);
@@ -698,11 +717,36 @@ class BornShotsGpu : public Operator<SEP::float2DReg, SEP::float3DReg>, public a
         });
         sumImages(parts, model->getVals(), n, add);
     }
-    void forwardWavefield(const bool, const std::shared_ptr<SEP::float2DReg>, std::shared_ptr<SEP::float3DReg>) {
-        aio_ops::fail("BornShotsGpu::forwardWavefield: saved Born wavefields are not available in this build");
+    // forward / adjoint of every shot, plus the coarse wavefields of shot wavefieldShotNumber when
+    // saveWavefield = 1 (F/src/BornShotsGpu.cpp:145-340, F/src/BornGpu.cpp:37-50): source and
+    // scattered wavefields (forward), the scaled receiver wavefield (adjoint); with
+    // saveWavefield = 0 the reference returns zero-filled containers, and so does this class.
+    void forwardWavefield(const bool add, const std::shared_ptr<SEP::float2DReg> model,
+                          std::shared_ptr<SEP::float3DReg> data) {
+        forward(add, model, data);
+        _srcWavefield = coarseWavefield();
+        _secWavefield = coarseWavefield();
+        if (_saveWavefield != 1 || _wavefieldShotNumber < 0 || _wavefieldShotNumber >= _nShot) return;
+        aio_ops::PreparedShot ps;
+        aio_shot sh = prepareOne(_wavefieldShotNumber, nullptr, ps);
+        std::vector<float> scratch((size_t)sh.nReceiversReg * fd()._nts);
+        sh.data = scratch.data();
+        aio_ops::ck(aio_born_forward_wavefield(context(0), model->getVals(), &sh, AIO_MEM_HOST,
+                                               _srcWavefield->getVals(), _secWavefield->getVals()));
     }
-    void adjointWavefield(const bool, const std::shared_ptr<SEP::float2DReg>, std::shared_ptr<SEP::float3DReg>) {
-        aio_ops::fail("BornShotsGpu::adjointWavefield: saved Born wavefields are not available in this build");
+    void adjointWavefield(const bool add, const std::shared_ptr<SEP::float2DReg> model,
+                          std::shared_ptr<SEP::float3DReg> data) {
+        adjoint(add, model, data);
+        _srcWavefield = coarseWavefield();
+        _secWavefield = coarseWavefield();
+        if (_saveWavefield != 1 || _wavefieldShotNumber < 0 || _wavefieldShotNumber >= _nShot) return;
+        aio_ops::PreparedShot ps;
+        aio_shot sh = prepareOne(_wavefieldShotNumber, &data, ps);
+        std::vector<float> image((size_t)model->size());
+        // the reference's adjoint wavefield driver returns the receiver wavefield only: the source
+        // wavefield container stays zero
+        aio_ops::ck(aio_born_adjoint_wavefield(context(0), image.data(), 0, &sh, AIO_MEM_HOST, nullptr,
+                                               _secWavefield->getVals()));
     }
     std::shared_ptr<SEP::float3DReg> getSrcWavefield() { return _srcWavefield; }
     std::shared_ptr<SEP::float3DReg> getSecWavefield() { return _secWavefield; }

@@ -1898,6 +1898,67 @@ struct Context {
         }
     }
 
+    // Full padded-grid wavefield output [nts][nx][nz] (zero FAT ring) from interior slices.
+    void wavefield_out(float* dst, const DevMem& src, int mem) {
+        const size_t bytes = (size_t)g.nts * g.nz * g.nx * 4;
+        if (mem == AIO_MEM_HOST) std::memset(dst, 0, bytes);
+        else AIO_CK(cudaMemsetAsync(dst, 0, bytes, st));
+        from_interior(dst, src.as<float>(), g.nts, mem);
+    }
+
+    // Born forward of one shot with its coarse source and scattered wavefields
+    // (BornShotsFwdGpuWavefield, F/src/BornShotsGpuFunctions.cu:390-535), per-fine-step stepper.
+    void born_forward_wavefield(const float* model, const aio_shot* shot, int mem, float* srcW, float* secW) {
+        begin_call();
+        require(srcW && secW, "wavefield output is NULL");
+        float* dm = stage_model(model, 1, mem, this->model);
+        scale_shared(dm, 1, 0);
+        Needs n;
+        n.nWavefields = 2;
+        n.ss = true;
+        require(wave_size(n, 1, shot) >= 1, "device memory budget cannot hold the wavefields of one shot");
+        setup_wave(n, 1, shot, mem, false, false);
+        source_wavefield(1, wf1);
+        const float* W = wf1.as<float>();
+        fwd_dense_pass(
+            1, [&](int t, long long slot) { img_fwd(1, slot, dm, 0, W, t); }, false, true, ACC_FULL, &wf2,
+            [](int, long long) {});
+        download_data(1, shot, mem);
+        wavefield_out(srcW, wf1, mem);
+        wavefield_out(secW, wf2, mem);
+        sync();
+    }
+
+    // Born adjoint of one shot with its receiver wavefield scaled by 2/v^3 v^2 dtw^2
+    // (BornShotsAdjGpuWavefield, F/src/BornShotsGpuFunctions.cu:959-1103, which returns only that
+    // one) and, when srcW is not null, its coarse source wavefield.
+    void born_adjoint_wavefield(float* modelOut, int add, const aio_shot* shot, int mem, float* srcW, float* recW) {
+        begin_call();
+        require(recW != nullptr, "wavefield output is NULL");
+        Needs n;
+        n.nWavefields = 2;
+        n.nImg = 1;
+        require(wave_size(n, 1, shot) >= 1, "device memory budget cannot hold the wavefields of one shot");
+        float* out = stage_out(modelOut, 1, add, mem);
+        setup_wave(n, 1, shot, mem, true, false);
+        source_wavefield(1, wf1);
+        zero_images(1, 1);
+        AIO_CK(cudaMemsetAsync(wf2.p, 0, (size_t)g.nts * g.isz * 4, st));
+        const float* W = wf1.as<float>();
+        std::vector<const float*> din(dataPtr.begin(), dataPtr.end());
+        adj_sparse_pass(1, din, nullptr, ACC_RING, nullptr, [&](int t, long long slot) {
+            k_record_scale<<<ew_grid(1, g.isz), 256, 0, st>>>(wf2.as<float>() + (long long)t * g.isz, ring_ptr(slot),
+                                                               rs.as<float>(), v2.as<float>(), g.isz);
+            kcheck();
+            img_adj(1, slot, W, t);
+        });
+        reduce_images(1, 1, 0, out, true);
+        write_model(modelOut, 1, add, mem, out);
+        if (srcW) wavefield_out(srcW, wf1, mem);
+        wavefield_out(recW, wf2, mem);
+        sync();
+    }
+
     // Extended (time-lag) Born adjoint (F/src/BornExtShotsGpuFunctions.cu:1525-1675).
     void born_ext_adjoint(float* modelOut, int add, int nShots, const aio_shot* shots, int mem) {
         begin_call();
@@ -2313,6 +2374,20 @@ AIO_API int aio_context_blocked_plan(aio_context* ctx, int nShots, int* plan) {
         plan[3] = pl.nChunks;
     });
 }
+AIO_API int aio_born_forward_wavefield(aio_context* ctx, const float* model, const aio_shot* shot, int memSpace,
+                                       float* srcWavefield, float* secWavefield) {
+    return guard([&] {
+        require(shot != nullptr, "shot is NULL");
+        ctx->c.born_forward_wavefield(model, shot, memSpace, srcWavefield, secWavefield);
+    });
+}
+AIO_API int aio_born_adjoint_wavefield(aio_context* ctx, float* modelOut, int add, const aio_shot* shot, int memSpace,
+                                       float* srcWavefield, float* recWavefield) {
+    return guard([&] {
+        require(shot != nullptr, "shot is NULL");
+        ctx->c.born_adjoint_wavefield(modelOut, add, shot, memSpace, srcWavefield, recWavefield);
+    });
+}
 AIO_API int aio_born_adjoint_shots(aio_context* ctx, float* const* images, int nShots, const aio_shot* shots,
                                    int memSpace) {
     return guard([&] { ctx->c.born_adjoint_shots(images, nShots, shots, memSpace); });
@@ -2427,6 +2502,26 @@ AIO_API int aio_BornShotsAdjGpu(float* model, float* dataRegDts, float* sourcesS
     return guard([&] {
         aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
         seam_ctx(AIO_BORN, iGpu).born_adjoint(model, 0, 1, &s, AIO_MEM_HOST);
+    });
+}
+
+AIO_API int aio_BornShotsFwdGpuWavefield(float* model, float* dataRegDts, float* sourcesSignals, int* sp, int ns,
+                                         int* rp, int nr, float* srcWavefield, float* scatWavefield, int iGpu,
+                                         int iGpuId) {
+    (void)iGpuId;
+    return guard([&] {
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
+        seam_ctx(AIO_BORN, iGpu).born_forward_wavefield(model, &s, AIO_MEM_HOST, srcWavefield, scatWavefield);
+    });
+}
+AIO_API int aio_BornShotsAdjGpuWavefield(float* model, float* dataRegDts, float* sourcesSignals, int* sp, int ns,
+                                         int* rp, int nr, float* srcWavefield, float* recWavefield, int iGpu,
+                                         int iGpuId) {
+    (void)iGpuId;
+    return guard([&] {
+        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
+        (void)srcWavefield;  // the reference's driver returns the receiver wavefield only
+        seam_ctx(AIO_BORN, iGpu).born_adjoint_wavefield(model, 0, &s, AIO_MEM_HOST, nullptr, recWavefield);
     });
 }
 

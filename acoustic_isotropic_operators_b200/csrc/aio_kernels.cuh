@@ -262,6 +262,11 @@ __global__ void k_img_time_adj(Acc* m, long long mSt, float* r, long long rSt, c
     }
 }
 
+// recordScaleWavefield (F/src/kernelsGpu.cu:145-153): W += r * rs * v2 (one coarse slice).
+__global__ void k_record_scale(float* W, const float* r, const float* rs, const float* v2, long long isz) {
+    AIO_GRID_STRIDE(i, isz) W[i] += r[i] * rs[i] * v2[i];
+}
+
 // ---- subsurface (horizontal) offsets, interior-slice layout (x*ip + z), x in [0, nxi) ----
 // imagingOffsetFwdGpu + scaleSecondarySourceFd (F/src/kernelsGpu.cu:381-395, 269-276):
 //   ss(x) = v2(x) * (ss(x) + sum_s m_{s+h}(x-s) W(x-2s)) over the offsets whose model point x-s

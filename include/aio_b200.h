@@ -132,6 +132,15 @@ int aio_born_adjoint(aio_context* ctx, float* model, int add, int nShots, const 
 /* Born adjoint returning each shot's own image: images[s] (nz*nx, overwritten, host or device
  * per memSpace). The shots still run together; used to batch independent requests. */
 int aio_born_adjoint_shots(aio_context* ctx, float* const* images, int nShots, const aio_shot* shots, int memSpace);
+/* Born of one shot with its coarse wavefields, [nts][nx][nz] each with a zero FAT ring (the
+ * reference's forwardWavefield / adjointWavefield, getSrcWfld / getSecWfld): forward returns the
+ * source and scattered wavefields (F/src/BornShotsGpuFunctions.cu:390-535), adjoint the receiver
+ * wavefield scaled by 2/v^3 v^2 dtw^2 (:959-1103) and, when srcWavefield is not NULL, the source
+ * wavefield. Per-fine-step stepper. */
+int aio_born_forward_wavefield(aio_context* ctx, const float* model, const aio_shot* shot, int memSpace,
+                               float* srcWavefield, float* secWavefield);
+int aio_born_adjoint_wavefield(aio_context* ctx, float* model, int add, const aio_shot* shot, int memSpace,
+                               float* srcWavefield, float* recWavefield);
 /* Extended (time-lag) Born: model nExt*nz*nx. */
 int aio_born_ext_forward(aio_context* ctx, const float* model, int nShots, const aio_shot* shots, int memSpace);
 int aio_born_ext_adjoint(aio_context* ctx, float* model, int add, int nShots, const aio_shot* shots, int memSpace);
@@ -201,6 +210,15 @@ int aio_BornShotsFwdGpu(float* model, float* dataRegDts, float* sourcesSignals, 
 int aio_BornShotsAdjGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
                         int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
                         float* recWavefield, int iGpu, int iGpuId);
+/* F/include/BornShotsGpuFunctions.h:17 (coarse source and scattered wavefields out, [nts][nx][nz]) */
+int aio_BornShotsFwdGpuWavefield(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                                 int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
+                                 float* scatWavefield, int iGpu, int iGpuId);
+/* F/include/BornShotsGpuFunctions.h:29 (scaled coarse receiver wavefield out; srcWavefield untouched, as in
+ * the reference) */
+int aio_BornShotsAdjGpuWavefield(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                                 int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
+                                 float* recWavefield, int iGpu, int iGpuId);
 /* F/include/BornExtShotsGpuFunctions.h:6-54 (time-lag extension) */
 int aio_initBornExtGpu(float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad, int blockSize,
                        float alphaCos, int nExt, int nGpu, int iGpuId, int iGpuAlloc);

@@ -577,8 +577,10 @@ static void nl_adj(const Grid<T>& g, T* model, const int* sp, int ns, const int*
 
 // Born forward, F/src/BornShotsGpuFunctions.cu:260-388.
 template <class T>
+// Wsec (optional): the coarse scattered wavefield (BornShotsFwdGpuWavefield,
+// F/src/BornShotsGpuFunctions.cu:390-535, interpWavefield of the scattered pass).
 static void born_fwd(const Grid<T>& g, const T* model, const T* sig, const int* sp, int ns, const int* rp, int nr,
-                     T* data, T* Wsrc) {
+                     T* data, T* Wsrc, T* Wsec = nullptr) {
     Work<T> w(g.N());
     const size_t N = g.N();
     std::vector<T> Wloc;
@@ -588,16 +590,29 @@ static void born_fwd(const Grid<T>& g, const T* model, const T* sig, const int* 
     std::vector<T> dm(model, model + N);
     scale_refl(g, dm.data());
     std::fill(data, data + (size_t)nr * g.nts, (T)0);
+    if (Wsec) std::fill(Wsec, Wsec + (size_t)g.nts * N, (T)0);
     scat_fwd_pass(
         g, w, [&](int t, T* ss) { imaging_fwd(g, dm.data(), ss, t, W); }, true,
-        [&](const T* p, int its, int it2) { record_data(g, p, data, its, it2, rp, nr); }, false,
-        [](int, T*) {});
+        [&](const T* p, int its, int it2) {
+            if (Wsec) interp_wavefield(g, Wsec, p, its, it2);
+            record_data(g, p, data, its, it2, rp, nr);
+        },
+        false, [](int, T*) {});
+}
+
+// recordScaleWavefield, F/src/kernelsGpu.cu:145-153: W[its] += r * rs * v2.
+template <class T>
+static void record_scale_wavefield(const Grid<T>& g, T* W, const T* r, int its) {
+    T* w = W + (size_t)its * g.N();
+    for_interior(g.nz, g.nx, [&](size_t i) { w[i] += r[i] * g.rs[i] * g.v2[i]; });
 }
 
 // Born adjoint, F/src/BornShotsGpuFunctions.cu:829-957.
 template <class T>
+// Wrec (optional): the coarse receiver wavefield scaled by 2/v^3 * v^2 dtw^2 (recordScaleWavefield,
+// F/src/kernelsGpu.cu:145-153, in BornShotsAdjGpuWavefield, F/src/BornShotsGpuFunctions.cu:959-1103).
 static void born_adj(const Grid<T>& g, T* model, const T* sig, const int* sp, int ns, const int* rp, int nr,
-                     const T* data, T* Wsrc) {
+                     const T* data, T* Wsrc, T* Wrec = nullptr) {
     Work<T> w(g.N());
     const size_t N = g.N();
     std::vector<T> Wloc;
@@ -619,9 +634,11 @@ static void born_adj(const Grid<T>& g, T* model, const T* sig, const int* sp, in
             std::swap(P0, P1);
         }
         imaging_adj(g, model, pR, W, its + 1);
+        if (Wrec) record_scale_wavefield(g, Wrec, pR, its + 1);
         std::swap(pR, pL);
         std::fill(pL, pL + N, (T)0);
     }
+    if (Wrec) record_scale_wavefield(g, Wrec, pR, 0);
     imaging_adj(g, model, pR, W, 0);
     scale_refl(g, model);
 }
@@ -987,14 +1004,14 @@ static Grid<T> grid_from(const OrcParams* p, const T* vel) {
         nl_adj<T>(g, model, sp, ns, rp, nr, data, W);                                                             \
     }                                                                                                             \
     ORC_EXPORT void orc_born_fwd_##SUF(const OrcParams* p, const T* vel, const T* model, const T* sig,            \
-                                       const int* sp, int ns, const int* rp, int nr, T* data, T* W) {             \
+                                       const int* sp, int ns, const int* rp, int nr, T* data, T* W, T* S) {       \
         Grid<T> g = grid_from<T>(p, vel);                                                                         \
-        born_fwd<T>(g, model, sig, sp, ns, rp, nr, data, W);                                                      \
+        born_fwd<T>(g, model, sig, sp, ns, rp, nr, data, W, S);                                                   \
     }                                                                                                             \
     ORC_EXPORT void orc_born_adj_##SUF(const OrcParams* p, const T* vel, T* model, const T* sig, const int* sp,   \
-                                       int ns, const int* rp, int nr, const T* data, T* W) {                      \
+                                       int ns, const int* rp, int nr, const T* data, T* W, T* R) {                \
         Grid<T> g = grid_from<T>(p, vel);                                                                         \
-        born_adj<T>(g, model, sig, sp, ns, rp, nr, data, W);                                                      \
+        born_adj<T>(g, model, sig, sp, ns, rp, nr, data, W, R);                                                   \
     }                                                                                                             \
     ORC_EXPORT void orc_bornext_fwd_##SUF(const OrcParams* p, const T* vel, const T* model, const T* sig,         \
                                           const int* sp, int ns, const int* rp, int nr, T* data, int sloth) {     \

@@ -114,23 +114,33 @@ def nl_adj(s, vel, data, src_pos, rec_pos, dtype=np.float64, wavefield=False):
     return (m, W) if wavefield else m
 
 
-def born_fwd(s, vel, model, sig_dtw, src_pos, rec_pos, dtype=np.float64, wavefield=False):
+def born_fwd(s, vel, model, sig_dtw, src_pos, rec_pos, dtype=np.float64, wavefield=False, secondary=False):
+    """Born forward data; wavefield=True also returns the coarse source wavefield, secondary=True
+    also the coarse scattered wavefield ((nts, nx, nz) each)."""
     vel = _arr(vel, dtype); m = _arr(model, dtype); sig = _arr(sig_dtw, dtype)
     d = np.zeros((len(rec_pos), s.nts), dtype)
-    W = np.zeros((s.nts, s.nx, s.nz), dtype) if wavefield else None
+    W = np.zeros((s.nts, s.nx, s.nz), dtype) if (wavefield or secondary) else None
+    S = np.zeros((s.nts, s.nx, s.nz), dtype) if secondary else None
     getattr(lib(), "orc_born_fwd_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(sig), _ip(src_pos),
                                                   len(src_pos), _ip(rec_pos), len(rec_pos), _p(d),
-                                                  _p(W) if W is not None else None)
+                                                  _p(W) if W is not None else None, _p(S) if S is not None else None)
+    if secondary:
+        return d, W, S
     return (d, W) if wavefield else d
 
 
-def born_adj(s, vel, data, sig_dtw, src_pos, rec_pos, dtype=np.float64, wavefield=False):
+def born_adj(s, vel, data, sig_dtw, src_pos, rec_pos, dtype=np.float64, wavefield=False, secondary=False):
+    """Born adjoint image; wavefield=True also returns the coarse source wavefield, secondary=True
+    also the scaled coarse receiver wavefield ((nts, nx, nz) each)."""
     vel = _arr(vel, dtype); d = _arr(data, dtype); sig = _arr(sig_dtw, dtype)
     m = np.zeros((s.nx, s.nz), dtype)
-    W = np.zeros((s.nts, s.nx, s.nz), dtype) if wavefield else None
+    W = np.zeros((s.nts, s.nx, s.nz), dtype) if (wavefield or secondary) else None
+    R = np.zeros((s.nts, s.nx, s.nz), dtype) if secondary else None
     getattr(lib(), "orc_born_adj_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(sig), _ip(src_pos),
                                                   len(src_pos), _ip(rec_pos), len(rec_pos), _p(d),
-                                                  _p(W) if W is not None else None)
+                                                  _p(W) if W is not None else None, _p(R) if R is not None else None)
+    if secondary:
+        return m, W, R
     return (m, W) if wavefield else m
 
 

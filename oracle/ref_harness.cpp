@@ -76,6 +76,15 @@ REF_EXPORT int ref_born_fwd(R* model, R* data, R* sig, int* sp, int ns, int* rp,
 REF_EXPORT int ref_born_adj(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
     GUARD(BornShotsAdjGpu(model, data, sig, sp, ns, rp, nr, nullptr, nullptr, 0, dev))
 }
+// wavefield drivers (F/include/BornShotsGpuFunctions.h:17,29): coarse [nts][nx][nz] wavefields out
+REF_EXPORT int ref_born_fwd_wfld(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, R* srcW, R* secW,
+                                 int dev) {
+    GUARD(BornShotsFwdGpuWavefield(model, data, sig, sp, ns, rp, nr, srcW, secW, 0, dev))
+}
+REF_EXPORT int ref_born_adj_wfld(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, R* srcW, R* recW,
+                                 int dev) {
+    GUARD(BornShotsAdjGpuWavefield(model, data, sig, sp, ns, rp, nr, srcW, recW, 0, dev))
+}
 // free-surface drivers (F/include/BornShotsGpuFunctions.h:20,32)
 REF_EXPORT int ref_born_fwd_fs(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
     GUARD(BornShotsFwdFsGpu(model, data, sig, sp, ns, rp, nr, nullptr, nullptr, 0, dev))

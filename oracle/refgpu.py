@@ -112,6 +112,30 @@ def born_adj(s, vel, data, sig, sp, rp, dtype=np.float32):
     return m
 
 
+def born_fwd_wavefields(s, vel, model, sig, sp, rp, dtype=np.float32):
+    """(data, source wavefield, scattered wavefield) from BornShotsFwdGpuWavefield."""
+    sp, rp = _i(sp), _i(rp)
+    m, g = _a(model, dtype), _a(sig, dtype)
+    d = np.zeros((len(rp), s.nts), dtype)
+    W = np.zeros((s.nts, s.nx, s.nz), dtype)
+    S = np.zeros_like(W)
+    _run("born", s, vel, dtype, lambda L: L.ref_born_fwd_wfld(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp),
+                                                              _p(W), _p(S), 0))
+    return d, W, S
+
+
+def born_adj_wavefields(s, vel, data, sig, sp, rp, dtype=np.float32):
+    """(image, source wavefield, scaled receiver wavefield) from BornShotsAdjGpuWavefield."""
+    sp, rp = _i(sp), _i(rp)
+    d, g = _a(data, dtype), _a(sig, dtype)
+    m = np.zeros((s.nx, s.nz), dtype)
+    W = np.zeros((s.nts, s.nx, s.nz), dtype)
+    R = np.zeros_like(W)
+    _run("born", s, vel, dtype, lambda L: L.ref_born_adj_wfld(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp),
+                                                              _p(W), _p(R), 0))
+    return m, W, R
+
+
 def bornext_fwd(s, vel, model, sig, sp, rp, sloth=0, dtype=np.float32):
     sp, rp = _i(sp), _i(rp)
     m, g = _a(model, dtype), _a(sig, dtype)

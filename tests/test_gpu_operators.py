@@ -147,3 +147,25 @@ def test_extension_must_be_named(api, setup):
                      xPadPlus=PAD, dz=10.0, dx=10.0, fMax=20.0, blockSize=16, fat=5, nShot=2, iGpu=[0], nExt=5)
     with pytest.raises(Exception):
         api.pyAcoustic_iso_float_born_ext.BornExtShotsGpu(st["v"], par, st["srcs"], [st["sig"]], [st["rec"]])
+
+
+def test_born_saved_wavefields(api, setup):
+    """BornShotsGpu.forwardWavefield with saveWavefield = 1 keeps the coarse source and scattered
+    wavefields of shot wavefieldShotNumber (getSrcWfld / getSecWfld), equal to the oracle's."""
+    st = setup
+    par = api.params(nts=NTS, dts=DTS, sub=SUB, nz=NZ, nx=NX, zPadMinus=PAD, zPadPlus=PAD, xPadMinus=PAD,
+                     xPadPlus=PAD, dz=10.0, dx=10.0, fMax=20.0, blockSize=16, fat=5, nShot=2, iGpu=[0],
+                     saveWavefield=1, wavefieldShotNumber=1)
+    rng = np.random.default_rng(4)
+    m = np.zeros((NX, NZ), np.float32)
+    m[5:-5, 5:-5] = rng.standard_normal((NXI, NZI))
+    op = api.pyAcoustic_iso_float_born.BornShotsGpu(st["v"], par, st["srcs"], [st["sig"]], [st["rec"]])
+    model = api.vector(m, [(NZ, 0.0, 10.0), (NX, 0.0, 10.0)])
+    data = data_vec(api)
+    op.forwardWavefield(False, model, data)
+    src, sec = op.getSrcWfld().getNdArray(), op.getSecWfld().getNdArray()
+    spos, sig = oracle_source(st, st["srcs"][1], True)
+    rpos = np.array(st["rec"].getRegPosUnique(), np.int32)
+    _, rW, rS = orc.born_fwd(st["scheme"], st["vel"], m, sig, spos, rpos, dtype=np.float32, secondary=True)
+    assert src.shape == (NTS, NX, NZ)
+    assert rel_l2(src, rW) < 1e-5 and rel_l2(sec, rS) < 1e-5
