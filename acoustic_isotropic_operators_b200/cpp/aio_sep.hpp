@@ -45,6 +45,7 @@ class hypercube {
     axis getAxis(int i) const { return (i >= 1 && i <= (int)_axes.size()) ? _axes[i - 1] : axis(1); }
     std::vector<axis> getAxes() const { return _axes; }
     int getNdim() const { return (int)_axes.size(); }
+    void addAxis(const axis& a) { _axes.push_back(a); }
     long long getN123() const {
         long long n = 1;
         for (const auto& a : _axes) n *= a.n;

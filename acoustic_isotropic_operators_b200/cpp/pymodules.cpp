@@ -9,6 +9,7 @@
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
 
+#include "aio_sepio.hpp"
 #include "aio_shots.hpp"
 
 namespace py = pybind11;
@@ -82,6 +83,38 @@ PYBIND11_MODULE(pySepLite, m) {
             return p;
         }))
         .def("set", &dictParams::set);
+    py::class_<SEP::argParams, paramObj, std::shared_ptr<SEP::argParams>>(m, "argParams")
+        .def(py::init<const std::vector<std::string>&>(), "parameters from key=value arguments and par= files")
+        .def("getInts", py::overload_cast<const std::string&>(&paramObj::getInts, py::const_));
+    // SEP .H datasets (genericIO.defaultIO.getVector / writeVector of the reference's Python)
+    m.def(
+        "getVector",
+        [](const std::string& path, int ndims) -> py::object {
+            SEP::genericRegFile f(path, usageIn);
+            auto h = f.getHyper();
+            if (ndims <= 0) ndims = h->getNdim();
+            if (ndims < h->getNdim() || ndims > 3)
+                throw std::runtime_error("SEP: " + path + " has " + std::to_string(h->getNdim()) +
+                                         " axes; vectors of 1 to 3 axes, at least as many as the file's");
+            while (h->getNdim() < ndims) h->addAxis(SEP::axis(1));
+            auto read = [&](auto v) -> py::object {
+                f.readFloatStream(v);
+                return py::cast(v);
+            };
+            if (ndims == 1) return read(std::make_shared<SEP::float1DReg>(h));
+            if (ndims == 2) return read(std::make_shared<SEP::float2DReg>(h));
+            return read(std::make_shared<SEP::float3DReg>(h));
+        },
+        py::arg("path"), py::arg("ndims") = 0);
+    m.def("writeVector", [](const std::string& p, std::shared_ptr<SEP::float1DReg> v, const std::string& f) {
+        SEP::writeVector(p, v, f);
+    }, py::arg("path"), py::arg("vec"), py::arg("data_format") = "xdr_float");
+    m.def("writeVector", [](const std::string& p, std::shared_ptr<SEP::float2DReg> v, const std::string& f) {
+        SEP::writeVector(p, v, f);
+    }, py::arg("path"), py::arg("vec"), py::arg("data_format") = "xdr_float");
+    m.def("writeVector", [](const std::string& p, std::shared_ptr<SEP::float3DReg> v, const std::string& f) {
+        SEP::writeVector(p, v, f);
+    }, py::arg("path"), py::arg("vec"), py::arg("data_format") = "xdr_float");
 }
 
 #elif AIO_MODULE == 1
@@ -106,7 +139,14 @@ PYBIND11_MODULE(pyAcoustic_iso_float_nl, m) {
         .def("getNDeviceIrreg", &deviceGpu::getNDeviceIrreg)
         .def("getRegPosUnique", [](deviceGpu& d) {
             return std::vector<int>(d.getRegPosUnique(), d.getRegPosUnique() + d.getNDeviceReg());
-        });
+        })
+        .def("getRegPos", [](deviceGpu& d) {  // corner grid indices, nCorner per device
+            return std::vector<int>(d.getRegPos(), d.getRegPos() + d.nCorner() * d.getNDeviceIrreg());
+        })
+        .def("getWeights", [](deviceGpu& d) {  // corner weights, same order as getRegPos
+            return std::vector<float>(d.getWeights(), d.getWeights() + d.nCorner() * d.getNDeviceIrreg());
+        })
+        .def("getNt", &deviceGpu::getNt);
     py::class_<nonlinearPropShotsGpu, std::shared_ptr<nonlinearPropShotsGpu>>(m, "nonlinearPropShotsGpu")
         .def(py::init<std::shared_ptr<SEP::float2DReg>, std::shared_ptr<paramObj>, std::vector<std::shared_ptr<deviceGpu>>,
                       std::vector<std::shared_ptr<deviceGpu>>>(),

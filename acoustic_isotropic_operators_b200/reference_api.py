@@ -5,8 +5,10 @@ and imports the six pybind11 modules built there by
 ``make -C acoustic_isotropic_operators_b200/cpp``:
 
 * ``pySepLite`` — SEP-compatible axis / hypercube / float1DReg / float2DReg /
-  float3DReg (``getNdArray()`` gives a writable numpy view, slowest axis first)
-  and ``dictParams`` (a paramObj built from a Python dict of par-file keys);
+  float3DReg (``getNdArray()`` gives a writable numpy view, slowest axis first),
+  ``dictParams`` (a paramObj built from a Python dict of par-file keys),
+  ``argParams`` (from ``key=value`` arguments and ``par=`` files) and the SEP .H
+  dataset reader / writer ``getVector`` / ``writeVector``;
 * ``pyAcoustic_iso_float_nl`` (``deviceGpu``, ``nonlinearPropShotsGpu``),
   ``pyAcoustic_iso_float_born`` (``BornShotsGpu``), ``pyAcoustic_iso_float_born_ext``
   (``BornExtShotsGpu``), ``pyAcoustic_iso_float_tomo`` (``tomoExtShotsGpu``),
@@ -43,3 +45,21 @@ def vector(values, axes):
 def params(**kw):
     """paramObj from keyword arguments (par-file keys, e.g. nts=1000, iGpu=[0, 1])."""
     return pySepLite.dictParams(kw)
+
+
+def io(params):
+    """paramObj from command-line arguments (``key=value`` and ``par=file``), as
+    ``genericIO.io(params=sys.argv)`` in the reference's Python programs."""
+    return pySepLite.argParams([str(a) for a in params])
+
+
+def getVector(path, ndims=0):
+    """SEP vector read from the .H dataset `path` (``genericIO.defaultIO.getVector``);
+    `ndims` pads the file's axes with n = 1 axes up to that many."""
+    return pySepLite.getVector(path, ndims)
+
+
+def writeVector(path, vec, data_format="xdr_float"):
+    """Writes `vec` as the .H dataset `path` with its data in `path@`
+    (``genericIO.defaultIO.writeVector``)."""
+    pySepLite.writeVector(path, vec, data_format)

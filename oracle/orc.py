@@ -214,3 +214,93 @@ def second_deriv(nt, dt, m, dtype=np.float64):
     d = np.zeros_like(m)
     getattr(lib(), "orc_second_deriv_" + _suf(dtype))(nt, C.c_double(dt), m.shape[0], _p(m), _p(d))
     return d
+
+
+# ------------------------------------------------------------------ devices (deviceGpu)
+# Restatement of the reference's device geometry (F/src/deviceGpu.cpp) in numpy, with
+# float32 where the reference computes in float and float64 where a double literal
+# promotes the expression, so corner indices and weights are bit-identical.
+
+def device_bilinear(zc, xc, nz, oz, dz, ox, dx, dipole=0, zshift=0.0, xshift=0.0):
+    """Corner indices and weights of devices at physical coordinates (constructor #1,
+    F/src/deviceGpu.cpp:8-81): 4 corners per device (8 with a dipole, whose corners
+    carry the negated weights of the shifted point). Returns (idx int32, w float32),
+    both of length nCorner * nDevice, device-major."""
+    f32 = np.float32
+    nc = 8 if dipole == 1 else 4
+    n = len(zc)
+    idx = np.zeros(nc * n, np.int32)
+    w = np.zeros(nc * n, np.float32)
+
+    def corners(i1, z, x, sign):
+        wz = f32(f32(f32(z) - f32(oz)) / f32(dz))
+        wx = f32(f32(f32(x) - f32(ox)) / f32(dx))
+        zr, xr = int(wz), int(wx)                    # truncation toward zero (int zReg = wz)
+        wz = f32(1.0 - float(f32(wz - f32(zr))))     # wz = wz - zReg; wz = 1.0 - wz
+        wx = f32(1.0 - float(f32(wx - f32(xr))))
+        base = xr * nz + zr
+        idx[i1:i1 + 4] = [base, base + 1, base + nz, base + nz + 1]
+        if sign > 0:
+            w[i1] = f32(wz * wx)
+            w[i1 + 1] = f32((1.0 - float(wz)) * float(wx))
+            w[i1 + 2] = f32(float(wz) * (1.0 - float(wx)))
+            w[i1 + 3] = f32((1.0 - float(wz)) * (1.0 - float(wx)))
+        else:
+            w[i1] = f32((-1.0 * float(wz)) * float(wx))
+            w[i1 + 1] = f32((-1.0 * (1.0 - float(wz))) * float(wx))
+            w[i1 + 2] = f32((-1.0 * float(wz)) * (1.0 - float(wx)))
+            w[i1 + 3] = f32((-1.0 * (1.0 - float(wz))) * (1.0 - float(wx)))
+
+    for i in range(n):
+        corners(i * nc, zc[i], xc[i], 1)
+        if nc == 8:
+            corners(i * nc + 4, f32(f32(zc[i]) + f32(zshift)), f32(f32(xc[i]) + f32(xshift)), -1)
+    return idx, w
+
+
+def device_on_grid(iz, ix, nz, dipole=0, zshift=0, xshift=0):
+    """Corner indices and weights of devices on grid points (constructors #2 and #3,
+    F/src/deviceGpu.cpp:84-190): weight 1 on the point (-1 on the dipole point), 0 on
+    the other three corners."""
+    nc = 8 if dipole == 1 else 4
+    idx = np.zeros(nc * len(iz), np.int32)
+    w = np.zeros(nc * len(iz), np.float32)
+    for i in range(len(iz)):
+        b = ix[i] * nz + iz[i]
+        idx[i * nc:i * nc + 4] = [b, b + 1, b + nz, b + nz + 1]
+        w[i * nc] = 1.0
+        if nc == 8:
+            b2 = (ix[i] + xshift) * nz + iz[i] + zshift
+            idx[i * nc + 4:i * nc + 8] = [b2, b2 + 1, b2 + nz, b2 + nz + 1]
+            w[i * nc + 4] = -1.0
+    return idx, w
+
+
+def device_unique(idx):
+    """Unique grid indices in order of first appearance and the trace of every corner
+    (convertIrregToReg, F/src/deviceGpu.cpp:192-214)."""
+    order, trace = {}, np.zeros(len(idx), np.int32)
+    for i, p in enumerate(idx):
+        trace[i] = order.setdefault(int(p), len(order))
+    return np.array(list(order), np.int32), trace
+
+
+def device_spread(idx, w, nc, sig_irreg):
+    """Device traces -> regular traces (deviceGpu::adjoint, F/src/deviceGpu.cpp:232-246),
+    float32 accumulation in device, corner order."""
+    uniq, trace = device_unique(idx)
+    sig_irreg = np.asarray(sig_irreg, np.float32)
+    reg = np.zeros((len(uniq), sig_irreg.shape[1]), np.float32)
+    for i1 in range(len(idx)):
+        reg[trace[i1]] += w[i1] * sig_irreg[i1 // nc]
+    return uniq, reg
+
+
+def device_gather(idx, w, nc, sig_reg):
+    """Regular traces -> device traces (deviceGpu::forward, F/src/deviceGpu.cpp:216-230)."""
+    _, trace = device_unique(idx)
+    sig_reg = np.asarray(sig_reg, np.float32)
+    out = np.zeros((len(idx) // nc, sig_reg.shape[1]), np.float32)
+    for i1 in range(len(idx)):
+        out[i1 // nc] += w[i1] * sig_reg[trace[i1]]
+    return out
