@@ -13,6 +13,7 @@
 // Header-only; link with libaio_b200.so.
 #pragma once
 #include <algorithm>
+#include <cmath>
 #include <iostream>
 #include <numeric>
 #include <thread>
@@ -103,6 +104,69 @@ class deviceGpu : public Operator<SEP::float2DReg, SEP::float2DReg> {
         unique();
     }
 
+    // Windowed-sinc devices (Hicks 2002, "Arbitrary source and receiver positioning in
+    // finite-difference schemes using Kaiser windowed sinc functions", Geophysics 67(1)):
+    // each device at physical coordinates spreads onto the (2r)^2 grid points around it
+    // with weights wz(iz) * wx(ix), w(i) = sinc(i - p) * K(i - p), p the coordinate in grid
+    // units, K(x) = I0(beta * sqrt(1 - (x/r)^2)) / I0(beta) the Kaiser window of half-width
+    // r = halfWidth. On a grid node the weights reduce to the node (sinc vanishes at the
+    // other integers). With a dipole the shifted point carries the negated weights. Not in
+    // the reference (its devices are bilinear); every stencil point must lie on the grid.
+    static std::shared_ptr<deviceGpu> windowedSinc(const std::shared_ptr<SEP::float1DReg> zCoord,
+                                                   const std::shared_ptr<SEP::float1DReg> xCoord,
+                                                   const std::shared_ptr<SEP::float2DReg> vel, int nt, int halfWidth = 4,
+                                                   float beta = 4.14f, int dipole = 0, float zDipoleShift = 0.f,
+                                                   float xDipoleShift = 0.f) {
+        if (halfWidth < 1 || halfWidth > 10) aio_ops::fail("windowed sinc: half-width must be 1 to 10");
+        const int w1 = 2 * halfWidth, nPt = w1 * w1;
+        std::shared_ptr<deviceGpu> d(new deviceGpu(nt, (dipole == 1 ? 2 : 1) * nPt));
+        const SEP::axis az = vel->getHyper()->getAxis(1), ax = vel->getHyper()->getAxis(2);
+        d->_nz = az.n;
+        d->_nDeviceIrreg = zCoord->getHyper()->getAxis(1).n;
+        d->_idx.resize((size_t)d->_nbCorner * d->_nDeviceIrreg);
+        d->_w.resize(d->_idx.size());
+        auto weights1d = [&](double p, int n, int& first, double* w) {
+            const int f = (int)std::floor(p);
+            first = f - halfWidth + 1;
+            if (first < 0 || first + w1 > n) aio_ops::fail("One of the device is out of bounds (windowed-sinc stencil)");
+            const double pi = 3.14159265358979323846, i0b = besselI0(beta);
+            for (int k = 0; k < w1; k++) {
+                const double x = first + k - p;
+                const double sinc = std::fabs(x) < 1e-12 ? 1.0 : std::sin(pi * x) / (pi * x);
+                const double u = x / halfWidth;
+                w[k] = std::fabs(u) <= 1.0 ? sinc * besselI0(beta * std::sqrt(1.0 - u * u)) / i0b : 0.0;
+            }
+        };
+        auto point = [&](int i1, float zc, float xc, double sign) {
+            double wz[20], wx[20];
+            int z0, x0;
+            weights1d(((double)zc - az.o) / az.d, az.n, z0, wz);
+            weights1d(((double)xc - ax.o) / ax.d, ax.n, x0, wx);
+            for (int jx = 0; jx < w1; jx++)
+                for (int jz = 0; jz < w1; jz++) {
+                    d->_idx[i1 + jx * w1 + jz] = (x0 + jx) * d->_nz + z0 + jz;
+                    d->_w[i1 + jx * w1 + jz] = (float)(sign * wz[jz] * wx[jx]);
+                }
+        };
+        for (int i = 0; i < d->_nDeviceIrreg; i++) {
+            const float zc = (*zCoord->_mat)[i], xc = (*xCoord->_mat)[i];
+            point(i * d->_nbCorner, zc, xc, 1.0);
+            if (dipole == 1) point(i * d->_nbCorner + nPt, zc + zDipoleShift, xc + xDipoleShift, -1.0);
+        }
+        d->unique();
+        return d;
+    }
+    // modified Bessel function of the first kind, order 0 (power series)
+    static double besselI0(double x) {
+        double sum = 1.0, term = 1.0;
+        for (int k = 1; k < 60; k++) {
+            term *= (x / (2.0 * k)) * (x / (2.0 * k));
+            sum += term;
+            if (term < 1e-17 * sum) break;
+        }
+        return sum;
+    }
+
     // regular [nDeviceReg][nt] -> irregular [nDeviceIrreg][nt]
     void forward(const bool add, const std::shared_ptr<SEP::float2DReg> signalReg,
                  std::shared_ptr<SEP::float2DReg> signalIrreg) const override {
@@ -128,6 +192,7 @@ class deviceGpu : public Operator<SEP::float2DReg, SEP::float2DReg> {
     int nCorner() const { return _nbCorner; }
 
   private:
+    deviceGpu(int nt, int nCorner) : _nt(nt), _nbCorner(nCorner) {}
     // Same float / double expression sequence as the reference's constructor #1.
     void bilinear(int i1, float zc, float xc, const SEP::axis& az, const SEP::axis& ax, double sign) {
         float wz = (zc - az.o) / az.d;

@@ -146,7 +146,11 @@ PYBIND11_MODULE(pyAcoustic_iso_float_nl, m) {
         .def("getWeights", [](deviceGpu& d) {  // corner weights, same order as getRegPos
             return std::vector<float>(d.getWeights(), d.getWeights() + d.nCorner() * d.getNDeviceIrreg());
         })
-        .def("getNt", &deviceGpu::getNt);
+        .def("getNt", &deviceGpu::getNt)
+        .def_static("windowedSinc", &deviceGpu::windowedSinc, "Kaiser-windowed sinc devices at coordinates",
+                    py::arg("zCoord"), py::arg("xCoord"), py::arg("vel"), py::arg("nt"), py::arg("halfWidth") = 4,
+                    py::arg("beta") = 4.14f, py::arg("dipole") = 0, py::arg("zDipoleShift") = 0.f,
+                    py::arg("xDipoleShift") = 0.f);
     py::class_<nonlinearPropShotsGpu, std::shared_ptr<nonlinearPropShotsGpu>>(m, "nonlinearPropShotsGpu")
         .def(py::init<std::shared_ptr<SEP::float2DReg>, std::shared_ptr<paramObj>, std::vector<std::shared_ptr<deviceGpu>>,
                       std::vector<std::shared_ptr<deviceGpu>>>(),

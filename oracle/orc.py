@@ -304,3 +304,40 @@ def device_gather(idx, w, nc, sig_reg):
     for i1 in range(len(idx)):
         out[i1 // nc] += w[i1] * sig_reg[trace[i1]]
     return out
+
+
+def device_sinc(zc, xc, nz, nx, oz, dz, ox, dx, r=4, beta=4.14, dipole=0, zshift=0.0, xshift=0.0):
+    """Kaiser-windowed sinc device weights (Hicks 2002, Geophysics 67(1)): (2r)^2 grid points per
+    point, w = wz(iz) * wx(ix), w(i) = sinc(i - p) I0(beta sqrt(1 - ((i - p)/r)^2)) / I0(beta) for
+    |i - p| <= r, p the coordinate in grid units; a dipole adds the shifted point with negated
+    weights. Returns (idx int32, w float32), device-major, x-major inside a point."""
+    from numpy import i0
+    w1 = 2 * r
+    npt = w1 * w1
+    nc = npt * (2 if dipole == 1 else 1)
+    idx = np.zeros(nc * len(zc), np.int32)
+    w = np.zeros(nc * len(zc), np.float32)
+
+    def one(p, n):
+        f = int(np.floor(p))
+        first = f - r + 1
+        assert first >= 0 and first + w1 <= n, "stencil off the grid"
+        x = first + np.arange(w1) - p
+        u = x / r
+        k = np.where(np.abs(u) <= 1, i0(beta * np.sqrt(np.clip(1 - u * u, 0, None))) / i0(beta), 0.0)
+        return first, np.sinc(x) * k
+
+    def point(i1, z, x, sign):
+        z0, wz = one((float(np.float32(z)) - float(np.float32(oz))) / float(np.float32(dz)), nz)
+        x0, wx = one((float(np.float32(x)) - float(np.float32(ox))) / float(np.float32(dx)), nx)
+        for jx in range(w1):
+            for jz in range(w1):
+                idx[i1 + jx * w1 + jz] = (x0 + jx) * nz + z0 + jz
+                w[i1 + jx * w1 + jz] = np.float32(sign * wz[jz] * wx[jx])
+
+    for i in range(len(zc)):
+        point(i * nc, zc[i], xc[i], 1.0)
+        if dipole == 1:
+            point(i * nc + npt, np.float32(np.float32(zc[i]) + np.float32(zshift)),
+                  np.float32(np.float32(xc[i]) + np.float32(xshift)), -1.0)
+    return idx, w

@@ -2,7 +2,8 @@
 restatement of the reference's geometry. Corner indices, weights and the unique grid
 points are integer / float work done with the reference's expression sequence, so the
 bar is bit-exact; spread and gather accumulate in the reference's device-corner order
-and are bit-exact too. CPU only."""
+and are bit-exact too. The Kaiser-windowed sinc devices (an addition: the reference's
+devices are bilinear) match the oracle's restatement to FP32 rounding. CPU only."""
 import numpy as np
 import pytest
 
@@ -96,3 +97,42 @@ def test_device_on_last_node_is_out_of_bounds(api):
     with pytest.raises(RuntimeError, match="out of bounds"):
         nl.deviceGpu(api.vector([zmax], [(1, 0, 1)]), api.vector([100.0], [(1, 0, 1)]), vel, 16, 0, 0.0, 0.0)
     nl.deviceGpu(api.vector([zmax - 0.5], [(1, 0, 1)]), api.vector([100.0], [(1, 0, 1)]), vel, 16, 0, 0.0, 0.0)
+
+
+@pytest.mark.parametrize("r,dipole", [(4, 0), (3, 1), (2, 0)])
+def test_windowed_sinc_devices(api, r, dipole):
+    """Kaiser-windowed sinc devices (Hicks 2002) against the oracle's restatement: same grid
+    points, weights to FP32 rounding (both evaluate the window in double)."""
+    nl = api.pyAcoustic_iso_float_nl
+    rng = np.random.default_rng(10 + r)
+    n = 7
+    z = rng.uniform(80.0, 300.0, n).astype(np.float32)
+    x = rng.uniform(80.0, 450.0, n).astype(np.float32)
+    dev = nl.deviceGpu.windowedSinc(api.vector(z, [(n, 0, 1)]), api.vector(x, [(n, 0, 1)]), _vel(api), 16, r, 4.14,
+                                    dipole, 13.0, 0.0)
+    idx, w = orc.device_sinc(z, x, NZ, NX, 0.0, D, 0.0, D, r, 4.14, dipole, 13.0, 0.0)
+    assert np.array_equal(np.array(dev.getRegPos(), np.int32), idx)
+    assert np.allclose(np.array(dev.getWeights(), np.float32), w, rtol=1e-6, atol=1e-7)
+    assert np.array_equal(np.array(dev.getRegPosUnique(), np.int32), orc.device_unique(idx)[0])
+    npt = (2 * r) ** 2
+    # a windowed sinc interpolates a constant to within a few per cent
+    assert np.allclose(w.reshape(n, -1)[:, :npt].sum(1), 1.0, atol=0.05)
+    reg = api.vector(None, [(16, 0, 1), (dev.getNDeviceReg(), 0, 1)])
+    irr = api.vector(None, [(16, 0, 1), (n, 0, 1)])
+    dev.setDomainRange(reg, irr)
+    assert dev.dotTest(False, 1e-5)
+
+
+def test_windowed_sinc_on_node_is_a_delta(api):
+    nl = api.pyAcoustic_iso_float_nl
+    z = np.array([100.0, 210.0], np.float32)
+    x = np.array([200.0, 330.0], np.float32)
+    dev = nl.deviceGpu.windowedSinc(api.vector(z, [(2, 0, 1)]), api.vector(x, [(2, 0, 1)]), _vel(api), 16)
+    w = np.array(dev.getWeights(), np.float32).reshape(2, -1)
+    pos = np.array(dev.getRegPos(), np.int32).reshape(2, -1)
+    for i in range(2):
+        k = int(np.argmax(np.abs(w[i])))
+        assert w[i, k] == 1.0 and pos[i, k] == int(x[i] / D) * NZ + int(z[i] / D)
+        assert np.max(np.abs(np.delete(w[i], k))) < 1e-7
+    with pytest.raises(RuntimeError, match="out of bounds"):
+        nl.deviceGpu.windowedSinc(api.vector([15.0], [(1, 0, 1)]), api.vector([200.0], [(1, 0, 1)]), _vel(api), 16)

@@ -3,7 +3,9 @@ nodes (bilinear, F/src/deviceGpu.cpp:8-81), receivers as dipoles, through the
 reference-named shot classes. The oracle chain is the oracle's own device geometry
 (orc.device_bilinear, bit-exact with the C++ class, tests/test_devices_cpu.py) -> spread ->
 d2/dt2 -> dtw^2 v^2 -> fine-time interpolation -> propagation at the unique grid points ->
-gather. Gates: relative L2 1e-5 against the FP32 oracle; dot tests 1e-5.
+gather. Kaiser-windowed sinc devices (deviceGpu.windowedSinc, 64 grid points per device) go
+through the same chain with the oracle's sinc weights (orc.device_sinc). Gates: relative L2
+1e-5 against the FP32 oracle; dot tests 1e-5.
 """
 import numpy as np
 import pytest
@@ -123,3 +125,60 @@ def test_born_off_grid(api, geo):
     assert rel_l2(img.getNdArray()[interior], want[interior]) < 1e-5
     op.setDomainRange(model, _data(api))
     assert op.dotTest(False, 1e-5)
+
+
+def _sinc_devices(api, geo, r=4):
+    nl = api.pyAcoustic_iso_float_nl
+    sz, sx = [np.float32(93.7), np.float32(121.2)], [np.float32(152.4), np.float32(388.9)]
+    srcs = [nl.deviceGpu.windowedSinc(api.vector([sz[i]], [(1, 0, 1)]), api.vector([sx[i]], [(1, 0, 1)]), geo["v"],
+                                      NTS, r) for i in range(2)]
+    rz = np.full(NREC, 81.5, np.float32)
+    rx = np.linspace(85.0, 470.0, NREC).astype(np.float32) + 0.37
+    rec = nl.deviceGpu.windowedSinc(api.vector(rz, [(NREC, 0, 1)]), api.vector(rx, [(NREC, 0, 1)]), geo["v"], NTS, r)
+    sgeo = [orc.device_sinc([sz[i]], [sx[i]], NZ, NX, 0.0, D, 0.0, D, r) for i in range(2)]
+    rgeo = orc.device_sinc(rz, rx, NZ, NX, 0.0, D, 0.0, D, r)
+    return srcs, rec, sgeo, rgeo
+
+
+def test_nonlinear_windowed_sinc(api, geo):
+    """Kaiser-windowed sinc sources and receivers (64 grid points each) through the nonlinear
+    shot class, against the oracle chain with the oracle's sinc weights; dot test."""
+    srcs, rec, sgeo, rgeo = _sinc_devices(api, geo)
+    op = api.pyAcoustic_iso_float_nl.nonlinearPropShotsGpu(geo["v"], geo["par"], srcs, [rec])
+    model = api.vector(geo["wav"][None, None, :], [(NTS, 0.0, DTS), (1, 0.0, 1.0), (1, 0.0, 1.0)])
+    data = _data(api)
+    op.forward(False, model, data)
+    nc_s, nc_r = len(sgeo[0][0]), len(rgeo[0]) // NREC
+    rpos = orc.device_unique(rgeo[0])[0]
+    dtw = np.float32(DTS / SUB)
+    vflat = geo["vel"].reshape(-1)
+    for i in range(2):
+        pos, reg = orc.device_spread(sgeo[i][0], sgeo[i][1], nc_s, geo["wav"][None, :])
+        reg = (reg * (dtw * dtw * vflat[pos] * vflat[pos])[:, None]).astype(np.float32)
+        sig = orc.time_interp_fwd(NTS, DTS, SUB, reg, dtype=np.float32)
+        dreg = orc.nl_fwd(geo["scheme"], geo["vel"], sig, pos, rpos, dtype=np.float32)
+        want = orc.device_gather(rgeo[0], rgeo[1], nc_r, dreg)
+        assert rel_l2(data.getNdArray()[i], want) < 1e-5
+    m1 = api.vector(None, [(NTS, 0.0, DTS), (1, 0.0, 1.0), (2, 0.0, 1.0)])
+    op.setDomainRange(m1, _data(api))
+    assert op.dotTest(False, 1e-5)
+
+
+def test_windowed_sinc_on_node_equals_grid_device(api, geo):
+    """On grid nodes the windowed sinc is a delta: the same data as grid-point devices."""
+    nl = api.pyAcoustic_iso_float_nl
+    v = geo["v"]
+    rz, rx = [8] * 20, list(range(10, 30))
+    grid_src = [nl.deviceGpu([9], [15], v, NTS, 0, 0, 0), nl.deviceGpu([11], [40], v, NTS, 0, 0, 0)]
+    grid_rec = nl.deviceGpu(rz, rx, v, NTS, 0, 0, 0)
+    f = lambda a: api.vector(np.asarray(a, np.float32) * D, [(len(a), 0, 1)])  # noqa: E731
+    sinc_src = [nl.deviceGpu.windowedSinc(f([9]), f([15]), v, NTS), nl.deviceGpu.windowedSinc(f([11]), f([40]), v, NTS)]
+    sinc_rec = nl.deviceGpu.windowedSinc(f(rz), f(rx), v, NTS)
+    model = api.vector(geo["wav"][None, None, :], [(NTS, 0.0, DTS), (1, 0.0, 1.0), (1, 0.0, 1.0)])
+    out = []
+    for s, r in ((grid_src, grid_rec), (sinc_src, sinc_rec)):
+        op = api.pyAcoustic_iso_float_nl.nonlinearPropShotsGpu(v, geo["par"], s, [r])
+        d = api.vector(None, [(NTS, 0.0, DTS), (20, 0.0, 1.0), (2, 0.0, 1.0)])
+        op.forward(False, model, d)
+        out.append(d.getNdArray().copy())
+    assert rel_l2(out[1], out[0]) < 1e-6
