@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <map>
@@ -222,7 +223,7 @@ struct Context {
         set_velocity(vel2Dtw2, reflScale);
         size_t fr = 0, tot = 0;
         AIO_CK(cudaMemGetInfo(&fr, &tot));
-        budget = p.memBudgetBytes > 0 ? p.memBudgetBytes : (long long)(0.9 * (double)fr);
+        budget = p.memBudgetBytes > 0 ? p.memBudgetBytes : (long long)(0.93 * (double)fr);
     }
 
     void set_velocity(const float* vel2Dtw2, const float* reflScale) {
@@ -295,7 +296,14 @@ struct Context {
         }
         int cap = capacity(n, maxSrc, maxRec);
         require(cap >= 1, "device memory budget cannot hold one shot for this operator");
-        return std::min(cap, nShots);
+        return balanced_wave(cap, nShots);
+    }
+    // Waves of (nearly) equal size: ceil(nShots / cap) waves rather than full waves and a
+    // small remainder, whose launches would use the GPU poorly.
+    static int balanced_wave(long long cap, int nShots) {
+        if (nShots <= cap) return nShots;
+        const long long waves = (nShots + cap - 1) / cap;
+        return (int)((nShots + waves - 1) / waves);
     }
 
     // Allocate wave buffers for nb shots and fill descriptors; traces are staged
@@ -882,7 +890,7 @@ struct Context {
     }
 
     // Measured autotuning of the blocked stepper's plan for waves of nb shots (chunkColumns
-    // == 0): strip heights {128, 112, 96, 64} rows x chunk counts around the model's choices
+    // == 0): strip heights {128, 112, 96, 80, 64} rows x chunk counts around the model's choices
     // (at least 4 waves of CTAs, and the cheapest count for any number of waves) are each timed
     // on the source-pass launch of interval 0 (idempotent: it reads one state set and
     // overwrites the other, the stored slice 0 and the partial sums), the fastest is cached
@@ -930,21 +938,24 @@ struct Context {
         }
         return m;
     }
+    // row quads of the k_tile variant a strip of NQ row quads runs on
+    static int tb_variant(int NQ) { return NQ <= KT_MAXQ_S ? KT_MAXQ_S : (NQ <= KT_MAXQ_M ? KT_MAXQ_M : KT_MAXQ); }
     // plan pl fits in shared memory in every mode
     bool tb_plan_fits(const TBPlan& pl, const TBEntries& e) const {
         int smemMax = 0;
         if (cudaDeviceGetAttribute(&smemMax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return false;
-        const int rs = kt_rs(pl.NQ <= KT_MAXQ_S ? KT_MAXQ_S : KT_MAXQ);
+        const int mq = tb_variant(pl.NQ);
         const std::pair<int, int> need[] = {{TB_SRC, e.fwd}, {TB_SCAT, e.scat}, {TB_ADJ, e.adj}, {TB_SCATW, 1}};
         for (const auto& mn : need)
-            if (kt_smem_bytes(mn.first, pl.threads, pl.iters, mn.second, rs) > (size_t)smemMax) return false;
+            if (kt_smem_bytes(mn.first, pl.threads, pl.iters, mn.second, kt_rs(mq), kt_v2s(mq)) > (size_t)smemMax)
+                return false;
         return true;
     }
 
     void tb_autotune(int nb, const aio_shot* shots) {
         if (P.chunkColumns != 0 || tbTuned.count(2 * nb)) return;
         std::vector<TBPlan> cand;
-        for (int maxHZ : {128, 112, 96, 64})
+        for (int maxHZ : {128, 112, 96, 80, 64})
             for (int minWaves : {4, 1}) {
                 const TBPlan m = tb_model_plan(nb, maxHZ, 0, 0, minWaves);
                 for (int d : {-2, -1, 0, 1, 2}) {
@@ -966,6 +977,8 @@ struct Context {
         TBPlan best = cand.front(), bestHeavy = cand.front();
         const long long saveLaunches = launches, saveKernels = kernels;
         const int saveProf = profEvery;
+        const char* logEnv = std::getenv("AIO_AUTOTUNE_LOG");  // print every candidate's timings
+        const bool logTune = logEnv && *logEnv && *logEnv != '0';
         profEvery = 0;
         for (const TBPlan& pl : cand) {
             const int maxEnt = tb_lists(pl, nb, shots, 1, false);
@@ -974,18 +987,29 @@ struct Context {
             KTArgs a = tb_args(pl, maxEnt, nullptr);
             a.its = 0;
             if (f16()) AIO_CK(cudaMemsetAsync(tbWmax.p, 0, (size_t)nb * g.nts * 4, st));
-            tb_launch<TB_SRC>(pl, nb, a, 0);  // warm-up (smem carve-out, caches)
-            AIO_CK(cudaEventRecord(e0, st));
-            tb_launch<TB_SRC>(pl, nb, a, 0);
-            tb_launch<TB_SRC>(pl, nb, a, 0);
-            AIO_CK(cudaEventRecord(e1, st));
-            AIO_CK(cudaEventSynchronize(e1));
-            float ms = 0.f;
-            AIO_CK(cudaEventElapsedTime(&ms, e0, e1));
+            // fastest of three timings of two launches each (after a warm-up launch: smem
+            // carve-out, caches), so that a disturbed timing does not decide the plan
+            auto timeMin = [&](auto launch) {
+                launch();
+                float best2 = 1e30f;
+                for (int rep = 0; rep < 3; rep++) {
+                    AIO_CK(cudaEventRecord(e0, st));
+                    launch();
+                    launch();
+                    AIO_CK(cudaEventRecord(e1, st));
+                    AIO_CK(cudaEventSynchronize(e1));
+                    float t = 0.f;
+                    AIO_CK(cudaEventElapsedTime(&t, e0, e1));
+                    best2 = std::min(best2, t);
+                }
+                return best2;
+            };
+            float ms = timeMin([&] { tb_launch<TB_SRC>(pl, nb, a, 0); });
             if (ms < bestMs) {
                 bestMs = ms;
                 best = pl;
             }
+            const float lightMs = ms;
             // heavy class: the time-lag scattered pass (reads W slices 0, 1 as its sources;
             // writes only the other state set)
             const int maxEntH = tb_lists(pl, nb, shots, 0, false);  // before tb_desc: it may move the lists
@@ -994,17 +1018,14 @@ struct Context {
             a.its = 0;
             a.rSlot = 0;
             a.rSlot0 = 1;
-            tb_launch<TB_SCATX>(pl, nb, a, 0);
-            AIO_CK(cudaEventRecord(e0, st));
-            tb_launch<TB_SCATX>(pl, nb, a, 0);
-            tb_launch<TB_SCATX>(pl, nb, a, 0);
-            AIO_CK(cudaEventRecord(e1, st));
-            AIO_CK(cudaEventSynchronize(e1));
-            AIO_CK(cudaEventElapsedTime(&ms, e0, e1));
+            ms = timeMin([&] { tb_launch<TB_SCATX>(pl, nb, a, 0); });
             if (ms < bestHeavyMs) {
                 bestHeavyMs = ms;
                 bestHeavy = pl;
             }
+            if (logTune)
+                std::fprintf(stderr, "aio autotune: shots %d strip %d x %d chunk %d x %d threads %d: light %.3f ms heavy %.3f ms\n",
+                             nb, pl.HZ, pl.nStrips, pl.LX, pl.nChunks, pl.threads, lightMs, ms);
         }
         AIO_CK(cudaEventDestroy(e0));
         AIO_CK(cudaEventDestroy(e1));
@@ -1153,7 +1174,7 @@ struct Context {
 
     template <int MODE, int WP, int MAXQ>
     void tb_launch_q(const TBPlan& pl, int nb, KTArgs& a, int v) {
-        const size_t smem = kt_smem_bytes(MODE, pl.threads, pl.iters, a.maxEnt, kt_rs(MAXQ));
+        const size_t smem = kt_smem_bytes(MODE, pl.threads, pl.iters, a.maxEnt, kt_rs(MAXQ), kt_v2s(MAXQ));
         static int attrDev = -1;
         static int smemMax = 0;
         if (attrDev != dev) {
@@ -1182,10 +1203,12 @@ struct Context {
         launches++;
         kernels++;
     }
-    // Short strips (<= 64 rows) use the variant with a narrower ring (two CTAs per SM).
+    // Short strips (<= 64 rows) and mid strips (<= 80 rows) use the variants with narrower
+    // rings (two CTAs per SM); taller strips the large one.
     template <int MODE, int WP>
     void tb_launch_t(const TBPlan& pl, int nb, KTArgs& a, int v) {
         if (pl.NQ <= KT_MAXQ_S) tb_launch_q<MODE, WP, KT_MAXQ_S>(pl, nb, a, v);
+        else if (pl.NQ <= KT_MAXQ_M) tb_launch_q<MODE, WP, KT_MAXQ_M>(pl, nb, a, v);
         else tb_launch_q<MODE, WP, KT_MAXQ>(pl, nb, a, v);
     }
     template <int MODE>
@@ -1728,7 +1751,7 @@ struct Context {
         long long shared = 4LL * g.isz * 4 + (64LL << 20);
         long long cap = (budget - shared) / per;
         require(cap >= 1, "device memory budget cannot hold one shot for this operator");
-        return (int)std::min<long long>(cap, nShots);
+        return balanced_wave(cap, nShots);
     }
 
     void born_forward_tb(const float* model, int nShots, const aio_shot* shots, int mem) {

@@ -44,6 +44,10 @@ constexpr int KT_RINGCOLS = KT_CB0 + (KT_T - 1) * KT_CB;
 constexpr int KT_PADQ = 2;     // zero quads above and below every ring column
 constexpr int KT_MAXQ = 42;    // row quads per strip (R <= 168, HZ <= 128)
 constexpr int KT_MAXQ_S = 26;  // short-strip variant (R <= 104, HZ <= 64): two CTAs per SM fit
+constexpr int KT_MAXQ_M = 30;  // mid-strip variant (R <= 120, HZ <= 80): two CTAs per SM fit (light modes)
+// Variants holding up to KT_MAXQ_M row quads run two CTAs per SM; they read v^2 of level 1
+// through L1 like the later levels instead of staging it in shared memory.
+__host__ __device__ constexpr bool kt_v2s(int maxq) { return maxq > KT_MAXQ_M; }
 // floats per ring column (compile-time offsets) of a variant holding up to maxq row quads
 __host__ __device__ constexpr int kt_rs(int maxq) { return (maxq + 2 * KT_PADQ) * 4; }
 constexpr int KT_RS = kt_rs(KT_MAXQ);
@@ -72,17 +76,20 @@ struct KTArgs {
 };
 
 // Per-thread staging slots (16 bytes each) filled by asynchronous copies: level-1 operands
-// of the next iteration (old level, v^2: slots 0-3) and the output operands of the current
-// iteration (partial sum: 4-5, stored wavefield: 6-7, FP64 image: 8-11).
-__host__ __device__ constexpr int kt_slots(int mode) {
-    return mode == TB_ADJ ? 12 : ((mode == TB_SRC || mode == TB_ADJR) ? 6 : (tb_scatlike(mode) ? 8 : 4));
+// of the next iteration (old level: slots 0-1; v^2: 2-3 when v2s) and the output operands of
+// the current iteration from slot kt_so(v2s) on (partial sum: +0..1, stored wavefield: +2..3,
+// FP64 image: +4..7; the scattered passes' sources: +0..3).
+__host__ __device__ constexpr int kt_so(bool v2s) { return v2s ? 4 : 2; }
+__host__ __device__ constexpr int kt_slots(int mode, bool v2s = true) {
+    return kt_so(v2s) +
+           (mode == TB_ADJ ? 8 : ((mode == TB_SRC || mode == TB_ADJR) ? 2 : (tb_scatlike(mode) ? 4 : 0)));
 }
 // Ring columns: levels 0..T-1, plus (scattered pass) the secondary sources dm*W[its] and
 // dm*W[its+1] of the last 32 level-1 columns, formed once at level 1 and read by levels 2..T.
 __host__ __device__ constexpr int kt_ringcols(int mode) { return KT_RINGCOLS + (tb_scatlike(mode) ? 2 * KT_CB : 0); }
 // rings, staging, column damping table, per-launch injection values (T per entry), entries
-inline size_t kt_smem_bytes(int mode, int threads, int iters, int maxEnt, int rs = KT_RS) {
-    return (size_t)kt_ringcols(mode) * rs * sizeof(float) + (size_t)kt_slots(mode) * threads * 16 +
+inline size_t kt_smem_bytes(int mode, int threads, int iters, int maxEnt, int rs = KT_RS, bool v2s = true) {
+    return (size_t)kt_ringcols(mode) * rs * sizeof(float) + (size_t)kt_slots(mode, v2s) * threads * 16 +
            (3 * ((size_t)iters * KT_BX + 64) + (size_t)maxEnt * KT_T) * sizeof(float) + (size_t)maxEnt * sizeof(TBEnt);
 }
 
@@ -203,12 +210,14 @@ __device__ __forceinline__ float2 kt_pair(const float4 (&Z)[5], int r) {
 }
 
 template <int MODE, int WPREC, int MAXQ = KT_MAXQ>
-__global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ? 2 : 1) k_tile(const KTArgs a) {
+__global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 2) k_tile(const KTArgs a) {
     constexpr int T = KT_T;
     extern __shared__ float4 kt_smem4[];
     const int NQ = a.NQ;
     constexpr int RS = kt_rs(MAXQ);
-    constexpr int NS = kt_slots(MODE);
+    constexpr bool V2S = kt_v2s(MAXQ);
+    constexpr int SO = kt_so(V2S);  // first output-operand slot
+    constexpr int NS = kt_slots(MODE, V2S);
     float* ring = reinterpret_cast<float*>(kt_smem4);         // level 0: [KT_CB0][RS], levels 1..T-1: [KT_CB][RS]
     float4* stg = reinterpret_cast<float4*>(ring + kt_ringcols(MODE) * RS);  // [NS][blockDim.x]
     float* dxt = reinterpret_cast<float*>(stg + NS * blockDim.x);      // column damping, columns xs-32 ...
@@ -346,16 +355,16 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
             const bool oko = zLoad && co >= 0 && co < nxi;
             kt_cp16(mySlot + j * bd, oko ? old + (long long)co * ip + zq : old, oko);
             const long long ic = (long long)min(max(co, 0), nxi - 1) * ip + zv;
-            kt_cp16_l1(mySlot + (2 + j) * bd, v2p + ic, true);
+            if (V2S) kt_cp16_l1(mySlot + (2 + j) * bd, v2p + ic, true);
             if (tb_scatlike(MODE)) {  // stored wavefield (or secondary sources) at its, its+1 (slots 4-7)
                 const void* wa = tb_wslice<WPREC>(sh.W, a.wStride, MODE == TB_SCAT ? its : a.rSlot);
                 const void* wb = tb_wslice<WPREC>(sh.W, a.wStride, MODE == TB_SCAT ? its + 1 : a.rSlot0);
                 if (WPREC == TBW_F32) {
-                    kt_cp16(mySlot + (4 + j) * bd, (const float*)wa + ic, true);
-                    kt_cp16(mySlot + (6 + j) * bd, (const float*)wb + ic, true);
+                    kt_cp16(mySlot + (SO + j) * bd, (const float*)wa + ic, true);
+                    kt_cp16(mySlot + (SO + 2 + j) * bd, (const float*)wb + ic, true);
                 } else {
-                    kt_cp8(mySlot + (4 + j) * bd, (const __nv_bfloat16*)wa + ic, true);
-                    kt_cp8(mySlot + (6 + j) * bd, (const __nv_bfloat16*)wb + ic, true);
+                    kt_cp8(mySlot + (SO + j) * bd, (const __nv_bfloat16*)wa + ic, true);
+                    kt_cp8(mySlot + (SO + 2 + j) * bd, (const __nv_bfloat16*)wb + ic, true);
                 }
             }
         }
@@ -380,13 +389,13 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
                 const int c = B - 5 * T + 2 * cp + j;
                 if (zOut && c >= x0 && c < x1) {
                     const long long idx = (long long)c * ip + zq;
-                    kt_cp16(mySlot + (4 + j) * bd, pPart + idx, true);
+                    kt_cp16(mySlot + (SO + j) * bd, pPart + idx, true);
                     if (MODE == TB_ADJ) {
                         const void* w = tb_wslice<WPREC>(sh.W, a.wStride, its + 1);
-                        if (WPREC == TBW_F32) kt_cp16(mySlot + (6 + j) * bd, (const float*)w + idx, true);
-                        else kt_cp8(mySlot + (6 + j) * bd, (const __nv_bfloat16*)w + idx, true);
-                        kt_cp16(mySlot + (8 + 2 * j) * bd, pImg + idx, true);
-                        kt_cp16(mySlot + (9 + 2 * j) * bd, pImg + idx + 2, true);
+                        if (WPREC == TBW_F32) kt_cp16(mySlot + (SO + 2 + j) * bd, (const float*)w + idx, true);
+                        else kt_cp8(mySlot + (SO + 2 + j) * bd, (const __nv_bfloat16*)w + idx, true);
+                        kt_cp16(mySlot + (SO + 4 + 2 * j) * bd, pImg + idx, true);
+                        kt_cp16(mySlot + (SO + 5 + 2 * j) * bd, pImg + idx + 2, true);
                     }
                 }
             }
@@ -426,8 +435,9 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
 #pragma unroll
                 for (int j = 0; j < 2; j++) {
                     const int c = c0 + j;
-                    // level 1: prefetched with the input; later levels re-read the same lines from L1
-                    vq[j] = (t == 1) ? mySlot[(2 + j) * bd]
+                    // level 1 (large-strip variant): prefetched with the input; otherwise read
+                    // from L1, where the lines of the previous levels' reads still are
+                    vq[j] = (V2S && t == 1) ? mySlot[(2 + j) * bd]
                                      : __ldg(reinterpret_cast<const float4*>(v2p + (long long)min(max(c, 0), nxi - 1) * ip + zv));
                     Dx[j] = dxt[c - xs + 32];
                 }
@@ -443,8 +453,8 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
                         if (t == 1) {
                             // imagingFwdGpu (F/src/kernelsGpu.cu:309-316): dm * W, kept for levels 2..T
                             // (SCATX, and SCATW / ADJX without dm: the sources are staged as they are)
-                            const float4 wa = kt_wfrom<WPREC>(mySlot[(4 + j) * bd], scA);
-                            const float4 wb = kt_wfrom<WPREC>(mySlot[(6 + j) * bd], scB);
+                            const float4 wa = kt_wfrom<WPREC>(mySlot[(SO + j) * bd], scA);
+                            const float4 wb = kt_wfrom<WPREC>(mySlot[(SO + 2 + j) * bd], scB);
                             if (MODE == TB_SCATX || (tb_dense_out(MODE) && dmp == nullptr)) {
                                 sa[j] = wa;
                                 sb[j] = wb;
@@ -568,7 +578,7 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
                     float wa[4], wb[4];
 #pragma unroll
                     for (int i = 0; i < 4; i++) {
-                        wa[i] = kt_el(mySlot[(4 + j) * bd], i);
+                        wa[i] = kt_el(mySlot[(SO + j) * bd], i);
                         wb[i] = 0.f;
 #pragma unroll
                         for (int l = 1; l <= T; l++) {
@@ -595,10 +605,10 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
                 } else if (MODE == TB_ADJ) {
                     float ra[4], rb[4];
                     double acc[4];
-                    const float4 oP = mySlot[(4 + j) * bd];
-                    const float4 oW = kt_wfrom<WPREC>(mySlot[(6 + j) * bd], scB);
-                    const double2* oI = reinterpret_cast<const double2*>(&mySlot[(8 + 2 * j) * bd]);
-                    const double2* oI2 = reinterpret_cast<const double2*>(&mySlot[(9 + 2 * j) * bd]);
+                    const float4 oP = mySlot[(SO + j) * bd];
+                    const float4 oW = kt_wfrom<WPREC>(mySlot[(SO + 2 + j) * bd], scB);
+                    const double2* oI = reinterpret_cast<const double2*>(&mySlot[(SO + 4 + 2 * j) * bd]);
+                    const double2* oI2 = reinterpret_cast<const double2*>(&mySlot[(SO + 5 + 2 * j) * bd]);
                     const double oImg[4] = {oI->x, oI->y, oI2->x, oI2->y};
                     float4 w0 = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (its == 0) w0 = kt_wload4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, 0), idx, sc0);
@@ -638,7 +648,7 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, MAXQ <= KT_MAXQ_S ?
                 } else if (MODE == TB_ADJR || MODE == TB_ADJX) {
                     float ra[4], rb[4];
                     const float4 oP = MODE == TB_ADJX ? __ldg(reinterpret_cast<const float4*>(pPart + idx))
-                                                      : mySlot[(4 + j) * bd];
+                                                      : mySlot[(SO + j) * bd];
 #pragma unroll
                     for (int i = 0; i < 4; i++) {
                         ra[i] = 0.f;

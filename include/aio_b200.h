@@ -64,7 +64,7 @@ typedef struct {
     int wavefieldPrecision;  /* AIO_WFLD_* for the stored source wavefield */
     int imageFp64;       /* 1: accumulate imaging conditions in FP64 on the GPU */
     int device;          /* CUDA device ordinal */
-    long long memBudgetBytes; /* cap on device memory for shot buffers; 0 = 90% of free */
+    long long memBudgetBytes; /* cap on device memory for shot buffers; 0 = 93% of free */
     int stepper;         /* AIO_STEPPER_*: how Born / nonlinear passes advance time */
     int chunkColumns;    /* blocked stepper x-chunk width: 0 = autotuned (measured once per wave size),
                             > 0 = fixed width (strips of at most 128 rows) */

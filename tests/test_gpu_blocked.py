@@ -265,3 +265,66 @@ def test_short_strip_variant():
     d = [c.rng.standard_normal((len(c.rec_pos[0]), c.scheme.nts)).astype(np.float32)]
     ga = ctx(c, stepper="blocked").born_adjoint(shots(c, d))
     assert rel_l2(ga, orc.born_adj(c.scheme, c.vel, d[0], c.sig[0], c.src_pos[0], c.rec_pos[0], dtype=np.float32)) < 1e-5
+
+
+def _strip_case(nzi, seed):
+    c = blocked_case(seed=seed, nzi=nzi, nxi=150, nts=26, nshots=2)
+    c.src_pos[0] = np.array([(5 + 40) * c.nz + 5 + 20, (5 + 90) * c.nz + 5 + nzi - 8], np.int32)
+    c.src_pos[1] = np.array([(5 + 70) * c.nz + 5 + nzi // 2], np.int32)
+    for i in range(2):
+        c.sig[i] = (c.rng.standard_normal((len(c.src_pos[i]), c.scheme.ntw)) * 1e-2).astype(np.float32)
+        c.rec_pos[i] = np.array([ix * c.nz + 5 + 9 for ix in range(5, c.nx - 5)], np.int32)
+    return c
+
+
+@pytest.mark.parametrize("nzi", [72, 80])
+def test_mid_strip_variant(nzi):
+    """Interiors of 65 to 80 rows run the mid-strip kernel variant (two CTAs per SM, v^2 of the
+    first level read through L1): every kind of blocked pass — nonlinear, Born forward / adjoint,
+    extended Born forward / adjoint, tomo and WEMVA with both legs — against the FP32 oracle
+    (relative L2 1e-5)."""
+    c = _strip_case(nzi, seed=13)
+    s = c.scheme
+    got = ctx(c, stepper="blocked").nonlinear_forward(shots(c))
+    for i in range(2):
+        r32 = orc.nl_fwd(s, c.vel, c.sig[i], c.src_pos[i], c.rec_pos[i], dtype=np.float32)
+        assert rel_l2(got[i], r32) < 1e-5
+    mask = interior_mask(c.nx, c.nz)
+    rng = np.random.default_rng(5)
+    m = (rng.standard_normal((c.nx, c.nz)) * mask).astype(np.float32)
+    gf = [x.copy() for x in ctx(c, stepper="blocked").born_forward(m, shots(c))]
+    for i in range(2):
+        assert rel_l2(gf[i], orc.born_fwd(s, c.vel, m, c.sig[i], c.src_pos[i], c.rec_pos[i], dtype=np.float32)) < 1e-5
+    d = [rng.standard_normal((len(r), s.nts)).astype(np.float32) for r in c.rec_pos]
+    ga = ctx(c, stepper="blocked").born_adjoint(shots(c, d))
+    ref = sum(orc.born_adj(s, c.vel, d[i], c.sig[i], c.src_pos[i], c.rec_pos[i], dtype=np.float32) for i in range(2))
+    assert rel_l2(ga, ref) < 1e-5
+    s5, e = _ext_ctx(c)
+    ext = (rng.standard_normal((5, c.nx, c.nz)) * mask).astype(np.float32)
+    fe = [x.copy() for x in e.born_ext_forward(ext, shots(c))]
+    assert e.last_launches == 2 * (s5.nts - 1)
+    for i in range(2):
+        r32 = orc.bornext_fwd(s5, c.vel, ext, c.sig[i], c.src_pos[i], c.rec_pos[i], dtype=np.float32)
+        assert rel_l2(fe[i], r32) < 1e-5
+    ae = e.born_ext_adjoint(shots(c, d))
+    ref = sum(orc.bornext_adj(s5, c.vel, d[i], c.sig[i], c.src_pos[i], c.rec_pos[i], dtype=np.float32)
+              for i in range(2))
+    assert rel_l2(ae, ref) < 1e-5
+    s5, t = _ext_ctx(c, leg1=1, leg2=1)
+    ft = [x.copy() for x in t.tomo_forward(m, ext, shots(c))]
+    assert t.last_launches == 5 * (s5.nts - 1)
+    for i in range(2):
+        r32 = orc.tomo_fwd(s5, c.vel, m, ext, c.sig[i], c.src_pos[i], c.rec_pos[i], dtype=np.float32)
+        assert rel_l2(ft[i], r32) < 1e-5
+    at = t.tomo_adjoint(ext, shots(c, d))
+    ref = sum(orc.tomo_adj(s5, c.vel, d[i], ext, c.sig[i], c.src_pos[i], c.rec_pos[i], dtype=np.float32)
+              for i in range(2))
+    assert rel_l2(at, ref) < 1e-5
+    fw = t.wemva_forward(m, _wshots(c, d)).copy()
+    ref = sum(orc.wemva_fwd(s5, c.vel, m, c.sig[i], c.src_pos[i], c.rec_pos[i], d[i], dtype=np.float32)
+              for i in range(2))
+    assert rel_l2(fw, ref) < 1e-5
+    aw = t.wemva_adjoint(ext, _wshots(c, d))
+    ref = sum(orc.wemva_adj(s5, c.vel, ext, c.sig[i], c.src_pos[i], c.rec_pos[i], d[i], dtype=np.float32)
+              for i in range(2))
+    assert rel_l2(aw, ref) < 1e-5
