@@ -841,10 +841,13 @@ struct Context {
     // nb: shots of the wave (one CTA column per shot)
     // Plan of a wave of nb shots: the autotuned plan when one was measured, else the model's.
     // Plans are tuned per wave size and kernel class: light modes (SRC, NL, ADJR: at most 6
-    // staging slots, no secondary-source rings) and heavy modes (SCAT, SCATX, SCATW, ADJX, ADJ),
-    // whose larger shared-memory footprint changes how many CTAs an SM holds.
-    TBPlan tb_plan(int nb, bool heavy = false) const {
-        auto it = tbTuned.find(2 * nb + (heavy ? 1 : 0));
+    // staging slots, no secondary-source rings), heavy modes (SCAT, SCATX, SCATW, ADJX), whose
+    // larger shared-memory footprint changes how many CTAs an SM holds, and the Born receiver
+    // pass (ADJ: 12 staging slots, FP64 image read-modify-write, receivers injected).
+    enum TBClass { TB_LIGHT = 0, TB_HEAVY = 1, TB_RECV = 2 };
+    TBPlan tb_plan(int nb, bool heavy = false) const { return tb_plan_c(nb, heavy ? TB_HEAVY : TB_LIGHT); }
+    TBPlan tb_plan_c(int nb, int cls) const {
+        auto it = tbTuned.find(3 * nb + cls);
         if (it != tbTuned.end()) return it->second;
         return tb_model_plan(nb, 4 * (KT_MAXQ - 10), P.chunkColumns > 0 ? P.chunkColumns : 0);
     }
@@ -953,7 +956,7 @@ struct Context {
     }
 
     void tb_autotune(int nb, const aio_shot* shots) {
-        if (P.chunkColumns != 0 || tbTuned.count(2 * nb)) return;
+        if (P.chunkColumns != 0 || tbTuned.count(3 * nb)) return;
         std::vector<TBPlan> cand;
         for (int maxHZ : {128, 112, 96, 80, 64})
             for (int minWaves : {4, 1}) {
@@ -973,8 +976,8 @@ struct Context {
         cudaEvent_t e0, e1;
         AIO_CK(cudaEventCreate(&e0));
         AIO_CK(cudaEventCreate(&e1));
-        float bestMs = 1e30f, bestHeavyMs = 1e30f;
-        TBPlan best = cand.front(), bestHeavy = cand.front();
+        float bestMs = 1e30f, bestHeavyMs = 1e30f, bestRecvMs = 1e30f;
+        TBPlan best = cand.front(), bestHeavy = cand.front(), bestRecv = cand.front();
         const long long saveLaunches = launches, saveKernels = kernels;
         const int saveProf = profEvery;
         const char* logEnv = std::getenv("AIO_AUTOTUNE_LOG");  // print every candidate's timings
@@ -1023,17 +1026,34 @@ struct Context {
                 bestHeavyMs = ms;
                 bestHeavy = pl;
             }
+            const float heavyMs = ms;
+            // receiver class: the Born receiver pass at the last interval (reads state set 0 and
+            // W[nts-1], writes the other state set and partial sums; its image accumulation is
+            // discarded: the pass zeroes the image first)
+            tbImg.ensure((size_t)nb * g.isz * 8);
+            const int maxEntR = tb_lists(pl, nb, shots, 2, false);
+            tb_desc(pl, nb, false, true, false, tbW.p, false);
+            a = tb_args(pl, maxEntR, nullptr);
+            a.its = g.nts - 2;
+            ms = timeMin([&] { tb_launch<TB_ADJ>(pl, nb, a, 0); });
+            if (ms < bestRecvMs) {
+                bestRecvMs = ms;
+                bestRecv = pl;
+            }
             if (logTune)
-                std::fprintf(stderr, "aio autotune: shots %d strip %d x %d chunk %d x %d threads %d: light %.3f ms heavy %.3f ms\n",
-                             nb, pl.HZ, pl.nStrips, pl.LX, pl.nChunks, pl.threads, lightMs, ms);
+                std::fprintf(stderr,
+                             "aio autotune: shots %d strip %d x %d chunk %d x %d threads %d: light %.3f ms heavy %.3f ms "
+                             "receiver %.3f ms\n",
+                             nb, pl.HZ, pl.nStrips, pl.LX, pl.nChunks, pl.threads, lightMs, heavyMs, ms);
         }
         AIO_CK(cudaEventDestroy(e0));
         AIO_CK(cudaEventDestroy(e1));
         launches = saveLaunches;
         kernels = saveKernels;
         profEvery = saveProf;
-        tbTuned[2 * nb] = best;
-        tbTuned[2 * nb + 1] = bestHeavy;
+        tbTuned[3 * nb + TB_LIGHT] = best;
+        tbTuned[3 * nb + TB_HEAVY] = bestHeavy;
+        tbTuned[3 * nb + TB_RECV] = bestRecv;
     }
 
     // Per-CTA sparse lists of every shot of a wave. inj: 0 none, 1 sources, 2 receivers
@@ -1264,7 +1284,7 @@ struct Context {
     // Launch L handles interval its = nts-2-L: it reads the partial R(its+1) written by
     // launch L-1 and writes R(its); state ping-pongs with L.
     void tb_adj_pass(int nb, const aio_shot* shots) {
-        const TBPlan pl = tb_plan(nb, true);
+        const TBPlan pl = tb_plan_c(nb, TB_RECV);
         const int maxEnt = tb_lists(pl, nb, shots, 2, false);
         tb_zero(nb, true);
         tb_desc(pl, nb, false, true, false, tbW.p, false);
