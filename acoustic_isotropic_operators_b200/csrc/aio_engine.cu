@@ -275,6 +275,7 @@ struct Context {
         if (n.ss) b += 2 * g.isz * 4;
         b += (long long)n.nWavefields * g.nts * g.isz * 4;
         b += (long long)n.nImg * g.isz * (P.imageFp64 ? 8 : 4);
+        if (offsets()) b += (long long)OFF_K * g.isz * 4;  // block of ring samples (img_offset_adj_block)
         b += (long long)maxSrc * g.ntw * 4 + 2LL * maxRec * g.nts * 4;
         b += 16LL * (g.tilesZ * g.tilesX + 2) + 16LL * (maxSrc + maxRec);
         return b;
@@ -744,26 +745,31 @@ struct Context {
                                                                    nullptr, g.isz, g.ip, g.nxi, g.hExt);
         kcheck();
     }
-    // image_e(x) += A(x+s) B(x-s) on the ring slot (then zeroed): Born form, A = ring * v2, B = W_t
-    // (scaleSecondarySourceFd + imagingOffsetAdjGpu); WEMVA form, A = R_t * v2, B = ring
-    // (imagingOffsetWemvaScaleFwdGpu).
-    void img_offset_adj(int nb, long long slot, const float* F, int t, bool wemvaForm) {
-        const long long mSt = (long long)g.nExt * g.isz;
-        const float* ring = ring_ptr(slot);
-        const float* Ft = F + (long long)t * g.isz;
-        const float* A = wemvaForm ? Ft : ring;
-        const float* B = wemvaForm ? ring : Ft;
-        const long long ASt = wemvaForm ? wfSt() : pairSt(), BSt = wemvaForm ? pairSt() : wfSt();
-        if (P.imageFp64)
-            k_img_offset_adj<double><<<ew_grid(nb, mSt), 256, 0, st>>>(img.as<double>(), mSt, A, ASt, B, BSt,
-                                                                       v2.as<float>(), g.isz, g.ip, g.nxi, g.hExt,
-                                                                       g.nExt, wemvaForm ? 1 : 0);
-        else
-            k_img_offset_adj<float><<<ew_grid(nb, mSt), 256, 0, st>>>(img.as<float>(), mSt, A, ASt, B, BSt,
-                                                                      v2.as<float>(), g.isz, g.ip, g.nxi, g.hExt,
-                                                                      g.nExt, wemvaForm ? 1 : 0);
-        kcheck();
+    // Subsurface-offset imaging in blocks of OFF_K coarse samples: the ring slot of sample t is
+    // copied into slice t % OFF_K of offBuf and zeroed; once the block holding t is complete
+    // (passes running backward in time: t % OFF_K == 0; forward: t % OFF_K == OFF_K - 1 or
+    // t == nts - 1), k_img_offset_block images all of its samples, reading and writing the image
+    // once per block.
+    DevMem offBuf;
+    void img_offset_adj_block(int nb, long long slot, const float* F, int t, bool wemvaForm, bool backward) {
+        offBuf.ensure((size_t)nb * OFF_K * g.isz * 4);
+        AIO_CK(cudaMemcpy2DAsync(offBuf.as<float>() + (long long)(t % OFF_K) * g.isz, (size_t)OFF_K * g.isz * 4,
+                                 ring_ptr(slot), (size_t)pairSt() * 4, (size_t)g.isz * 4, nb,
+                                 cudaMemcpyDeviceToDevice, st));
         zero_slot(ringb, nb, slot);
+        const bool done = backward ? (t % OFF_K == 0) : (t % OFF_K == OFF_K - 1 || t == g.nts - 1);
+        if (!done) return;
+        const int tlo = t - t % OFF_K, thi = std::min(tlo + OFF_K - 1, g.nts - 1);
+        const long long mSt = (long long)g.nExt * g.isz, RSt = (long long)OFF_K * g.isz;
+        if (P.imageFp64)
+            k_img_offset_block<double><<<ew_grid(nb, g.isz), 256, 0, st>>>(
+                img.as<double>(), mSt, offBuf.as<float>(), RSt, F, wfSt(), v2.as<float>(), (int)g.isz, g.ip, g.nxi,
+                g.hExt, g.nExt, tlo, thi, wemvaForm ? 1 : 0);
+        else
+            k_img_offset_block<float><<<ew_grid(nb, g.isz), 256, 0, st>>>(
+                img.as<float>(), mSt, offBuf.as<float>(), RSt, F, wfSt(), v2.as<float>(), (int)g.isz, g.ip, g.nxi,
+                g.hExt, g.nExt, tlo, thi, wemvaForm ? 1 : 0);
+        kcheck();
     }
 
     void scale_shared(float* m, int nSlices, int mode) {
@@ -2020,7 +2026,7 @@ struct Context {
             std::vector<const float*> din(dataPtr.begin(), dataPtr.end());
             // subsurface offsets: BornOffsetShotsAdjGpu, F/src/BornExtShotsGpuFunctions.cu:1848-1990
             adj_sparse_pass(nb, din, nullptr, ACC_RING, nullptr, [&](int t, long long slot) {
-                if (offsets()) img_offset_adj(nb, slot, W, t, false);
+                if (offsets()) img_offset_adj_block(nb, slot, W, t, false, true);
                 else img_time_adj(nb, slot, W, t, +1);
             });
             reduce_images(nb, g.nExt, offsets() ? 3 : (P.sloth ? 2 : 1), out, true);
@@ -2166,14 +2172,14 @@ struct Context {
                 fwd_dense_pass(
                     nb, [&](int t, long long slot) { img_fwd(nb, slot, dm, 0, W2, t); }, false, false, ACC_RING,
                     nullptr, [&](int t, long long slot) {
-                        if (offsets()) img_offset_adj(nb, slot, R, t, true);
+                        if (offsets()) img_offset_adj_block(nb, slot, R, t, true, false);
                         else img_time_adj(nb, slot, R, t, -1);
                     });
             if (P.leg2)
                 adj_dense_pass(
                     nb, [&](int t, long long slot) { img_fwd(nb, slot, dm, 0, R, t); }, false,
                     [&](int t, long long slot) {
-                        if (offsets()) img_offset_adj(nb, slot, W2, t, false);
+                        if (offsets()) img_offset_adj_block(nb, slot, W2, t, false, true);
                         else img_time_adj(nb, slot, W2, t, +1);
                     });
             reduce_images(nb, g.nExt, offsets() ? 3 : 1, out, true);

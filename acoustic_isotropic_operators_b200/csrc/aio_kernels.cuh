@@ -303,34 +303,52 @@ __global__ void k_img_offset_tomo_adj(float* ss, long long ssSt, const float* m,
         ss[i] = v2Out ? acc * v2Out[i] : acc;
     }
 }
-// imagingOffsetAdjGpu (:397-411): img_e(x) += A(x+s) B(x-s), s = e-h, x in [h, nxi-h).
-// wemvaForm = 0: (A(x+s) * scaleA(x+s)) * B(x-s) — the receiver sample scaled by
-//   scaleSecondarySourceFd (:269-276) before imagingOffsetAdjGpu;
-// wemvaForm = 1: (B(x-s) * A(x+s)) * scaleA(x+s) — imagingOffsetWemvaScaleFwdGpu (:429-443) with
-//   A the receiver wavefield and B the scattered sample.
-// scaleA may be null (factor 1).
+// Subsurface-offset imaging of a block of coarse samples tlo..thi: imagingOffsetAdjGpu
+// (F/src/kernelsGpu.cu:397-411, img_e(x) += A(x+s) B(x-s), s = e-h, x in [h, nxi-h)) applied at
+// every sample of the block. R holds the block's ring samples (slice t - tlo, stride isz), F the
+// full coarse field (slice t).
+//   Born form (wemvaForm = 0): img_e(x) += sum_t (R_t(x+s) v2(x+s)) F_t(x-s) — the receiver
+//     sample scaled by scaleSecondarySourceFd (:269-276) before imagingOffsetAdjGpu;
+//   WEMVA form (1): img_e(x) += sum_t (R_t(x-s) F_t(x+s)) v2(x+s) — imagingOffsetWemvaScaleFwdGpu
+//     (:429-443) with F the receiver wavefield and R the scattered samples.
+// Each term is the reference's per-sample float product; the block's terms are summed in the
+// accumulator type and added to the image once per block instead of once per sample.
+constexpr int OFF_K = 32;
 template <typename Acc>
-__global__ void k_img_offset_adj(Acc* img, long long mSt, const float* A, long long ASt, const float* B, long long BSt,
-                                 const float* scaleA, long long isz, int ip, int nxi, int hExt, int nExt,
-                                 int wemvaForm) {
+__global__ void k_img_offset_block(Acc* img, long long mSt, const float* R, long long RSt, const float* F,
+                                   long long FSt, const float* v2, int isz, int ip, int nxi, int hExt, int nExt,
+                                   int tlo, int thi, int wemvaForm) {
     const int b = blockIdx.y;
-    img += b * mSt; A += b * ASt; B += b * BSt;
-    const long long n = (long long)nExt * isz;
-    AIO_GRID_STRIDE(k, n) {
-        const int e = (int)(k / isz);
-        const long long i = k - (long long)e * isz;
-        const int x = (int)(i / ip), s = e - hExt;
+    img += b * mSt;
+    R += b * RSt;
+    F += b * FSt + (long long)tlo * isz;
+    const int nk = thi - tlo + 1;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < isz; i += gridDim.x * blockDim.x) {
+        const int x = i / ip;
         if (x < hExt || x >= nxi - hExt) continue;
-        const long long ja = i + (long long)s * ip, jb = i - (long long)s * ip;
-        float v;
-        if (wemvaForm) {
-            v = B[jb] * A[ja];
-            if (scaleA) v = v * scaleA[ja];
-        } else {
-            const float a = scaleA ? A[ja] * scaleA[ja] : A[ja];
-            v = a * B[jb];
+        for (int e = 0; e < nExt; e++) {
+            const int s = e - hExt;
+            const int ja = i + s * ip, jb = i - s * ip;
+            const float sa = __ldg(v2 + ja);
+            Acc acc = 0;
+            const float* r = R;
+            const float* f = F;
+#pragma unroll 8
+            for (int k = 0; k < nk; k++) {
+                float v;
+                if (wemvaForm) {
+                    v = __ldg(r + jb) * __ldg(f + ja);
+                    v = v * sa;
+                } else {
+                    const float a = __ldg(r + ja) * sa;
+                    v = a * __ldg(f + jb);
+                }
+                acc += (Acc)v;
+                r += isz;
+                f += isz;
+            }
+            img[(long long)e * isz + i] += acc;
         }
-        img[k] += (Acc)v;
     }
 }
 

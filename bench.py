@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--nl", action="store_true",
                     help="instead of the Born step: time the nonlinear forward of one shot on the 200x400 grid "
                          "(304x512 interior, nts=1000) per call and print that line")
+    ap.add_argument("--variants", type=int, default=0,
+                    help="N > 0: time the free-surface Born and subsurface-offset extended Born operators on N shots")
     ap.add_argument("--plain", type=int, default=0,
                     help="instead of the batched step: time N shots one per call on the per-fine-step "
                          "stepper (the reference's schedule), FP32, and print that line")
@@ -322,6 +324,51 @@ def run_tomo(args):
     return 0
 
 
+def run_variants(args):
+    """The free-surface and subsurface-offset operators (per-fine-step stepper) on the Born
+    benchmark grid (512x1312 interior, nts from --nts): free-surface Born forward + adjoint and
+    the subsurface-offset extended Born adjoint (nExt = 31), N shots per call through the C ABI
+    with host buffers; each call is made twice and the second one timed."""
+    import torch
+    from acoustic_isotropic_operators_b200 import _capi, synthetic as S
+    from acoustic_isotropic_operators_b200.batch import Context, Shot
+    n_ext = 31
+    w = S.born_workload(nshots=args.variants, nts=args.nts)
+    lib = _capi.lib()
+    v2 = np.zeros(w.nz * w.nx, np.float32)
+    rs = np.zeros_like(v2)
+    velf = np.ascontiguousarray(w.vel.reshape(-1), np.float32)
+    lib.aio_fd_precompute(w.nz, w.nx, C.c_float(w.dts), w.sub, velf.ctypes.data_as(C.c_void_p),
+                          v2.ctypes.data_as(C.c_void_p), rs.ctypes.data_as(C.c_void_p))
+    sigs = prepare_signals(w, lib)
+    rng = np.random.default_rng(8)
+    shots = [Shot(a.src_pos, a.rec_pos, sg, (rng.standard_normal((len(a.rec_pos), w.nts)) * 1e-3).astype(np.float32))
+             for a, sg in zip(w.shots, sigs)]
+    model = np.ascontiguousarray(w.model, np.float32)
+    n, steps = w.n_interior, w.fine_steps
+    out = {}
+    geo = (w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs)
+    cases = [("free_surface_born_forward_adjoint", 4, dict(image_fp64=True, free_surface=1),
+              lambda c: (c.born_forward(model, shots), c.born_adjoint(shots))),
+             ("offset_extended_born_adjoint", 2, dict(nExt=n_ext, image_fp64=True, extension="offset"),
+              lambda c: c.born_ext_adjoint(shots))]
+    for name, passes, kw, fn in cases:
+        ctx = Context(*geo, **kw)   # one context at a time: each sizes its waves by the free memory
+        fn(ctx)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn(ctx)
+        t = time.perf_counter() - t0
+        ctx.close()
+        out[name] = {"seconds": t, "passes": passes, "Gpts_s": n * steps * passes * len(shots) / t / 1e9,
+                     "seconds_per_shot": t / len(shots)}
+    print(json.dumps({"impl": "this engine, free-surface and subsurface-offset operators (per-fine-step stepper, "
+                              "FP32, host buffers)", "metric": "Gpts/s", "unit": UNIT, "ops": out,
+                      "shots": len(shots), "nExt": n_ext, "interior": [w.nz - 10, w.nx - 10], "nts": w.nts,
+                      "data": "synthetic (seeded)"}))
+    return 0
+
+
 def run_nl(args):
     """Nonlinear forward of one shot on the 200x400 physical grid with Gaussian blobs (304x512
     interior, nts = 1000, 400 receivers), one call per shot through the C ABI with host buffers:
@@ -369,6 +416,8 @@ def main():
         return run_ext(args)
     if args.tomo:
         return run_tomo(args)
+    if args.variants:
+        return run_variants(args)
     if args.nl:
         return run_nl(args)
 

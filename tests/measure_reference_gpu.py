@@ -7,6 +7,8 @@ shots/s). Run on a GPU machine with oracle/_ref built:
 
     python tests/measure_reference_gpu.py [--nts 2000] [--repeats 2]
     python tests/measure_reference_gpu.py --nl     # nonlinear forward, 1 shot, 304x512 interior, nts=1000
+    python tests/measure_reference_gpu.py --variants   # free-surface Born forward + adjoint and the
+                                                        # subsurface-offset extended Born adjoint (nExt = 31)
 """
 import argparse
 import json
@@ -27,6 +29,7 @@ def main():
     ap.add_argument("--nts", type=int, default=2000)
     ap.add_argument("--repeats", type=int, default=2)
     ap.add_argument("--nl", action="store_true")
+    ap.add_argument("--variants", action="store_true")
     a = ap.parse_args()
     import orc
     import refgpu
@@ -66,6 +69,29 @@ def main():
     sig = bench.prepare_signals(w, _capi.lib())[0]
     sh = w.shots[0]
     s = orc.Scheme(nz=w.nz, nx=w.nx, nts=w.nts, dts=w.dts, sub=w.sub, dz=w.dz, dx=w.dx, minPad=w.minPad)
+    if a.variants:
+        import dataclasses
+        out = {}
+        sfs = dataclasses.replace(s, freeSurface=1)
+        soff = dataclasses.replace(s, extension=1, nExt=31)
+        d0 = (np.random.default_rng(8).standard_normal((len(sh.rec_pos), s.nts)) * 1e-3).astype(np.float32)
+        cases = [("free_surface_born_forward_adjoint", 4,
+                  lambda: refgpu.born_adj(sfs, w.vel, refgpu.born_fwd(sfs, w.vel, w.model, sig, sh.src_pos, sh.rec_pos),
+                                          sig, sh.src_pos, sh.rec_pos)),
+                 ("offset_extended_born_adjoint", 2,
+                  lambda: refgpu.bornext_adj(soff, w.vel, d0, sig, sh.src_pos, sh.rec_pos))]
+        for name, passes, fn in cases:
+            times = []
+            for _ in range(a.repeats + 1):
+                t0 = time.perf_counter()
+                fn()
+                times.append(time.perf_counter() - t0)
+            t = float(np.mean(times[1:]))
+            out[name] = {"seconds_per_shot": t, "passes": passes,
+                         "Gpts_s": w.n_interior * w.fine_steps * passes / t / 1e9}
+        print(json.dumps({"impl": "reference-gpu (own sm_100a build, one shot per call)",
+                          "workload": "512x1312 interior, nts=%d, nExt=31 for offsets" % w.nts, "ops": out}))
+        return
     times = []
     for _ in range(a.repeats + 1):
         t0 = time.perf_counter()

@@ -147,3 +147,23 @@ def test_vs_reference_offset_drivers(case):
                   refgpu.wemva_fwd(s, case.vel, m, sig, sp, rp, d)) < 1e-5
     assert rel_l2(ctx.wemva_adjoint(ext, [Shot(sp, rp, sig, None, d)]),
                   refgpu.wemva_adj(s, case.vel, ext, sig, sp, rp, d)) < 1e-5
+
+
+@pytest.mark.parametrize("n_ext", [33, 35])
+def test_wide_offsets(n_ext):
+    """Wide offset ranges (hExt = 16, 17) through the blocked offset imaging: extended Born adjoint
+    and WEMVA forward (the two imaging forms, in passes running backward and forward in time)
+    against the FP32 oracle; nts = 70 spans three blocks of 32 coarse samples, the last one partial."""
+    c = make_case(seed=19, nxi=80, nts=70, nExt=n_ext, nshots=1)
+    s = dataclasses.replace(c.scheme, extension=1)
+    c.scheme = s
+    ctx = ctx_for(c, extension="offset", image_fp64=True)
+    rng = np.random.default_rng(20)
+    d = [rng.standard_normal((len(r), s.nts)).astype(np.float32) for r in c.rec_pos]
+    ad = ctx.born_ext_adjoint(shots_for(c, data=d))
+    ref = orc.bornext_adj(s, c.vel, d[0], c.sig[0], c.src_pos[0], c.rec_pos[0], dtype=np.float32)
+    assert rel_l2(ad, ref) < 1e-5
+    m = (rng.standard_normal((c.nx, c.nz)) * interior_mask(c.nx, c.nz)).astype(np.float32)
+    fimg = ctx.wemva_forward(m, shots_for(c, wemva=d))
+    ref_f = orc.wemva_fwd(s, c.vel, m, c.sig[0], c.src_pos[0], c.rec_pos[0], d[0], dtype=np.float32)
+    assert rel_l2(fimg, ref_f) < 1e-5
