@@ -1305,7 +1305,8 @@ struct Context {
     // on the blocked stepper: launch L (interval its = nts-2-L) finishes the coarse receiver
     // sample R(its+1) (and R(0) at its == 0) into a ring of LAG_K slices; each time the lowest
     // sample of a block [bK, bK+K) has arrived, k_img_lag_block correlates the block with the
-    // stored wavefield (imagingTimeAdjGpu, F/src/kernelsGpu.cu:352-364, for every t of it).
+    // stored wavefield (imagingTimeAdjGpu, F/src/kernelsGpu.cu:352-364, for every t of it), or
+    // with subsurface offsets k_img_offset_block (imagingOffsetAdjGpu, :397-411).
     void tb_adjx_pass(int nb, const aio_shot* shots) {
         const TBPlan pl = tb_plan(nb);
         const int maxEnt = tb_lists(pl, nb, shots, 2, false);
@@ -1321,8 +1322,23 @@ struct Context {
             AIO_CK(cudaFuncSetAttribute(k_img_lag_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
             lagAttr = dev;
         }
-        require(lagSmem <= 200 * 1024, "extension too long for the blocked lag imaging");
+        require(offsets() || lagSmem <= 200 * 1024, "extension too long for the blocked lag imaging");
         auto image = [&](int tlo, int thi) {
+            if (offsets()) {
+                // subsurface offsets (BornOffsetShotsAdjGpu, F/src/BornExtShotsGpuFunctions.cu:1848-1990):
+                // U-form samples carry the v2 of scaleSecondarySourceFd already
+                const long long RSt = (long long)LAG_K * g.isz;
+                if (P.imageFp64)
+                    k_img_offset_block<double><<<ew_grid(nb, g.isz), 256, 0, st>>>(
+                        img.as<double>(), mSt, tbR.as<float>(), RSt, tbW.as<float>(), wfSt(), nullptr, (int)g.isz,
+                        g.ip, g.nxi, g.hExt, g.nExt, tlo, thi, 0);
+                else
+                    k_img_offset_block<float><<<ew_grid(nb, g.isz), 256, 0, st>>>(
+                        img.as<float>(), mSt, tbR.as<float>(), RSt, tbW.as<float>(), wfSt(), nullptr, (int)g.isz,
+                        g.ip, g.nxi, g.hExt, g.nExt, tlo, thi, 0);
+                kcheck();
+                return;
+            }
             const dim3 grid((unsigned)((g.isz + nP - 1) / nP), nb);
             if (P.imageFp64)
                 k_img_lag_block<double><<<grid, nP, lagSmem, st>>>(img.as<double>(), mSt, tbR.as<float>(),
@@ -1419,8 +1435,9 @@ struct Context {
             zero_images(nb, g.nExt);
             tb_adjx_pass(nb, shots + s0);
             // images of U = v2 * receiver wavefield: the reference's rs*v2 scaling reduces to rs,
-            // the sloth scaling -(m*v2) to a sign change
-            reduce_images(nb, g.nExt, P.sloth ? 4 : 3, out, true);
+            // the sloth scaling -(m*v2) to a sign change; subsurface offsets: rs (2/v^3) only, the
+            // v2 of their scaleSecondarySourceFd being the one U carries
+            reduce_images(nb, g.nExt, (P.sloth && !offsets()) ? 4 : 3, out, true);
             sync();
             s0 += nb;
         }
@@ -2011,7 +2028,7 @@ struct Context {
     // Extended (time-lag) Born adjoint (F/src/BornExtShotsGpuFunctions.cu:1525-1675).
     void born_ext_adjoint(float* modelOut, int add, int nShots, const aio_shot* shots, int mem) {
         begin_call();
-        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32 && !offsets())
+        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32)
             return born_ext_adjoint_tb(modelOut, add, nShots, shots, mem);
         Needs n;
         n.nWavefields = 1;

@@ -312,7 +312,8 @@ __global__ void k_img_offset_tomo_adj(float* ss, long long ssSt, const float* m,
 //   WEMVA form (1): img_e(x) += sum_t (R_t(x-s) F_t(x+s)) v2(x+s) — imagingOffsetWemvaScaleFwdGpu
 //     (:429-443) with F the receiver wavefield and R the scattered samples.
 // Each term is the reference's per-sample float product; the block's terms are summed in the
-// accumulator type and added to the image once per block instead of once per sample.
+// accumulator type and added to the image once per block instead of once per sample. v2 may be
+// null (factor 1: receiver samples in U-form, v2 * S, carry it already).
 constexpr int OFF_K = 32;
 template <typename Acc>
 __global__ void k_img_offset_block(Acc* img, long long mSt, const float* R, long long RSt, const float* F,
@@ -322,30 +323,37 @@ __global__ void k_img_offset_block(Acc* img, long long mSt, const float* R, long
     img += b * mSt;
     R += b * RSt;
     F += b * FSt + (long long)tlo * isz;
-    const int nk = thi - tlo + 1;
+    const int nk = min(thi - tlo + 1, OFF_K);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < isz; i += gridDim.x * blockDim.x) {
         const int x = i / ip;
         if (x < hExt || x >= nxi - hExt) continue;
         for (int e = 0; e < nExt; e++) {
             const int s = e - hExt;
             const int ja = i + s * ip, jb = i - s * ip;
-            const float sa = __ldg(v2 + ja);
+            const float sa = v2 ? __ldg(v2 + ja) : 1.f;
+            // all of the block's operands are loaded before the first product (the kernel is
+            // bound by load latency otherwise)
+            const int jr = wemvaForm ? jb : ja, jf = wemvaForm ? ja : jb;
+            float rv[OFF_K], fv[OFF_K];
+#pragma unroll
+            for (int k = 0; k < OFF_K; k++) {
+                rv[k] = k < nk ? __ldg(R + (long long)k * isz + jr) : 0.f;
+                fv[k] = k < nk ? __ldg(F + (long long)k * isz + jf) : 0.f;
+            }
             Acc acc = 0;
-            const float* r = R;
-            const float* f = F;
-#pragma unroll 8
-            for (int k = 0; k < nk; k++) {
-                float v;
-                if (wemvaForm) {
-                    v = __ldg(r + jb) * __ldg(f + ja);
-                    v = v * sa;
-                } else {
-                    const float a = __ldg(r + ja) * sa;
-                    v = a * __ldg(f + jb);
+#pragma unroll
+            for (int k = 0; k < OFF_K; k++) {
+                if (k < nk) {
+                    float v;
+                    if (wemvaForm) {
+                        v = rv[k] * fv[k];
+                        v = v * sa;
+                    } else {
+                        const float a = rv[k] * sa;
+                        v = a * fv[k];
+                    }
+                    acc += (Acc)v;
                 }
-                acc += (Acc)v;
-                r += isz;
-                f += isz;
             }
             img[(long long)e * isz + i] += acc;
         }
