@@ -203,8 +203,6 @@ struct Context {
                 "extension must be AIO_EXT_TIME or AIO_EXT_OFFSET");
         require(p.extension != AIO_EXT_OFFSET || 2 * ((p.nExt - 1) / 2) < p.nx - 2 * FAT,
                 "subsurface offsets longer than the interior width");
-        require(!(p.freeSurface && p.stepper == AIO_STEPPER_BLOCKED),
-                "the free surface runs on the per-fine-step stepper (stepper AUTO or FINE)");
         require(p.wavefieldPrecision == AIO_WFLD_FP32 || (p.stepper != AIO_STEPPER_FINE && p.sub == 4),
                 "compressed stored wavefields need the interval-blocked stepper (sub == 4)");
         g = make_geom(p.nz, p.nx, p.nts, p.sub, p.minPad, p.nExt);
@@ -840,7 +838,7 @@ struct Context {
         int T = KT_T, HZ = 0, nStrips = 0, LX = 0, nChunks = 0, iters = 0, threads = 0, NQ = 0;
     };
 
-    bool tb_enabled() const { return P.stepper != AIO_STEPPER_FINE && g.sub == KT_T && !P.freeSurface; }
+    bool tb_enabled() const { return P.stepper != AIO_STEPPER_FINE && g.sub == KT_T; }
     int wbytes() const { return P.wavefieldPrecision == AIO_WFLD_FP32 ? 4 : 2; }
     bool f16() const { return P.wavefieldPrecision == AIO_WFLD_FP16; }
 
@@ -947,8 +945,12 @@ struct Context {
         }
         return m;
     }
-    // row quads of the k_tile variant a strip of NQ row quads runs on
-    static int tb_variant(int NQ) { return NQ <= KT_MAXQ_S ? KT_MAXQ_S : (NQ <= KT_MAXQ_M ? KT_MAXQ_M : KT_MAXQ); }
+    // row quads of the k_tile variant a strip of NQ row quads runs on (the free surface: the
+    // large-strip variant only)
+    int tb_variant(int NQ) const {
+        if (P.freeSurface) return KT_MAXQ;
+        return NQ <= KT_MAXQ_S ? KT_MAXQ_S : (NQ <= KT_MAXQ_M ? KT_MAXQ_M : KT_MAXQ);
+    }
     // plan pl fits in shared memory in every mode
     bool tb_plan_fits(const TBPlan& pl, const TBEntries& e) const {
         int smemMax = 0;
@@ -1198,14 +1200,14 @@ struct Context {
         return a;
     }
 
-    template <int MODE, int WP, int MAXQ>
+    template <int MODE, int WP, int MAXQ, bool FS = false>
     void tb_launch_q(const TBPlan& pl, int nb, KTArgs& a, int v) {
         const size_t smem = kt_smem_bytes(MODE, pl.threads, pl.iters, a.maxEnt, kt_rs(MAXQ), kt_v2s(MAXQ));
         static int attrDev = -1;
         static int smemMax = 0;
         if (attrDev != dev) {
             AIO_CK(cudaDeviceGetAttribute(&smemMax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-            AIO_CK(cudaFuncSetAttribute(k_tile<MODE, WP, MAXQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, smemMax));
+            AIO_CK(cudaFuncSetAttribute(k_tile<MODE, WP, MAXQ, FS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smemMax));
             attrDev = dev;
         }
         require(smem <= (size_t)smemMax, "blocked stepper: shared memory plan of " + std::to_string(smem) +
@@ -1219,7 +1221,7 @@ struct Context {
             ev = take_events();
             AIO_CK(cudaEventRecord(ev.first, st));
         }
-        k_tile<MODE, WP, MAXQ><<<dim3(pl.nStrips, pl.nChunks, nb), pl.threads, smem, st>>>(a);
+        k_tile<MODE, WP, MAXQ, FS><<<dim3(pl.nStrips, pl.nChunks, nb), pl.threads, smem, st>>>(a);
         AIO_CK(cudaGetLastError());
         if (timed) {
             AIO_CK(cudaEventRecord(ev.second, st));
@@ -1233,7 +1235,8 @@ struct Context {
     // rings (two CTAs per SM); taller strips the large one.
     template <int MODE, int WP>
     void tb_launch_t(const TBPlan& pl, int nb, KTArgs& a, int v) {
-        if (pl.NQ <= KT_MAXQ_S) tb_launch_q<MODE, WP, KT_MAXQ_S>(pl, nb, a, v);
+        if (P.freeSurface) tb_launch_q<MODE, WP, KT_MAXQ, true>(pl, nb, a, v);
+        else if (pl.NQ <= KT_MAXQ_S) tb_launch_q<MODE, WP, KT_MAXQ_S>(pl, nb, a, v);
         else if (pl.NQ <= KT_MAXQ_M) tb_launch_q<MODE, WP, KT_MAXQ_M>(pl, nb, a, v);
         else tb_launch_q<MODE, WP, KT_MAXQ>(pl, nb, a, v);
     }

@@ -209,7 +209,37 @@ __device__ __forceinline__ float2 kt_pair(const float4 (&Z)[5], int r) {
     return make_float2(kt_el(Z[i >> 2], i & 3), kt_el(Z[(i + 1) >> 2], (i + 1) & 3));
 }
 
-template <int MODE, int WPREC, int MAXQ = KT_MAXQ>
+// element idx (0..19) of the 20-row window held as quads Z[0..4]
+__device__ __forceinline__ float kt_win(const float4 (&Z)[5], int idx) { return kt_el(Z[idx >> 2], idx & 3); }
+// Free surface, forward modes (setFsConditionFwdGpu, F/src/kernelsGpu.cu:555-567): the stencil
+// sees the current level with its top interior row zeroed and rows -1..-5 set to minus rows
+// 1..5. Applied to the z-window (rows zq-8 .. zq+11) of the threads whose outputs read row 0
+// or above: zq = 0 (rows 0..3) and zq = 4 (rows 4..7), in whichever strip computes them.
+__device__ __forceinline__ void kt_fs_window(float4 (&Z)[5], int zq) {
+    float w[20];
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+        w[4 * i] = Z[i].x;
+        w[4 * i + 1] = Z[i].y;
+        w[4 * i + 2] = Z[i].z;
+        w[4 * i + 3] = Z[i].w;
+    }
+    if (zq == 0) {  // row r at index r + 8
+        w[8] = 0.f;
+#pragma unroll
+        for (int r = 1; r <= 5; r++) w[8 - r] = -w[8 + r];
+    } else {        // zq == 4: row r at index r + 4
+        w[4] = 0.f;
+#pragma unroll
+        for (int r = 1; r <= 4; r++) w[4 - r] = -w[4 + r];
+    }
+#pragma unroll
+    for (int i = 0; i < 5; i++) Z[i] = make_float4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+}
+__host__ __device__ constexpr bool kt_adj(int mode) { return mode == TB_ADJ || mode == TB_ADJR || mode == TB_ADJX; }
+
+// FS: free surface at the top interior row (runs on the large-strip variant only)
+template <int MODE, int WPREC, int MAXQ = KT_MAXQ, bool FS = false>
 __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 2) k_tile(const KTArgs a) {
     constexpr int T = KT_T;
     extern __shared__ float4 kt_smem4[];
@@ -316,7 +346,7 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
         const int z = zq + i;
         float d = 0.f;
         if (z >= 0 && z < nzi) {
-            const int dd = min(z, nzi - 1 - z);
+            const int dd = FS ? nzi - 1 - z : min(z, nzi - 1 - z);  // dampCosineEdgeFs: no top taper
             d = dd < g.minPad ? __ldg(a.taper + dd) : 1.f;
         }
         Dz[i] = d;
@@ -430,6 +460,22 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
                     ol[0] = kt_ld4(col(t - 2, c0));
                     ol[1] = kt_ld4(col(t - 2, c0 + 1));
                 }
+                // free surface: forward modes see row 0 zeroed and rows above it mirrored (also
+                // row 0 of the old level); adjoint modes are corrected below
+                const bool fsTop = FS && (zq == 0 || zq == 4);  // quads of rows 0..3 and 4..7
+                if (!kt_adj(MODE) && fsTop) {
+#pragma unroll
+                    for (int j = 0; j < 2; j++) kt_fs_window(zq4[j], zq);
+                    if (zq == 0) {
+#pragma unroll
+                        for (int d = 0; d < 5; d++) {
+                            xm[d].x = 0.f;
+                            xp[d].x = 0.f;
+                        }
+                        ol[0].x = 0.f;
+                        ol[1].x = 0.f;
+                    }
+                }
                 float4 vq[2];
                 float Dx[2];
 #pragma unroll
@@ -494,6 +540,25 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
 #pragma unroll
                         for (int kk = 1; kk <= 5; kk++)
                             lz = __ffma2_rn(zc2[kk], __fadd2_rn(kt_pair(zq4[j], a0 + kk), kt_pair(zq4[j], a0 - kk)), lz);
+                        if (kt_adj(MODE) && fsTop) {
+                            // stepAdjFsGpu (F/src/kernelsGpu.cu:613-740), U-form: rows zi = 1..4 drop
+                            // the mirror terms, lz(zi) -= sum_{k=zi+1..5} zc[k] U(k - zi)
+                            if (zq == 0) {
+#pragma unroll
+                                for (int h = 0; h < 2; h++) {
+                                    const int zi = a0 + h;  // window index of row r: r + 8
+                                    if (zi >= 1 && zi <= 4) {
+                                        float c = h ? lz.y : lz.x;
+#pragma unroll
+                                        for (int k = zi + 1; k <= 5; k++) c = c - a.c.zc[k] * kt_win(zq4[j], k - zi + 8);
+                                        if (h) lz.y = c;
+                                        else lz.x = c;
+                                    }
+                                }
+                            } else if (P == 0) {  // zq == 4: row 4 (index 8), k = 5 reads row 1 (index 5)
+                                lz.x = lz.x - a.c.zc[5] * kt_win(zq4[j], 5);
+                            }
+                        }
                         float2 lx = __fmul2_rn(xc2[0], ctr);
 #pragma unroll
                         for (int kk = 1; kk <= 5; kk++)
@@ -501,6 +566,8 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
                         float2 n = __ffma2_rn(kt_half(vq[j], P), __fadd2_rn(lz, lx), ctr);
                         n = __fadd2_rn(n, ctr);
                         n = __ffma2_rn(make_float2(-Dm[j][a0], -Dm[j][a0 + 1]), kt_half(ol[j], P), n);
+                        // free surface, adjoint modes: the top row keeps the old level (D o)
+                        if (kt_adj(MODE) && fsTop && zq == 0 && P == 0) n.x = Dm[j][0] * ol[j].x;
                         if (tb_scatlike(MODE)) {
                             // injectSecondarySource (F/src/kernelsGpu.cu:102-107): forward fine step it2 = t
                             // weighs ss(its), ss(its+1) by h[it2-1], h[H+it2-1]; adjoint step it2 = T-t by

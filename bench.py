@@ -326,9 +326,9 @@ def run_tomo(args):
 
 def run_variants(args):
     """The free-surface and subsurface-offset operators on the Born benchmark grid (512x1312
-    interior, nts from --nts): free-surface Born forward + adjoint (per-fine-step stepper) and the
-    subsurface-offset extended Born adjoint (nExt = 31, blocked stepper), N shots per call through
-    the C ABI with host buffers; each call is made twice and the second one timed."""
+    interior, nts from --nts): free-surface Born forward + adjoint and the subsurface-offset
+    extended Born adjoint (nExt = 31), both on the blocked stepper, N shots per call through the
+    C ABI with host buffers; each call is made twice and the second one timed."""
     import torch
     from acoustic_isotropic_operators_b200 import _capi, synthetic as S
     from acoustic_isotropic_operators_b200.batch import Context, Shot
@@ -362,8 +362,8 @@ def run_variants(args):
         ctx.close()
         out[name] = {"seconds": t, "passes": passes, "Gpts_s": n * steps * passes * len(shots) / t / 1e9,
                      "seconds_per_shot": t / len(shots)}
-    print(json.dumps({"impl": "this engine, free-surface Born (per-fine-step stepper) and subsurface-offset "
-                              "extended Born adjoint (blocked stepper), FP32, host buffers",
+    print(json.dumps({"impl": "this engine, free-surface Born and subsurface-offset extended Born adjoint "
+                              "(blocked stepper), FP32, host buffers",
                       "metric": "Gpts/s", "unit": UNIT, "ops": out,
                       "shots": len(shots), "nExt": n_ext, "interior": [w.nz - 10, w.nx - 10], "nts": w.nts,
                       "data": "synthetic (seeded)"}))

@@ -69,7 +69,7 @@ typedef struct {
     int chunkColumns;    /* blocked stepper x-chunk width: 0 = autotuned (measured once per wave size),
                             > 0 = fixed width (strips of at most 128 rows) */
     int freeSurface;     /* 1: free surface at the top interior row (reference par freeSurface;
-                            the *FsGpu drivers); runs on the per-fine-step stepper */
+                            the *FsGpu drivers); both steppers */
     int extension;       /* AIO_EXT_*: extension axis of the extended Born / tomo / WEMVA operators
                             (reference par extension "time" / "offset") */
 } aio_params;
@@ -243,8 +243,8 @@ int aio_tomoTimeShotsAdjGpu(float* model, float* dataRegDts, float* extReflectiv
                             int* sourcesPositionReg, int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
                             float* tomoSrcWavefieldDt2, float* tomoSecWavefield1, float* tomoSecWavefield2,
                             int sloth, int iGpu, int iGpuId, int saveWavefield);
-/* Free-surface drivers (reference freeSurface == 1): same arguments as the plain calls of the family;
- * they run on the per-fine-step stepper with the top interior row as a pressure-free surface. */
+/* Free-surface drivers (reference freeSurface == 1): same arguments as the plain calls of the family,
+ * with the top interior row as a pressure-free surface. */
 /* F/include/nonlinearShotsGpuFunctions.h:15 */
 int aio_propShotsFwdFsGpu(float* modelRegDtw, float* dataRegDts, int* sourcesPositionReg, int nSourcesReg,
                           int* receiversPositionReg, int nReceiversReg, float* wavefieldDts, int iGpu, int iGpuId);

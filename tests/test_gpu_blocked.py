@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 import orc
+import refgpu
 from cases import Case, interior_mask, rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -359,3 +360,89 @@ def test_born_ext_offset_adjoint_blocked(case, n_ext):
     a32 = sum(float(np.sum(r32[i].astype(np.float64) * d[i])) for i in range(len(d)))
     b32 = float(np.sum(m.astype(np.float64) * ref))
     assert abs(a - b) / abs(b) < max(1e-5, 2 * abs(a32 - b32) / abs(b32))
+
+
+def _fs_case():
+    import dataclasses
+    c = blocked_case(seed=21, nts=40)
+    c.scheme = dataclasses.replace(c.scheme, freeSurface=1)
+    # a source 3 rows below the surface in each shot: the surface reflection reaches the receivers
+    for i in range(len(c.src_pos)):
+        c.src_pos[i] = np.concatenate([c.src_pos[i], np.array([(5 + 100 + 50 * i) * c.nz + 5 + 3], np.int32)])
+        c.sig[i] = (c.rng.standard_normal((len(c.src_pos[i]), c.scheme.ntw)) * 1e-2).astype(np.float32)
+    return c
+
+
+def test_free_surface_blocked():
+    """Free surface on the blocked stepper (forward modes: the top row zeroed and the rows above it
+    mirrored; adjoint modes: stepAdjFsGpu's corrections, in U-form): nonlinear forward / adjoint,
+    Born forward / adjoint, extended (time-lag) Born forward / adjoint and tomo with both legs
+    against the FP32 oracle with the free surface (relative L2 1e-5), one launch per interval and
+    pass, and the Born dot test."""
+    from acoustic_isotropic_operators_b200.batch import Shot
+    c = _fs_case()
+    s = c.scheme
+    k = lambda **kw: ctx(c, free_surface=1, **kw)  # noqa: E731
+    nl = k().nonlinear_forward(shots(c))
+    for i in range(2):
+        r32 = orc.nl_fwd(s, c.vel, c.sig[i], c.src_pos[i], c.rec_pos[i], dtype=np.float32)
+        assert rel_l2(nl[i], r32) < 1e-5
+    plain = ctx(c).nonlinear_forward(shots(c))[0]
+    assert rel_l2(plain, nl[0]) > 1e-3                   # the surface changes the answer
+    rng = np.random.default_rng(22)
+    d = [rng.standard_normal((len(r), s.nts)).astype(np.float32) for r in c.rec_pos]
+    na = k().nonlinear_adjoint([Shot(c.src_pos[i], c.rec_pos[i], None, d[i]) for i in range(2)])
+    for i in range(2):
+        assert rel_l2(na[i], orc.nl_adj(s, c.vel, d[i], c.src_pos[i], c.rec_pos[i], dtype=np.float32)) < 1e-5
+    mask = interior_mask(c.nx, c.nz)
+    m = (rng.standard_normal((c.nx, c.nz)) * mask).astype(np.float32)
+    b = k(image_fp64=True)
+    fm = [x.copy() for x in b.born_forward(m, shots(c))]
+    assert b.last_launches == 2 * (s.nts - 1)
+    for i in range(2):
+        assert rel_l2(fm[i], orc.born_fwd(s, c.vel, m, c.sig[i], c.src_pos[i], c.rec_pos[i], dtype=np.float32)) < 1e-5
+    ad = b.born_adjoint(shots(c, d))
+    assert b.last_launches == 2 * (s.nts - 1)
+    ref = sum(orc.born_adj(s, c.vel, d[i], c.sig[i], c.src_pos[i], c.rec_pos[i], dtype=np.float32) for i in range(2))
+    assert rel_l2(ad, ref) < 1e-5
+    a_ = sum(float(np.sum(fm[i].astype(np.float64) * d[i])) for i in range(2))
+    b_ = float(np.sum(m.astype(np.float64) * ad))
+    assert abs(a_ - b_) / abs(b_) < 1e-5
+    s5, e = _ext_ctx(c, free_surface=1)
+    ext = (rng.standard_normal((5, c.nx, c.nz)) * mask).astype(np.float32)
+    fe = [x.copy() for x in e.born_ext_forward(ext, shots(c))]
+    assert e.last_launches == 2 * (s5.nts - 1)
+    for i in range(2):
+        assert rel_l2(fe[i], orc.bornext_fwd(s5, c.vel, ext, c.sig[i], c.src_pos[i], c.rec_pos[i],
+                                             dtype=np.float32)) < 1e-5
+    ae = e.born_ext_adjoint(shots(c, d))
+    ref = sum(orc.bornext_adj(s5, c.vel, d[i], c.sig[i], c.src_pos[i], c.rec_pos[i], dtype=np.float32)
+              for i in range(2))
+    assert rel_l2(ae, ref) < 1e-5
+    s5, t = _ext_ctx(c, free_surface=1, leg1=1, leg2=1)
+    ft = [x.copy() for x in t.tomo_forward(m, ext, shots(c))]
+    assert t.last_launches == 5 * (s5.nts - 1)
+    for i in range(2):
+        assert rel_l2(ft[i], orc.tomo_fwd(s5, c.vel, m, ext, c.sig[i], c.src_pos[i], c.rec_pos[i],
+                                          dtype=np.float32)) < 1e-5
+    at = t.tomo_adjoint(ext, shots(c, d))
+    ref = sum(orc.tomo_adj(s5, c.vel, d[i], ext, c.sig[i], c.src_pos[i], c.rec_pos[i], dtype=np.float32)
+              for i in range(2))
+    assert rel_l2(at, ref) < 1e-5
+
+
+@pytest.mark.skipif(not refgpu.available("born"), reason="oracle/_ref not built (make -C oracle ref)")
+def test_free_surface_blocked_vs_reference_drivers():
+    """Blocked stepper with the free surface against the reference's own free-surface drivers
+    (nonlinear forward, Born forward / adjoint; one shot)."""
+    from acoustic_isotropic_operators_b200.batch import Shot
+    c = _fs_case()
+    s = c.scheme
+    sp, rp, sig = c.src_pos[0], c.rec_pos[0], c.sig[0]
+    one = [Shot(sp, rp, sig)]
+    b = ctx(c, free_surface=1, image_fp64=True)
+    assert rel_l2(b.nonlinear_forward(one)[0], refgpu.nl_fwd(s, c.vel, sig, sp, rp)) < 1e-5
+    m = (np.random.default_rng(23).standard_normal((c.nx, c.nz)) * interior_mask(c.nx, c.nz)).astype(np.float32)
+    assert rel_l2(b.born_forward(m, one)[0], refgpu.born_fwd(s, c.vel, m, sig, sp, rp)) < 1e-5
+    d = (np.random.default_rng(24).standard_normal((len(rp), s.nts)) * 1e-2).astype(np.float32)
+    assert rel_l2(b.born_adjoint([Shot(sp, rp, sig, d)]), refgpu.born_adj(s, c.vel, d, sig, sp, rp)) < 1e-5

@@ -78,15 +78,15 @@ def test_born_fs(case):
     assert abs(a - _dot(m, ad)) / abs(_dot(m, ad)) < 1e-5
 
 
-def test_born_fs_sub4_runs_per_fine_step():
-    """With sub = 4 the automatic stepper would be the interval-blocked one; the free surface
-    runs on the per-fine-step stepper (one launch per fine step) and matches the oracle."""
+def test_born_fs_sub4_runs_blocked():
+    """With sub = 4 the free surface runs on the interval-blocked stepper (one launch per coarse
+    interval and pass) and matches the oracle."""
     c = make_case(seed=8, nts=30, sub=4)
     c.scheme = dataclasses.replace(c.scheme, freeSurface=1)
     ctx = ctx_for(c, free_surface=1)
     m = (np.random.default_rng(4).standard_normal((c.nx, c.nz)) * interior_mask(c.nx, c.nz)).astype(np.float32)
     got = ctx.born_forward(m, shots_for(c))
-    assert ctx.last_launches == 2 * (c.scheme.nts - 1) * 4
+    assert ctx.last_launches == 2 * (c.scheme.nts - 1)
     for i in range(len(got)):
         assert rel_l2(got[i], orc.born_fwd(c.scheme, c.vel, m, c.sig[i], c.src_pos[i], c.rec_pos[i],
                                            dtype=np.float32)) < 1e-5
