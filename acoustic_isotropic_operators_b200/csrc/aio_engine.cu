@@ -1382,9 +1382,23 @@ struct Context {
             AIO_CK(cudaFuncSetAttribute(k_ss_lag_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
             ssAttr = dev;
         }
-        require(lagSmem <= 200 * 1024, "extension too long for the blocked lag imaging");
+        require(offsets() || lagSmem <= 200 * 1024, "extension too long for the blocked lag imaging");
         auto sources = [&](int tlo) {
             const int thi = std::min(tlo + LAG_K - 1, g.nts - 1);
+            if (offsets()) {
+                // subsurface offsets (imagingOffsetFwdGpu + scaleSecondarySourceFd): one slice per
+                // sample, formed into the zeroed ring slots of the block
+                const long long rSt = (long long)ring * g.isz;
+                AIO_CK(cudaMemset2DAsync(tbSS.as<float>() + (long long)(tlo % ring) * g.isz, (size_t)rSt * 4, 0,
+                                         (size_t)(thi - tlo + 1) * g.isz * 4, nb, st));
+                const float* Fs = F ? F : tbW.as<float>();
+                for (int t = tlo; t <= thi; t++)
+                    k_img_offset_fwd<<<ew_grid(nb, g.isz), 256, 0, st>>>(
+                        tbSS.as<float>() + (long long)(t % ring) * g.isz, rSt, ext, 0, Fs + (long long)t * g.isz,
+                        wfSt(), v2.as<float>(), g.isz, g.ip, g.nxi, g.hExt);
+                kcheck();
+                return;
+            }
             const dim3 grid((unsigned)((g.isz + nP - 1) / nP), nb);
             k_ss_lag_block<<<grid, nP, lagSmem, st>>>(tbSS.as<float>(), (long long)ring * g.isz, ring, ext,
                                                       F ? F : tbW.as<float>(), wfSt(), g.isz, tlo, thi, g.nts, g.hExt,
@@ -1403,7 +1417,8 @@ struct Context {
 
     void born_ext_forward_tb(const float* model, int nShots, const aio_shot* shots, int mem) {
         float* ext = stage_model(model, g.nExt, mem, this->model);
-        scale_shared(ext, g.nExt, P.sloth ? 2 : 1);
+        // subsurface offsets: 2/v^3 only, v^2 applied to each secondary-source slice
+        scale_shared(ext, g.nExt, offsets() ? 3 : (P.sloth ? 2 : 1));
         Needs n;
         for (int s0 = 0; s0 < nShots;) {
             const int nb = tb_wave_size(nShots - s0, shots + s0, true, false);
@@ -1940,7 +1955,7 @@ struct Context {
     // Extended (time-lag) Born forward (F/src/BornExtShotsGpuFunctions.cu:269-419).
     void born_ext_forward(const float* model, int nShots, const aio_shot* shots, int mem) {
         begin_call();
-        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32 && !offsets())
+        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32)
             return born_ext_forward_tb(model, nShots, shots, mem);
         Needs n;
         n.nWavefields = 1;

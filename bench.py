@@ -327,8 +327,8 @@ def run_tomo(args):
 def run_variants(args):
     """The free-surface and subsurface-offset operators on the Born benchmark grid (512x1312
     interior, nts from --nts): free-surface Born forward + adjoint and the subsurface-offset
-    extended Born adjoint (nExt = 31), both on the blocked stepper, N shots per call through the
-    C ABI with host buffers; each call is made twice and the second one timed."""
+    extended Born forward and adjoint (nExt = 31), on the blocked stepper, N shots per call through
+    the C ABI with host buffers; each call is made twice and the second one timed."""
     import torch
     from acoustic_isotropic_operators_b200 import _capi, synthetic as S
     from acoustic_isotropic_operators_b200.batch import Context, Shot
@@ -345,11 +345,14 @@ def run_variants(args):
     shots = [Shot(a.src_pos, a.rec_pos, sg, (rng.standard_normal((len(a.rec_pos), w.nts)) * 1e-3).astype(np.float32))
              for a, sg in zip(w.shots, sigs)]
     model = np.ascontiguousarray(w.model, np.float32)
+    ext_model = np.ascontiguousarray(np.repeat(model[None], n_ext, axis=0) / n_ext, np.float32)
     n, steps = w.n_interior, w.fine_steps
     out = {}
     geo = (w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs)
     cases = [("free_surface_born_forward_adjoint", 4, dict(image_fp64=True, free_surface=1),
               lambda c: (c.born_forward(model, shots), c.born_adjoint(shots))),
+             ("offset_extended_born_forward", 2, dict(nExt=n_ext, image_fp64=True, extension="offset"),
+              lambda c: c.born_ext_forward(ext_model, shots)),
              ("offset_extended_born_adjoint", 2, dict(nExt=n_ext, image_fp64=True, extension="offset"),
               lambda c: c.born_ext_adjoint(shots))]
     for name, passes, kw, fn in cases:
@@ -362,7 +365,7 @@ def run_variants(args):
         ctx.close()
         out[name] = {"seconds": t, "passes": passes, "Gpts_s": n * steps * passes * len(shots) / t / 1e9,
                      "seconds_per_shot": t / len(shots)}
-    print(json.dumps({"impl": "this engine, free-surface Born and subsurface-offset extended Born adjoint "
+    print(json.dumps({"impl": "this engine, free-surface Born and subsurface-offset extended Born "
                               "(blocked stepper), FP32, host buffers",
                       "metric": "Gpts/s", "unit": UNIT, "ops": out,
                       "shots": len(shots), "nExt": n_ext, "interior": [w.nz - 10, w.nx - 10], "nts": w.nts,

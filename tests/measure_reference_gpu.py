@@ -8,7 +8,8 @@ shots/s). Run on a GPU machine with oracle/_ref built:
     python tests/measure_reference_gpu.py [--nts 2000] [--repeats 2]
     python tests/measure_reference_gpu.py --nl     # nonlinear forward, 1 shot, 304x512 interior, nts=1000
     python tests/measure_reference_gpu.py --variants   # free-surface Born forward + adjoint and the
-                                                        # subsurface-offset extended Born adjoint (nExt = 31)
+                                                        # subsurface-offset extended Born forward and
+                                                        # adjoint (nExt = 31)
 """
 import argparse
 import json
@@ -75,9 +76,12 @@ def main():
         sfs = dataclasses.replace(s, freeSurface=1)
         soff = dataclasses.replace(s, extension=1, nExt=31)
         d0 = (np.random.default_rng(8).standard_normal((len(sh.rec_pos), s.nts)) * 1e-3).astype(np.float32)
+        ext_model = np.ascontiguousarray(np.repeat(w.model[None], 31, axis=0) / 31, np.float32)
         cases = [("free_surface_born_forward_adjoint", 4,
                   lambda: refgpu.born_adj(sfs, w.vel, refgpu.born_fwd(sfs, w.vel, w.model, sig, sh.src_pos, sh.rec_pos),
                                           sig, sh.src_pos, sh.rec_pos)),
+                 ("offset_extended_born_forward", 2,
+                  lambda: refgpu.bornext_fwd(soff, w.vel, ext_model, sig, sh.src_pos, sh.rec_pos)),
                  ("offset_extended_born_adjoint", 2,
                   lambda: refgpu.bornext_adj(soff, w.vel, d0, sig, sh.src_pos, sh.rec_pos))]
         for name, passes, fn in cases:

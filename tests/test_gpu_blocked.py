@@ -333,9 +333,9 @@ def test_mid_strip_variant(nzi):
 
 @pytest.mark.parametrize("n_ext", [5, 31])
 def test_born_ext_offset_adjoint_blocked(case, n_ext):
-    """Extended Born adjoint with subsurface offsets on the blocked stepper (ADJR receiver pass,
-    offset imaging in blocks of 32 coarse samples): vs the FP32 oracle (1e-5), and the dot test
-    against the offset forward (per-fine-step stepper)."""
+    """Extended Born forward and adjoint with subsurface offsets on the blocked stepper (SCATX pass
+    fed by per-sample offset sources; ADJR receiver pass with offset imaging in blocks of 32 coarse
+    samples): vs the FP32 oracle (1e-5), and the dot test."""
     import dataclasses
     from acoustic_isotropic_operators_b200.batch import Context
     s = dataclasses.replace(case.scheme, nExt=n_ext, extension=1)
@@ -351,6 +351,7 @@ def test_born_ext_offset_adjoint_blocked(case, n_ext):
     assert rel_l2(got, ref) < 1e-5
     m = (rng.standard_normal((n_ext, case.nx, case.nz)) * interior_mask(case.nx, case.nz)).astype(np.float32)
     fm = [x.copy() for x in c.born_ext_forward(m, shots(case))]
+    assert c.last_launches == 2 * (s.nts - 1)          # forward on the blocked stepper too
     r32 = [orc.bornext_fwd(s, case.vel, m, case.sig[i], case.src_pos[i], case.rec_pos[i], dtype=np.float32)
            for i in range(len(fm))]
     for i in range(len(fm)):
