@@ -1636,7 +1636,7 @@ struct Context {
         const long long shared = (4LL + 2 * g.nExt) * g.isz * 4 + (64LL << 20);
         const long long cap = (budget - shared) / per;
         require(cap >= 1, "device memory budget cannot hold one shot for this operator");
-        return (int)std::min<long long>(cap, nShots);
+        return balanced_wave(cap, nShots);
     }
     void tb_fields_alloc(int nb) {
         tb_alloc(nb, false);
