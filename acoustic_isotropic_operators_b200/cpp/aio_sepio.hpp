@@ -13,6 +13,7 @@
 // name the data file `<header path>@`, or `$DATAPATH<header file name>@` when the
 // DATAPATH environment variable is set.
 #pragma once
+#include <algorithm>
 #include <cctype>
 #include <cstdint>
 #include <cstdio>
@@ -155,10 +156,15 @@ class genericRegFile {
     }
     void writeFloatStream(const float* p, long long n) {
         if (!_data || _usage == usageIn) throw std::runtime_error("SEP: writeDescription before writing " + _header);
-        std::vector<float> buf(p, p + n);
-        if (swap()) swapBytes(buf.data(), n);
-        if (std::fwrite(buf.data(), 4, (size_t)n, _data) != (size_t)n)
-            throw std::runtime_error("SEP: short write to " + _dataPath);
+        const long long chunk = 1 << 20;  // byte-swapped through a bounded buffer
+        std::vector<float> buf((size_t)std::min(n, chunk));
+        for (long long o = 0; o < n; o += chunk) {
+            const long long m = std::min(chunk, n - o);
+            std::copy(p + o, p + o + m, buf.begin());
+            if (swap()) swapBytes(buf.data(), m);
+            if (std::fwrite(buf.data(), 4, (size_t)m, _data) != (size_t)m)
+                throw std::runtime_error("SEP: short write to " + _dataPath);
+        }
         std::fflush(_data);
     }
     template <class V>
