@@ -56,6 +56,10 @@ EXPORTED = [
     "aio_tomoOffsetShotsFwdFsGpu", "aio_tomoOffsetShotsAdjFsGpu", "aio_wemvaOffsetShotsFwdGpu",
     "aio_wemvaOffsetShotsAdjGpu", "aio_born_forward_wavefield", "aio_born_adjoint_wavefield",
     "aio_BornShotsFwdGpuWavefield", "aio_BornShotsAdjGpuWavefield",
+    "aio_born_ext_forward_wavefield", "aio_born_ext_adjoint_wavefield",
+    "aio_BornTimeShotsFwdGpuWavefield", "aio_BornOffsetShotsFwdGpuWavefield", "aio_BornTimeShotsFwdFsGpuWavefield",
+    "aio_BornOffsetShotsFwdFsGpuWavefield", "aio_BornTimeShotsAdjGpuWavefield", "aio_BornOffsetShotsAdjGpuWavefield",
+    "aio_BornTimeShotsAdjFsGpuWavefield", "aio_BornOffsetShotsAdjFsGpuWavefield",
 ]
 
 

@@ -195,6 +195,28 @@ class Context:
                                                    A.fptr(rec)))
         return out, src, rec
 
+    def born_ext_forward_wavefield(self, model, shot: Shot):
+        """Extended Born forward of one shot: (data, source wavefield, scattered wavefield), the
+        wavefields (nts, nx, nz) with a zero FAT ring (non-sloth time-lag scaling)."""
+        m = self._model(model, self.nExt)
+        arr = self._shots([shot], data_out=True)
+        src = np.zeros((self.nts, self.nx, self.nz), np.float32)
+        sec = np.zeros_like(src)
+        A.check(A.lib().aio_born_ext_forward_wavefield(self._h, A.fptr(m), arr, A.AIO_MEM_HOST, A.fptr(src),
+                                                       A.fptr(sec)))
+        return shot.data, src, sec
+
+    def born_ext_adjoint_wavefield(self, shot: Shot):
+        """Extended Born adjoint of one shot: (image (nExt, nx, nz), source wavefield, receiver
+        wavefield scaled by 2/v^3 v^2 dtw^2 for time lags, by v^2 dtw^2 for offsets)."""
+        out = np.zeros((self.nExt, self.nx, self.nz), np.float32)
+        arr = self._shots([shot], data_out=False)
+        src = np.zeros((self.nts, self.nx, self.nz), np.float32)
+        rec = np.zeros_like(src)
+        A.check(A.lib().aio_born_ext_adjoint_wavefield(self._h, A.fptr(out), 0, arr, A.AIO_MEM_HOST, A.fptr(src),
+                                                       A.fptr(rec)))
+        return out, src, rec
+
     def born_ext_forward(self, model, shots: List[Shot]) -> List[np.ndarray]:
         m = self._model(model, self.nExt)
         arr = self._shots(shots, data_out=True)

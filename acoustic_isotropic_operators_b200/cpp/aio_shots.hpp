@@ -848,16 +848,43 @@ class BornExtShotsGpu : public Operator<SEP::float3DReg, SEP::float3DReg>, publi
         });
         sumImages(parts, model->getVals(), n, add);
     }
-    void forwardWavefield(const bool, const std::shared_ptr<SEP::float3DReg>, std::shared_ptr<SEP::float3DReg>) {
-        aio_ops::fail("BornExtShotsGpu::forwardWavefield: saved wavefields are not available in this build");
+    // forward / adjoint of every shot, plus the coarse wavefields of shot wavefieldShotNumber when
+    // saveWavefield = 1 (F/src/BornExtShotsGpu.cpp:143-340, F/src/BornExtGpu.cpp:37-110): source and
+    // scattered wavefields (forward), source and receiver wavefields (adjoint), computed like the
+    // reference's *Wavefield drivers (non-sloth time-lag scaling); with saveWavefield = 0 the
+    // containers stay zero-filled.
+    void forwardWavefield(const bool add, const std::shared_ptr<SEP::float3DReg> model,
+                          std::shared_ptr<SEP::float3DReg> data) {
+        forward(add, model, data);
+        _srcWavefield = coarseWavefield();
+        _secWavefield = coarseWavefield();
+        if (_saveWavefield != 1 || _wavefieldShotNumber < 0 || _wavefieldShotNumber >= _nShot) return;
+        aio_ops::PreparedShot ps;
+        aio_shot sh = prepareOne(_wavefieldShotNumber, nullptr, ps);
+        std::vector<float> scratch((size_t)sh.nReceiversReg * fd()._nts);
+        sh.data = scratch.data();
+        aio_ops::ck(aio_born_ext_forward_wavefield(context(0), model->getVals(), &sh, AIO_MEM_HOST,
+                                                   _srcWavefield->getVals(), _secWavefield->getVals()));
     }
-    void adjointWavefield(const bool, std::shared_ptr<SEP::float3DReg>, const std::shared_ptr<SEP::float3DReg>) {
-        aio_ops::fail("BornExtShotsGpu::adjointWavefield: saved wavefields are not available in this build");
+    void adjointWavefield(const bool add, std::shared_ptr<SEP::float3DReg> model,
+                          const std::shared_ptr<SEP::float3DReg> data) {
+        adjoint(add, model, data);
+        _srcWavefield = coarseWavefield();
+        _secWavefield = coarseWavefield();
+        if (_saveWavefield != 1 || _wavefieldShotNumber < 0 || _wavefieldShotNumber >= _nShot) return;
+        aio_ops::PreparedShot ps;
+        aio_shot sh = prepareOne(_wavefieldShotNumber, &data, ps);
+        std::vector<float> image((size_t)model->size());
+        aio_ops::ck(aio_born_ext_adjoint_wavefield(context(0), image.data(), 0, &sh, AIO_MEM_HOST,
+                                                   _srcWavefield->getVals(), _secWavefield->getVals()));
     }
-    std::shared_ptr<SEP::float3DReg> getSrcWavefield() { return nullptr; }
-    std::shared_ptr<SEP::float3DReg> getSecWavefield() { return nullptr; }
+    std::shared_ptr<SEP::float3DReg> getSrcWavefield() { return _srcWavefield; }
+    std::shared_ptr<SEP::float3DReg> getSecWavefield() { return _secWavefield; }
     std::shared_ptr<SEP::float2DReg> getVel() { return _vel; }
     void setVel(std::shared_ptr<SEP::float2DReg> vel) { setVelocity(vel); }
+
+  private:
+    std::shared_ptr<SEP::float3DReg> _srcWavefield, _secWavefield;
 };
 
 // Extended tomo: velocity perturbation [nx][nz] -> data, background extended reflectivity

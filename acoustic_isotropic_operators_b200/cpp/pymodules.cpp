@@ -200,6 +200,8 @@ PYBIND11_MODULE(pyAcoustic_iso_float_born_ext, m) {
         .def("adjointWavefield", &BornExtShotsGpu::adjointWavefield, "Adjoint wavefield")
         .def("setVel", &BornExtShotsGpu::setVel, "Function to set background velocity")
         .def("getVel", &BornExtShotsGpu::getVel, "Function to get background velocity")
+        .def("getSrcWfld", &BornExtShotsGpu::getSrcWavefield, "Function to get src wfld")
+        .def("getSecWfld", &BornExtShotsGpu::getSecWavefield, "Function to get scattered / receiver wfld")
         .def("dotTest", &BornExtShotsGpu::dotTest, "Dot-Product Test", py::arg("verbose") = false,
              py::arg("maxError") = 1e-5f);
 }

@@ -2043,6 +2043,68 @@ struct Context {
         sync();
     }
 
+    // Extended Born forward of one shot with its coarse source and scattered wavefields
+    // (BornTimeShotsFwdGpuWavefield, F/src/BornExtShotsGpuFunctions.cu:420-580; offsets :726-884;
+    // free surface :1038-1205, :1356-1524), per-fine-step stepper. Like those drivers, the
+    // time-lag model scaling is the non-sloth one.
+    void born_ext_forward_wavefield(const float* model, const aio_shot* shot, int mem, float* srcW, float* secW) {
+        begin_call();
+        require(srcW && secW, "wavefield output is NULL");
+        float* dm = stage_model(model, g.nExt, mem, this->model);
+        scale_shared(dm, g.nExt, offsets() ? 3 : 1);
+        Needs n;
+        n.nWavefields = 2;
+        n.ss = true;
+        require(wave_size(n, 1, shot) >= 1, "device memory budget cannot hold the wavefields of one shot");
+        setup_wave(n, 1, shot, mem, false, false);
+        source_wavefield(1, wf1);
+        const float* W = wf1.as<float>();
+        fwd_dense_pass(
+            1,
+            [&](int t, long long slot) {
+                if (offsets()) img_offset_fwd(1, slot, dm, W, t);
+                else img_time_fwd(1, slot, dm, W, t);
+            },
+            true, true, ACC_FULL, &wf2, [](int, long long) {});
+        download_data(1, shot, mem);
+        wavefield_out(srcW, wf1, mem);
+        wavefield_out(secW, wf2, mem);
+        sync();
+    }
+    // Extended Born adjoint of one shot with its coarse source wavefield and receiver wavefield
+    // (BornTimeShotsAdjGpuWavefield, F/src/BornExtShotsGpuFunctions.cu:1680-1847: the receiver
+    // samples scaled by 2/v^3 v^2 dtw^2; offsets :1991-2151: by v^2 dtw^2 only; free surface
+    // :2306-2476, :2623-2783), per-fine-step stepper, non-sloth time-lag scaling.
+    void born_ext_adjoint_wavefield(float* modelOut, int add, const aio_shot* shot, int mem, float* srcW,
+                                    float* recW) {
+        begin_call();
+        require(recW != nullptr, "wavefield output is NULL");
+        Needs n;
+        n.nWavefields = 2;
+        n.nImg = g.nExt;
+        require(wave_size(n, 1, shot) >= 1, "device memory budget cannot hold the wavefields of one shot");
+        float* out = stage_out(modelOut, g.nExt, add, mem);
+        setup_wave(n, 1, shot, mem, true, false);
+        source_wavefield(1, wf1);
+        zero_images(1, g.nExt);
+        AIO_CK(cudaMemsetAsync(wf2.p, 0, (size_t)g.nts * g.isz * 4, st));
+        const float* W = wf1.as<float>();
+        std::vector<const float*> din(dataPtr.begin(), dataPtr.end());
+        adj_sparse_pass(1, din, nullptr, ACC_RING, nullptr, [&](int t, long long slot) {
+            k_record_scale<<<ew_grid(1, g.isz), 256, 0, st>>>(wf2.as<float>() + (long long)t * g.isz, ring_ptr(slot),
+                                                               offsets() ? nullptr : rs.as<float>(), v2.as<float>(),
+                                                               g.isz);
+            kcheck();
+            if (offsets()) img_offset_adj_block(1, slot, W, t, false, true);
+            else img_time_adj(1, slot, W, t, +1);
+        });
+        reduce_images(1, g.nExt, offsets() ? 3 : 1, out, true);
+        write_model(modelOut, g.nExt, add, mem, out);
+        if (srcW) wavefield_out(srcW, wf1, mem);
+        wavefield_out(recW, wf2, mem);
+        sync();
+    }
+
     // Extended (time-lag) Born adjoint (F/src/BornExtShotsGpuFunctions.cu:1525-1675).
     void born_ext_adjoint(float* modelOut, int add, int nShots, const aio_shot* shots, int mem) {
         begin_call();
@@ -2472,6 +2534,20 @@ AIO_API int aio_born_adjoint_wavefield(aio_context* ctx, float* modelOut, int ad
         ctx->c.born_adjoint_wavefield(modelOut, add, shot, memSpace, srcWavefield, recWavefield);
     });
 }
+AIO_API int aio_born_ext_forward_wavefield(aio_context* ctx, const float* model, const aio_shot* shot, int memSpace,
+                                           float* srcWavefield, float* secWavefield) {
+    return guard([&] {
+        require(shot != nullptr, "shot is NULL");
+        ctx->c.born_ext_forward_wavefield(model, shot, memSpace, srcWavefield, secWavefield);
+    });
+}
+AIO_API int aio_born_ext_adjoint_wavefield(aio_context* ctx, float* modelOut, int add, const aio_shot* shot,
+                                           int memSpace, float* srcWavefield, float* recWavefield) {
+    return guard([&] {
+        require(shot != nullptr, "shot is NULL");
+        ctx->c.born_ext_adjoint_wavefield(modelOut, add, shot, memSpace, srcWavefield, recWavefield);
+    });
+}
 AIO_API int aio_born_adjoint_shots(aio_context* ctx, float* const* images, int nShots, const aio_shot* shots,
                                    int memSpace) {
     return guard([&] { ctx->c.born_adjoint_shots(images, nShots, shots, memSpace); });
@@ -2843,6 +2919,44 @@ AIO_API int aio_BornOffsetShotsAdjFsGpu(float* model, float* dataRegDts, float* 
     (void)srcWavefield; (void)recWavefield; (void)iGpuId;
     return guard([&] { seam_born_offset(model, dataRegDts, sourcesSignals, sp, ns, rp, nr, iGpu, true, true); });
 }
+// Extended Born with saved wavefields (the reference's *Wavefield drivers): offsets / free surface as named.
+static void seam_born_ext_wfld(float* model, float* dataRegDts, float* sig, int* sp, int ns, int* rp, int nr, int iGpu,
+                               bool adjoint, bool offset, bool fs, float* srcW, float* secW) {
+    Context& c = seam_ctx(AIO_BORN_EXT, iGpu);
+    const int ext = c.P.extension, fs0 = c.P.freeSurface;
+    c.P.extension = offset ? AIO_EXT_OFFSET : AIO_EXT_TIME;
+    c.P.freeSurface = fs ? 1 : 0;
+    aio_shot s = one_shot(sig, sp, ns, rp, nr, dataRegDts);
+    try {
+        if (adjoint) c.born_ext_adjoint_wavefield(model, 0, &s, AIO_MEM_HOST, srcW, secW);
+        else c.born_ext_forward_wavefield(model, &s, AIO_MEM_HOST, srcW, secW);
+    } catch (...) {
+        c.P.extension = ext;
+        c.P.freeSurface = fs0;
+        throw;
+    }
+    c.P.extension = ext;
+    c.P.freeSurface = fs0;
+}
+#define AIO_BORN_EXT_WFLD(NAME, ADJ, OFF, FS)                                                                   \
+    AIO_API int NAME(float* model, float* dataRegDts, float* sourcesSignals, int* sp, int ns, int* rp, int nr,  \
+                     float* srcWavefield, float* secWavefield, int iGpu, int iGpuId) {                          \
+        (void)iGpuId;                                                                                           \
+        return guard([&] {                                                                                      \
+            seam_born_ext_wfld(model, dataRegDts, sourcesSignals, sp, ns, rp, nr, iGpu, ADJ, OFF, FS,           \
+                               srcWavefield, secWavefield);                                                    \
+        });                                                                                                     \
+    }
+AIO_BORN_EXT_WFLD(aio_BornTimeShotsFwdGpuWavefield, false, false, false)
+AIO_BORN_EXT_WFLD(aio_BornOffsetShotsFwdGpuWavefield, false, true, false)
+AIO_BORN_EXT_WFLD(aio_BornTimeShotsFwdFsGpuWavefield, false, false, true)
+AIO_BORN_EXT_WFLD(aio_BornOffsetShotsFwdFsGpuWavefield, false, true, true)
+AIO_BORN_EXT_WFLD(aio_BornTimeShotsAdjGpuWavefield, true, false, false)
+AIO_BORN_EXT_WFLD(aio_BornOffsetShotsAdjGpuWavefield, true, true, false)
+AIO_BORN_EXT_WFLD(aio_BornTimeShotsAdjFsGpuWavefield, true, false, true)
+AIO_BORN_EXT_WFLD(aio_BornOffsetShotsAdjFsGpuWavefield, true, true, true)
+#undef AIO_BORN_EXT_WFLD
+
 static void seam_tomo_offset(float* model, float* dataRegDts, float* ext, float* sig, int* sp, int ns, int* rp, int nr,
                              int iGpu, int saveWavefield, bool adjoint, bool fs) {
     require(saveWavefield == 0, "saveWavefield=1 is not available for tomo in this build");

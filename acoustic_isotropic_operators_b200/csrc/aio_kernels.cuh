@@ -262,9 +262,11 @@ __global__ void k_img_time_adj(Acc* m, long long mSt, float* r, long long rSt, c
     }
 }
 
-// recordScaleWavefield (F/src/kernelsGpu.cu:145-153): W += r * rs * v2 (one coarse slice).
+// recordScaleWavefield (F/src/kernelsGpu.cu:145-153): W += r * rs * v2 (one coarse slice); with
+// rs null, scaleSecondarySourceFd then recordWavefield (:269-276, :138-143): W += r * v2.
 __global__ void k_record_scale(float* W, const float* r, const float* rs, const float* v2, long long isz) {
-    AIO_GRID_STRIDE(i, isz) W[i] += r[i] * rs[i] * v2[i];
+    if (rs) AIO_GRID_STRIDE(i, isz) W[i] += r[i] * rs[i] * v2[i];
+    else AIO_GRID_STRIDE(i, isz) W[i] += r[i] * v2[i];
 }
 
 // ---- subsurface (horizontal) offsets, interior-slice layout (x*ip + z), x in [0, nxi) ----

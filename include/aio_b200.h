@@ -141,6 +141,15 @@ int aio_born_forward_wavefield(aio_context* ctx, const float* model, const aio_s
                                float* srcWavefield, float* secWavefield);
 int aio_born_adjoint_wavefield(aio_context* ctx, float* model, int add, const aio_shot* shot, int memSpace,
                                float* srcWavefield, float* recWavefield);
+/* Extended Born of one shot with saved wavefields (the reference's *Wavefield drivers of
+ * F/src/BornExtShotsGpuFunctions.cu, :420-580 forward, :1680-1847 adjoint): forward returns the
+ * source and scattered wavefields; adjoint the receiver wavefield (time lags: scaled by
+ * 2/v^3 v^2 dtw^2; offsets: by v^2 dtw^2) and, when srcWavefield is not NULL, the source
+ * wavefield. Per-fine-step stepper; non-sloth time-lag scaling. */
+int aio_born_ext_forward_wavefield(aio_context* ctx, const float* model, const aio_shot* shot, int memSpace,
+                                   float* srcWavefield, float* secWavefield);
+int aio_born_ext_adjoint_wavefield(aio_context* ctx, float* model, int add, const aio_shot* shot, int memSpace,
+                                   float* srcWavefield, float* recWavefield);
 /* Extended (time-lag) Born: model nExt*nz*nx. */
 int aio_born_ext_forward(aio_context* ctx, const float* model, int nShots, const aio_shot* shots, int memSpace);
 int aio_born_ext_adjoint(aio_context* ctx, float* model, int add, int nShots, const aio_shot* shots, int memSpace);
@@ -303,6 +312,37 @@ int aio_BornOffsetShotsFwdFsGpu(float* model, float* dataRegDts, float* sourcesS
 int aio_BornOffsetShotsAdjFsGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
                                 int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
                                 float* recWavefield, int iGpu, int iGpuId);
+/* Extended Born with saved wavefields, [nts][nx][nz] with a zero FAT ring (per-fine-step stepper; the
+ * time-lag scaling is the non-sloth one, as in the reference's drivers). Forward: coarse source and
+ * scattered wavefields; adjoint: coarse source wavefield and receiver wavefield (time lags: scaled by
+ * 2/v^3 v^2 dtw^2; offsets: by v^2 dtw^2). F/include/BornExtShotsGpuFunctions.h:19, 23, 28, 32, 41, 45,
+ * 50, 54 in the order below. */
+int aio_BornTimeShotsFwdGpuWavefield(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                                     int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
+                                     float* srcWavefield, float* scatWavefield, int iGpu, int iGpuId);
+int aio_BornOffsetShotsFwdGpuWavefield(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                                       int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
+                                       float* srcWavefield, float* scatWavefield, int iGpu, int iGpuId);
+int aio_BornTimeShotsFwdFsGpuWavefield(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                                       int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
+                                       float* srcWavefield, float* scatWavefield, int iGpu, int iGpuId);
+int aio_BornOffsetShotsFwdFsGpuWavefield(float* model, float* dataRegDts, float* sourcesSignals,
+                                         int* sourcesPositionReg, int nSourcesReg, int* receiversPositionReg,
+                                         int nReceiversReg, float* srcWavefield, float* scatWavefield, int iGpu,
+                                         int iGpuId);
+int aio_BornTimeShotsAdjGpuWavefield(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                                     int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
+                                     float* srcWavefield, float* recWavefield, int iGpu, int iGpuId);
+int aio_BornOffsetShotsAdjGpuWavefield(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                                       int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
+                                       float* srcWavefield, float* recWavefield, int iGpu, int iGpuId);
+int aio_BornTimeShotsAdjFsGpuWavefield(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
+                                       int nSourcesReg, int* receiversPositionReg, int nReceiversReg,
+                                       float* srcWavefield, float* recWavefield, int iGpu, int iGpuId);
+int aio_BornOffsetShotsAdjFsGpuWavefield(float* model, float* dataRegDts, float* sourcesSignals,
+                                         int* sourcesPositionReg, int nSourcesReg, int* receiversPositionReg,
+                                         int nReceiversReg, float* srcWavefield, float* recWavefield, int iGpu,
+                                         int iGpuId);
 /* F/include/tomoExtShotsGpuFunctions.h:17 */
 int aio_tomoOffsetShotsFwdGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
                               int* sourcesPositionReg, int nSourcesReg, int* receiversPositionReg, int nReceiversReg,

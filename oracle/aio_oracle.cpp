@@ -644,13 +644,19 @@ static void born_adj(const Grid<T>& g, T* model, const T* sig, const int* sp, in
 }
 
 // Extended (time-lag) Born forward, F/src/BornExtShotsGpuFunctions.cu:269-419.
+// Wsrc / Wsec (optional): the coarse source and scattered wavefields (BornTimeShotsFwdGpuWavefield,
+// :420-580, and BornOffsetShotsFwdGpuWavefield, :726-884: interpWavefield of the scattered pass;
+// those drivers take no sloth flag).
 template <class T>
 static void bornext_fwd(const Grid<T>& g, const T* model, const T* sig, const int* sp, int ns, const int* rp,
-                        int nr, T* data, int sloth) {
+                        int nr, T* data, int sloth, T* Wsrc = nullptr, T* Wsec = nullptr) {
     Work<T> w(g.N());
     const size_t N = g.N();
-    std::vector<T> W((size_t)g.nts * N);
-    source_wavefield(g, w, sig, sp, ns, W.data());
+    std::vector<T> Wloc;
+    T* Wp = Wsrc;
+    if (!Wp) { Wloc.resize((size_t)g.nts * N); Wp = Wloc.data(); }
+    source_wavefield(g, w, sig, sp, ns, Wp);
+    if (Wsec) std::fill(Wsec, Wsec + (size_t)g.nts * N, (T)0);
     std::vector<T> dm(model, model + (size_t)g.nExt * N);
     // subsurface offsets: BornOffsetShotsFwdGpu, F/src/BornExtShotsGpuFunctions.cu:582-724
     if (g.offset) scale_refl_lin_ext(g, dm.data());
@@ -660,26 +666,43 @@ static void bornext_fwd(const Grid<T>& g, const T* model, const T* sig, const in
         g, w,
         [&](int t, T* ss) {
             if (g.offset) {
-                imaging_offset_fwd(g, dm.data(), ss, W.data(), t);
+                imaging_offset_fwd(g, dm.data(), ss, Wp, t);
                 scale_ss_fd(g, ss);
                 return;
             }
             int e0, e1;
             lag_bounds_src(g, t, e0, e1);
-            imaging_time_fwd(g, dm.data(), ss, W.data(), t, e0, e1);
+            imaging_time_fwd(g, dm.data(), ss, Wp, t, e0, e1);
         },
-        true, [&](const T* p, int its, int it2) { record_data(g, p, data, its, it2, rp, nr); }, false,
-        [](int, T*) {});
+        true,
+        [&](const T* p, int its, int it2) {
+            if (Wsec) interp_wavefield(g, Wsec, p, its, it2);
+            record_data(g, p, data, its, it2, rp, nr);
+        },
+        false, [](int, T*) {});
+}
+
+// recordWavefield (F/src/kernelsGpu.cu:138-143): W[its] += r.
+template <class T>
+static void record_wavefield(const Grid<T>& g, T* W, const T* r, int its) {
+    T* w = W + (size_t)its * g.N();
+    for_interior(g.nz, g.nx, [&](size_t i) { w[i] += r[i]; });
 }
 
 // Extended (time-lag) Born adjoint, F/src/BornExtShotsGpuFunctions.cu:1525-1675.
+// Wsrc / Wrec (optional): the coarse source wavefield and the receiver wavefield
+// (BornTimeShotsAdjGpuWavefield, :1680-1847: recordScaleWavefield before each imaging step;
+// BornOffsetShotsAdjGpuWavefield, :1991-2151: recordWavefield of the v2-scaled sample).
 template <class T>
 static void bornext_adj(const Grid<T>& g, T* model, const T* sig, const int* sp, int ns, const int* rp, int nr,
-                        const T* data, int sloth) {
+                        const T* data, int sloth, T* Wsrc = nullptr, T* Wrec = nullptr) {
     Work<T> w(g.N());
     const size_t N = g.N();
-    std::vector<T> W((size_t)g.nts * N);
-    source_wavefield(g, w, sig, sp, ns, W.data());
+    std::vector<T> Wloc;
+    T* Wp = Wsrc;
+    if (!Wp) { Wloc.resize((size_t)g.nts * N); Wp = Wloc.data(); }
+    source_wavefield(g, w, sig, sp, ns, Wp);
+    if (Wrec) std::fill(Wrec, Wrec + (size_t)g.nts * N, (T)0);
     std::fill(model, model + (size_t)g.nExt * N, (T)0);
     std::vector<T> L(N, 0), R(N, 0);
     T *pL = L.data(), *pR = R.data();
@@ -696,22 +719,26 @@ static void bornext_adj(const Grid<T>& g, T* model, const T* sig, const int* sp,
         }
         if (g.offset) {  // BornOffsetShotsAdjGpu, F/src/BornExtShotsGpuFunctions.cu:1848-1990
             scale_ss_fd(g, pR);
-            imaging_offset_adj(g, model, pR, W.data(), its + 1);
+            if (Wrec) record_wavefield(g, Wrec, pR, its + 1);
+            imaging_offset_adj(g, model, pR, Wp, its + 1);
         } else {
+            if (Wrec) record_scale_wavefield(g, Wrec, pR, its + 1);
             lag_bounds_src(g, its + 1, e0, e1);
-            imaging_time_adj(g, model, pR, W.data(), its + 1, e0, e1);
+            imaging_time_adj(g, model, pR, Wp, its + 1, e0, e1);
         }
         std::swap(pR, pL);
         std::fill(pL, pL + N, (T)0);
     }
     if (g.offset) {
         scale_ss_fd(g, pR);
-        imaging_offset_adj(g, model, pR, W.data(), 0);
+        if (Wrec) record_wavefield(g, Wrec, pR, 0);
+        imaging_offset_adj(g, model, pR, Wp, 0);
         scale_refl_lin_ext(g, model);
         return;
     }
+    if (Wrec) record_scale_wavefield(g, Wrec, pR, 0);
     lag_bounds_src(g, 0, e0, e1);
-    imaging_time_adj(g, model, pR, W.data(), 0, e0, e1);
+    imaging_time_adj(g, model, pR, Wp, 0, e0, e1);
     scale_refl_ext(g, model, sloth);
 }
 
@@ -1023,6 +1050,18 @@ static Grid<T> grid_from(const OrcParams* p, const T* vel) {
                                           int sloth) {                                                            \
         Grid<T> g = grid_from<T>(p, vel);                                                                         \
         bornext_adj<T>(g, model, sig, sp, ns, rp, nr, data, sloth);                                               \
+    }                                                                                                             \
+    ORC_EXPORT void orc_bornext_fwd_wfld_##SUF(const OrcParams* p, const T* vel, const T* model, const T* sig,    \
+                                               const int* sp, int ns, const int* rp, int nr, T* data, T* W,       \
+                                               T* S) {                                                            \
+        Grid<T> g = grid_from<T>(p, vel);                                                                         \
+        bornext_fwd<T>(g, model, sig, sp, ns, rp, nr, data, 0, W, S);                                             \
+    }                                                                                                             \
+    ORC_EXPORT void orc_bornext_adj_wfld_##SUF(const OrcParams* p, const T* vel, T* model, const T* sig,          \
+                                               const int* sp, int ns, const int* rp, int nr, const T* data, T* W, \
+                                               T* R) {                                                            \
+        Grid<T> g = grid_from<T>(p, vel);                                                                         \
+        bornext_adj<T>(g, model, sig, sp, ns, rp, nr, data, 0, W, R);                                             \
     }                                                                                                             \
     ORC_EXPORT void orc_tomo_fwd_##SUF(const OrcParams* p, const T* vel, const T* model, const T* ext,            \
                                        const T* sig, const int* sp, int ns, const int* rp, int nr, T* data,       \

@@ -144,17 +144,35 @@ def born_adj(s, vel, data, sig_dtw, src_pos, rec_pos, dtype=np.float64, wavefiel
     return (m, W) if wavefield else m
 
 
-def bornext_fwd(s, vel, model_ext, sig_dtw, src_pos, rec_pos, dtype=np.float64, sloth=0):
+def bornext_fwd(s, vel, model_ext, sig_dtw, src_pos, rec_pos, dtype=np.float64, sloth=0, secondary=False):
+    """Extended Born forward data; secondary=True (non-sloth scaling, as the reference's wavefield
+    drivers) returns (data, coarse source wavefield, coarse scattered wavefield)."""
     vel = _arr(vel, dtype); m = _arr(model_ext, dtype); sig = _arr(sig_dtw, dtype)
     d = np.zeros((len(rec_pos), s.nts), dtype)
+    if secondary:
+        W = np.zeros((s.nts, s.nx, s.nz), dtype)
+        S = np.zeros_like(W)
+        getattr(lib(), "orc_bornext_fwd_wfld_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(sig),
+                                                              _ip(src_pos), len(src_pos), _ip(rec_pos),
+                                                              len(rec_pos), _p(d), _p(W), _p(S))
+        return d, W, S
     getattr(lib(), "orc_bornext_fwd_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(sig), _ip(src_pos),
                                                      len(src_pos), _ip(rec_pos), len(rec_pos), _p(d), sloth)
     return d
 
 
-def bornext_adj(s, vel, data, sig_dtw, src_pos, rec_pos, dtype=np.float64, sloth=0):
+def bornext_adj(s, vel, data, sig_dtw, src_pos, rec_pos, dtype=np.float64, sloth=0, secondary=False):
+    """Extended Born adjoint image; secondary=True (non-sloth scaling) returns (image, coarse source
+    wavefield, receiver wavefield: scaled by 2/v^3 v^2 dtw^2 for time lags, by v^2 dtw^2 for offsets)."""
     vel = _arr(vel, dtype); d = _arr(data, dtype); sig = _arr(sig_dtw, dtype)
     m = np.zeros((s.nExt, s.nx, s.nz), dtype)
+    if secondary:
+        W = np.zeros((s.nts, s.nx, s.nz), dtype)
+        R = np.zeros_like(W)
+        getattr(lib(), "orc_bornext_adj_wfld_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(sig),
+                                                              _ip(src_pos), len(src_pos), _ip(rec_pos),
+                                                              len(rec_pos), _p(d), _p(W), _p(R))
+        return m, W, R
     getattr(lib(), "orc_bornext_adj_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(sig), _ip(src_pos),
                                                      len(src_pos), _ip(rec_pos), len(rec_pos), _p(d), sloth)
     return m

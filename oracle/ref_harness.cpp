@@ -121,6 +121,22 @@ REF_EXPORT int ref_bornext_fwd_fs(R* model, R* data, R* sig, int* sp, int ns, in
 REF_EXPORT int ref_bornext_adj_fs(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
     GUARD(BornTimeShotsAdjFsGpu(model, data, sig, sp, ns, rp, nr, nullptr, nullptr, 0, dev))
 }
+// wavefield drivers (F/include/BornExtShotsGpuFunctions.h:19,23,28,32 forward; :41,45,50,54 adjoint):
+// coarse [nts][nx][nz] wavefields out; off / fs select the offset and free-surface forms
+REF_EXPORT int ref_bornext_fwd_wfld(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, R* srcW, R* secW,
+                                    int off, int fs, int dev) {
+    if (off && fs) { GUARD(BornOffsetShotsFwdFsGpuWavefield(model, data, sig, sp, ns, rp, nr, srcW, secW, 0, dev)) }
+    if (off) { GUARD(BornOffsetShotsFwdGpuWavefield(model, data, sig, sp, ns, rp, nr, srcW, secW, 0, dev)) }
+    if (fs) { GUARD(BornTimeShotsFwdFsGpuWavefield(model, data, sig, sp, ns, rp, nr, srcW, secW, 0, dev)) }
+    GUARD(BornTimeShotsFwdGpuWavefield(model, data, sig, sp, ns, rp, nr, srcW, secW, 0, dev))
+}
+REF_EXPORT int ref_bornext_adj_wfld(R* model, R* data, R* sig, int* sp, int ns, int* rp, int nr, R* srcW, R* recW,
+                                    int off, int fs, int dev) {
+    if (off && fs) { GUARD(BornOffsetShotsAdjFsGpuWavefield(model, data, sig, sp, ns, rp, nr, srcW, recW, 0, dev)) }
+    if (off) { GUARD(BornOffsetShotsAdjGpuWavefield(model, data, sig, sp, ns, rp, nr, srcW, recW, 0, dev)) }
+    if (fs) { GUARD(BornTimeShotsAdjFsGpuWavefield(model, data, sig, sp, ns, rp, nr, srcW, recW, 0, dev)) }
+    GUARD(BornTimeShotsAdjGpuWavefield(model, data, sig, sp, ns, rp, nr, srcW, recW, 0, dev))
+}
 #elif defined(REF_FAMILY_TOMO)
 // F/include/tomoExtShotsGpuFunctions.h:6-33
 REF_EXPORT int ref_init(R dz, R dx, int nz, int nx, int nts, R dts, int sub, int minPad, R alphaCos, int nExt,

@@ -158,6 +158,33 @@ def bornext_adj(s, vel, data, sig, sp, rp, sloth=0, dtype=np.float32):
     return m
 
 
+def bornext_fwd_wavefields(s, vel, model, sig, sp, rp, dtype=np.float32):
+    """(data, source wavefield, scattered wavefield) from the extended Born forward wavefield drivers
+    (time lags or offsets, with or without the free surface, by the scheme)."""
+    sp, rp = _i(sp), _i(rp)
+    m, g = _a(model, dtype), _a(sig, dtype)
+    d = np.zeros((len(rp), s.nts), dtype)
+    W = np.zeros((s.nts, s.nx, s.nz), dtype)
+    S = np.zeros_like(W)
+    _run("bornext", s, vel, dtype,
+         lambda L: L.ref_bornext_fwd_wfld(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), _p(W), _p(S),
+                                          int(_off(s)), int(_fs(s)), 0), nExt=s.nExt)
+    return d, W, S
+
+
+def bornext_adj_wavefields(s, vel, data, sig, sp, rp, dtype=np.float32):
+    """(image, source wavefield, receiver wavefield) from the extended Born adjoint wavefield drivers."""
+    sp, rp = _i(sp), _i(rp)
+    d, g = _a(data, dtype), _a(sig, dtype)
+    m = np.zeros((s.nExt, s.nx, s.nz), dtype)
+    W = np.zeros((s.nts, s.nx, s.nz), dtype)
+    R = np.zeros_like(W)
+    _run("bornext", s, vel, dtype,
+         lambda L: L.ref_bornext_adj_wfld(_p(m), _p(d), _p(g), _p(sp), len(sp), _p(rp), len(rp), _p(W), _p(R),
+                                          int(_off(s)), int(_fs(s)), 0), nExt=s.nExt)
+    return m, W, R
+
+
 def tomo_fwd(s, vel, model, ext, sig, sp, rp, sloth=0, leg1=1, leg2=1, dtype=np.float32):
     sp, rp = _i(sp), _i(rp)
     m, e, g = _a(model, dtype), _a(ext, dtype), _a(sig, dtype)

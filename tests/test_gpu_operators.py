@@ -169,3 +169,31 @@ def test_born_saved_wavefields(api, setup):
     _, rW, rS = orc.born_fwd(st["scheme"], st["vel"], m, sig, spos, rpos, dtype=np.float32, secondary=True)
     assert src.shape == (NTS, NX, NZ)
     assert rel_l2(src, rW) < 1e-5 and rel_l2(sec, rS) < 1e-5
+
+
+def test_born_ext_saved_wavefields(api, setup):
+    """BornExtShotsGpu.forwardWavefield / adjointWavefield with saveWavefield = 1 keep the coarse
+    wavefields of shot wavefieldShotNumber (getSrcWfld / getSecWfld), equal to the oracle's."""
+    st = setup
+    par = api.params(nts=NTS, dts=DTS, sub=SUB, nz=NZ, nx=NX, zPadMinus=PAD, zPadPlus=PAD, xPadMinus=PAD,
+                     xPadPlus=PAD, dz=10.0, dx=10.0, fMax=20.0, blockSize=16, fat=5, nShot=2, iGpu=[0], nExt=5,
+                     extension="time", saveWavefield=1, wavefieldShotNumber=1)
+    rng = np.random.default_rng(6)
+    m = np.zeros((5, NX, NZ), np.float32)
+    m[:, 5:-5, 5:-5] = rng.standard_normal((5, NXI, NZI))
+    op = api.pyAcoustic_iso_float_born_ext.BornExtShotsGpu(st["v"], par, st["srcs"], [st["sig"]], [st["rec"]])
+    model = api.vector(m, [(NZ, 0.0, 10.0), (NX, 0.0, 10.0), (5, -2 * DTS, DTS)])
+    data = data_vec(api)
+    op.forwardWavefield(False, model, data)
+    spos, sig = oracle_source(st, st["srcs"][1], True)
+    rpos = np.array(st["rec"].getRegPosUnique(), np.int32)
+    _, rW, rS = orc.bornext_fwd(st["scheme"], st["vel"], m, sig, spos, rpos, dtype=np.float32, secondary=True)
+    assert rel_l2(op.getSrcWfld().getNdArray(), rW) < 1e-5 and rel_l2(op.getSecWfld().getNdArray(), rS) < 1e-5
+    d = (rng.standard_normal((2, 40, NTS)) * 1e-2).astype(np.float32)
+    op.adjointWavefield(False, model, data_vec(api, d))
+    dreg = np.zeros((len(rpos), NTS), np.float32)
+    index = {p: i for i, p in enumerate(rpos)}
+    for r in range(40):
+        dreg[index[(8 + r) * NZ + 8]] = d[1, r]
+    _, rW, rR = orc.bornext_adj(st["scheme"], st["vel"], dreg, sig, spos, rpos, dtype=np.float32, secondary=True)
+    assert rel_l2(op.getSrcWfld().getNdArray(), rW) < 1e-5 and rel_l2(op.getSecWfld().getNdArray(), rR) < 1e-5
