@@ -60,6 +60,7 @@ EXPORTED = [
     "aio_BornTimeShotsFwdGpuWavefield", "aio_BornOffsetShotsFwdGpuWavefield", "aio_BornTimeShotsFwdFsGpuWavefield",
     "aio_BornOffsetShotsFwdFsGpuWavefield", "aio_BornTimeShotsAdjGpuWavefield", "aio_BornOffsetShotsAdjGpuWavefield",
     "aio_BornTimeShotsAdjFsGpuWavefield", "aio_BornOffsetShotsAdjFsGpuWavefield",
+    "aio_dot_f64",
 ]
 
 
@@ -103,6 +104,8 @@ def lib():
         L.aio_context_wave_capacity.argtypes = [C.c_void_p, C.c_int]
         L.aio_context_stream.restype = C.c_void_p
         L.aio_context_stream.argtypes = [C.c_void_p]
+        L.aio_dot_f64.argtypes = [C.c_int, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p,
+                                  C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -124,3 +127,17 @@ def iptr(a):
         return None
     assert a.dtype == np.int32 and a.flags.c_contiguous
     return a.ctypes.data_as(C.c_void_p)
+
+
+def dot_f64(a, b, device: int = 0) -> float:
+    """sum(a * b) of two float32 host arrays of the same size, reduced in FP64 on the GPU
+    (aio_dot_f64): the inner product of the dot-product tests."""
+    a = np.ascontiguousarray(a, dtype=np.float32).reshape(-1)
+    b = np.ascontiguousarray(b, dtype=np.float32).reshape(-1)
+    assert a.size == b.size
+    out = C.c_double()
+    code = lib().aio_dot_f64(device, AIO_MEM_HOST, a.size, a.ctypes.data_as(C.c_void_p),
+                             b.ctypes.data_as(C.c_void_p), C.byref(out))
+    if code != AIO_OK:
+        raise AioError(code, "aio_dot_f64 failed (see stderr)")
+    return float(out.value)

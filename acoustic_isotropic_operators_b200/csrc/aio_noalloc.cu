@@ -1,10 +1,11 @@
 // Allocation-free nonlinear forward propagation of one shot.
 //
-// Some callers cannot let a library allocate device memory: code that records
-// work into a CUDA graph (cudaMalloc is illegal while a stream is being
-// captured), services that pre-plan every byte of device memory up front and
-// forbid allocations on the request path, and hosts whose own allocator owns
-// the device heap. This entry point serves them: the caller passes its inputs
+// Some callers cannot let a library allocate device memory: services that
+// pre-plan every byte of device memory up front and forbid allocations on the
+// request path (an allocation there can stall on the device or fail under
+// fragmentation), and hosts whose own allocator owns the device heap (a second
+// allocator beside it would take memory it has already counted as free). This
+// entry point serves them: the caller passes its inputs
 // and output as device pointers and a stream, and every temporary the stepper
 // needs (the two fine time levels, the interior copy of v^2 dtw^2, the damping
 // table, the shot descriptor and the sparse device lists) lives in one

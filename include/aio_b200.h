@@ -387,10 +387,9 @@ int aio_wemvaTimeShotsAdjGpu(float* model, float* wemvaExtImage, float* sourcesS
                              float* wemvaSrcWavefieldDt2, float* wemvaSecWavefield1, float* wemvaSecWavefield2,
                              int iGpu, int iGpuId, int saveWavefield);
 /* Allocation-free nonlinear forward of one shot. No counterpart in the reference.
- * For callers that cannot let a library allocate device memory: work recorded
- * into a CUDA graph (cudaMalloc is not allowed during stream capture), services
- * that plan all device memory ahead and forbid allocation on the request path,
- * and hosts whose own allocator owns the device heap. Inputs and output are
+ * For callers that cannot let a library allocate device memory: services that
+ * plan all device memory ahead and forbid allocation on the request path, and
+ * hosts whose own allocator owns the device heap. Inputs and output are
  * device pointers (vel2Dtw2: nz*nx; modelRegDtw: [nSourcesReg][ntw]; dataRegDts:
  * [nReceiversReg][nts], overwritten); positions are host arrays; work is queued
  * on `stream` (a cudaStream_t, NULL = default stream) and not waited for.
@@ -404,6 +403,11 @@ int aio_propShotsFwdGpu_noalloc(float dz, float dx, int nz, int nx, int nts, flo
                                 float alphaCos, const float* vel2Dtw2, const float* modelRegDtw,
                                 const int* sourcesPositionReg, int nSourcesReg, const int* receiversPositionReg,
                                 int nReceiversReg, float* dataRegDts, void* stream);
+/* FP64 inner product sum(a[i]*b[i]) of two FP32 arrays of n elements, reduced on GPU `device`
+ * (host arrays are copied there first when memSpace is AIO_MEM_HOST): the reduction of the
+ * dot-product test, F/include/operator.h:50-88 (which takes SEP vector dot products). Products are
+ * exact in FP64 and summed in a fixed order, so the result is reproducible. */
+int aio_dot_f64(int device, int memSpace, long long n, const float* a, const float* b, double* result);
 /* F/src/nonlinearShotsGpuFunctions.cu:18-84: validates a GPU id list (info printing dropped). */
 int aio_getGpuInfo(const int* gpuList, int nGpuList, int info, int deviceNumberInfo);
 

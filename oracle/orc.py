@@ -359,3 +359,25 @@ def device_sinc(zc, xc, nz, nx, oz, dz, ox, dx, r=4, beta=4.14, dipole=0, zshift
             point(i * nc + npt, np.float32(np.float32(zc[i]) + np.float32(zshift)),
                   np.float32(np.float32(xc[i]) + np.float32(xshift)), -1.0)
     return idx, w
+
+
+def prepare_source(wavelets, cidx, weights, n_reg, pos, nts, dts, sub, vel, second_derivative=True):
+    """The reference's source chain of the Born-family operators (seismicOperator2D::setSources,
+    F/include/seismicOperator2D.cpp:10-39) in FP32: device traces spread to their unique grid
+    points (deviceGpu::adjoint, F/src/deviceGpu.cpp:232-246), second time derivative
+    (F/src/secondTimeDerivative.cpp:14-39, skipped for the nonlinear operator), scaled by
+    dtw^2 v^2 at each point (scaleSeismicSource, F/include/seismicOperator2D.cpp:72-86), then
+    linearly interpolated to the fine time axis (F/src/interpTimeLinTbb.cpp:26-61).
+    wavelets: (nDevice, nts); cidx / weights: (nDevice, nCorner) unique-point index and weight of
+    every corner; pos: the n_reg unique grid indices. Returns (n_reg, ntw) float32."""
+    wavelets = np.asarray(wavelets, np.float32)
+    reg = np.zeros((n_reg, nts), np.float32)
+    for d in range(cidx.shape[0]):
+        for c in range(cidx.shape[1]):
+            reg[cidx[d, c]] += np.float32(weights[d, c]) * wavelets[d]
+    if second_derivative:
+        reg = second_deriv(nts, dts, reg, dtype=np.float32)
+    dtw = np.float32(np.float32(dts) / np.float32(sub))
+    v = np.asarray(vel, np.float32).reshape(-1)[np.asarray(pos)]
+    reg = reg * ((dtw * dtw) * v * v)[:, None].astype(np.float32)
+    return time_interp_fwd(nts, dts, sub, reg, dtype=np.float32)

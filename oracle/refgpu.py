@@ -94,6 +94,26 @@ def nl_adj(s, vel, data, sp, rp, dtype=np.float32):
     return m
 
 
+def nl_fwd_wavefield(s, vel, model_dtw, sp, rp, dtype=np.float32):
+    """(data, coarse wavefield [nts][nx][nz]) from propShotsFwdGpuWavefield."""
+    sp, rp = _i(sp), _i(rp)
+    m = _a(model_dtw, dtype)
+    d = np.zeros((len(rp), s.nts), dtype)
+    W = np.zeros((s.nts, s.nx, s.nz), dtype)
+    _run("nl", s, vel, dtype, lambda L: L.ref_nl_fwd(_p(m), _p(d), _p(sp), len(sp), _p(rp), len(rp), _p(W), 0))
+    return d, W
+
+
+def nl_adj_wavefield(s, vel, data, sp, rp, dtype=np.float32):
+    """(fine source traces, coarse adjoint wavefield) from propShotsAdjGpuWavefield."""
+    sp, rp = _i(sp), _i(rp)
+    d = _a(data, dtype)
+    m = np.zeros((len(sp), s.ntw), dtype)
+    W = np.zeros((s.nts, s.nx, s.nz), dtype)
+    _run("nl", s, vel, dtype, lambda L: L.ref_nl_adj(_p(m), _p(d), _p(sp), len(sp), _p(rp), len(rp), _p(W), 0))
+    return m, W
+
+
 def born_fwd(s, vel, model, sig, sp, rp, dtype=np.float32):
     sp, rp = _i(sp), _i(rp)
     m, g = _a(model, dtype), _a(sig, dtype)

@@ -1,8 +1,8 @@
 """Allocation-free nonlinear forward (aio_propShotsFwdGpu_noalloc).
 
 This entry point is for callers that cannot let a library allocate device
-memory — work captured into a CUDA graph, services that plan all device memory
-ahead, hosts whose allocator owns the device heap. It keeps every temporary in
+memory — services that plan all device memory ahead, hosts whose allocator
+owns the device heap. It keeps every temporary in
 one fixed file-scope device array, so this test checks it against the regular
 engine entry point on two calls in a row with different shots: anything left
 over in the shared scratch from the first call would corrupt the second.
