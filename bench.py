@@ -78,6 +78,8 @@ def parse():
     ap.add_argument("--plain", type=int, default=0,
                     help="instead of the batched step: time N shots one per call on the per-fine-step "
                          "stepper (the reference's schedule), FP32, and print that line")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="leave out the other configurations' sub-objects of the default line")
     return ap.parse_args()
 
 
@@ -167,8 +169,10 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     w = workload(args, 1)
-    from acoustic_isotropic_operators_b200 import _capi
-    sigs = prepare_signals(w, _capi.lib())
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc  # the CPU port's own source preparation: this arm loads no product code
+    sigs = [orc.prepare_source(np.repeat(w.wavelet[None, :], a.src_cidx.shape[0], axis=0), a.src_cidx, a.src_w,
+                               len(a.src_pos), a.src_pos, w.nts, w.dts, w.sub, w.vel) for a in w.shots]
     nts_sample = args.cpu_nts or 150
     vals = []
     for i in range(args.warmup + args.steps):
@@ -204,18 +208,35 @@ def config_dict(args, w):
             "parallelism": f"dp{args.gpus} (shots)", "l2": "inputs larger than L2 (5.4 GB wavefield per shot)"}
 
 
-def run_plain(args):
-    """One shot per call, per-fine-step stepper, FP32 wavefield: the plain GPU path."""
+def fields(w, lib):
+    """v^2 dtw^2 and 2/v^3 of a workload through the product's host code (aio_fd_precompute)."""
+    v2 = np.zeros(w.nz * w.nx, np.float32)
+    rs = np.zeros_like(v2)
+    velf = np.ascontiguousarray(w.vel.reshape(-1), np.float32)
+    assert lib.aio_fd_precompute(w.nz, w.nx, C.c_float(w.dts), w.sub, velf.ctypes.data_as(C.c_void_p),
+                                 v2.ctypes.data_as(C.c_void_p), rs.ctypes.data_as(C.c_void_p)) == 0
+    return v2, rs
+
+
+def hbm_peak():
+    """(GB/s, 'measured' | 'fallback'): the measured copy bandwidth of this GPU pool."""
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        v = json.load(open(pk)).get("hbm_gbs")
+        if v:
+            return float(v), "measured"
+    return 6650.0, "fallback"
+
+
+def run_plain(args, emit=True):
+    """One shot per call, per-fine-step stepper, FP32 wavefield: the plain GPU path (the
+    reference's schedule on this engine), Born forward + adjoint of each shot, host buffers."""
     import torch
     from acoustic_isotropic_operators_b200 import _capi
     from acoustic_isotropic_operators_b200.batch import Context, Shot
     w = workload(args, args.plain)
     lib = _capi.lib()
-    v2 = np.zeros(w.nz * w.nx, np.float32)
-    rs = np.zeros_like(v2)
-    velf = np.ascontiguousarray(w.vel.reshape(-1), np.float32)
-    lib.aio_fd_precompute(w.nz, w.nx, C.c_float(w.dts), w.sub, velf.ctypes.data_as(C.c_void_p),
-                          v2.ctypes.data_as(C.c_void_p), rs.ctypes.data_as(C.c_void_p))
+    v2, rs = fields(w, lib)
     sigs = prepare_signals(w, lib)
     model = np.ascontiguousarray(w.model, np.float32)
     times = []
@@ -231,13 +252,17 @@ def run_plain(args):
         ctx.close()
     t = statistics.mean(times[1:] if len(times) > 1 else times)
     pts = w.n_interior * w.fine_steps * PASSES
-    print(json.dumps({"impl": "plain (this engine, one shot per call, per-fine-step stepper, FP32 W)",
-                      "metric": METRIC, "value": pts / t / 1e9, "unit": UNIT, "seconds_per_shot": t,
-                      "shots_per_s": 1.0 / t, "shots": len(times), "config": config_dict(args, w)}))
-    return 0
+    out = {"impl": "plain (this engine, one shot per call, per-fine-step stepper, FP32 W)",
+           "metric": METRIC, "value": pts / t / 1e9, "unit": UNIT, "seconds_per_shot": t,
+           "shots_per_s": 1.0 / t, "shots": len(times), "timed_shots": max(1, len(times) - 1),
+           "inputs": "host buffers (copies inside the timed call)"}
+    if emit:
+        print(json.dumps(dict(out, config=config_dict(args, w))))
+        return 0
+    return out
 
 
-def run_ext(args):
+def run_ext(args, emit=True):
     """Extended (time-lag, nExt = 31) Born adjoint of N shots on the 500x1500 physical grid
     (608x1600 interior), host buffers, one call after one warm-up call."""
     import torch
@@ -246,11 +271,7 @@ def run_ext(args):
     n_ext = 31
     w = S.born_workload(nz_phys=500, nx_phys=1500, nshots=args.ext, nts=args.nts)
     lib = _capi.lib()
-    v2 = np.zeros(w.nz * w.nx, np.float32)
-    rs = np.zeros_like(v2)
-    velf = np.ascontiguousarray(w.vel.reshape(-1), np.float32)
-    lib.aio_fd_precompute(w.nz, w.nx, C.c_float(w.dts), w.sub, velf.ctypes.data_as(C.c_void_p),
-                          v2.ctypes.data_as(C.c_void_p), rs.ctypes.data_as(C.c_void_p))
+    v2, rs = fields(w, lib)
     sigs = prepare_signals(w, lib)
     rng = np.random.default_rng(4)
     shots = [Shot(a.src_pos, a.rec_pos, sg, (rng.standard_normal((len(a.rec_pos), w.nts)) * 1e-3).astype(np.float32))
@@ -264,15 +285,24 @@ def run_ext(args):
     n, steps, T = w.n_interior, w.fine_steps, w.nts - 1
     pts = n * steps * 2 * len(shots)
     algo = len(shots) * n * (2 * 16 * steps + 4 * w.nts + (4 + 4) * T + 8 * n_ext)
-    print(json.dumps({"impl": "this engine, extended Born adjoint (blocked stepper, blocked lag imaging, FP32 W)",
-                      "metric": "Gpts/s, extended (time-lag) Born adjoint", "value": pts / t / 1e9, "unit": UNIT,
-                      "seconds": t, "shots": len(shots), "nExt": n_ext, "interior": [w.nz - 10, w.nx - 10],
-                      "nts": w.nts, "algorithmic_GBps": algo / t / 1e9, "data": "synthetic (seeded)"}))
+    peak, src = hbm_peak()
+    out = {"impl": "this engine, extended Born adjoint (blocked stepper, blocked lag imaging, FP32 W)",
+           "metric": "Gpts/s, extended (time-lag) Born adjoint", "value": pts / t / 1e9, "unit": UNIT,
+           "seconds": t, "shots": len(shots), "shots_per_s": len(shots) / t, "nExt": n_ext,
+           "interior": [w.nz - 10, w.nx - 10], "nts": w.nts,
+           "roofline": {"bound": "hbm", "achieved": algo / t / 1e9, "peak": peak, "peak_source": src,
+                        "unit": "GB/s", "frac": algo / t / 1e9 / peak,
+                        "what": "whole call (host buffers), algorithmic bytes 16 B per update + stored / read W, "
+                                "receiver samples and the FP32 extended image"},
+           "inputs": "host buffers (copies inside the timed call)", "data": "synthetic (seeded)"}
     ctx.close()
-    return 0
+    if emit:
+        print(json.dumps(out))
+        return 0
+    return out
 
 
-def run_tomo(args):
+def run_tomo(args, emit=True):
     """Extended tomo and WEMVA forward and adjoint (time lags, nExt = 41) of N shots on the
     800x3000 physical grid (912x3104 interior, nts = 3000), host buffers; every operator is
     called twice and the second call is timed (the first one includes the stepper autotuning)."""
@@ -281,11 +311,7 @@ def run_tomo(args):
     from acoustic_isotropic_operators_b200.batch import Context, Shot
     w = S.tomo_workload(nshots=args.tomo, nts=args.tomo_nts)
     lib = _capi.lib()
-    v2 = np.zeros(w.nz * w.nx, np.float32)
-    rs = np.zeros_like(v2)
-    velf = np.ascontiguousarray(w.vel.reshape(-1), np.float32)
-    lib.aio_fd_precompute(w.nz, w.nx, C.c_float(w.dts), w.sub, velf.ctypes.data_as(C.c_void_p),
-                          v2.ctypes.data_as(C.c_void_p), rs.ctypes.data_as(C.c_void_p))
+    v2, rs = fields(w, lib)
     sigs = prepare_signals(w, lib)
     rng = np.random.default_rng(6)
     noise = lambda a: (rng.standard_normal((len(a.rec_pos), w.nts)) * 1e-3).astype(np.float32)
@@ -315,13 +341,20 @@ def run_tomo(args):
         tot_t += t
         tot_bytes += nbytes
     stepper = {"auto": "blocked stepper", "blocked": "blocked stepper", "fine": "per-fine-step stepper"}[args.stepper]
-    print(json.dumps({"impl": f"this engine, extended tomo + WEMVA ({stepper}, FP32 wavefields)",
-                      "metric": "Gpts/s, extended tomo + WEMVA forward and adjoint", "value": tot_pts / tot_t / 1e9,
-                      "unit": UNIT, "seconds": tot_t, "algorithmic_GBps": tot_bytes / tot_t / 1e9, "ops": res,
-                      "shots": len(shots), "nExt": w.nExt,
-                      "interior": [w.nz - 10, w.nx - 10], "nts": w.nts, "data": "synthetic (seeded)"}))
+    peak, src = hbm_peak()
+    out = {"impl": f"this engine, extended tomo + WEMVA ({stepper}, FP32 wavefields)",
+           "metric": "Gpts/s, extended tomo + WEMVA forward and adjoint", "value": tot_pts / tot_t / 1e9,
+           "unit": UNIT, "seconds": tot_t, "ops": res, "shots": len(shots), "nExt": w.nExt,
+           "interior": [w.nz - 10, w.nx - 10], "nts": w.nts,
+           "roofline": {"bound": "hbm", "achieved": tot_bytes / tot_t / 1e9, "peak": peak, "peak_source": src,
+                        "unit": "GB/s", "frac": tot_bytes / tot_t / 1e9 / peak,
+                        "what": "whole calls (host buffers), algorithmic bytes 16 B per update + coarse-field sweeps"},
+           "inputs": "host buffers (copies inside the timed calls)", "data": "synthetic (seeded)"}
     ctx.close()
-    return 0
+    if emit:
+        print(json.dumps(out))
+        return 0
+    return out
 
 
 def run_variants(args):
@@ -373,7 +406,7 @@ def run_variants(args):
     return 0
 
 
-def run_nl(args):
+def run_nl(args, emit=True):
     """Nonlinear forward of one shot on the 200x400 physical grid with Gaussian blobs (304x512
     interior, nts = 1000, 400 receivers), one call per shot through the C ABI with host buffers:
     the latency-bound single-shot case (its three state slices fit in L2)."""
@@ -382,11 +415,7 @@ def run_nl(args):
     from acoustic_isotropic_operators_b200.batch import Context, Shot
     w = S.nonlinear_workload()
     lib = _capi.lib()
-    v2 = np.zeros(w.nz * w.nx, np.float32)
-    rs = np.zeros_like(v2)
-    velf = np.ascontiguousarray(w.vel.reshape(-1), np.float32)
-    lib.aio_fd_precompute(w.nz, w.nx, C.c_float(w.dts), w.sub, velf.ctypes.data_as(C.c_void_p),
-                          v2.ctypes.data_as(C.c_void_p), rs.ctypes.data_as(C.c_void_p))
+    v2, rs = fields(w, lib)
     sig = prepare_signals(w, lib)[0]
     shot = Shot(w.shots[0].src_pos, w.shots[0].rec_pos, sig)
     out = {}
@@ -403,11 +432,44 @@ def run_nl(args):
         out["blocked" if stepper == "auto" else "per_fine_step"] = {
             "seconds_per_call": t, "Gpts_s": w.n_interior * w.fine_steps / t / 1e9}
         ctx.close()
-    print(json.dumps({"impl": "this engine, nonlinear forward, one shot per call (host buffers)",
-                      "metric": "Gpts/s, nonlinear forward", "unit": UNIT, "value": out["blocked"]["Gpts_s"],
-                      "steppers": out, "interior": [w.nz - 10, w.nx - 10], "nts": w.nts, "sub": w.sub,
-                      "receivers": len(w.shots[0].rec_pos), "data": "synthetic (seeded)"}))
-    return 0
+    peak, src = hbm_peak()
+    t = out["blocked"]["seconds_per_call"]
+    algo = 16.0 * w.n_interior * w.fine_steps
+    res = {"impl": "this engine, nonlinear forward, one shot per call (host buffers)",
+           "metric": "Gpts/s, nonlinear forward", "unit": UNIT, "value": out["blocked"]["Gpts_s"],
+           "shots_per_s": 1.0 / t, "steppers": out, "interior": [w.nz - 10, w.nx - 10], "nts": w.nts,
+           "sub": w.sub, "receivers": len(w.shots[0].rec_pos),
+           "roofline": {"bound": "hbm", "achieved": algo / t / 1e9, "peak": peak, "peak_source": src, "unit": "GB/s",
+                        "frac": algo / t / 1e9 / peak,
+                        "what": "whole call, 16 B per update; the three state slices (0.6 MB each) stay in L2"},
+           "inputs": "host buffers (copies inside the timed call)", "data": "synthetic (seeded)"}
+    if emit:
+        print(json.dumps(res))
+        return 0
+    return res
+
+
+def other_configs(args, batched_value):
+    """The other benchmark configurations, each timed once after the headline (1 GPU): the
+    single-shot nonlinear forward (200x400), the plain one-shot-per-call path on the headline's
+    grid, the extended Born adjoint (500x1500, nExt = 31, 64 shots) and the extended tomo + WEMVA
+    operators (800x3000, nExt = 41, 2 of 96 shots: the shots one FP32 wave holds)."""
+    import copy
+    out = {}
+    a = copy.copy(args)
+    out["nonlinear_forward_1_shot"] = run_nl(a, emit=False)
+    a = copy.copy(args)
+    a.plain, a.nts = 3, args.nts
+    plain = run_plain(a, emit=False)
+    plain["batched_over_plain"] = batched_value / plain["value"]
+    out["plain_one_shot_per_call"] = plain
+    a = copy.copy(args)
+    a.ext, a.nts = 64, 2000
+    out["extended_born_adjoint_64_shots"] = run_ext(a, emit=False)
+    a = copy.copy(args)
+    a.tomo, a.tomo_nts, a.stepper = 2, 3000, "auto"
+    out["tomo_wemva_2_shots"] = run_tomo(a, emit=False)
+    return out
 
 
 def main():
@@ -551,6 +613,11 @@ def main():
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"1 shot, Born forward+adjoint, full grid, nts={nts_sample} ({dt:.1f} s)"}
 
+    ctx.close()
+    configs = None
+    if world == 1 and not args.no_configs:
+        configs = other_configs(args, value)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -563,8 +630,9 @@ def main():
                              "algorithmic_bytes_per_step": algo_step, "timed_launches": n_timed,
                              "stepper_ms_share": (step_ms * 16 / ms) if ms > 0 else None},
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": kernels, "clocks": clk.summary()}
+        if configs is not None:
+            line["configs"] = configs
         print(json.dumps(line))
-    ctx.close()
     if dist:
         dist.destroy_process_group()
     return 0
