@@ -82,6 +82,11 @@ class Context:
         return int(A.lib().aio_context_wave_capacity(self._h, family))
 
     @property
+    def graph_replays(self) -> int:
+        """Interval loops replayed from CUDA graphs since the context was created."""
+        return int(A.lib().aio_context_graph_replays(self._h))
+
+    @property
     def stream_ptr(self) -> int:
         return int(A.lib().aio_context_stream(self._h) or 0)
 

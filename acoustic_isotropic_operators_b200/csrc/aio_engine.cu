@@ -222,6 +222,8 @@ struct Context {
         size_t fr = 0, tot = 0;
         AIO_CK(cudaMemGetInfo(&fr, &tot));
         budget = p.memBudgetBytes > 0 ? p.memBudgetBytes : (long long)(0.93 * (double)fr);
+        const char* gEnv = std::getenv("AIO_GRAPHS");  // AIO_GRAPHS=0: launch every interval directly
+        graphsOn = !(gEnv && gEnv[0] == '0');
     }
 
     void set_velocity(const float* vel2Dtw2, const float* reflScale) {
@@ -234,6 +236,7 @@ struct Context {
     }
 
     void destroy() {
+        drop_graphs();
         for (auto& e : evFree) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
         for (auto& e : evBusy) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
         evFree.clear();
@@ -244,6 +247,69 @@ struct Context {
     void kcheck() {
         AIO_CK(cudaGetLastError());
         kernels++;
+    }
+
+    // ------------------------------------------------------------- graph-captured time loops
+    // A pass's per-interval launches (one blocked-stepper launch per coarse interval, ~2000 per
+    // pass) are a fixed sequence once the pass's key is fixed: plan, entry capacity and the device
+    // addresses baked into the launch arguments (descriptors, stored wavefield, model). The first
+    // run of a key launches directly; the second is captured into a CUDA graph, which this and
+    // every later run with the same key replay with one cudaGraphLaunch. Off while live stepper
+    // timing brackets single launches with events, and with AIO_GRAPHS=0.
+    struct GraphEntry {
+        cudaGraphExec_t exec = nullptr;
+        long long launches = 0, kernels = 0;
+    };
+    std::map<std::vector<long long>, GraphEntry> graphs;
+    std::map<std::vector<long long>, int> graphRuns;
+    bool graphsOn = true;
+    long long graphReplays = 0;
+
+    void drop_graphs() {
+        for (auto& e : graphs)
+            if (e.second.exec) cudaGraphExecDestroy(e.second.exec);
+        graphs.clear();
+        graphRuns.clear();
+    }
+    // key: the pass's own fields; the settings that select kernel variants (free surface,
+    // stored precision) are appended here so no pass can replay another variant's graph
+    template <class Body>
+    void graph_loop(std::vector<long long> key, Body&& body) {
+        if (!graphsOn || profEvery > 0) {
+            body();
+            return;
+        }
+        key.insert(key.end(), {P.freeSurface, P.wavefieldPrecision, P.extension, P.sloth, P.stepper});
+        auto it = graphs.find(key);
+        if (it != graphs.end()) {
+            AIO_CK(cudaGraphLaunch(it->second.exec, st));
+            launches += it->second.launches;
+            kernels += it->second.kernels;
+            graphReplays++;
+            return;
+        }
+        if (graphRuns[key]++ == 0) {  // first run: direct launches (also sets kernel attributes)
+            body();
+            return;
+        }
+        if (graphs.size() >= 64) drop_graphs();
+        const long long l0 = launches, k0 = kernels;
+        AIO_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        cudaGraph_t gph = nullptr;
+        try {
+            body();
+        } catch (...) {
+            cudaStreamEndCapture(st, &gph);
+            if (gph) cudaGraphDestroy(gph);
+            throw;
+        }
+        AIO_CK(cudaStreamEndCapture(st, &gph));
+        cudaGraphExec_t ex = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&ex, gph, 0);
+        cudaGraphDestroy(gph);
+        AIO_CK(e);
+        graphs[key] = GraphEntry{ex, launches - l0, kernels - k0};
+        AIO_CK(cudaGraphLaunch(ex, st));
     }
 
     // full nz*nx (per slice) <-> interior pitched slices
@@ -829,6 +895,7 @@ struct Context {
     // images use interior slices; the stored wavefield is FP32 or BF16.
     DevMem tbState, tbPart, tbImg, tbW, tbEnt, tbStart, tbDesc, shotImg;
     DevMem tbWscale, tbWmax, tbWstage;  // FP16 stored wavefield: per-slice scales, max |W|, FP32 staging
+    DevMem tbWover;                     // FP16 stored wavefield: overflow flag of the speculative scales
     DevMem tbR;                         // extended adjoint: coarse receiver samples [shot][LAG_K][isz]
     DevMem tbSS;                        // extended forward: secondary sources [shot][2 LAG_K][isz]
     DevMem tbF2;                        // tomo / WEMVA: second full coarse field [shot][nts][isz]
@@ -848,10 +915,12 @@ struct Context {
     // staging slots, no secondary-source rings), heavy modes (SCAT, SCATX, SCATW, ADJX), whose
     // larger shared-memory footprint changes how many CTAs an SM holds, and the Born receiver
     // pass (ADJ: 12 staging slots, FP64 image read-modify-write, receivers injected).
-    enum TBClass { TB_LIGHT = 0, TB_HEAVY = 1, TB_RECV = 2 };
+    // The nonlinear forward (NL: sources in, receivers recorded, no stored wavefield) is tuned as
+    // its own class: its single-shot calls are the small, latency-bound waves.
+    enum TBClass { TB_LIGHT = 0, TB_HEAVY = 1, TB_RECV = 2, TB_NLC = 3 };
     TBPlan tb_plan(int nb, bool heavy = false) const { return tb_plan_c(nb, heavy ? TB_HEAVY : TB_LIGHT); }
     TBPlan tb_plan_c(int nb, int cls) const {
-        auto it = tbTuned.find(3 * nb + cls);
+        auto it = tbTuned.find(4 * nb + cls);
         if (it != tbTuned.end()) return it->second;
         return tb_model_plan(nb, 4 * (KT_MAXQ - 10), P.chunkColumns > 0 ? P.chunkColumns : 0);
     }
@@ -963,15 +1032,31 @@ struct Context {
         return true;
     }
 
-    void tb_autotune(int nb, const aio_shot* shots) {
-        if (P.chunkColumns != 0 || tbTuned.count(3 * nb)) return;
+    // Candidates: strip heights {128 .. 64} rows (and, for waves too small to fill the GPU with
+    // 128-row strips, 48 and 32 rows) x chunk counts around the model's choices; for those small
+    // waves also the chunk counts that give one or two CTAs per SM, with chunks down to 16
+    // columns. nonlinear: the NL class alone is timed (its launch with recording off).
+    void tb_autotune(int nb, const aio_shot* shots, bool nonlinear = false) {
+        if (P.chunkColumns != 0 || tbTuned.count(4 * nb + (nonlinear ? TB_NLC : TB_LIGHT))) return;
+        const bool small = (long long)tb_model_plan(nb, 128, 0, 0, 1).nStrips * std::max(1, g.nxi / 48) * nb <
+                           2LL * smCount;
+        std::vector<int> heights = {128, 112, 96, 80, 64};
+        if (small) heights.insert(heights.end(), {48, 32});
+        const int maxChunks = std::max(1, g.nxi / (small ? 16 : 32));
         std::vector<TBPlan> cand;
-        for (int maxHZ : {128, 112, 96, 80, 64})
-            for (int minWaves : {4, 1}) {
-                const TBPlan m = tb_model_plan(nb, maxHZ, 0, 0, minWaves);
-                for (int d : {-2, -1, 0, 1, 2}) {
+        for (int maxHZ : heights)
+            for (int minWaves : {4, 1, 0}) {
+                TBPlan m;
+                if (minWaves > 0) {
+                    m = tb_model_plan(nb, maxHZ, 0, 0, minWaves);
+                } else {  // small waves: about one and two CTAs per SM
+                    if (!small) continue;
+                    m = tb_model_plan(nb, maxHZ, 0, 1);
+                    m.nChunks = std::max(1, (int)(smCount / std::max(1LL, (long long)m.nStrips * nb)));
+                }
+                for (int d : {-2, -1, 0, 1, 2, minWaves == 0 ? m.nChunks : 0}) {
                     const int nc = m.nChunks + d;
-                    if (nc < 1 || nc > std::max(1, g.nxi / 32)) continue;
+                    if (nc < 1 || nc > maxChunks) continue;
                     TBPlan c = tb_model_plan(nb, maxHZ, 0, nc);
                     bool dup = false;
                     for (auto& o : cand) dup |= (o.HZ == c.HZ && o.nChunks == c.nChunks);
@@ -994,9 +1079,34 @@ struct Context {
         for (const TBPlan& pl : cand) {
             const int maxEnt = tb_lists(pl, nb, shots, 1, false);
             tb_zero(nb, false);
-            tb_desc(pl, nb, true, false, false, tbW.p, false);
+            tb_desc(pl, nb, true, false, false, nonlinear ? nullptr : tbW.p, false);
             KTArgs a = tb_args(pl, maxEnt, nullptr);
             a.its = 0;
+            if (nonlinear) {  // NL class: the launch without recording (the data stay untouched)
+                const float ms = [&] {
+                    tb_launch<TB_NL>(pl, nb, a, 0);
+                    float best2 = 1e30f;
+                    for (int rep = 0; rep < 3; rep++) {
+                        AIO_CK(cudaEventRecord(e0, st));
+                        tb_launch<TB_NL>(pl, nb, a, 0);
+                        tb_launch<TB_NL>(pl, nb, a, 0);
+                        AIO_CK(cudaEventRecord(e1, st));
+                        AIO_CK(cudaEventSynchronize(e1));
+                        float t = 0.f;
+                        AIO_CK(cudaEventElapsedTime(&t, e0, e1));
+                        best2 = std::min(best2, t);
+                    }
+                    return best2;
+                }();
+                if (ms < bestMs) {
+                    bestMs = ms;
+                    best = pl;
+                }
+                if (logTune)
+                    std::fprintf(stderr, "aio autotune (NL): shots %d strip %d x %d chunk %d x %d threads %d: %.3f ms\n",
+                                 nb, pl.HZ, pl.nStrips, pl.LX, pl.nChunks, pl.threads, ms);
+                continue;
+            }
             if (f16()) AIO_CK(cudaMemsetAsync(tbWmax.p, 0, (size_t)nb * g.nts * 4, st));
             // fastest of three timings of two launches each (after a warm-up launch: smem
             // carve-out, caches), so that a disturbed timing does not decide the plan
@@ -1059,9 +1169,13 @@ struct Context {
         launches = saveLaunches;
         kernels = saveKernels;
         profEvery = saveProf;
-        tbTuned[3 * nb + TB_LIGHT] = best;
-        tbTuned[3 * nb + TB_HEAVY] = bestHeavy;
-        tbTuned[3 * nb + TB_RECV] = bestRecv;
+        if (nonlinear) {
+            tbTuned[4 * nb + TB_NLC] = best;
+        } else {
+            tbTuned[4 * nb + TB_LIGHT] = best;
+            tbTuned[4 * nb + TB_HEAVY] = bestHeavy;
+            tbTuned[4 * nb + TB_RECV] = bestRecv;
+        }
     }
 
     // Per-CTA sparse lists of every shot of a wave. inj: 0 none, 1 sources, 2 receivers
@@ -1132,6 +1246,7 @@ struct Context {
             tbWscale.ensure((size_t)nb * g.nts * 4);
             tbWmax.ensure((size_t)nb * g.nts * 4);
             tbWstage.ensure((size_t)nb * 2 * g.isz * 4);
+            tbWover.ensure(4);
         }
     }
 
@@ -1140,8 +1255,11 @@ struct Context {
     // wSlices: coarse slices per shot in W (the stored wavefield: nts; a secondary-source ring: its length)
     // out / outSlices: per-shot slices written by ADJR / SCATW / ADJX (default: the LAG_K ring tbR)
     // dataIn: traces injected when injData (default: the wave's data)
+    // W: the stored source wavefield (elements of wbytes()) or, with wSlices > 0, an FP32 ring of
+    // wSlices secondary-source slices
     void tb_desc(const TBPlan& pl, int nb, bool injSources, bool injData, bool recData, void* W, bool partFlip,
                  int wSlices = 0, float* out = nullptr, int outSlices = 0, const float* const* dataIn = nullptr) {
+        const int wElem = wSlices > 0 ? 4 : wbytes();
         if (wSlices <= 0) wSlices = g.nts;
         if (!out && tbR.p) {
             out = tbR.as<float>();
@@ -1168,13 +1286,14 @@ struct Context {
                 t.recLd = g.nts;
                 t.entStart = tbStart.as<int4>() + (size_t)s * nCTA;
                 t.ent = tbEnt.as<TBEnt>();
-                t.W = W ? (void*)((char*)W + (size_t)s * wSlices * g.isz * wbytes()) : nullptr;
+                t.W = W ? (void*)((char*)W + (size_t)s * wSlices * g.isz * wElem) : nullptr;
                 t.img = tbImg.p ? tbImg.as<double>() + (size_t)s * g.isz : nullptr;
                 t.rcoarse = out ? out + (size_t)s * outSlices * g.isz : nullptr;
                 if (f16()) {
                     t.wscale = tbWscale.as<float>() + (size_t)s * g.nts;
                     t.wmax = tbWmax.as<unsigned>() + (size_t)s * g.nts;
                     t.wstage = tbWstage.as<float>() + (size_t)s * 2 * g.isz;
+                    t.wover = tbWover.as<unsigned>();
                 }
             }
         AIO_CK(cudaMemcpyAsync(tbDesc.p, d.data(), d.size() * sizeof(TBShot), cudaMemcpyHostToDevice, st));
@@ -1242,7 +1361,10 @@ struct Context {
     }
     template <int MODE>
     void tb_launch(const TBPlan& pl, int nb, KTArgs& a, int v) {
-        if (P.wavefieldPrecision == AIO_WFLD_BF16) tb_launch_t<MODE, TBW_BF16>(pl, nb, a, v);
+        // the dense-source modes read FP32 rings of secondary sources, and the receiver-sample
+        // pass reads no stored wavefield: those run on FP32 whatever the stored precision
+        if (MODE == TB_SCATX || MODE == TB_SCATW || MODE == TB_ADJX || MODE == TB_ADJR) tb_launch_t<MODE, TBW_F32>(pl, nb, a, v);
+        else if (P.wavefieldPrecision == AIO_WFLD_BF16) tb_launch_t<MODE, TBW_BF16>(pl, nb, a, v);
         else if (P.wavefieldPrecision == AIO_WFLD_FP16) tb_launch_t<MODE, TBW_F16>(pl, nb, a, v);
         else tb_launch_t<MODE, TBW_F32>(pl, nb, a, v);
     }
@@ -1255,25 +1377,44 @@ struct Context {
 
     // Source pass storing W[nts] (F/src/BornShotsGpuFunctions.cu:297-321), or the
     // nonlinear forward when recordData (F/src/nonlinearShotsGpuFunctions.cu:269-295).
-    void tb_src_pass(int nb, const aio_shot* shots, bool nonlinear) {
-        if (!nonlinear) tb_autotune(nb, shots);
-        const TBPlan pl = tb_plan(nb);
+    // FP16 stored wavefield: slices are stored with speculative power-of-two scales from the
+    // previous slice's max (kt_f16_spec_scale); if any slice outgrew its scale's headroom the
+    // pass is run again with every slice staged in FP32 and quantized with its exact max.
+    void tb_src_pass(int nb, const aio_shot* shots, bool nonlinear, bool exactF16 = false) {
+        tb_autotune(nb, shots, nonlinear);
+        const TBPlan pl = nonlinear ? tb_plan_c(nb, TB_NLC) : tb_plan(nb);
         const int maxEnt = tb_lists(pl, nb, shots, 1, nonlinear);
         tb_zero(nb, false);
         tb_desc(pl, nb, true, false, nonlinear, nonlinear ? nullptr : tbW.p, false);
         KTArgs a = tb_args(pl, maxEnt, nullptr);
+        const bool spec = !nonlinear && f16() && !exactF16;
+        a.f16spec = spec ? 1 : 0;
         if (!nonlinear && f16()) AIO_CK(cudaMemsetAsync(tbWmax.p, 0, (size_t)nb * g.nts * 4, st));
-        for (int its = 0; its < g.nts - 1; its++) {
-            a.its = its;
-            if (nonlinear) tb_launch<TB_NL>(pl, nb, a, its & 1);
-            else tb_launch<TB_SRC>(pl, nb, a, its & 1);
-        }
+        if (spec) AIO_CK(cudaMemsetAsync(tbWover.p, 0, 4, st));
+        tbLast = pl;
+        graph_loop({1, nonlinear, nb, pl.HZ, pl.nStrips, pl.LX, pl.nChunks, maxEnt, (long long)tbDesc.p,
+                    (long long)tbW.p, a.f16spec, P.wavefieldPrecision},
+                   [&] {
+                       for (int its = 0; its < g.nts - 1; its++) {
+                           a.its = its;
+                           if (nonlinear) tb_launch<TB_NL>(pl, nb, a, its & 1);
+                           else tb_launch<TB_SRC>(pl, nb, a, its & 1);
+                       }
+                   });
         if (!nonlinear && f16()) {  // last two slices and the per-slice scales
             k_f16_finish<<<dim3(std::max(1, smCount), nb), 256, 0, st>>>(tbDesc.as<TBShot>(), g.isz, g.ip, g.nzi,
-                                                                          g.nxi, g.nts);
+                                                                          g.nxi, g.nts, a.f16spec);
             kcheck();
         }
+        if (spec) {
+            unsigned over = 0;
+            AIO_CK(cudaMemcpyAsync(&over, tbWover.p, 4, cudaMemcpyDeviceToHost, st));
+            AIO_CK(cudaStreamSynchronize(st));
+            f16Reruns += over ? 1 : 0;
+            if (over) tb_src_pass(nb, shots, nonlinear, true);
+        }
     }
+    long long f16Reruns = 0;  // FP16 source passes run again with exact scales (speculative overflow)
 
     // Scattered pass with data recording (F/src/BornShotsGpuFunctions.cu:323-376); W: the stored
     // field the secondary sources dm * W come from (default: the source wavefield tbW).
@@ -1283,10 +1424,15 @@ struct Context {
         tb_zero(nb, false);
         tb_desc(pl, nb, false, false, true, W ? (void*)W : tbW.p, false);
         KTArgs a = tb_args(pl, maxEnt, dm);
-        for (int its = 0; its < g.nts - 1; its++) {
-            a.its = its;
-            tb_launch<TB_SCAT>(pl, nb, a, its & 1);
-        }
+        tbLast = pl;
+        graph_loop({2, nb, pl.HZ, pl.nStrips, pl.LX, pl.nChunks, maxEnt, (long long)tbDesc.p, (long long)dm,
+                    (long long)(W ? (const void*)W : tbW.p), P.wavefieldPrecision},
+                   [&] {
+                       for (int its = 0; its < g.nts - 1; its++) {
+                           a.its = its;
+                           tb_launch<TB_SCAT>(pl, nb, a, its & 1);
+                       }
+                   });
     }
 
     // Receiver pass with imaging (F/src/BornShotsGpuFunctions.cu:880-950), on U = v2*p.
@@ -1298,10 +1444,15 @@ struct Context {
         tb_zero(nb, true);
         tb_desc(pl, nb, false, true, false, tbW.p, false);
         KTArgs a = tb_args(pl, maxEnt, nullptr);
-        for (int L = 0; L < g.nts - 1; L++) {
-            a.its = g.nts - 2 - L;
-            tb_launch<TB_ADJ>(pl, nb, a, L & 1);
-        }
+        tbLast = pl;
+        graph_loop({3, nb, pl.HZ, pl.nStrips, pl.LX, pl.nChunks, maxEnt, (long long)tbDesc.p, (long long)tbW.p,
+                    P.wavefieldPrecision},
+                   [&] {
+                       for (int L = 0; L < g.nts - 1; L++) {
+                           a.its = g.nts - 2 - L;
+                           tb_launch<TB_ADJ>(pl, nb, a, L & 1);
+                       }
+                   });
     }
 
     // Receiver pass of the extended (time-lag) adjoint (F/src/BornExtShotsGpuFunctions.cu:1525-1675)
@@ -1323,6 +1474,10 @@ struct Context {
         if (lagAttr != dev) {
             AIO_CK(cudaFuncSetAttribute(k_img_lag_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
             AIO_CK(cudaFuncSetAttribute(k_img_lag_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            AIO_CK(cudaFuncSetAttribute(k_img_lag_block<double, TBW_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            AIO_CK(cudaFuncSetAttribute(k_img_lag_block<float, TBW_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            AIO_CK(cudaFuncSetAttribute(k_img_lag_block<double, TBW_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            AIO_CK(cudaFuncSetAttribute(k_img_lag_block<float, TBW_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
             lagAttr = dev;
         }
         require(offsets() || lagSmem <= 200 * 1024, "extension too long for the blocked lag imaging");
@@ -1343,14 +1498,22 @@ struct Context {
                 return;
             }
             const dim3 grid((unsigned)((g.isz + nP - 1) / nP), nb);
-            if (P.imageFp64)
-                k_img_lag_block<double><<<grid, nP, lagSmem, st>>>(img.as<double>(), mSt, tbR.as<float>(),
-                                                                    (long long)LAG_K * g.isz, LAG_K, tbW.as<float>(),
-                                                                    wfSt(), g.isz, tlo, thi, g.nts, g.hExt, g.nExt, 1);
-            else
-                k_img_lag_block<float><<<grid, nP, lagSmem, st>>>(img.as<float>(), mSt, tbR.as<float>(),
-                                                                   (long long)LAG_K * g.isz, LAG_K, tbW.as<float>(),
-                                                                   wfSt(), g.isz, tlo, thi, g.nts, g.hExt, g.nExt, 1);
+            const long long rSt = (long long)LAG_K * g.isz;
+            const float* sc = f16() ? tbWscale.as<float>() : nullptr;
+#define AIO_LAG_IMG(ACC, WP)                                                                                          \
+    k_img_lag_block<ACC, WP><<<grid, nP, lagSmem, st>>>(img.as<ACC>(), mSt, tbR.as<float>(), rSt, LAG_K, tbW.p, wfSt(), \
+                                                        g.isz, tlo, thi, g.nts, g.hExt, g.nExt, 1, sc)
+            if (P.wavefieldPrecision == AIO_WFLD_BF16) {
+                if (P.imageFp64) AIO_LAG_IMG(double, TBW_BF16);
+                else AIO_LAG_IMG(float, TBW_BF16);
+            } else if (f16()) {
+                if (P.imageFp64) AIO_LAG_IMG(double, TBW_F16);
+                else AIO_LAG_IMG(float, TBW_F16);
+            } else {
+                if (P.imageFp64) AIO_LAG_IMG(double, TBW_F32);
+                else AIO_LAG_IMG(float, TBW_F32);
+            }
+#undef AIO_LAG_IMG
             kcheck();
         };
         for (int L = 0; L < g.nts - 1; L++) {
@@ -1379,7 +1542,9 @@ struct Context {
         const size_t lagSmem = (size_t)lag_window_len(g.hExt) * nP * 4;
         static int ssAttr = -1;
         if (ssAttr != dev) {
-            AIO_CK(cudaFuncSetAttribute(k_ss_lag_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            AIO_CK(cudaFuncSetAttribute(k_ss_lag_block<TBW_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            AIO_CK(cudaFuncSetAttribute(k_ss_lag_block<TBW_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+            AIO_CK(cudaFuncSetAttribute(k_ss_lag_block<TBW_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
             ssAttr = dev;
         }
         require(offsets() || lagSmem <= 200 * 1024, "extension too long for the blocked lag imaging");
@@ -1400,9 +1565,22 @@ struct Context {
                 return;
             }
             const dim3 grid((unsigned)((g.isz + nP - 1) / nP), nb);
-            k_ss_lag_block<<<grid, nP, lagSmem, st>>>(tbSS.as<float>(), (long long)ring * g.isz, ring, ext,
-                                                      F ? F : tbW.as<float>(), wfSt(), g.isz, tlo, thi, g.nts, g.hExt,
-                                                      g.nExt, 1);
+            // F (a caller's FP32 field) or the stored source wavefield in its precision
+            const int wp = F ? AIO_WFLD_FP32 : P.wavefieldPrecision;
+            const void* Ws = F ? (const void*)F : tbW.p;
+            const float* sc = (!F && f16()) ? tbWscale.as<float>() : nullptr;
+            if (wp == AIO_WFLD_BF16)
+                k_ss_lag_block<TBW_BF16><<<grid, nP, lagSmem, st>>>(tbSS.as<float>(), (long long)ring * g.isz, ring, ext,
+                                                                    Ws, wfSt(), g.isz, tlo, thi, g.nts, g.hExt, g.nExt,
+                                                                    1, sc);
+            else if (wp == AIO_WFLD_FP16)
+                k_ss_lag_block<TBW_F16><<<grid, nP, lagSmem, st>>>(tbSS.as<float>(), (long long)ring * g.isz, ring, ext,
+                                                                   Ws, wfSt(), g.isz, tlo, thi, g.nts, g.hExt, g.nExt,
+                                                                   1, sc);
+            else
+                k_ss_lag_block<TBW_F32><<<grid, nP, lagSmem, st>>>(tbSS.as<float>(), (long long)ring * g.isz, ring, ext,
+                                                                   Ws, wfSt(), g.isz, tlo, thi, g.nts, g.hExt, g.nExt,
+                                                                   1, sc);
             kcheck();
         };
         for (int its = 0; its < g.nts - 1; its++) {
@@ -1424,7 +1602,7 @@ struct Context {
             const int nb = tb_wave_size(nShots - s0, shots + s0, true, false);
             setup_wave(n, nb, shots + s0, mem, false, false);
             tb_alloc(nb, false);
-            tbW.ensure((size_t)nb * g.nts * g.isz * 4);
+            tbW.ensure((size_t)nb * g.nts * g.isz * wbytes());
             tbSS.ensure((size_t)nb * 2 * LAG_K * g.isz * 4);
             tb_src_pass(nb, shots + s0, false);
             tb_scatx_pass(nb, shots + s0, ext);
@@ -1435,8 +1613,8 @@ struct Context {
     }
 
     void born_ext_adjoint_tb(float* modelOut, int add, int nShots, const aio_shot* shots, int mem) {
-        require(P.wavefieldPrecision == AIO_WFLD_FP32,
-                "the extended operators keep the stored wavefield in FP32 (wavefieldPrecision)");
+        require(P.wavefieldPrecision == AIO_WFLD_FP32 || !offsets(),
+                "the subsurface-offset extension keeps the stored wavefield in FP32 (wavefieldPrecision)");
         Needs n;
         n.nImg = g.nExt;
         float* out = stage_out(modelOut, g.nExt, add, mem);
@@ -1447,7 +1625,7 @@ struct Context {
             nb = std::max(1, std::min<int>(nb, (int)std::max<long long>(1, (budget / 2) / perImg)));
             setup_wave(n, nb, shots + s0, mem, true, false);
             tb_alloc(nb, false);
-            tbW.ensure((size_t)nb * g.nts * g.isz * 4);
+            tbW.ensure((size_t)nb * g.nts * g.isz * wbytes());
             tbR.ensure((size_t)nb * LAG_K * g.isz * 4);
             tb_src_pass(nb, shots + s0, false);
             zero_images(nb, g.nExt);
@@ -1488,7 +1666,7 @@ struct Context {
         if (lagDev == dev) return;
         AIO_CK(cudaFuncSetAttribute(k_img_lag_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         AIO_CK(cudaFuncSetAttribute(k_img_lag_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        AIO_CK(cudaFuncSetAttribute(k_ss_lag_block, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        AIO_CK(cudaFuncSetAttribute(k_ss_lag_block<TBW_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         lagDev = dev;
     }
     size_t tb_lag_smem(int hExt) const {
@@ -1501,7 +1679,7 @@ struct Context {
         tb_lag_attr();
         const int nP = LAG_NP;
         const dim3 grid((unsigned)((g.isz + nP - 1) / nP), nb);
-        k_ss_lag_block<<<grid, nP, tb_lag_smem(g.hExt), st>>>(tbSS.as<float>(), (long long)TB_RING * g.isz, TB_RING,
+        k_ss_lag_block<TBW_F32><<<grid, nP, tb_lag_smem(g.hExt), st>>>(tbSS.as<float>(), (long long)TB_RING * g.isz, TB_RING,
                                                                 src.ext, src.F, wfSt(), g.isz, tlo, thi, g.nts, g.hExt,
                                                                 g.nExt, src.sign);
         kcheck();
@@ -1952,11 +2130,19 @@ struct Context {
         return outv.as<float>();
     }
 
+    // Operators whose stored fields stay in FP32 refuse a compressed stored-wavefield setting
+    // instead of running with FP32 fields under it.
+    void require_fp32_fields(const char* what) {
+        require(P.wavefieldPrecision == AIO_WFLD_FP32,
+                std::string(what) + " keep their stored wavefields in FP32 (wavefieldPrecision must be AIO_WFLD_FP32)");
+    }
+
     // Extended (time-lag) Born forward (F/src/BornExtShotsGpuFunctions.cu:269-419).
     void born_ext_forward(const float* model, int nShots, const aio_shot* shots, int mem) {
         begin_call();
-        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32)
-            return born_ext_forward_tb(model, nShots, shots, mem);
+        require(P.wavefieldPrecision == AIO_WFLD_FP32 || !offsets(),
+                "the subsurface-offset extension keeps the stored wavefield in FP32 (wavefieldPrecision)");
+        if (tb_enabled()) return born_ext_forward_tb(model, nShots, shots, mem);
         Needs n;
         n.nWavefields = 1;
         n.ss = true;
@@ -2108,8 +2294,9 @@ struct Context {
     // Extended (time-lag) Born adjoint (F/src/BornExtShotsGpuFunctions.cu:1525-1675).
     void born_ext_adjoint(float* modelOut, int add, int nShots, const aio_shot* shots, int mem) {
         begin_call();
-        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32)
-            return born_ext_adjoint_tb(modelOut, add, nShots, shots, mem);
+        require(P.wavefieldPrecision == AIO_WFLD_FP32 || !offsets(),
+                "the subsurface-offset extension keeps the stored wavefield in FP32 (wavefieldPrecision)");
+        if (tb_enabled()) return born_ext_adjoint_tb(modelOut, add, nShots, shots, mem);
         Needs n;
         n.nWavefields = 1;
         n.nImg = g.nExt;
@@ -2149,6 +2336,7 @@ struct Context {
     // Extended tomo forward (F/src/tomoExtShotsGpuFunctions.cu:355-465, legs :1554-1881).
     void tomo_forward(const float* model, const float* extRefl, int nShots, const aio_shot* shots, int mem) {
         begin_call();
+        require_fp32_fields("tomo and WEMVA");
         Needs n;
         n.nWavefields = 2;
         n.ss = true;
@@ -2157,7 +2345,7 @@ struct Context {
         float* ex = stage_model(extRefl, g.nExt, mem, this->ext);
         // subsurface offsets (tomoOffsetShotsFwdGpu, F/src/tomoExtShotsGpuFunctions.cu:467-575): 2/v^3 only
         scale_shared(ex, g.nExt, offsets() ? 3 : (P.sloth ? 2 : 1));
-        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32 && !offsets())
+        if (tb_enabled() && !offsets())
             return tomo_forward_tb(dm, ex, nShots, shots, mem);
         auto ext_src = [&](int nb, long long slot, const float* F, int t) {
             if (offsets()) img_offset_fwd(nb, slot, ex, F, t);
@@ -2193,6 +2381,7 @@ struct Context {
     // Extended tomo adjoint (F/src/tomoExtShotsGpuFunctions.cu:797-910, legs :2442-2701).
     void tomo_adjoint(float* modelOut, int add, const float* extRefl, int nShots, const aio_shot* shots, int mem) {
         begin_call();
+        require_fp32_fields("tomo and WEMVA");
         Needs n;
         n.nWavefields = 2;
         n.ss = true;
@@ -2201,7 +2390,7 @@ struct Context {
         // subsurface offsets (tomoOffsetShotsAdjGpu, F/src/tomoExtShotsGpuFunctions.cu:912-1023): 2/v^3 only
         scale_shared(ex, g.nExt, offsets() ? 3 : (P.sloth ? 2 : 1));
         float* out = stage_out(modelOut, 1, add, mem);
-        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32 && !offsets()) {
+        if (tb_enabled() && !offsets()) {
             tomo_adjoint_tb(out, ex, nShots, shots, mem);
             write_model(modelOut, 1, add, mem, out);
             sync();
@@ -2243,6 +2432,7 @@ struct Context {
     // Extended WEMVA forward (F/src/wemvaExtShotsGpuFunctions.cu:344-456, legs :961-1122).
     void wemva_forward(const float* model, float* imageOut, int add, int nShots, const aio_shot* shots, int mem) {
         begin_call();
+        require_fp32_fields("tomo and WEMVA");
         Needs n;
         n.nWavefields = 2;
         n.ss = true;
@@ -2250,7 +2440,7 @@ struct Context {
         float* dm = stage_model(model, 1, mem, this->model);
         scale_shared(dm, 1, 0);
         float* out = stage_out(imageOut, g.nExt, add, mem);
-        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32 && !offsets()) {
+        if (tb_enabled() && !offsets()) {
             wemva_forward_tb(dm, out, nShots, shots, mem);
             write_model(imageOut, g.nExt, add, mem, out);
             sync();
@@ -2290,6 +2480,7 @@ struct Context {
     // Extended WEMVA adjoint (F/src/wemvaExtShotsGpuFunctions.cu:575-688, legs :1270-1426).
     void wemva_adjoint(float* modelOut, int add, const float* image, int nShots, const aio_shot* shots, int mem) {
         begin_call();
+        require_fp32_fields("tomo and WEMVA");
         Needs n;
         n.nWavefields = 2;
         n.ss = true;
@@ -2298,7 +2489,7 @@ struct Context {
         // subsurface offsets (wemvaOffsetShotsAdjGpu, F/src/wemvaExtShotsGpuFunctions.cu:689-810): 2/v^3 only
         scale_shared(im, g.nExt, offsets() ? 3 : 1);
         float* out = stage_out(modelOut, 1, add, mem);
-        if (tb_enabled() && P.wavefieldPrecision == AIO_WFLD_FP32 && !offsets()) {
+        if (tb_enabled() && !offsets()) {
             wemva_adjoint_tb(out, im, nShots, shots, mem);
             write_model(modelOut, 1, add, mem, out);
             sync();
@@ -2477,6 +2668,7 @@ AIO_API int aio_context_stats(aio_context* ctx, long long* kernels, double* step
     if (stepperPoints) *stepperPoints = ctx->c.stepPoints;
     return AIO_OK;
 }
+AIO_API long long aio_context_graph_replays(aio_context* ctx) { return ctx ? ctx->c.graphReplays : 0; }
 AIO_API int aio_context_reset_stats(aio_context* ctx) {
     ctx->c.kernels = 0;
     ctx->c.stepMs = 0.0;

@@ -13,7 +13,11 @@
 // stores each level once (damped once) and applies the second damping factor
 // when it reads p_old, which produces the same values with one store per point.
 #pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "aio_common.cuh"
+#include "aio_tb.cuh"
 
 namespace aio {
 
@@ -378,39 +382,54 @@ constexpr int LAG_K = 32;
 constexpr int LAG_B = 8;
 constexpr int LAG_NP = 128;  // threads per block (points), a compile-time shared-memory stride
 __host__ __device__ constexpr int lag_window_len(int hExt) { return LAG_K + 4 * hExt; }
+// Sample tau of a stored wavefield at element idx: FP32, BF16, or FP16 in units of the slice's
+// scale sc[tau] (the stored source wavefield of aio_tb.cuh).
+template <int WP>
+__device__ __forceinline__ float lag_wsample(const void* __restrict__ W, long long idx, const float* __restrict__ sc,
+                                             int tau) {
+    if (WP == TBW_F32) return __ldg(reinterpret_cast<const float*>(W) + idx);
+    const unsigned short u = __ldg(reinterpret_cast<const unsigned short*>(W) + idx);
+    if (WP == TBW_BF16) return __bfloat162float(__ushort_as_bfloat16(u));
+    return __half2float(__ushort_as_half(u)) * __ldg(sc + tau);
+}
 // W slices tlo-2h .. of point p into this thread's shared column, zero outside [0, nts). The
 // column holds consecutive samples in pairs (one float2 per pair): every lag offset 2h - 2(e-h)
 // is even, so sample pairs (k, k+1) of any lag are one aligned float2 and the inner products
-// run on paired FP32 instructions.
-__device__ __forceinline__ void lag_window(float2* W2, const float* __restrict__ W, long long isz, long long p, int tlo,
-                                           int hExt, int nts) {
+// run on paired FP32 instructions. W is stored in FP32, BF16 or FP16 with per-slice scales sc.
+template <int WP = TBW_F32>
+__device__ __forceinline__ void lag_window(float2* W2, const void* __restrict__ W, const float* __restrict__ sc,
+                                           long long isz, long long p, int tlo, int hExt, int nts) {
     const int n = lag_window_len(hExt), t0 = tlo - 2 * hExt;
     for (int k0 = 0; k0 < n; k0 += 2 * LAG_B) {
         float v[2 * LAG_B];
 #pragma unroll
         for (int j = 0; j < 2 * LAG_B; j++) {
             const int tau = t0 + k0 + j;
-            v[j] = (k0 + j < n && tau >= 0 && tau < nts) ? __ldg(W + (long long)tau * isz + p) : 0.f;
+            v[j] = (k0 + j < n && tau >= 0 && tau < nts) ? lag_wsample<WP>(W, (long long)tau * isz + p, sc, tau) : 0.f;
         }
 #pragma unroll
         for (int j = 0; j < 2 * LAG_B; j += 2)
             if (k0 + j < n) W2[((k0 + j) >> 1) * LAG_NP] = make_float2(v[j], v[j + 1]);
     }
 }
-template <typename Acc>
+// W: stored wavefield of WSt elements per shot (FP32, or BF16 / FP16 with nts scales per shot
+// in wsc when WP says so).
+template <typename Acc, int WP = TBW_F32>
 __global__ void __launch_bounds__(LAG_NP) k_img_lag_block(Acc* __restrict__ img, long long mSt, const float* __restrict__ R,
-                                                          long long rSt, int rRing, const float* __restrict__ W,
+                                                          long long rSt, int rRing, const void* __restrict__ W,
                                                           long long WSt, long long isz, int tlo, int thi, int nts,
-                                                          int hExt, int nExt, int sign) {
+                                                          int hExt, int nExt, int sign,
+                                                          const float* __restrict__ wsc = nullptr) {
     extern __shared__ float2 lag_smem2[];
     const int b = blockIdx.y, tid = threadIdx.x;
     const long long p = (long long)blockIdx.x * LAG_NP + tid;
     if (p >= isz) return;
     R += b * rSt;
-    W += b * WSt;
+    const void* Wb = reinterpret_cast<const char*>(W) + b * WSt * (WP == TBW_F32 ? 4 : 2);
+    const float* scb = WP == TBW_F16 ? wsc + (long long)b * nts : nullptr;
     img += b * mSt;
     float2* W2 = lag_smem2 + tid;
-    lag_window(W2, W, isz, p, tlo, hExt, nts);
+    lag_window<WP>(W2, Wb, scb, isz, p, tlo, hExt, nts);
     float2 r2[LAG_K / 2];
     int slot = tlo % rRing;  // ring slot of sample tlo; the block's slots follow with one wrap at most
 #pragma unroll
@@ -450,18 +469,21 @@ __global__ void __launch_bounds__(LAG_NP) k_img_lag_block(Acc* __restrict__ img,
 // the block live in shared memory (own column only, zero outside [0, nts)), so W is read once
 // per block, and ext once per block (lags outer, the block's samples accumulated in registers,
 // in lag order, two samples per paired instruction).
+template <int WP = TBW_F32>
 __global__ void __launch_bounds__(LAG_NP) k_ss_lag_block(float* __restrict__ ss, long long ssSt, int ring,
-                                                         const float* __restrict__ ext, const float* __restrict__ W,
+                                                         const float* __restrict__ ext, const void* __restrict__ W,
                                                          long long WSt, long long isz, int tlo, int thi, int nts,
-                                                         int hExt, int nExt, int sign) {
+                                                         int hExt, int nExt, int sign,
+                                                         const float* __restrict__ wsc = nullptr) {
     extern __shared__ float2 lag_smem2[];
     const int b = blockIdx.y, tid = threadIdx.x;
     const long long p = (long long)blockIdx.x * LAG_NP + tid;
     if (p >= isz) return;
     ss += b * ssSt;
-    W += b * WSt;
+    const void* Wb = reinterpret_cast<const char*>(W) + b * WSt * (WP == TBW_F32 ? 4 : 2);
+    const float* scb = WP == TBW_F16 ? wsc + (long long)b * nts : nullptr;
     float2* W2 = lag_smem2 + tid;
-    lag_window(W2, W, isz, p, tlo, hExt, nts);
+    lag_window<WP>(W2, Wb, scb, isz, p, tlo, hExt, nts);
     float2 acc[LAG_K / 2];
 #pragma unroll
     for (int k = 0; k < LAG_K / 2; k++) acc[k] = make_float2(0.f, 0.f);

@@ -22,6 +22,8 @@
 #include <cstring>
 #include <mutex>
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "aio_b200.h"

@@ -54,6 +54,7 @@ struct TBShot {
     float* wscale;        // [nts] value of one FP16 unit of slice t
     float* wstage;        // [2][isz] FP32 slices its and its+1 being accumulated (SRC)
     unsigned* wmax;       // [nts] max |W| of slice t as float bits (SRC)
+    unsigned* wover;      // set to 1 when a slice stored with a speculative scale overflowed FP16 (SRC)
     float* rcoarse;       // ADJR / SCATW / ADJX: slices of coarse samples written by the launch
 };
 

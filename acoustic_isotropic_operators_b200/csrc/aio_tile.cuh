@@ -73,6 +73,7 @@ struct KTArgs {
     int rSlot, rSlot0;     // ADJR: ring slots of R(its+1) and (its == 0) R(0);
                            // SCATX / SCATW / ADJX: slices of W holding the sources at its, its+1
     int oA, oB;            // SCATW / ADJX: slices of rcoarse receiving the samples its, its+1
+    int f16spec;           // FP16 source pass: store slices with the speculative scale where allowed
 };
 
 // Per-thread staging slots (16 bytes each) filled by asynchronous copies: level-1 operands
@@ -157,6 +158,24 @@ __device__ __forceinline__ float kt_f16_scale(unsigned maxBits) {
     const float m = __uint_as_float(maxBits);
     return m > 0.f ? m * (1.f / 32768.f) : 1.f;
 }
+// Speculative FP16 unit of slice t from the finished slice t-1 (max bits prevBits): the power of
+// two 2^(e - 11) for a previous max in [2^e, 2^(e+1)), which maps that max into [2^11, 2^12).
+// FP16 keeps 11 significant bits over its whole normal range, so this scale loses no precision
+// against the exact one; it leaves headroom for slice t to grow 16x (up to 65504) before an
+// overflow, which the source pass flags so the pass is run again with exact scales. Usable when
+// the previous max is a normal float of at least 2^-115 (then the unit is a normal float too).
+__host__ __device__ __forceinline__ bool kt_f16_spec_ok(unsigned prevBits) {
+    const unsigned e = (prevBits >> 23) & 0xffu;
+    return e >= 12u && e < 255u;
+}
+__device__ __forceinline__ float kt_f16_spec_scale(unsigned prevBits) {
+    return __uint_as_float((((prevBits >> 23) & 0xffu) - 11u) << 23);
+}
+// slice t of a source pass was stored directly with the speculative scale (else staged in FP32
+// and quantized with its exact max); slice 0 and the last slice are always staged
+__device__ __forceinline__ bool kt_f16_spec_slice(const unsigned* wmax, int t, int nts, int spec) {
+    return spec && t >= 1 && t <= nts - 2 && kt_f16_spec_ok(wmax[t - 1]);
+}
 // quantize four FP32 samples to FP16 units of `sc`
 __device__ __forceinline__ uint2 kt_f16_pack(const float4& v, float sc) {
     const float inv = 1.f / sc;
@@ -183,13 +202,17 @@ __device__ __forceinline__ void kt_f16_quantize(const TBShot& sh, long long wStr
     }
 }
 
-// Finishes the last two slices (nts-2, nts-1) of an FP16 source pass and records the scales.
-__global__ void k_f16_finish(const TBShot* shots, long long wStride, int ip, int nzi, int nxi, int nts) {
+// Finishes the last two slices (nts-2, nts-1) of an FP16 source pass (those staged in FP32) and
+// records every slice's scale: the speculative one where the slice was stored directly.
+__global__ void k_f16_finish(const TBShot* shots, long long wStride, int ip, int nzi, int nxi, int nts, int spec) {
     const TBShot sh = shots[blockIdx.y];
     const int nthr = gridDim.x * blockDim.x, tid = blockIdx.x * blockDim.x + threadIdx.x;
-    for (int t = nts - 2; t < nts; t++) kt_f16_quantize(sh, wStride, ip, t, 0, nzi, 0, nxi, tid, nthr);
+    for (int t = nts - 2; t < nts; t++)
+        if (!kt_f16_spec_slice(sh.wmax, t, nts, spec)) kt_f16_quantize(sh, wStride, ip, t, 0, nzi, 0, nxi, tid, nthr);
     if (tid == 0)
-        for (int t = 0; t < nts; t++) sh.wscale[t] = kt_f16_scale(sh.wmax[t]);
+        for (int t = 0; t < nts; t++)
+            sh.wscale[t] = kt_f16_spec_slice(sh.wmax, t, nts, spec) ? kt_f16_spec_scale(sh.wmax[t - 1])
+                                                                    : kt_f16_scale(sh.wmax[t]);
 }
 
 __device__ __forceinline__ float4 kt_ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
@@ -399,8 +422,13 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
             }
         }
     };
-    if (WPREC == TBW_F16 && MODE == TB_SRC && its > 0) {
-        // slice its-1 is complete (previous launch): quantize this CTA's output region of it
+    // FP16 source pass: slice its is stored directly with the speculative scale of slice its-1's
+    // max when that max allows it (the same decision in every CTA), else staged in FP32
+    const bool f16Spec = WPREC == TBW_F16 && MODE == TB_SRC && kt_f16_spec_slice(sh.wmax, its, g.nts, a.f16spec);
+    const float f16Sc = f16Spec ? kt_f16_spec_scale(sh.wmax[its - 1]) : 1.f;
+    if (WPREC == TBW_F16 && MODE == TB_SRC && its > 0 && !kt_f16_spec_slice(sh.wmax, its - 1, g.nts, a.f16spec)) {
+        // slice its-1 was staged and is complete (previous launch): quantize this CTA's output
+        // region of it with its exact max
         kt_f16_quantize(sh, a.wStride, ip, its - 1, z0, min(z0 + a.HZ, nzi), x0, x1, tid, blockDim.x);
         __syncthreads();  // the region's staging slots are rewritten below (slice its+1 at the end)
     }
@@ -408,6 +436,9 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
     kt_commit();
     kt_wait<0>();
     __syncthreads();
+    // FP16 source pass: max |W| of this thread's points of slice its (and its+1 at the end),
+    // folded into the slice maxima once per warp after the last iteration
+    float wmaxA = 0.f, wmaxB = 0.f;
 
     for (int k = 0; k < a.iters; k++) {
         const int B = xs + KT_BX * k;
@@ -655,15 +686,22 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
                     }
                     kt_st4(pPartOut + idx, wb);
                     if (WPREC == TBW_F16) {
-                        // FP32 slice its (and its+1 at the end) into the staging buffer; the
-                        // next launch (or k_f16_finish) quantizes it with the slice's exact max
-                        kt_st4(sh.wstage + (long long)(its & 1) * a.wStride + idx, wa);
+                        // slice its: FP16 with the speculative scale, or FP32 into the staging
+                        // buffer (the next launch or k_f16_finish quantizes it with the slice's
+                        // exact max); slice its+1 at the end is always staged
                         float m = fmaxf(fmaxf(fabsf(wa[0]), fabsf(wa[1])), fmaxf(fabsf(wa[2]), fabsf(wa[3])));
-                        if (m > 0.f) atomicMax(sh.wmax + its, __float_as_uint(m));
+                        if (f16Spec) {
+                            *reinterpret_cast<uint2*>((unsigned short*)sh.W + (long long)its * a.wStride + idx) =
+                                kt_f16_pack(make_float4(wa[0], wa[1], wa[2], wa[3]), f16Sc);
+                            if (m >= 65504.f * f16Sc) atomicOr(sh.wover, 1u);  // FP16 overflow: redo exactly
+                        } else {
+                            kt_st4(sh.wstage + (long long)(its & 1) * a.wStride + idx, wa);
+                        }
+                        wmaxA = fmaxf(wmaxA, m);
                         if (its == g.nts - 2) {
                             kt_st4(sh.wstage + (long long)((its + 1) & 1) * a.wStride + idx, wb);
                             m = fmaxf(fmaxf(fabsf(wb[0]), fabsf(wb[1])), fmaxf(fabsf(wb[2]), fabsf(wb[3])));
-                            if (m > 0.f) atomicMax(sh.wmax + its + 1, __float_as_uint(m));
+                            wmaxB = fmaxf(wmaxB, m);
                         }
                     } else {
                         kt_wstore4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, its), idx, wa);
@@ -756,6 +794,15 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
         }
         kt_wait<0>();     // the next input block and level-1 operands have landed
         __syncthreads();  // ... for every thread; outputs done before level 1 reuses ring slots
+    }
+    if (WPREC == TBW_F16 && MODE == TB_SRC) {
+        // non-negative floats order like their bit patterns: one warp max, one atomic per warp
+        const unsigned ma = __reduce_max_sync(0xffffffffu, __float_as_uint(wmaxA));
+        const unsigned mb = __reduce_max_sync(0xffffffffu, __float_as_uint(wmaxB));
+        if ((tid & 31) == 0) {
+            if (ma) atomicMax(sh.wmax + its, ma);
+            if (mb) atomicMax(sh.wmax + its + 1, mb);
+        }
     }
 }
 

@@ -276,7 +276,8 @@ def run_ext(args, emit=True):
     rng = np.random.default_rng(4)
     shots = [Shot(a.src_pos, a.rec_pos, sg, (rng.standard_normal((len(a.rec_pos), w.nts)) * 1e-3).astype(np.float32))
              for a, sg in zip(w.shots, sigs)]
-    ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs, nExt=n_ext, image_fp64=True)
+    ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs, nExt=n_ext, image_fp64=True,
+                  wavefield=args.wavefield)
     ctx.born_ext_adjoint(shots)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -284,9 +285,11 @@ def run_ext(args, emit=True):
     t = time.perf_counter() - t0
     n, steps, T = w.n_interior, w.fine_steps, w.nts - 1
     pts = n * steps * 2 * len(shots)
-    algo = len(shots) * n * (2 * 16 * steps + 4 * w.nts + (4 + 4) * T + 8 * n_ext)
+    wb = 4 if args.wavefield == "fp32" else 2
+    algo = len(shots) * n * (2 * 16 * steps + wb * w.nts + (4 + wb) * T + 8 * n_ext)
     peak, src = hbm_peak()
-    out = {"impl": "this engine, extended Born adjoint (blocked stepper, blocked lag imaging, FP32 W)",
+    out = {"impl": f"this engine, extended Born adjoint (blocked stepper, blocked lag imaging, "
+                   f"{args.wavefield.upper()} stored W)", "wavefield": args.wavefield,
            "metric": "Gpts/s, extended (time-lag) Born adjoint", "value": pts / t / 1e9, "unit": UNIT,
            "seconds": t, "shots": len(shots), "shots_per_s": len(shots) / t, "nExt": n_ext,
            "interior": [w.nz - 10, w.nx - 10], "nts": w.nts,
@@ -463,9 +466,10 @@ def other_configs(args, batched_value):
     plain = run_plain(a, emit=False)
     plain["batched_over_plain"] = batched_value / plain["value"]
     out["plain_one_shot_per_call"] = plain
-    a = copy.copy(args)
-    a.ext, a.nts = 64, 2000
-    out["extended_born_adjoint_64_shots"] = run_ext(a, emit=False)
+    for wf in ("fp32", "fp16", "bf16"):
+        a = copy.copy(args)
+        a.ext, a.nts, a.wavefield = 64, 2000, wf
+        out[f"extended_born_adjoint_64_shots_{wf}"] = run_ext(a, emit=False)
     a = copy.copy(args)
     a.tomo, a.tomo_nts, a.stepper = 2, 3000, "auto"
     out["tomo_wemva_2_shots"] = run_tomo(a, emit=False)

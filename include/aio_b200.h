@@ -117,6 +117,12 @@ int aio_context_profile(aio_context* ctx, int sampleEvery);
 int aio_context_stats(aio_context* ctx, long long* kernels, double* stepperMs, long long* stepperTimed,
                       double* stepperPoints);
 int aio_context_reset_stats(aio_context* ctx);
+/* Interval loops replayed from CUDA graphs since the context was created. A blocked pass's
+ * per-interval launches run directly the first time a (plan, buffers) key is seen, are captured
+ * into a CUDA graph the second time and replayed from it afterwards; AIO_GRAPHS=0 in the
+ * environment (read at context creation) and live stepper timing (aio_context_profile) keep the
+ * direct launches. */
+long long aio_context_graph_replays(aio_context* ctx);
 
 /* Nonlinear: model = source traces (sourcesSignals), data per shot. */
 int aio_nonlinear_forward(aio_context* ctx, int nShots, const aio_shot* shots, int memSpace);
