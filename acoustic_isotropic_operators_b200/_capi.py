@@ -60,7 +60,7 @@ EXPORTED = [
     "aio_BornTimeShotsFwdGpuWavefield", "aio_BornOffsetShotsFwdGpuWavefield", "aio_BornTimeShotsFwdFsGpuWavefield",
     "aio_BornOffsetShotsFwdFsGpuWavefield", "aio_BornTimeShotsAdjGpuWavefield", "aio_BornOffsetShotsAdjGpuWavefield",
     "aio_BornTimeShotsAdjFsGpuWavefield", "aio_BornOffsetShotsAdjFsGpuWavefield",
-    "aio_dot_f64", "aio_context_graph_replays",
+    "aio_dot_f64", "aio_context_graph_replays", "aio_context_set_budget",
 ]
 
 
@@ -104,6 +104,7 @@ def lib():
         L.aio_context_wave_capacity.argtypes = [C.c_void_p, C.c_int]
         L.aio_context_stream.restype = C.c_void_p
         L.aio_context_stream.argtypes = [C.c_void_p]
+        L.aio_context_set_budget.argtypes = [C.c_void_p, C.c_longlong]
         L.aio_context_graph_replays.restype = C.c_longlong
         L.aio_context_graph_replays.argtypes = [C.c_void_p]
         L.aio_dot_f64.argtypes = [C.c_int, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p,

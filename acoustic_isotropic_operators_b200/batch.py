@@ -78,6 +78,10 @@ class Context:
     def last_launches(self) -> int:
         return int(A.lib().aio_context_last_launches(self._h))
 
+    def set_budget(self, nbytes: int) -> None:
+        """Device-memory budget for shot buffers from now on (<= 0: 93 % of free memory)."""
+        A.check(A.lib().aio_context_set_budget(self._h, int(nbytes)))
+
     def capacity(self, family: int) -> int:
         return int(A.lib().aio_context_wave_capacity(self._h, family))
 

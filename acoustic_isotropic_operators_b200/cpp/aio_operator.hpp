@@ -7,6 +7,10 @@
 #include <iomanip>
 #include <iostream>
 #include <memory>
+#include <stdexcept>
+#include <string>
+
+#include "aio_b200.h"
 
 template <class V1, class V2>
 class Operator {
@@ -29,7 +33,9 @@ class Operator {
     }
 
     // <F m, d> against <m, F* d> for random m and d, without and with add; relative
-    // error of each pair must not exceed maxError. Dot products accumulate in FP64.
+    // error of each pair must not exceed maxError. The inner products accumulate in FP64: for the
+    // GPU operators (dotTestDevice() >= 0) exact FP64 products reduced on that GPU in a fixed
+    // order (aio_dot_f64), for host operators on the host.
     bool dotTest(const bool verbose = false, const float maxError = .00001f) const {
         auto m1 = _domain->clone(), m2 = _domain->clone();
         auto d1 = _range->clone(), d2 = _range->clone();
@@ -37,11 +43,11 @@ class Operator {
         d1->random();
         forward(false, m1, d2);
         adjoint(false, m2, d1);
-        const double a1 = d1->dot(d2), b1 = m1->dot(m2);
+        const double a1 = gpuDot(d1, d2), b1 = gpuDot(m1, m2);
         const double eNoAdd = std::fabs((a1 - b1) / b1);
         forward(true, m1, d2);
         adjoint(true, m2, d1);
-        const double a2 = d1->dot(d2), b2 = m1->dot(m2);
+        const double a2 = gpuDot(d1, d2), b2 = gpuDot(m1, m2);
         const double eAdd = std::fabs((a2 - b2) / b2);
         if (verbose) {
             std::cout << std::setprecision(16) << "WITHOUT ADD: <F m, d> = " << a1 << ", <m, F* d> = " << b1
@@ -52,6 +58,10 @@ class Operator {
         return eNoAdd <= maxError && eAdd <= maxError;
     }
 
+    // GPU of the dot-product test's reductions (the shot operators: their first GPU), or -1 for
+    // host reductions (host operators such as deviceGpu)
+    virtual int dotTestDevice() const { return -1; }
+
     void setDomainRange(const std::shared_ptr<V1> dom, const std::shared_ptr<V2> rng) {
         _domain = dom->cloneSpace();
         _range = rng->cloneSpace();
@@ -61,6 +71,17 @@ class Operator {
 
   protected:
     Operator() = default;
+
+    template <class V>
+    double gpuDot(const std::shared_ptr<V>& a, const std::shared_ptr<V>& b) const {
+        if (dotTestDevice() < 0) return a->dot(b);
+        double r = 0.0;
+        const long long n = a->getHyper()->getN123();
+        if (n != b->getHyper()->getN123()) throw std::runtime_error("dotTest: vectors of different sizes");
+        if (aio_dot_f64(dotTestDevice(), AIO_MEM_HOST, n, a->getVals(), b->getVals(), &r) != AIO_OK)
+            throw std::runtime_error("dotTest: FP64 reduction on the GPU failed");
+        return r;
+    }
 
   private:
     std::shared_ptr<V1> _domain;

@@ -551,6 +551,8 @@ class ShotLoop {
 // (F/src/nonlinearPropShotsGpu.cpp, F/src/nonlinearPropGpu.cpp).
 class nonlinearPropShotsGpu : public Operator<SEP::float3DReg, SEP::float3DReg>, public aio_ops::ShotLoop {
   public:
+    // the dot-product test reduces on the first GPU of the operator's list
+    int dotTestDevice() const override { return _gpuList.empty() || _gpuList[0] < 0 ? 0 : _gpuList[0]; }
     nonlinearPropShotsGpu(std::shared_ptr<SEP::float2DReg> vel, std::shared_ptr<paramObj> par,
                           std::vector<std::shared_ptr<deviceGpu>> sourcesVector,
                           std::vector<std::shared_ptr<deviceGpu>> receiversVector)
@@ -758,6 +760,8 @@ class BornFamily : public ShotLoop {
 // Born: model [nx][nz] -> data [nShot][nRecIrreg][nts] (F/src/BornShotsGpu.cpp, F/src/BornGpu.cpp).
 class BornShotsGpu : public Operator<SEP::float2DReg, SEP::float3DReg>, public aio_ops::BornFamily<SEP::float2DReg> {
   public:
+    // the dot-product test reduces on the first GPU of the operator's list
+    int dotTestDevice() const override { return _gpuList.empty() || _gpuList[0] < 0 ? 0 : _gpuList[0]; }
     BornShotsGpu(std::shared_ptr<SEP::float2DReg> vel, std::shared_ptr<paramObj> par,
                  std::vector<std::shared_ptr<deviceGpu>> sourcesVector,
                  std::vector<std::shared_ptr<SEP::float2DReg>> sourcesSignalsVector,
@@ -824,6 +828,8 @@ class BornShotsGpu : public Operator<SEP::float2DReg, SEP::float3DReg>, public a
 // Extended (time-lag) Born: model [nExt][nx][nz] -> data (F/src/BornExtShotsGpu.cpp).
 class BornExtShotsGpu : public Operator<SEP::float3DReg, SEP::float3DReg>, public aio_ops::BornFamily<SEP::float3DReg> {
   public:
+    // the dot-product test reduces on the first GPU of the operator's list
+    int dotTestDevice() const override { return _gpuList.empty() || _gpuList[0] < 0 ? 0 : _gpuList[0]; }
     BornExtShotsGpu(std::shared_ptr<SEP::float2DReg> vel, std::shared_ptr<paramObj> par,
                     std::vector<std::shared_ptr<deviceGpu>> sourcesVector,
                     std::vector<std::shared_ptr<SEP::float2DReg>> sourcesSignalsVector,
@@ -891,6 +897,8 @@ class BornExtShotsGpu : public Operator<SEP::float3DReg, SEP::float3DReg>, publi
 // [nExt][nx][nz] (F/src/tomoExtShotsGpu.cpp).
 class tomoExtShotsGpu : public Operator<SEP::float2DReg, SEP::float3DReg>, public aio_ops::BornFamily<SEP::float2DReg> {
   public:
+    // the dot-product test reduces on the first GPU of the operator's list
+    int dotTestDevice() const override { return _gpuList.empty() || _gpuList[0] < 0 ? 0 : _gpuList[0]; }
     tomoExtShotsGpu(std::shared_ptr<SEP::float2DReg> vel, std::shared_ptr<paramObj> par,
                     std::vector<std::shared_ptr<deviceGpu>> sourcesVector,
                     std::vector<std::shared_ptr<SEP::float2DReg>> sourcesSignalsVector,
@@ -939,6 +947,8 @@ class tomoExtShotsGpu : public Operator<SEP::float2DReg, SEP::float3DReg>, publi
 // observed data of every shot driving the receiver wavefield (F/src/wemvaExtShotsGpu.cpp).
 class wemvaExtShotsGpu : public Operator<SEP::float2DReg, SEP::float3DReg>, public aio_ops::BornFamily<SEP::float2DReg> {
   public:
+    // the dot-product test reduces on the first GPU of the operator's list
+    int dotTestDevice() const override { return _gpuList.empty() || _gpuList[0] < 0 ? 0 : _gpuList[0]; }
     wemvaExtShotsGpu(std::shared_ptr<SEP::float2DReg> vel, std::shared_ptr<paramObj> par,
                      std::vector<std::shared_ptr<deviceGpu>> sourcesVector,
                      std::vector<std::shared_ptr<SEP::float2DReg>> sourcesSignalsVector,

@@ -2669,6 +2669,21 @@ AIO_API int aio_context_stats(aio_context* ctx, long long* kernels, double* step
     return AIO_OK;
 }
 AIO_API long long aio_context_graph_replays(aio_context* ctx) { return ctx ? ctx->c.graphReplays : 0; }
+AIO_API int aio_context_set_budget(aio_context* ctx, long long bytes) {
+    return guard([&] {
+        require(ctx != nullptr, "context is NULL");
+        Context& c = ctx->c;
+        AIO_CK(cudaSetDevice(c.dev));
+        if (bytes > 0) {
+            c.budget = bytes;
+        } else {
+            size_t fr = 0, tot = 0;
+            AIO_CK(cudaMemGetInfo(&fr, &tot));
+            c.budget = (long long)(0.93 * (double)fr);
+        }
+        c.P.memBudgetBytes = bytes > 0 ? bytes : 0;
+    });
+}
 AIO_API int aio_context_reset_stats(aio_context* ctx) {
     ctx->c.kernels = 0;
     ctx->c.stepMs = 0.0;

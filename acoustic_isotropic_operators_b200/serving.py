@@ -74,21 +74,42 @@ class Request:
         return (self.op, self.grid, self.velocity_id, self.model_id if self.op == "born_forward" else "")
 
 
+def _slices(g: Grid):
+    """(interior slice, halo slice) sizes in floats, as the engine lays them out."""
+    nzi, nxi = g.nz - 10, g.nx - 10
+    isz = ((nzi + 31) // 32 * 32) * nxi
+    hsz = (32 + (nzi + 31) // 32 * 32 + 32) * ((nxi + 31) // 32 * 32 + 10)
+    return isz, hsz
+
+
 def shot_bytes(req: Request, wavefield_bytes: int = 4) -> int:
-    """Device memory one shot of `req` needs in a batch (state, partial sums, stored wavefield, image)."""
+    """Device memory one shot of `req` takes in a wave of the blocked stepper: the engine's own
+    per-shot figure (state and partial-sum slices, stored wavefield and, for FP16, its staging and
+    scales, FP64 image, traces, halo levels), so that server and engine plan with one number."""
     g = req.grid
-    isz = ((g.nz - 10 + 31) // 32 * 32) * (g.nx - 10)
-    b = 4 * isz * 4 + 2 * isz * 4                       # 4 state slices + 2 partial-sum slices
-    if req.op != "nonlinear_forward":
-        b += g.nts * isz * wavefield_bytes              # stored source wavefield
+    isz, hsz = _slices(g)
+    wavefield = req.op != "nonlinear_forward"
+    b = 6 * isz * 4 + 2 * hsz * 4 + 2 * isz * 4 + (1 << 16)
+    if wavefield:
+        b += g.nts * isz * wavefield_bytes
+        if wavefield_bytes == 2:
+            b += 2 * isz * 4 + 8 * g.nts
     if req.op == "born_adjoint":
-        b += isz * 8                                    # FP64 image
-    b += (len(req.shot.src_pos) * g.ntw + 2 * len(req.shot.rec_pos) * g.nts) * 4
+        b += isz * 8
+    b += len(req.shot.src_pos) * g.ntw * 4 + 2 * len(req.shot.rec_pos) * g.nts * 4
     return b
 
 
-def _engine_batch(ctx_cache: Dict, worker: int, reqs: List[Request], device: int, wavefield: str):
-    """Run one batch on this worker's context for the batch's grid (created on first use)."""
+def batch_shared_bytes(g: Grid) -> int:
+    """Device memory a wave needs besides its shots (the engine's shared figure)."""
+    isz, _ = _slices(g)
+    return 4 * isz * 4 + (64 << 20)
+
+
+def _engine_batch(ctx_cache: Dict, worker: int, reqs: List[Request], device: int, wavefield: str,
+                  reserved: int = 0):
+    """Run one batch on this worker's context for the batch's grid (created on first use), with
+    the context's device-memory budget set to the bytes the server reserved for the batch."""
     from .batch import Context
     r0 = reqs[0]
     g = r0.grid
@@ -96,8 +117,10 @@ def _engine_batch(ctx_cache: Dict, worker: int, reqs: List[Request], device: int
     ctx = ctx_cache.get(key)
     if ctx is None:
         ctx = Context(g.nz, g.nx, g.nts, g.dts, g.sub, g.dz, g.dx, g.minPad, r0.vel2dtw2, r0.refl_scale,
-                      image_fp64=True, device=device, wavefield=wavefield)
+                      image_fp64=True, device=device, wavefield=wavefield, mem_budget_bytes=max(reserved, 1))
         ctx_cache[key] = ctx
+    if reserved > 0:
+        ctx.set_budget(reserved)
     shots = [r.shot for r in reqs]
     if r0.op == "nonlinear_forward":
         return ctx.nonlinear_forward(shots)
@@ -126,12 +149,15 @@ class Server:
         self.budget = int(mem_budget_bytes)
         self.in_use = 0
         self._ctx: Dict = {}
-        self._run = run_batch or (lambda w, reqs: _engine_batch(self._ctx, w, reqs, device, wavefield))
+        self._engine = run_batch is None
+        self._run = run_batch or (lambda w, reqs, reserved=0: _engine_batch(self._ctx, w, reqs, device, wavefield,
+                                                                               reserved))
         self._queue: deque = deque()
         self._idle = list(range(workers))
         self._lock = threading.Condition()
         self._closing = False
         self.finished: List[Request] = []
+        self._reserved: Dict[int, int] = {}    # bytes reserved per running batch (by its head request)
         self.batches: List[Tuple[int, int]] = []   # (worker, batch size)
         self._threads: List[threading.Thread] = []
         self._sched = threading.Thread(target=self._schedule, daemon=True)
@@ -141,7 +167,7 @@ class Server:
     def submit(self, req: Request) -> Future:
         if req.op not in OPS:
             raise ValueError(f"unknown operator {req.op!r}")
-        need = shot_bytes(req, self.wbytes)
+        need = batch_shared_bytes(req.grid) + shot_bytes(req, self.wbytes)
         if need > self.budget:
             raise ValueError(f"request needs {need} bytes, above the budget of {self.budget}")
         with self._lock:
@@ -166,7 +192,7 @@ class Server:
     def _take_batch(self) -> Optional[List[Request]]:
         """Oldest waiting request plus compatible waiting ones that fit in free memory."""
         head = self._queue[0]
-        need = shot_bytes(head, self.wbytes)
+        need = batch_shared_bytes(head.grid) + shot_bytes(head, self.wbytes)
         if self.in_use + need > self.budget:
             return None                                   # wait for memory; no overtaking of the head
         batch, used = [head], need
@@ -182,6 +208,7 @@ class Server:
         for r in batch:
             self._queue.remove(r)
         self.in_use += used
+        self._reserved[id(batch[0])] = used
         return batch
 
     def _schedule(self):
@@ -205,13 +232,14 @@ class Server:
         for r in batch:
             r.start = t0
         err = None
+        reserved = self._reserved[id(batch[0])]
         try:
-            results = self._run(w, batch)
+            results = self._run(w, batch, reserved) if self._engine else self._run(w, batch)
         except Exception as e:  # reported through every future of the batch
             err, results = e, [None] * len(batch)
         t1 = time.perf_counter()
         with self._lock:
-            self.in_use -= sum(shot_bytes(r, self.wbytes) for r in batch)
+            self.in_use -= self._reserved.pop(id(batch[0]))
             self._idle.append(w)
             self.batches.append((w, len(batch)))
             for r, res in zip(batch, results):

@@ -99,6 +99,10 @@ int aio_context_create(const aio_params* params, const float* vel2Dtw2, const fl
 int aio_context_destroy(aio_context* ctx);
 /* Replace the velocity-derived fields (reference setVel + fdParam precompute). */
 int aio_context_set_velocity(aio_context* ctx, const float* vel2Dtw2, const float* reflectivityScale);
+/* Device-memory budget for the context's shot buffers from now on (bytes; <= 0: 93 % of the
+ * device's free memory, sampled now). A server that admits work by its own HBM budget hands each
+ * context the bytes it reserved for that context's batch, so both plan with the same number. */
+int aio_context_set_budget(aio_context* ctx, long long bytes);
 /* Maximum number of shots one wave can hold for operator `family` under the memory budget. */
 int aio_context_wave_capacity(aio_context* ctx, int family);
 /* Number of stepper launches issued by the most recent operator call. */

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from acoustic_isotropic_operators_b200.batch import Shot
-from acoustic_isotropic_operators_b200.serving import Grid, Request, Server, shot_bytes
+from acoustic_isotropic_operators_b200.serving import Grid, Request, Server, batch_shared_bytes, shot_bytes
 
 
 def req(op, grid, tag, vid="v0"):
@@ -62,7 +62,7 @@ def test_batches_compatible_requests_and_keeps_fifo_head():
 
 def test_memory_budget_limits_concurrency():
     eng = FakeEngine(delay=0.1)
-    one = shot_bytes(req("born_adjoint", G2, 0))
+    one = batch_shared_bytes(G2) + shot_bytes(req("born_adjoint", G2, 0))  # one single-shot batch
     srv = Server(workers=4, max_batch=1, mem_budget_bytes=2 * one, run_batch=eng)
     futs = [srv.submit(req("born_adjoint", G2, i, vid=f"v{i}")) for i in range(6)]
     [f.result(timeout=10) for f in futs]
