@@ -61,6 +61,8 @@ EXPORTED = [
     "aio_BornOffsetShotsFwdFsGpuWavefield", "aio_BornTimeShotsAdjGpuWavefield", "aio_BornOffsetShotsAdjGpuWavefield",
     "aio_BornTimeShotsAdjFsGpuWavefield", "aio_BornOffsetShotsAdjFsGpuWavefield",
     "aio_dot_f64", "aio_context_graph_replays", "aio_context_set_budget",
+    "aio_tomo_ext_forward_wavefield", "aio_tomo_ext_adjoint_wavefield", "aio_wemva_ext_forward_wavefield",
+    "aio_wemva_ext_adjoint_wavefield",
 ]
 
 

@@ -226,6 +226,53 @@ class Context:
                                                        A.fptr(rec)))
         return out, src, rec
 
+    def _w3(self):
+        return [np.zeros((self.nts, self.nx, self.nz), np.float32) for _ in range(3)]
+
+    def tomo_forward_wavefield(self, model, ext_reflectivity, shot: Shot):
+        """Tomo forward of one shot: (data, d2/dt2 of the source wavefield, the last leg's first
+        and second scattered wavefields), the wavefields (nts, nx, nz) with a zero FAT ring."""
+        m = self._model(model, 1)
+        e = self._model(ext_reflectivity, self.nExt)
+        arr = self._shots([shot], data_out=True)
+        W = self._w3()
+        A.check(A.lib().aio_tomo_ext_forward_wavefield(self._h, A.fptr(m), A.fptr(e), arr, A.AIO_MEM_HOST,
+                                                       *[A.fptr(x) for x in W]))
+        return (shot.data, *W)
+
+    def tomo_adjoint_wavefield(self, ext_reflectivity, shot: Shot):
+        """Tomo adjoint of one shot: (model, d2/dt2 of the source wavefield, receiver wavefield, the
+        last leg's scattered coarse samples)."""
+        out = np.zeros((self.nx, self.nz), np.float32)
+        e = self._model(ext_reflectivity, self.nExt)
+        arr = self._shots([shot], data_out=False)
+        W = self._w3()
+        A.check(A.lib().aio_tomo_ext_adjoint_wavefield(self._h, A.fptr(out), 0, A.fptr(e), arr, A.AIO_MEM_HOST,
+                                                       *[A.fptr(x) for x in W]))
+        return (out, *W)
+
+    def wemva_forward_wavefield(self, model, shot: Shot):
+        """WEMVA forward of one shot: (extended image, d2/dt2 of the source wavefield, receiver
+        wavefield, the last leg's scattered coarse samples)."""
+        m = self._model(model, 1)
+        out = np.zeros((self.nExt, self.nx, self.nz), np.float32)
+        arr = self._shots([shot], data_out=False)
+        W = self._w3()
+        A.check(A.lib().aio_wemva_ext_forward_wavefield(self._h, A.fptr(m), A.fptr(out), 0, arr, A.AIO_MEM_HOST,
+                                                        *[A.fptr(x) for x in W]))
+        return (out, *W)
+
+    def wemva_adjoint_wavefield(self, image, shot: Shot):
+        """WEMVA adjoint of one shot: (model, d2/dt2 of the source wavefield, receiver wavefield,
+        the last leg's scattered coarse samples)."""
+        im = self._model(image, self.nExt)
+        out = np.zeros((self.nx, self.nz), np.float32)
+        arr = self._shots([shot], data_out=False)
+        W = self._w3()
+        A.check(A.lib().aio_wemva_ext_adjoint_wavefield(self._h, A.fptr(out), 0, A.fptr(im), arr, A.AIO_MEM_HOST,
+                                                        *[A.fptr(x) for x in W]))
+        return (out, *W)
+
     def born_ext_forward(self, model, shots: List[Shot]) -> List[np.ndarray]:
         m = self._model(model, self.nExt)
         arr = self._shots(shots, data_out=True)

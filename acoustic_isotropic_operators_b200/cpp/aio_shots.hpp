@@ -723,8 +723,10 @@ class BornFamily : public ShotLoop {
             body(g, s0, s1, ps, shots);
         });
     }
-    // Prepare shot i alone (sources, receivers, optional input data) for a one-shot call.
-    aio_shot prepareOne(int i, const std::shared_ptr<SEP::float3DReg>* dataIn, PreparedShot& s) const {
+    // Prepare shot i alone (sources, receivers, optional input data, optional WEMVA data) for a
+    // one-shot call.
+    aio_shot prepareOne(int i, const std::shared_ptr<SEP::float3DReg>* dataIn, PreparedShot& s,
+                        bool wemvaData = false) const {
         const fdParam& f = fd();
         prepareSource(*_sourcesVector[i], _sourcesSignalsVector[sigIndex(_sourcesSignalsVector.size(), i)]->getVals(),
                       true, s);
@@ -734,8 +736,24 @@ class BornFamily : public ShotLoop {
             spreadData(const_cast<std::vector<std::shared_ptr<deviceGpu>>&>(_receiversVector), i,
                        (*dataIn)->getVals() + (size_t)i * nRecIrreg * f._nts, s.dataReg);
         }
+        if (wemvaData) {
+            auto& rs = *_receiversSignalsVector[sigIndex(_receiversSignalsVector.size(), i)];
+            spreadData(const_cast<std::vector<std::shared_ptr<deviceGpu>>&>(_receiversVector), i, rs.getVals(),
+                       s.wemvaReg);
+        }
+        if (s.dataReg.empty()) s.dataReg.assign((size_t)s.recPos.size() * f._nts, 0.f);
         return toShot(s);
     }
+    // The three saved-wavefield containers of tomo and WEMVA, zero-filled (setAllWavefields(1)).
+    void resetWavefields3() {
+        _wSrc = coarseWavefield();
+        _wSec1 = coarseWavefield();
+        _wSec2 = coarseWavefield();
+    }
+    bool wavefieldShotValid() const {
+        return _saveWavefield == 1 && _wavefieldShotNumber >= 0 && _wavefieldShotNumber < _nShot;
+    }
+    std::shared_ptr<SEP::float3DReg> _wSrc, _wSec1, _wSec2;
     // A coarse wavefield container [nts][nx][nz] (zeros), as the reference's setAllWavefields(1).
     std::shared_ptr<SEP::float3DReg> coarseWavefield() const {
         const fdParam& f = fd();
@@ -927,15 +945,37 @@ class tomoExtShotsGpu : public Operator<SEP::float2DReg, SEP::float3DReg>, publi
         });
         sumImages(parts, model->getVals(), n, add);
     }
-    void forwardWavefield(const bool, const std::shared_ptr<SEP::float2DReg>, std::shared_ptr<SEP::float3DReg>) {
-        aio_ops::fail("tomoExtShotsGpu::forwardWavefield: saved wavefields are not available in this build");
+    // forward / adjoint of every shot, plus, with saveWavefield = 1, the saved wavefields of shot
+    // wavefieldShotNumber (F/src/tomoExtShotsGpu.cpp:147-245, :343-440): d2/dt2 of the source
+    // wavefield and the two secondary wavefields the drivers fill (forward: the last leg's first and
+    // recorded scattered wavefields; adjoint: the receiver wavefield and the last leg's scattered
+    // samples). With saveWavefield = 0 the containers stay zero-filled.
+    void forwardWavefield(const bool add, const std::shared_ptr<SEP::float2DReg> model,
+                          std::shared_ptr<SEP::float3DReg> data) {
+        forward(add, model, data);
+        resetWavefields3();
+        if (!wavefieldShotValid()) return;
+        aio_ops::PreparedShot ps;
+        aio_shot sh = prepareOne(_wavefieldShotNumber, nullptr, ps);
+        aio_ops::ck(aio_tomo_ext_forward_wavefield(context(0), model->getVals(), _reflectivityExt->getVals(), &sh,
+                                                   AIO_MEM_HOST, _wSrc->getVals(), _wSec1->getVals(),
+                                                   _wSec2->getVals()));
     }
-    void adjointWavefield(const bool, std::shared_ptr<SEP::float2DReg>, const std::shared_ptr<SEP::float3DReg>) {
-        aio_ops::fail("tomoExtShotsGpu::adjointWavefield: saved wavefields are not available in this build");
+    void adjointWavefield(const bool add, std::shared_ptr<SEP::float2DReg> model,
+                          const std::shared_ptr<SEP::float3DReg> data) {
+        adjoint(add, model, data);
+        resetWavefields3();
+        if (!wavefieldShotValid()) return;
+        aio_ops::PreparedShot ps;
+        aio_shot sh = prepareOne(_wavefieldShotNumber, &data, ps);
+        std::vector<float> image((size_t)model->size());
+        aio_ops::ck(aio_tomo_ext_adjoint_wavefield(context(0), image.data(), 0, _reflectivityExt->getVals(), &sh,
+                                                   AIO_MEM_HOST, _wSrc->getVals(), _wSec1->getVals(),
+                                                   _wSec2->getVals()));
     }
-    std::shared_ptr<SEP::float3DReg> getSrcWavefield() { return nullptr; }
-    std::shared_ptr<SEP::float3DReg> getSecWavefield1() { return nullptr; }
-    std::shared_ptr<SEP::float3DReg> getSecWavefield2() { return nullptr; }
+    std::shared_ptr<SEP::float3DReg> getSrcWavefield() { return _wSrc; }
+    std::shared_ptr<SEP::float3DReg> getSecWavefield1() { return _wSec1; }
+    std::shared_ptr<SEP::float3DReg> getSecWavefield2() { return _wSec2; }
     void setVel(std::shared_ptr<SEP::float2DReg> vel) { setVelocity(vel); }
     void setReflectivityExt(std::shared_ptr<SEP::float3DReg> reflectivityExt) { _reflectivityExt = reflectivityExt; }
 
@@ -981,15 +1021,35 @@ class wemvaExtShotsGpu : public Operator<SEP::float2DReg, SEP::float3DReg>, publ
         });
         sumImages(parts, model->getVals(), n, add);
     }
-    void forwardWavefield(const bool, const std::shared_ptr<SEP::float2DReg>, std::shared_ptr<SEP::float3DReg>) {
-        aio_ops::fail("wemvaExtShotsGpu::forwardWavefield: saved wavefields are not available in this build");
+    // forward / adjoint of every shot, plus, with saveWavefield = 1, the saved wavefields of shot
+    // wavefieldShotNumber (F/src/wemvaExtShotsGpu.cpp forwardWavefield / adjointWavefield): d2/dt2
+    // of the source wavefield, the receiver wavefield and the last leg's scattered samples. With
+    // saveWavefield = 0 the containers stay zero-filled.
+    void forwardWavefield(const bool add, const std::shared_ptr<SEP::float2DReg> model,
+                          std::shared_ptr<SEP::float3DReg> data) {
+        forward(add, model, data);
+        resetWavefields3();
+        if (!wavefieldShotValid()) return;
+        aio_ops::PreparedShot ps;
+        aio_shot sh = prepareOne(_wavefieldShotNumber, nullptr, ps, true);
+        std::vector<float> image((size_t)data->size());
+        aio_ops::ck(aio_wemva_ext_forward_wavefield(context(0), model->getVals(), image.data(), 0, &sh, AIO_MEM_HOST,
+                                                    _wSrc->getVals(), _wSec1->getVals(), _wSec2->getVals()));
     }
-    void adjointWavefield(const bool, std::shared_ptr<SEP::float2DReg>, const std::shared_ptr<SEP::float3DReg>) {
-        aio_ops::fail("wemvaExtShotsGpu::adjointWavefield: saved wavefields are not available in this build");
+    void adjointWavefield(const bool add, std::shared_ptr<SEP::float2DReg> model,
+                          const std::shared_ptr<SEP::float3DReg> data) {
+        adjoint(add, model, data);
+        resetWavefields3();
+        if (!wavefieldShotValid()) return;
+        aio_ops::PreparedShot ps;
+        aio_shot sh = prepareOne(_wavefieldShotNumber, nullptr, ps, true);
+        std::vector<float> m((size_t)model->size());
+        aio_ops::ck(aio_wemva_ext_adjoint_wavefield(context(0), m.data(), 0, data->getVals(), &sh, AIO_MEM_HOST,
+                                                    _wSrc->getVals(), _wSec1->getVals(), _wSec2->getVals()));
     }
-    std::shared_ptr<SEP::float3DReg> getSrcWavefield() { return nullptr; }
-    std::shared_ptr<SEP::float3DReg> getSecWavefield1() { return nullptr; }
-    std::shared_ptr<SEP::float3DReg> getSecWavefield2() { return nullptr; }
+    std::shared_ptr<SEP::float3DReg> getSrcWavefield() { return _wSrc; }
+    std::shared_ptr<SEP::float3DReg> getSecWavefield1() { return _wSec1; }
+    std::shared_ptr<SEP::float3DReg> getSecWavefield2() { return _wSec2; }
     void setVel(std::shared_ptr<SEP::float2DReg> vel) { setVelocity(vel); }
     void setReceiversSignalsVector(std::vector<std::shared_ptr<SEP::float2DReg>> v) { _receiversSignalsVector = v; }
 };

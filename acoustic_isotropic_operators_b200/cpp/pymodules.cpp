@@ -220,6 +220,9 @@ PYBIND11_MODULE(pyAcoustic_iso_float_tomo, m) {
         .def("adjoint", &tomoExtShotsGpu::adjoint, "Adjoint")
         .def("forwardWavefield", &tomoExtShotsGpu::forwardWavefield, "Forward wavefield")
         .def("adjointWavefield", &tomoExtShotsGpu::adjointWavefield, "Adjoint wavefield")
+        .def("getSrcWavefield", &tomoExtShotsGpu::getSrcWavefield, "Saved d2/dt2 of the source wavefield")
+        .def("getSecWavefield1", &tomoExtShotsGpu::getSecWavefield1, "First saved secondary wavefield")
+        .def("getSecWavefield2", &tomoExtShotsGpu::getSecWavefield2, "Second saved secondary wavefield")
         .def("setVel", &tomoExtShotsGpu::setVel, "Function to set background velocity")
         .def("setReflectivityExt", &tomoExtShotsGpu::setReflectivityExt, "Function to set reflectivity")
         .def("dotTest", &tomoExtShotsGpu::dotTest, "Dot-Product Test", py::arg("verbose") = false,
@@ -240,6 +243,9 @@ PYBIND11_MODULE(pyAcoustic_iso_float_wemva, m) {
         .def("adjoint", &wemvaExtShotsGpu::adjoint, "Adjoint")
         .def("forwardWavefield", &wemvaExtShotsGpu::forwardWavefield, "Forward wavefield")
         .def("adjointWavefield", &wemvaExtShotsGpu::adjointWavefield, "Adjoint wavefield")
+        .def("getSrcWavefield", &wemvaExtShotsGpu::getSrcWavefield, "Saved d2/dt2 of the source wavefield")
+        .def("getSecWavefield1", &wemvaExtShotsGpu::getSecWavefield1, "First saved secondary wavefield")
+        .def("getSecWavefield2", &wemvaExtShotsGpu::getSecWavefield2, "Second saved secondary wavefield")
         .def("setVel", &wemvaExtShotsGpu::setVel, "Function to set background velocity")
         .def("setReceiversSignalsVector", &wemvaExtShotsGpu::setReceiversSignalsVector, "Set the WEMVA data")
         .def("dotTest", &wemvaExtShotsGpu::dotTest, "Dot-Product Test", py::arg("verbose") = false,

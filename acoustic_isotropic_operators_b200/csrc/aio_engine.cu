@@ -171,7 +171,7 @@ struct Context {
     cudaStream_t st = nullptr;
     DevMem v2, rs, taper;
     // per-wave buffers
-    DevMem pbuf, ringb, ssb, wf1, wf2, img, lists, desc, sig, dat, aux, model, ext, outv;
+    DevMem pbuf, ringb, ssb, wf1, wf2, wf3, img, lists, desc, sig, dat, aux, model, ext, outv;
     std::vector<ShotDesc> hdesc;
     long long launches = 0;      // stepper launches of the last operator call
     long long kernels = 0;       // every kernel launched since the last stats reset
@@ -384,6 +384,7 @@ struct Context {
         if (n.ss) ssb.ensure((size_t)nb * 2 * g.isz * 4);
         if (n.nWavefields >= 1) wf1.ensure((size_t)nb * g.nts * g.isz * 4);
         if (n.nWavefields >= 2) wf2.ensure((size_t)nb * g.nts * g.isz * 4);
+        if (n.nWavefields >= 3) wf3.ensure((size_t)nb * g.nts * g.isz * 4);
         if (n.nImg) img.ensure((size_t)nb * n.nImg * g.isz * (P.imageFp64 ? 8 : 4));
         AIO_CK(cudaMemsetAsync(pbuf.p, 0, (size_t)nb * 2 * g.hsz * 4, st));
         AIO_CK(cudaMemsetAsync(ringb.p, 0, (size_t)nb * 2 * g.isz * 4, st));
@@ -2321,6 +2322,78 @@ struct Context {
         sync();
     }
 
+    // Saved wavefields of one tomo / WEMVA shot (the reference drivers' saveWavefield = 1):
+    // d2/dt2 of the source wavefield, and two secondary fields, each [nts][nx][nz]. While `save`
+    // is set the four operators run one shot on the per-fine-step stepper with a third full
+    // wavefield (wf3) for the second secondary field.
+    struct SaveOut {
+        float* src;
+        float* sec1;
+        float* sec2;
+    };
+    const SaveOut* save = nullptr;
+    struct SaveScope {
+        Context* c;
+        SaveScope(Context* x, const SaveOut* o) : c(x) { c->save = o; }
+        ~SaveScope() { c->save = nullptr; }
+    };
+    // Coarse sample t of a scattered field, taken from its ring slot before the imaging call that
+    // clears the slot (the drivers' per-sample cudaMemcpy of scatLeft / scatRight). `scaled`
+    // stores it times v^2 dtw^2: the subsurface-offset WEMVA forward saves its second-leg samples
+    // after scaleSecondarySourceFd (F/src/wemvaExtShotsGpuFunctions.cu:1232-1239).
+    void keep(int t, long long slot, bool scaled = false) {
+        if (!save) return;
+        float* dst = wf3.as<float>() + (long long)t * g.isz;
+        if (scaled) {
+            AIO_CK(cudaMemsetAsync(dst, 0, (size_t)g.isz * 4, st));
+            k_record_scale<<<ew_grid(1, g.isz), 256, 0, st>>>(dst, ring_ptr(slot), nullptr, v2.as<float>(), g.isz);
+            kcheck();
+        } else {
+            AIO_CK(cudaMemcpyAsync(dst, ring_ptr(slot), (size_t)g.isz * 4, cudaMemcpyDeviceToDevice, st));
+        }
+    }
+    // The three saved fields of the shot to the caller: source d2/dt2 (wf2), first secondary
+    // field (wf1: the receiver wavefield, or the tomo forward's first scattered field), second
+    // secondary field (wf3).
+    void save_out(int mem) {
+        if (!save) return;
+        wavefield_out(save->src, wf2, mem);
+        wavefield_out(save->sec1, wf1, mem);
+        wavefield_out(save->sec2, wf3, mem);
+    }
+    int fields_needed() const { return save ? 3 : 2; }
+    void one_shot_saving(int nShots) {
+        if (save) require(nShots == 1, "saved wavefields are returned for one shot per call");
+    }
+    void tomo_forward_wavefield(const float* model, const float* extRefl, const aio_shot* shot, int mem, float* w0,
+                                float* w1, float* w2) {
+        require(w0 && w1 && w2, "wavefield output is NULL");
+        const SaveOut o{w0, w1, w2};
+        SaveScope sc(this, &o);
+        tomo_forward(model, extRefl, 1, shot, mem);
+    }
+    void tomo_adjoint_wavefield(float* modelOut, int add, const float* extRefl, const aio_shot* shot, int mem,
+                                float* w0, float* w1, float* w2) {
+        require(w0 && w1 && w2, "wavefield output is NULL");
+        const SaveOut o{w0, w1, w2};
+        SaveScope sc(this, &o);
+        tomo_adjoint(modelOut, add, extRefl, 1, shot, mem);
+    }
+    void wemva_forward_wavefield(const float* model, float* imageOut, int add, const aio_shot* shot, int mem,
+                                 float* w0, float* w1, float* w2) {
+        require(w0 && w1 && w2, "wavefield output is NULL");
+        const SaveOut o{w0, w1, w2};
+        SaveScope sc(this, &o);
+        wemva_forward(model, imageOut, add, 1, shot, mem);
+    }
+    void wemva_adjoint_wavefield(float* modelOut, int add, const float* image, const aio_shot* shot, int mem,
+                                 float* w0, float* w1, float* w2) {
+        require(w0 && w1 && w2, "wavefield output is NULL");
+        const SaveOut o{w0, w1, w2};
+        SaveScope sc(this, &o);
+        wemva_adjoint(modelOut, add, image, 1, shot, mem);
+    }
+
     // Source wavefield with coarse second time derivative (computeTomoSrcWfldDt2,
     // F/src/tomoExtShotsGpuFunctions.cu:1251-1361).
     void source_wavefield_dt2(int nb, DevMem& W) {
@@ -2337,16 +2410,21 @@ struct Context {
     void tomo_forward(const float* model, const float* extRefl, int nShots, const aio_shot* shots, int mem) {
         begin_call();
         require_fp32_fields("tomo and WEMVA");
+        one_shot_saving(nShots);
         Needs n;
-        n.nWavefields = 2;
+        n.nWavefields = fields_needed();
         n.ss = true;
         float* dm = stage_model(model, 1, mem, this->model);
         scale_shared(dm, 1, 0);
         float* ex = stage_model(extRefl, g.nExt, mem, this->ext);
         // subsurface offsets (tomoOffsetShotsFwdGpu, F/src/tomoExtShotsGpuFunctions.cu:467-575): 2/v^3 only
         scale_shared(ex, g.nExt, offsets() ? 3 : (P.sloth ? 2 : 1));
-        if (tb_enabled() && !offsets())
+        if (tb_enabled() && !offsets() && !save)
             return tomo_forward_tb(dm, ex, nShots, shots, mem);
+        // saving: the recorded (second) pass of each leg also accumulates its coarse field into wf3
+        // (interpWavefield into tomoSecWavefield2, F/src/tomoExtShotsGpuFunctions.cu:1640-1641)
+        const AccMode secondAcc = save ? ACC_FULL : ACC_NONE;
+        DevMem* second = save ? &wf3 : nullptr;
         auto ext_src = [&](int nb, long long slot, const float* F, int t) {
             if (offsets()) img_offset_fwd(nb, slot, ex, F, t);
             else img_time_fwd(nb, slot, ex, F, t);
@@ -2362,17 +2440,18 @@ struct Context {
                 fwd_dense_pass(
                     nb, [&](int t, long long slot) { ext_src(nb, slot, W2, t); }, true, false, ACC_FULL, &wf1, nop);
                 fwd_dense_pass(
-                    nb, [&](int t, long long slot) { img_fwd(nb, slot, dm, 0, W1, t); }, false, true, ACC_NONE,
-                    nullptr, nop);
+                    nb, [&](int t, long long slot) { img_fwd(nb, slot, dm, 0, W1, t); }, false, true, secondAcc,
+                    second, nop);
             }
             if (P.leg2) {
                 fwd_dense_pass(
                     nb, [&](int t, long long slot) { img_fwd(nb, slot, dm, 0, W2, t); }, false, false, ACC_FULL, &wf1,
                     nop);
                 fwd_dense_pass(
-                    nb, [&](int t, long long slot) { ext_src(nb, slot, W1, t); }, true, true, ACC_NONE, nullptr, nop);
+                    nb, [&](int t, long long slot) { ext_src(nb, slot, W1, t); }, true, true, secondAcc, second, nop);
             }
             download_data(nb, shots + s0, mem);
+            save_out(mem);
             sync();
             s0 += nb;
         }
@@ -2382,15 +2461,16 @@ struct Context {
     void tomo_adjoint(float* modelOut, int add, const float* extRefl, int nShots, const aio_shot* shots, int mem) {
         begin_call();
         require_fp32_fields("tomo and WEMVA");
+        one_shot_saving(nShots);
         Needs n;
-        n.nWavefields = 2;
+        n.nWavefields = fields_needed();
         n.ss = true;
         n.nImg = 1;
         float* ex = stage_model(extRefl, g.nExt, mem, this->ext);
         // subsurface offsets (tomoOffsetShotsAdjGpu, F/src/tomoExtShotsGpuFunctions.cu:912-1023): 2/v^3 only
         scale_shared(ex, g.nExt, offsets() ? 3 : (P.sloth ? 2 : 1));
         float* out = stage_out(modelOut, 1, add, mem);
-        if (tb_enabled() && !offsets()) {
+        if (tb_enabled() && !offsets() && !save) {
             tomo_adjoint_tb(out, ex, nShots, shots, mem);
             write_model(modelOut, 1, add, mem, out);
             sync();
@@ -2412,7 +2492,10 @@ struct Context {
                         if (offsets()) img_offset_fwd(nb, slot, ex, W2, t);
                         else img_time_fwd(nb, slot, ex, W2, t);
                     },
-                    true, false, ACC_RING, nullptr, [&](int t, long long slot) { img_adj(nb, slot, R, t); });
+                    true, false, ACC_RING, nullptr, [&](int t, long long slot) {
+                        keep(t, slot);
+                        img_adj(nb, slot, R, t);
+                    });
             if (P.leg2)
                 adj_dense_pass(
                     nb,
@@ -2420,8 +2503,12 @@ struct Context {
                         if (offsets()) img_offset_tomo_adj(nb, slot, ex, R, t);
                         else img_time_tomo_adj(nb, slot, ex, R, t);
                     },
-                    true, [&](int t, long long slot) { img_adj(nb, slot, W2, t); });
+                    true, [&](int t, long long slot) {
+                        keep(t, slot);
+                        img_adj(nb, slot, W2, t);
+                    });
             reduce_images(nb, 1, 0, out, true);
+            save_out(mem);
             sync();
             s0 += nb;
         }
@@ -2433,14 +2520,15 @@ struct Context {
     void wemva_forward(const float* model, float* imageOut, int add, int nShots, const aio_shot* shots, int mem) {
         begin_call();
         require_fp32_fields("tomo and WEMVA");
+        one_shot_saving(nShots);
         Needs n;
-        n.nWavefields = 2;
+        n.nWavefields = fields_needed();
         n.ss = true;
         n.nImg = g.nExt;
         float* dm = stage_model(model, 1, mem, this->model);
         scale_shared(dm, 1, 0);
         float* out = stage_out(imageOut, g.nExt, add, mem);
-        if (tb_enabled() && !offsets()) {
+        if (tb_enabled() && !offsets() && !save) {
             wemva_forward_tb(dm, out, nShots, shots, mem);
             write_model(imageOut, g.nExt, add, mem, out);
             sync();
@@ -2459,6 +2547,7 @@ struct Context {
                 fwd_dense_pass(
                     nb, [&](int t, long long slot) { img_fwd(nb, slot, dm, 0, W2, t); }, false, false, ACC_RING,
                     nullptr, [&](int t, long long slot) {
+                        keep(t, slot);
                         if (offsets()) img_offset_adj_block(nb, slot, R, t, true, false);
                         else img_time_adj(nb, slot, R, t, -1);
                     });
@@ -2466,10 +2555,12 @@ struct Context {
                 adj_dense_pass(
                     nb, [&](int t, long long slot) { img_fwd(nb, slot, dm, 0, R, t); }, false,
                     [&](int t, long long slot) {
+                        keep(t, slot, offsets());
                         if (offsets()) img_offset_adj_block(nb, slot, W2, t, false, true);
                         else img_time_adj(nb, slot, W2, t, +1);
                     });
             reduce_images(nb, g.nExt, offsets() ? 3 : 1, out, true);
+            save_out(mem);
             sync();
             s0 += nb;
         }
@@ -2481,15 +2572,16 @@ struct Context {
     void wemva_adjoint(float* modelOut, int add, const float* image, int nShots, const aio_shot* shots, int mem) {
         begin_call();
         require_fp32_fields("tomo and WEMVA");
+        one_shot_saving(nShots);
         Needs n;
-        n.nWavefields = 2;
+        n.nWavefields = fields_needed();
         n.ss = true;
         n.nImg = 1;
         float* im = stage_model(image, g.nExt, mem, this->ext);
         // subsurface offsets (wemvaOffsetShotsAdjGpu, F/src/wemvaExtShotsGpuFunctions.cu:689-810): 2/v^3 only
         scale_shared(im, g.nExt, offsets() ? 3 : 1);
         float* out = stage_out(modelOut, 1, add, mem);
-        if (tb_enabled() && !offsets()) {
+        if (tb_enabled() && !offsets() && !save) {
             wemva_adjoint_tb(out, im, nShots, shots, mem);
             write_model(modelOut, 1, add, mem, out);
             sync();
@@ -2510,7 +2602,10 @@ struct Context {
                         if (offsets()) img_offset_tomo_adj(nb, slot, im, R, t);
                         else img_time_tomo_adj(nb, slot, im, R, t);
                     },
-                    true, [&](int t, long long slot) { img_adj(nb, slot, W2, t); });
+                    true, [&](int t, long long slot) {
+                        keep(t, slot);
+                        img_adj(nb, slot, W2, t);
+                    });
             if (P.leg2)
                 fwd_dense_pass(
                     nb,
@@ -2518,8 +2613,12 @@ struct Context {
                         if (offsets()) img_offset_fwd(nb, slot, im, W2, t);
                         else img_time_fwd(nb, slot, im, W2, t);
                     },
-                    true, false, ACC_RING, nullptr, [&](int t, long long slot) { img_adj(nb, slot, R, t); });
+                    true, false, ACC_RING, nullptr, [&](int t, long long slot) {
+                        keep(t, slot);
+                        img_adj(nb, slot, R, t);
+                    });
             reduce_images(nb, 1, 0, out, true);
+            save_out(mem);
             sync();
             s0 += nb;
         }
@@ -2779,6 +2878,28 @@ AIO_API int aio_wemva_ext_forward(aio_context* ctx, const float* model, float* i
                                   const aio_shot* shots, int memSpace) {
     return guard([&] { ctx->c.wemva_forward(model, image, add, nShots, shots, memSpace); });
 }
+AIO_API int aio_tomo_ext_forward_wavefield(aio_context* ctx, const float* model, const float* extReflectivity,
+                                           const aio_shot* shot, int memSpace, float* srcDt2, float* sec1,
+                                           float* sec2) {
+    return guard([&] { ctx->c.tomo_forward_wavefield(model, extReflectivity, shot, memSpace, srcDt2, sec1, sec2); });
+}
+AIO_API int aio_tomo_ext_adjoint_wavefield(aio_context* ctx, float* model, int add, const float* extReflectivity,
+                                           const aio_shot* shot, int memSpace, float* srcDt2, float* sec1,
+                                           float* sec2) {
+    return guard([&] {
+        ctx->c.tomo_adjoint_wavefield(model, add, extReflectivity, shot, memSpace, srcDt2, sec1, sec2);
+    });
+}
+AIO_API int aio_wemva_ext_forward_wavefield(aio_context* ctx, const float* model, float* image, int add,
+                                            const aio_shot* shot, int memSpace, float* srcDt2, float* sec1,
+                                            float* sec2) {
+    return guard([&] { ctx->c.wemva_forward_wavefield(model, image, add, shot, memSpace, srcDt2, sec1, sec2); });
+}
+AIO_API int aio_wemva_ext_adjoint_wavefield(aio_context* ctx, float* model, int add, const float* image,
+                                            const aio_shot* shot, int memSpace, float* srcDt2, float* sec1,
+                                            float* sec2) {
+    return guard([&] { ctx->c.wemva_adjoint_wavefield(model, add, image, shot, memSpace, srcDt2, sec1, sec2); });
+}
 AIO_API int aio_wemva_ext_adjoint(aio_context* ctx, float* model, int add, const float* image, int nShots,
                                   const aio_shot* shots, int memSpace) {
     return guard([&] { ctx->c.wemva_adjoint(model, add, image, nShots, shots, memSpace); });
@@ -2943,28 +3064,55 @@ AIO_API int aio_deallocateTomoExtShotsGpu(int iGpu, int iGpuId) {
     (void)iGpuId;
     return guard([&] { seam_deallocate(AIO_TOMO_EXT, iGpu); });
 }
+// saveWavefield = 1 (the reference drivers' flag): the call also returns, for its one shot, d2/dt2
+// of the source wavefield in w0 and the two secondary wavefields in w1 and w2, each
+// [nts][nx][nz] (F/src/tomoExtShotsGpuFunctions.cu:396,429-432,843-850,877;
+// F/src/wemvaExtShotsGpuFunctions.cu:46,55,78-80). Any other value returns none of them.
+static void seam_tomo(Context& c, bool adjoint, float* model, float* data, float* ext, float* sig, int* sp, int ns,
+                      int* rp, int nr, float* w0, float* w1, float* w2, int saveWavefield) {
+    aio_shot s = one_shot(sig, sp, ns, rp, nr, data);
+    if (saveWavefield == 1) {
+        if (adjoint) c.tomo_adjoint_wavefield(model, 0, ext, &s, AIO_MEM_HOST, w0, w1, w2);
+        else c.tomo_forward_wavefield(model, ext, &s, AIO_MEM_HOST, w0, w1, w2);
+    } else if (adjoint) {
+        c.tomo_adjoint(model, 0, ext, 1, &s, AIO_MEM_HOST);
+    } else {
+        c.tomo_forward(model, ext, 1, &s, AIO_MEM_HOST);
+    }
+}
+static void seam_wemva(Context& c, bool adjoint, float* model, float* image, float* sig, int* sp, int ns,
+                       float* wemvaData, int* rp, int nr, float* w0, float* w1, float* w2, int saveWavefield) {
+    aio_shot s = one_shot(sig, sp, ns, rp, nr, nullptr);
+    s.wemvaData = wemvaData;
+    if (saveWavefield == 1) {
+        if (adjoint) c.wemva_adjoint_wavefield(model, 0, image, &s, AIO_MEM_HOST, w0, w1, w2);
+        else c.wemva_forward_wavefield(model, image, 0, &s, AIO_MEM_HOST, w0, w1, w2);
+    } else if (adjoint) {
+        c.wemva_adjoint(model, 0, image, 1, &s, AIO_MEM_HOST);
+    } else {
+        c.wemva_forward(model, image, 0, 1, &s, AIO_MEM_HOST);
+    }
+}
 AIO_API int aio_tomoTimeShotsFwdGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
                                     int* sp, int ns, int* rp, int nr, float* w0, float* w1, float* w2, int sloth,
                                     int iGpu, int iGpuId, int saveWavefield) {
-    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    (void)iGpuId;
     return guard([&] {
-        require(saveWavefield == 0, "saveWavefield=1 is not available for tomo in this build");
         Context& c = seam_ctx(AIO_TOMO_EXT, iGpu);
         c.P.sloth = sloth;
-        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
-        c.tomo_forward(model, extReflectivity, 1, &s, AIO_MEM_HOST);
+        seam_tomo(c, false, model, dataRegDts, extReflectivity, sourcesSignals, sp, ns, rp, nr, w0, w1, w2,
+                  saveWavefield);
     });
 }
 AIO_API int aio_tomoTimeShotsAdjGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
                                     int* sp, int ns, int* rp, int nr, float* w0, float* w1, float* w2, int sloth,
                                     int iGpu, int iGpuId, int saveWavefield) {
-    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    (void)iGpuId;
     return guard([&] {
-        require(saveWavefield == 0, "saveWavefield=1 is not available for tomo in this build");
         Context& c = seam_ctx(AIO_TOMO_EXT, iGpu);
         c.P.sloth = sloth;
-        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
-        c.tomo_adjoint(model, 0, extReflectivity, 1, &s, AIO_MEM_HOST);
+        seam_tomo(c, true, model, dataRegDts, extReflectivity, sourcesSignals, sp, ns, rp, nr, w0, w1, w2,
+                  saveWavefield);
     });
 }
 
@@ -3061,23 +3209,21 @@ AIO_API int aio_BornTimeShotsAdjFsGpu(float* model, float* dataRegDts, float* so
 AIO_API int aio_tomoTimeShotsFwdFsGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
                                       int* sp, int ns, int* rp, int nr, float* w0, float* w1, float* w2, int iGpu,
                                       int iGpuId, int saveWavefield) {
-    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    (void)iGpuId;
     return guard([&] {
-        require(saveWavefield == 0, "saveWavefield=1 is not available for tomo in this build");
         SeamFs fs(seam_ctx(AIO_TOMO_EXT, iGpu));
-        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
-        fs.c.tomo_forward(model, extReflectivity, 1, &s, AIO_MEM_HOST);
+        seam_tomo(fs.c, false, model, dataRegDts, extReflectivity, sourcesSignals, sp, ns, rp, nr, w0, w1, w2,
+                  saveWavefield);
     });
 }
 AIO_API int aio_tomoTimeShotsAdjFsGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
                                       int* sp, int ns, int* rp, int nr, float* w0, float* w1, float* w2, int iGpu,
                                       int iGpuId, int saveWavefield) {
-    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    (void)iGpuId;
     return guard([&] {
-        require(saveWavefield == 0, "saveWavefield=1 is not available for tomo in this build");
         SeamFs fs(seam_ctx(AIO_TOMO_EXT, iGpu));
-        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, dataRegDts);
-        fs.c.tomo_adjoint(model, 0, extReflectivity, 1, &s, AIO_MEM_HOST);
+        seam_tomo(fs.c, true, model, dataRegDts, extReflectivity, sourcesSignals, sp, ns, rp, nr, w0, w1, w2,
+                  saveWavefield);
     });
 }
 
@@ -3165,46 +3311,47 @@ AIO_BORN_EXT_WFLD(aio_BornOffsetShotsAdjFsGpuWavefield, true, true, true)
 #undef AIO_BORN_EXT_WFLD
 
 static void seam_tomo_offset(float* model, float* dataRegDts, float* ext, float* sig, int* sp, int ns, int* rp, int nr,
-                             int iGpu, int saveWavefield, bool adjoint, bool fs) {
-    require(saveWavefield == 0, "saveWavefield=1 is not available for tomo in this build");
+                             int iGpu, float* w0, float* w1, float* w2, int saveWavefield, bool adjoint, bool fs) {
     SeamExt x(seam_ctx(AIO_TOMO_EXT, iGpu), fs);
-    aio_shot s = one_shot(sig, sp, ns, rp, nr, dataRegDts);
-    if (adjoint) x.c.tomo_adjoint(model, 0, ext, 1, &s, AIO_MEM_HOST);
-    else x.c.tomo_forward(model, ext, 1, &s, AIO_MEM_HOST);
+    seam_tomo(x.c, adjoint, model, dataRegDts, ext, sig, sp, ns, rp, nr, w0, w1, w2, saveWavefield);
 }
 AIO_API int aio_tomoOffsetShotsFwdGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
                                       int* sp, int ns, int* rp, int nr, float* w0, float* w1, float* w2, int iGpu,
                                       int iGpuId, int saveWavefield) {
-    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    (void)iGpuId;
     return guard([&] {
-        seam_tomo_offset(model, dataRegDts, extReflectivity, sourcesSignals, sp, ns, rp, nr, iGpu, saveWavefield,
+        seam_tomo_offset(model, dataRegDts, extReflectivity, sourcesSignals, sp, ns, rp, nr, iGpu, w0, w1, w2,
+                         saveWavefield,
                          false, false);
     });
 }
 AIO_API int aio_tomoOffsetShotsAdjGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
                                       int* sp, int ns, int* rp, int nr, float* w0, float* w1, float* w2, int iGpu,
                                       int iGpuId, int saveWavefield) {
-    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    (void)iGpuId;
     return guard([&] {
-        seam_tomo_offset(model, dataRegDts, extReflectivity, sourcesSignals, sp, ns, rp, nr, iGpu, saveWavefield,
+        seam_tomo_offset(model, dataRegDts, extReflectivity, sourcesSignals, sp, ns, rp, nr, iGpu, w0, w1, w2,
+                         saveWavefield,
                          true, false);
     });
 }
 AIO_API int aio_tomoOffsetShotsFwdFsGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
                                         int* sp, int ns, int* rp, int nr, float* w0, float* w1, float* w2, int iGpu,
                                         int iGpuId, int saveWavefield) {
-    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    (void)iGpuId;
     return guard([&] {
-        seam_tomo_offset(model, dataRegDts, extReflectivity, sourcesSignals, sp, ns, rp, nr, iGpu, saveWavefield,
+        seam_tomo_offset(model, dataRegDts, extReflectivity, sourcesSignals, sp, ns, rp, nr, iGpu, w0, w1, w2,
+                         saveWavefield,
                          false, true);
     });
 }
 AIO_API int aio_tomoOffsetShotsAdjFsGpu(float* model, float* dataRegDts, float* extReflectivity, float* sourcesSignals,
                                         int* sp, int ns, int* rp, int nr, float* w0, float* w1, float* w2, int iGpu,
                                         int iGpuId, int saveWavefield) {
-    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    (void)iGpuId;
     return guard([&] {
-        seam_tomo_offset(model, dataRegDts, extReflectivity, sourcesSignals, sp, ns, rp, nr, iGpu, saveWavefield,
+        seam_tomo_offset(model, dataRegDts, extReflectivity, sourcesSignals, sp, ns, rp, nr, iGpu, w0, w1, w2,
+                         saveWavefield,
                          true, true);
     });
 }
@@ -3227,46 +3374,38 @@ AIO_API int aio_deallocateWemvaExtShotsGpu(int iGpu, int iGpuId) {
 AIO_API int aio_wemvaTimeShotsFwdGpu(float* model, float* wemvaExtImage, float* sourcesSignals, int* sp, int ns,
                                      float* wemvaDataRegDts, int* rp, int nr, float* w0, float* w1, float* w2,
                                      int iGpu, int iGpuId, int saveWavefield) {
-    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    (void)iGpuId;
     return guard([&] {
-        require(saveWavefield == 0, "saveWavefield=1 is not available for WEMVA in this build");
-        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, nullptr);
-        s.wemvaData = wemvaDataRegDts;
-        seam_ctx(AIO_WEMVA_EXT, iGpu).wemva_forward(model, wemvaExtImage, 0, 1, &s, AIO_MEM_HOST);
+        seam_wemva(seam_ctx(AIO_WEMVA_EXT, iGpu), false, model, wemvaExtImage, sourcesSignals, sp, ns,
+                   wemvaDataRegDts, rp, nr, w0, w1, w2, saveWavefield);
     });
 }
 AIO_API int aio_wemvaOffsetShotsFwdGpu(float* model, float* wemvaExtImage, float* sourcesSignals, int* sp, int ns,
                                        float* wemvaDataRegDts, int* rp, int nr, float* w0, float* w1, float* w2,
                                        int iGpu, int iGpuId, int saveWavefield) {
-    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    (void)iGpuId;
     return guard([&] {
-        require(saveWavefield == 0, "saveWavefield=1 is not available for WEMVA in this build");
         SeamExt x(seam_ctx(AIO_WEMVA_EXT, iGpu), false);
-        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, nullptr);
-        s.wemvaData = wemvaDataRegDts;
-        x.c.wemva_forward(model, wemvaExtImage, 0, 1, &s, AIO_MEM_HOST);
+        seam_wemva(x.c, false, model, wemvaExtImage, sourcesSignals, sp, ns, wemvaDataRegDts, rp, nr, w0, w1, w2,
+                   saveWavefield);
     });
 }
 AIO_API int aio_wemvaOffsetShotsAdjGpu(float* model, float* wemvaExtImage, float* sourcesSignals, int* sp, int ns,
                                        float* wemvaDataRegDts, int* rp, int nr, float* w0, float* w1, float* w2,
                                        int iGpu, int iGpuId, int saveWavefield) {
-    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    (void)iGpuId;
     return guard([&] {
-        require(saveWavefield == 0, "saveWavefield=1 is not available for WEMVA in this build");
         SeamExt x(seam_ctx(AIO_WEMVA_EXT, iGpu), false);
-        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, nullptr);
-        s.wemvaData = wemvaDataRegDts;
-        x.c.wemva_adjoint(model, 0, wemvaExtImage, 1, &s, AIO_MEM_HOST);
+        seam_wemva(x.c, true, model, wemvaExtImage, sourcesSignals, sp, ns, wemvaDataRegDts, rp, nr, w0, w1, w2,
+                   saveWavefield);
     });
 }
 AIO_API int aio_wemvaTimeShotsAdjGpu(float* model, float* wemvaExtImage, float* sourcesSignals, int* sp, int ns,
                                      float* wemvaDataRegDts, int* rp, int nr, float* w0, float* w1, float* w2,
                                      int iGpu, int iGpuId, int saveWavefield) {
-    (void)w0; (void)w1; (void)w2; (void)iGpuId;
+    (void)iGpuId;
     return guard([&] {
-        require(saveWavefield == 0, "saveWavefield=1 is not available for WEMVA in this build");
-        aio_shot s = one_shot(sourcesSignals, sp, ns, rp, nr, nullptr);
-        s.wemvaData = wemvaDataRegDts;
-        seam_ctx(AIO_WEMVA_EXT, iGpu).wemva_adjoint(model, 0, wemvaExtImage, 1, &s, AIO_MEM_HOST);
+        seam_wemva(seam_ctx(AIO_WEMVA_EXT, iGpu), true, model, wemvaExtImage, sourcesSignals, sp, ns,
+                   wemvaDataRegDts, rp, nr, w0, w1, w2, saveWavefield);
     });
 }

@@ -173,6 +173,21 @@ int aio_wemva_ext_forward(aio_context* ctx, const float* model, float* image, in
                           const aio_shot* shots, int memSpace);
 int aio_wemva_ext_adjoint(aio_context* ctx, float* model, int add, const float* image, int nShots,
                           const aio_shot* shots, int memSpace);
+/* Tomo and WEMVA of one shot with the saved wavefields of the reference's saveWavefield = 1
+ * drivers, each [nts][nx][nz] with a zero FAT ring: srcDt2 = d2/dt2 of the source wavefield.
+ * Tomo forward (F/src/tomoExtShotsGpuFunctions.cu:355-465): sec1 = the last leg's first
+ * scattered wavefield, sec2 = its second (recorded) scattered wavefield. Tomo adjoint
+ * (:797-910) and WEMVA forward / adjoint (F/src/wemvaExtShotsGpuFunctions.cu:344-456, :575-688):
+ * sec1 = the receiver wavefield, sec2 = the coarse samples of the last leg's scattered
+ * wavefield. Per-fine-step stepper, FP32 fields (wavefieldPrecision AIO_WFLD_FP32). */
+int aio_tomo_ext_forward_wavefield(aio_context* ctx, const float* model, const float* extReflectivity,
+                                   const aio_shot* shot, int memSpace, float* srcDt2, float* sec1, float* sec2);
+int aio_tomo_ext_adjoint_wavefield(aio_context* ctx, float* model, int add, const float* extReflectivity,
+                                   const aio_shot* shot, int memSpace, float* srcDt2, float* sec1, float* sec2);
+int aio_wemva_ext_forward_wavefield(aio_context* ctx, const float* model, float* image, int add,
+                                    const aio_shot* shot, int memSpace, float* srcDt2, float* sec1, float* sec2);
+int aio_wemva_ext_adjoint_wavefield(aio_context* ctx, float* model, int add, const float* image,
+                                    const aio_shot* shot, int memSpace, float* srcDt2, float* sec1, float* sec2);
 
 /* ------------------------------------------------------------ host preparation
  * The reference's host-side numerics, FP32 expressions unchanged; arrays are
@@ -249,7 +264,9 @@ int aio_BornTimeShotsFwdGpu(float* model, float* dataRegDts, float* sourcesSigna
 int aio_BornTimeShotsAdjGpu(float* model, float* dataRegDts, float* sourcesSignals, int* sourcesPositionReg,
                             int nSourcesReg, int* receiversPositionReg, int nReceiversReg, float* srcWavefield,
                             float* recWavefield, int sloth, int iGpu, int iGpuId);
-/* F/include/tomoExtShotsGpuFunctions.h:6-33 (time-lag extension) */
+/* F/include/tomoExtShotsGpuFunctions.h:6-33 (time-lag extension). saveWavefield = 1 fills the three
+ * wavefield arrays of the call as aio_tomo_ext_{forward,adjoint}_wavefield describe; the WEMVA
+ * calls below do the same with aio_wemva_ext_{forward,adjoint}_wavefield's fields. */
 int aio_initTomoExtGpu(float dz, float dx, int nz, int nx, int nts, float dts, int sub, int minPad, int blockSize,
                        float alphaCos, int nExt, int leg1, int leg2, int nGpu, int iGpuId, int iGpuAlloc);
 int aio_allocateTomoExtShotsGpu(float* vel2Dtw2, float* reflectivityScale, int iGpu, int iGpuId);

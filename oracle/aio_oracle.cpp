@@ -549,6 +549,16 @@ static void receiver_wavefield(const Grid<T>& g, Work<T>& w, const T* data, cons
     rec_pass(g, w, data, pos, n, [&](const T* p, int its, int it2) { interp_wavefield(g, R, p, its, it2); });
 }
 
+// Saved wavefields (saveWavefield = 1): copy a whole [nts][nx][nz] field, or one coarse slice t.
+template <class T>
+static void copy_out(const Grid<T>& g, const std::vector<T>& W, T* out) {
+    if (out) std::copy(W.begin(), W.begin() + (size_t)g.nts * g.N(), out);
+}
+template <class T>
+static void save_slice(const Grid<T>& g, T* out, const T* C, int t) {
+    if (out) std::copy(C, C + g.N(), out + (size_t)t * g.N());
+}
+
 // ============================ operators =====================================
 
 // Nonlinear forward, F/src/nonlinearShotsGpuFunctions.cu:227-309 (and :310-395 with W).
@@ -745,8 +755,14 @@ static void bornext_adj(const Grid<T>& g, T* model, const T* sig, const int* sp,
 // Extended tomo forward, F/src/tomoExtShotsGpuFunctions.cu:355-465 with
 // legs :1554-1656 (s->i->m->d) and :1782-1881 (s->m->i->d).
 template <class T>
+//
+// Saved wavefields (non-null Wsrc, Wsec1, Wsec2: the drivers' saveWavefield = 1): d2/dt2 of the
+// source wavefield; the last leg's first scattered wavefield (tomoSecWavefield1, :429-432);
+// the last leg's recorded scattered wavefield, accumulated per leg from zero
+// (tomoSecWavefield2, :1615-1641, :1839-1871).
 static void tomo_fwd(const Grid<T>& g, const T* model, const T* extRefl, const T* sig, const int* sp, int ns,
-                     const int* rp, int nr, T* data, int sloth, int leg1, int leg2) {
+                     const int* rp, int nr, T* data, int sloth, int leg1, int leg2, T* Wsrc = nullptr,
+                     T* Wsec1 = nullptr, T* Wsec2 = nullptr) {
     Work<T> w(g.N());
     const size_t N = g.N();
     std::vector<T> W2((size_t)g.nts * N), W1((size_t)g.nts * N);
@@ -771,11 +787,19 @@ static void tomo_fwd(const Grid<T>& g, const T* model, const T* extRefl, const T
         };
     };
     auto store_W1 = [&](const T* p, int its, int it2) { interp_wavefield(g, W1.data(), p, its, it2); };
-    auto rec = [&](const T* p, int its, int it2) { record_data(g, p, data, its, it2, rp, nr); };
+    auto rec = [&](const T* p, int its, int it2) {
+        if (Wsec2) interp_wavefield(g, Wsec2, p, its, it2);
+        record_data(g, p, data, its, it2, rp, nr);
+    };
     auto nop = [](int, T*) {};
+    copy_out(g, W2, Wsrc);
+    auto clear_sec2 = [&] {
+        if (Wsec2) std::fill(Wsec2, Wsec2 + (size_t)g.nts * N, (T)0);
+    };
     if (leg1) {
         std::fill(W1.begin(), W1.end(), (T)0);
         scat_fwd_pass(g, w, ext_src(W2.data()), true, store_W1, false, nop);
+        clear_sec2();
         scat_fwd_pass(g, w, [&](int t, T* ss) { imaging_fwd(g, dm.data(), ss, t, W1.data()); }, false, rec,
                       false, nop);
     }
@@ -783,20 +807,29 @@ static void tomo_fwd(const Grid<T>& g, const T* model, const T* extRefl, const T
         std::fill(W1.begin(), W1.end(), (T)0);
         scat_fwd_pass(g, w, [&](int t, T* ss) { imaging_fwd(g, dm.data(), ss, t, W2.data()); }, false, store_W1,
                       false, nop);
+        clear_sec2();
         scat_fwd_pass(g, w, ext_src(W1.data()), true, rec, false, nop);
     }
+    copy_out(g, W1, Wsec1);
 }
 
 // Extended tomo adjoint, F/src/tomoExtShotsGpuFunctions.cu:797-910 with legs
 // :2442-2527 (leg 1) and :2619-2701 (leg 2).
 template <class T>
+//
+// Saved wavefields: d2/dt2 of the source wavefield, the receiver wavefield (tomoSecWavefield1,
+// :850) and the coarse samples of the last leg's scattered wavefield, taken as they are imaged
+// (tomoSecWavefield2, :2507-2525, :2680-2700).
 static void tomo_adj(const Grid<T>& g, T* model, const T* extRefl, const T* sig, const int* sp, int ns,
-                     const int* rp, int nr, const T* data, int sloth, int leg1, int leg2) {
+                     const int* rp, int nr, const T* data, int sloth, int leg1, int leg2, T* Wsrc = nullptr,
+                     T* Wsec1 = nullptr, T* Wsec2 = nullptr) {
     Work<T> w(g.N());
     const size_t N = g.N();
     std::vector<T> W2((size_t)g.nts * N), R((size_t)g.nts * N);
     source_wavefield_dt2(g, w, sig, sp, ns, W2.data());
     receiver_wavefield(g, w, data, rp, nr, R.data());
+    copy_out(g, W2, Wsrc);
+    copy_out(g, R, Wsec1);
     std::vector<T> ext(extRefl, extRefl + (size_t)g.nExt * N);
     // subsurface offsets: tomoOffsetShotsAdjGpu, F/src/tomoExtShotsGpuFunctions.cu:912-1023, legs :2788-2866, :2949-3021
     if (g.offset) scale_refl_lin_ext(g, ext.data());
@@ -816,7 +849,10 @@ static void tomo_adj(const Grid<T>& g, T* model, const T* extRefl, const T* sig,
                 imaging_time_fwd(g, ext.data(), ss, W2.data(), t, e0, e1);
             },
             true, [](const T*, int, int) {}, true,
-            [&](int t, T* C) { imaging_adj(g, model, C, R.data(), t); });
+            [&](int t, T* C) {
+                save_slice(g, Wsec2, C, t);
+                imaging_adj(g, model, C, R.data(), t);
+            });
     }
     if (leg2) {
         scat_adj_pass(
@@ -830,7 +866,10 @@ static void tomo_adj(const Grid<T>& g, T* model, const T* extRefl, const T* sig,
                 lag_bounds_rec(g, t, e0, e1);
                 imaging_time_tomo_adj(g, R.data(), ss, ext.data(), t, e0, e1);
             },
-            true, [&](int t, T* C) { imaging_adj(g, model, C, W2.data(), t); });
+            true, [&](int t, T* C) {
+                save_slice(g, Wsec2, C, t);
+                imaging_adj(g, model, C, W2.data(), t);
+            });
     }
     scale_refl(g, model);
 }
@@ -839,13 +878,21 @@ static void tomo_adj(const Grid<T>& g, T* model, const T* extRefl, const T* sig,
 // :961-1037 (s->m->i<-d) and :1038-1122 (s->i<-m<-d). `rdata` is the regular-grid
 // WEMVA data that drives the receiver wavefield.
 template <class T>
+//
+// Saved wavefields: d2/dt2 of the source wavefield, the receiver wavefield (wemvaSecWavefield1,
+// :55) and the coarse samples of the last leg's scattered wavefield as they are imaged
+// (wemvaSecWavefield2, :1009, :1033, :1091, :1117; the offset second leg saves them after the
+// v^2 dtw^2 scaling, :1232-1239).
 static void wemva_fwd(const Grid<T>& g, const T* model, const T* sig, const int* sp, int ns, const int* rp, int nr,
-                      const T* rdata, T* image, int leg1, int leg2) {
+                      const T* rdata, T* image, int leg1, int leg2, T* Wsrc = nullptr, T* Wsec1 = nullptr,
+                      T* Wsec2 = nullptr) {
     Work<T> w(g.N());
     const size_t N = g.N();
     std::vector<T> W2((size_t)g.nts * N), R((size_t)g.nts * N);
     source_wavefield_dt2(g, w, sig, sp, ns, W2.data());
     receiver_wavefield(g, w, rdata, rp, nr, R.data());
+    copy_out(g, W2, Wsrc);
+    copy_out(g, R, Wsec1);
     std::vector<T> dm(model, model + N);
     scale_refl(g, dm.data());
     std::fill(image, image + (size_t)g.nExt * N, (T)0);
@@ -853,6 +900,7 @@ static void wemva_fwd(const Grid<T>& g, const T* model, const T* sig, const int*
         scat_fwd_pass(
             g, w, [&](int t, T* ss) { imaging_fwd(g, dm.data(), ss, t, W2.data()); }, false,
             [](const T*, int, int) {}, true, [&](int t, T* C) {
+                save_slice(g, Wsec2, C, t);
                 if (g.offset) {  // wemvaOffsetShotsFwdGpu (:458-574) legs, F/src/wemvaExtShotsGpuFunctions.cu:1123-1269
                     imaging_offset_wemva_scale_fwd(g, image, C, R.data(), t);
                     return;
@@ -867,9 +915,11 @@ static void wemva_fwd(const Grid<T>& g, const T* model, const T* sig, const int*
             g, w, [&](int t, T* ss) { imaging_fwd(g, dm.data(), ss, t, R.data()); }, false, [&](int t, T* C) {
                 if (g.offset) {
                     scale_ss_fd(g, C);
+                    save_slice(g, Wsec2, C, t);
                     imaging_offset_adj(g, image, C, W2.data(), t);
                     return;
                 }
+                save_slice(g, Wsec2, C, t);
                 int e0, e1;
                 lag_bounds_src(g, t, e0, e1);
                 imaging_time_adj(g, image, C, W2.data(), t, e0, e1);
@@ -882,13 +932,18 @@ static void wemva_fwd(const Grid<T>& g, const T* model, const T* sig, const int*
 // Extended WEMVA adjoint, F/src/wemvaExtShotsGpuFunctions.cu:575-688 with legs
 // :1270-1350 (leg 1) and :1352-1426 (leg 2).
 template <class T>
+//
+// Saved wavefields: as wemva_fwd (wemvaSecWavefield2 from :1325, :1347, :1401, :1422).
 static void wemva_adj(const Grid<T>& g, T* model, const T* sig, const int* sp, int ns, const int* rp, int nr,
-                      const T* rdata, const T* imageIn, int leg1, int leg2) {
+                      const T* rdata, const T* imageIn, int leg1, int leg2, T* Wsrc = nullptr, T* Wsec1 = nullptr,
+                      T* Wsec2 = nullptr) {
     Work<T> w(g.N());
     const size_t N = g.N();
     std::vector<T> W2((size_t)g.nts * N), R((size_t)g.nts * N);
     source_wavefield_dt2(g, w, sig, sp, ns, W2.data());
     receiver_wavefield(g, w, rdata, rp, nr, R.data());
+    copy_out(g, W2, Wsrc);
+    copy_out(g, R, Wsec1);
     std::vector<T> img(imageIn, imageIn + (size_t)g.nExt * N);
     // subsurface offsets: wemvaOffsetShotsAdjGpu, F/src/wemvaExtShotsGpuFunctions.cu:689-810, legs :1428-1580
     if (g.offset) scale_refl_lin_ext(g, img.data());
@@ -906,7 +961,10 @@ static void wemva_adj(const Grid<T>& g, T* model, const T* sig, const int* sp, i
                 lag_bounds_rec(g, t, e0, e1);
                 imaging_time_tomo_adj(g, R.data(), ss, img.data(), t, e0, e1);
             },
-            true, [&](int t, T* C) { imaging_adj(g, model, C, W2.data(), t); });
+            true, [&](int t, T* C) {
+                save_slice(g, Wsec2, C, t);
+                imaging_adj(g, model, C, W2.data(), t);
+            });
     }
     if (leg2) {
         scat_fwd_pass(
@@ -921,7 +979,10 @@ static void wemva_adj(const Grid<T>& g, T* model, const T* sig, const int* sp, i
                 lag_bounds_src(g, t, e0, e1);
                 imaging_time_fwd(g, img.data(), ss, W2.data(), t, e0, e1);
             },
-            true, [](const T*, int, int) {}, true, [&](int t, T* C) { imaging_adj(g, model, C, R.data(), t); });
+            true, [](const T*, int, int) {}, true, [&](int t, T* C) {
+                save_slice(g, Wsec2, C, t);
+                imaging_adj(g, model, C, R.data(), t);
+            });
     }
     scale_refl(g, model);
 }
@@ -1065,27 +1126,27 @@ static Grid<T> grid_from(const OrcParams* p, const T* vel) {
     }                                                                                                             \
     ORC_EXPORT void orc_tomo_fwd_##SUF(const OrcParams* p, const T* vel, const T* model, const T* ext,            \
                                        const T* sig, const int* sp, int ns, const int* rp, int nr, T* data,       \
-                                       int sloth, int leg1, int leg2) {                                           \
+                                       int sloth, int leg1, int leg2, T* W0, T* W1, T* W2) {                      \
         Grid<T> g = grid_from<T>(p, vel);                                                                         \
-        tomo_fwd<T>(g, model, ext, sig, sp, ns, rp, nr, data, sloth, leg1, leg2);                                 \
+        tomo_fwd<T>(g, model, ext, sig, sp, ns, rp, nr, data, sloth, leg1, leg2, W0, W1, W2);                     \
     }                                                                                                             \
     ORC_EXPORT void orc_tomo_adj_##SUF(const OrcParams* p, const T* vel, T* model, const T* ext, const T* sig,    \
                                        const int* sp, int ns, const int* rp, int nr, const T* data, int sloth,    \
-                                       int leg1, int leg2) {                                                      \
+                                       int leg1, int leg2, T* W0, T* W1, T* W2) {                                 \
         Grid<T> g = grid_from<T>(p, vel);                                                                         \
-        tomo_adj<T>(g, model, ext, sig, sp, ns, rp, nr, data, sloth, leg1, leg2);                                 \
+        tomo_adj<T>(g, model, ext, sig, sp, ns, rp, nr, data, sloth, leg1, leg2, W0, W1, W2);                     \
     }                                                                                                             \
     ORC_EXPORT void orc_wemva_fwd_##SUF(const OrcParams* p, const T* vel, const T* model, const T* sig,           \
                                         const int* sp, int ns, const int* rp, int nr, const T* rdata, T* image,   \
-                                        int leg1, int leg2) {                                                     \
+                                        int leg1, int leg2, T* W0, T* W1, T* W2) {                                \
         Grid<T> g = grid_from<T>(p, vel);                                                                         \
-        wemva_fwd<T>(g, model, sig, sp, ns, rp, nr, rdata, image, leg1, leg2);                                    \
+        wemva_fwd<T>(g, model, sig, sp, ns, rp, nr, rdata, image, leg1, leg2, W0, W1, W2);                        \
     }                                                                                                             \
     ORC_EXPORT void orc_wemva_adj_##SUF(const OrcParams* p, const T* vel, T* model, const T* sig, const int* sp,  \
                                         int ns, const int* rp, int nr, const T* rdata, const T* image, int leg1,  \
-                                        int leg2) {                                                               \
+                                        int leg2, T* W0, T* W1, T* W2) {                                          \
         Grid<T> g = grid_from<T>(p, vel);                                                                         \
-        wemva_adj<T>(g, model, sig, sp, ns, rp, nr, rdata, image, leg1, leg2);                                    \
+        wemva_adj<T>(g, model, sig, sp, ns, rp, nr, rdata, image, leg1, leg2, W0, W1, W2);                        \
     }                                                                                                             \
     ORC_EXPORT void orc_time_interp_fwd_##SUF(int nts, double dts, double ots, int sub, int nDev, const T* m,      \
                                               T* d) {                                                             \

@@ -178,38 +178,62 @@ def bornext_adj(s, vel, data, sig_dtw, src_pos, rec_pos, dtype=np.float64, sloth
     return m
 
 
-def tomo_fwd(s, vel, model, ext_refl, sig_dtw, src_pos, rec_pos, dtype=np.float64, sloth=0, leg1=1, leg2=1):
+def _wfld(s, dtype, on):
+    """Three [nts][nx][nz] arrays for saved wavefields (and their pointers), or null pointers."""
+    if not on:
+        return [], [None, None, None]
+    W = [np.zeros((s.nts, s.nx, s.nz), dtype) for _ in range(3)]
+    return W, [_p(x) for x in W]
+
+
+def tomo_fwd(s, vel, model, ext_refl, sig_dtw, src_pos, rec_pos, dtype=np.float64, sloth=0, leg1=1, leg2=1,
+             wavefields=False):
+    """Tomo forward data; with wavefields=True (data, source d2/dt2, the last leg's first
+    scattered wavefield, its recorded scattered wavefield)."""
     vel = _arr(vel, dtype); m = _arr(model, dtype); e = _arr(ext_refl, dtype); sig = _arr(sig_dtw, dtype)
     d = np.zeros((len(rec_pos), s.nts), dtype)
+    W, wp = _wfld(s, dtype, wavefields)
     getattr(lib(), "orc_tomo_fwd_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(e), _p(sig), _ip(src_pos),
-                                                  len(src_pos), _ip(rec_pos), len(rec_pos), _p(d), sloth, leg1, leg2)
-    return d
+                                                  len(src_pos), _ip(rec_pos), len(rec_pos), _p(d), sloth, leg1, leg2,
+                                                  *wp)
+    return (d, *W) if wavefields else d
 
 
-def tomo_adj(s, vel, data, ext_refl, sig_dtw, src_pos, rec_pos, dtype=np.float64, sloth=0, leg1=1, leg2=1):
+def tomo_adj(s, vel, data, ext_refl, sig_dtw, src_pos, rec_pos, dtype=np.float64, sloth=0, leg1=1, leg2=1,
+             wavefields=False):
+    """Tomo adjoint model; with wavefields=True (model, source d2/dt2, receiver wavefield, the
+    last leg's scattered coarse samples)."""
     vel = _arr(vel, dtype); d = _arr(data, dtype); e = _arr(ext_refl, dtype); sig = _arr(sig_dtw, dtype)
     m = np.zeros((s.nx, s.nz), dtype)
+    W, wp = _wfld(s, dtype, wavefields)
     getattr(lib(), "orc_tomo_adj_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(e), _p(sig), _ip(src_pos),
-                                                  len(src_pos), _ip(rec_pos), len(rec_pos), _p(d), sloth, leg1, leg2)
-    return m
+                                                  len(src_pos), _ip(rec_pos), len(rec_pos), _p(d), sloth, leg1, leg2,
+                                                  *wp)
+    return (m, *W) if wavefields else m
 
 
-def wemva_fwd(s, vel, model, sig_dtw, src_pos, rec_pos, rdata, dtype=np.float64, leg1=1, leg2=1):
+def wemva_fwd(s, vel, model, sig_dtw, src_pos, rec_pos, rdata, dtype=np.float64, leg1=1, leg2=1, wavefields=False):
+    """WEMVA forward extended image; with wavefields=True (image, source d2/dt2, receiver
+    wavefield, the last leg's scattered coarse samples)."""
     vel = _arr(vel, dtype); m = _arr(model, dtype); sig = _arr(sig_dtw, dtype); r = _arr(rdata, dtype)
     img = np.zeros((s.nExt, s.nx, s.nz), dtype)
+    W, wp = _wfld(s, dtype, wavefields)
     getattr(lib(), "orc_wemva_fwd_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(sig), _ip(src_pos),
                                                    len(src_pos), _ip(rec_pos), len(rec_pos), _p(r), _p(img),
-                                                   leg1, leg2)
-    return img
+                                                   leg1, leg2, *wp)
+    return (img, *W) if wavefields else img
 
 
-def wemva_adj(s, vel, image, sig_dtw, src_pos, rec_pos, rdata, dtype=np.float64, leg1=1, leg2=1):
+def wemva_adj(s, vel, image, sig_dtw, src_pos, rec_pos, rdata, dtype=np.float64, leg1=1, leg2=1, wavefields=False):
+    """WEMVA adjoint model; with wavefields=True (model, source d2/dt2, receiver wavefield, the
+    last leg's scattered coarse samples)."""
     vel = _arr(vel, dtype); img = _arr(image, dtype); sig = _arr(sig_dtw, dtype); r = _arr(rdata, dtype)
     m = np.zeros((s.nx, s.nz), dtype)
+    W, wp = _wfld(s, dtype, wavefields)
     getattr(lib(), "orc_wemva_adj_" + _suf(dtype))(C.byref(s.c()), _p(vel), _p(m), _p(sig), _ip(src_pos),
                                                    len(src_pos), _ip(rec_pos), len(rec_pos), _p(r), _p(img),
-                                                   leg1, leg2)
-    return m
+                                                   leg1, leg2, *wp)
+    return (m, *W) if wavefields else m
 
 
 def time_interp_fwd(nts, dts, sub, m, ots=0.0, dtype=np.float64):

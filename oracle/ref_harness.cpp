@@ -167,6 +167,22 @@ REF_EXPORT int ref_tomo_fwd_fs(R* model, R* data, R* ext, R* sig, int* sp, int n
 REF_EXPORT int ref_tomo_adj_fs(R* model, R* data, R* ext, R* sig, int* sp, int ns, int* rp, int nr, int dev) {
     GUARD(tomoTimeShotsAdjFsGpu(model, data, ext, sig, sp, ns, rp, nr, nullptr, nullptr, nullptr, 0, dev, 0))
 }
+// saveWavefield = 1: source d2/dt2 and the two secondary wavefields out ([nts][nx][nz] each);
+// off / fs select the offset and free-surface drivers (sloth applies to the plain time-lag one)
+REF_EXPORT int ref_tomo_fwd_wfld(R* model, R* data, R* ext, R* sig, int* sp, int ns, int* rp, int nr, R* W0, R* W1,
+                                 R* W2, int off, int fs, int sloth, int dev) {
+    if (off && fs) { GUARD(tomoOffsetShotsFwdFsGpu(model, data, ext, sig, sp, ns, rp, nr, W0, W1, W2, 0, dev, 1)) }
+    if (off) { GUARD(tomoOffsetShotsFwdGpu(model, data, ext, sig, sp, ns, rp, nr, W0, W1, W2, 0, dev, 1)) }
+    if (fs) { GUARD(tomoTimeShotsFwdFsGpu(model, data, ext, sig, sp, ns, rp, nr, W0, W1, W2, 0, dev, 1)) }
+    GUARD(tomoTimeShotsFwdGpu(model, data, ext, sig, sp, ns, rp, nr, W0, W1, W2, sloth, 0, dev, 1))
+}
+REF_EXPORT int ref_tomo_adj_wfld(R* model, R* data, R* ext, R* sig, int* sp, int ns, int* rp, int nr, R* W0, R* W1,
+                                 R* W2, int off, int fs, int sloth, int dev) {
+    if (off && fs) { GUARD(tomoOffsetShotsAdjFsGpu(model, data, ext, sig, sp, ns, rp, nr, W0, W1, W2, 0, dev, 1)) }
+    if (off) { GUARD(tomoOffsetShotsAdjGpu(model, data, ext, sig, sp, ns, rp, nr, W0, W1, W2, 0, dev, 1)) }
+    if (fs) { GUARD(tomoTimeShotsAdjFsGpu(model, data, ext, sig, sp, ns, rp, nr, W0, W1, W2, 0, dev, 1)) }
+    GUARD(tomoTimeShotsAdjGpu(model, data, ext, sig, sp, ns, rp, nr, W0, W1, W2, sloth, 0, dev, 1))
+}
 #elif defined(REF_FAMILY_WEMVA)
 // F/include/wemvaExtShotsGpuFunctions.h:6-17
 REF_EXPORT int ref_init(R dz, R dx, int nz, int nx, int nts, R dts, int sub, int minPad, R alphaCos, int nExt,
@@ -187,5 +203,16 @@ REF_EXPORT int ref_wemva_fwd_off(R* model, R* image, R* sig, int* sp, int ns, R*
 }
 REF_EXPORT int ref_wemva_adj_off(R* model, R* image, R* sig, int* sp, int ns, R* rdata, int* rp, int nr, int dev) {
     GUARD(wemvaOffsetShotsAdjGpu(model, image, sig, sp, ns, rdata, rp, nr, nullptr, nullptr, nullptr, 0, dev, 0))
+}
+// saveWavefield = 1: source d2/dt2 and the two secondary wavefields out; off selects the offset drivers
+REF_EXPORT int ref_wemva_fwd_wfld(R* model, R* image, R* sig, int* sp, int ns, R* rdata, int* rp, int nr, R* W0,
+                                  R* W1, R* W2, int off, int dev) {
+    if (off) { GUARD(wemvaOffsetShotsFwdGpu(model, image, sig, sp, ns, rdata, rp, nr, W0, W1, W2, 0, dev, 1)) }
+    GUARD(wemvaTimeShotsFwdGpu(model, image, sig, sp, ns, rdata, rp, nr, W0, W1, W2, 0, dev, 1))
+}
+REF_EXPORT int ref_wemva_adj_wfld(R* model, R* image, R* sig, int* sp, int ns, R* rdata, int* rp, int nr, R* W0,
+                                  R* W1, R* W2, int off, int dev) {
+    if (off) { GUARD(wemvaOffsetShotsAdjGpu(model, image, sig, sp, ns, rdata, rp, nr, W0, W1, W2, 0, dev, 1)) }
+    GUARD(wemvaTimeShotsAdjGpu(model, image, sig, sp, ns, rdata, rp, nr, W0, W1, W2, 0, dev, 1))
 }
 #endif

@@ -249,3 +249,61 @@ def wemva_adj(s, vel, image, sig, sp, rp, rdata, leg1=1, leg2=1, dtype=np.float3
              _p(m), _p(img), _p(g), _p(sp), len(sp), _p(r), _p(rp), len(rp), 0),
          nExt=s.nExt, leg1=leg1, leg2=leg2)
     return m
+
+
+def _w3(s, dtype):
+    return [np.zeros((s.nts, s.nx, s.nz), dtype) for _ in range(3)]
+
+
+def tomo_fwd_wavefields(s, vel, model, ext, sig, sp, rp, sloth=0, leg1=1, leg2=1, dtype=np.float32):
+    """(data, source d2/dt2, secondary 1, secondary 2) from the tomo forward drivers with
+    saveWavefield = 1 (time lags or offsets, with or without the free surface, by the scheme)."""
+    sp, rp = _i(sp), _i(rp)
+    m, e, g = _a(model, dtype), _a(ext, dtype), _a(sig, dtype)
+    d = np.zeros((len(rp), s.nts), dtype)
+    W = _w3(s, dtype)
+    _run("tomo", s, vel, dtype, lambda L: L.ref_tomo_fwd_wfld(_p(m), _p(d), _p(e), _p(g), _p(sp), len(sp), _p(rp),
+                                                              len(rp), *[_p(x) for x in W], int(_off(s)),
+                                                              int(_fs(s)), sloth, 0),
+         nExt=s.nExt, leg1=leg1, leg2=leg2)
+    return (d, *W)
+
+
+def tomo_adj_wavefields(s, vel, data, ext, sig, sp, rp, sloth=0, leg1=1, leg2=1, dtype=np.float32):
+    """(model, source d2/dt2, receiver wavefield, the last leg's scattered coarse samples) from
+    the tomo adjoint drivers with saveWavefield = 1."""
+    sp, rp = _i(sp), _i(rp)
+    d, e, g = _a(data, dtype), _a(ext, dtype), _a(sig, dtype)
+    m = np.zeros((s.nx, s.nz), dtype)
+    W = _w3(s, dtype)
+    _run("tomo", s, vel, dtype, lambda L: L.ref_tomo_adj_wfld(_p(m), _p(d), _p(e), _p(g), _p(sp), len(sp), _p(rp),
+                                                              len(rp), *[_p(x) for x in W], int(_off(s)),
+                                                              int(_fs(s)), sloth, 0),
+         nExt=s.nExt, leg1=leg1, leg2=leg2)
+    return (m, *W)
+
+
+def wemva_fwd_wavefields(s, vel, model, sig, sp, rp, rdata, leg1=1, leg2=1, dtype=np.float32):
+    """(image, source d2/dt2, receiver wavefield, the last leg's scattered coarse samples) from
+    the WEMVA forward drivers with saveWavefield = 1."""
+    sp, rp = _i(sp), _i(rp)
+    m, g, r = _a(model, dtype), _a(sig, dtype), _a(rdata, dtype)
+    img = np.zeros((s.nExt, s.nx, s.nz), dtype)
+    W = _w3(s, dtype)
+    _run("wemva", s, vel, dtype, lambda L: L.ref_wemva_fwd_wfld(_p(m), _p(img), _p(g), _p(sp), len(sp), _p(r), _p(rp),
+                                                                len(rp), *[_p(x) for x in W], int(_off(s)), 0),
+         nExt=s.nExt, leg1=leg1, leg2=leg2)
+    return (img, *W)
+
+
+def wemva_adj_wavefields(s, vel, image, sig, sp, rp, rdata, leg1=1, leg2=1, dtype=np.float32):
+    """(model, source d2/dt2, receiver wavefield, the last leg's scattered coarse samples) from
+    the WEMVA adjoint drivers with saveWavefield = 1."""
+    sp, rp = _i(sp), _i(rp)
+    img, g, r = _a(image, dtype), _a(sig, dtype), _a(rdata, dtype)
+    m = np.zeros((s.nx, s.nz), dtype)
+    W = _w3(s, dtype)
+    _run("wemva", s, vel, dtype, lambda L: L.ref_wemva_adj_wfld(_p(m), _p(img), _p(g), _p(sp), len(sp), _p(r), _p(rp),
+                                                                len(rp), *[_p(x) for x in W], int(_off(s)), 0),
+         nExt=s.nExt, leg1=leg1, leg2=leg2)
+    return (m, *W)

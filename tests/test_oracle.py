@@ -60,3 +60,32 @@ def test_host_prep_adjoints():
     b = rng.standard_normal((3, nts))
     assert abs(dot(orc.second_deriv(nts, dts, a), b) - dot(a, orc.second_deriv(nts, dts, b))) < 1e-9 * abs(
         dot(a, a)) / dts ** 2
+
+
+def test_tomo_wemva_saved_wavefields_leave_outputs_unchanged():
+    """Asking the oracle for the saved wavefields changes none of the operators' outputs; the
+    source d2/dt2 and the receiver wavefield are shared by the calls that compute them, and the
+    secondary fields are non-zero."""
+    import numpy as np
+    from cases import interior_mask, make_case
+    c = make_case(seed=22, nts=16, nshots=1, nExt=3, nzi=24, nxi=32)
+    s, sp, rp, sig = c.scheme, c.src_pos[0], c.rec_pos[0], c.sig[0]
+    rng = np.random.default_rng(1)
+    mask = interior_mask(c.nx, c.nz)
+    dv = rng.standard_normal((c.nx, c.nz)) * mask
+    ext = rng.standard_normal((s.nExt, c.nx, c.nz)) * mask
+    d = rng.standard_normal((len(rp), s.nts))
+    v = c.vel.astype(np.float64)
+    f = orc.tomo_fwd(s, v, dv, ext, sig, sp, rp, wavefields=True)
+    assert np.array_equal(f[0], orc.tomo_fwd(s, v, dv, ext, sig, sp, rp))
+    a = orc.tomo_adj(s, v, d, ext, sig, sp, rp, wavefields=True)
+    assert np.array_equal(a[0], orc.tomo_adj(s, v, d, ext, sig, sp, rp))
+    np.testing.assert_array_equal(f[1], a[1])
+    wf = orc.wemva_fwd(s, v, dv, sig, sp, rp, d, wavefields=True)
+    assert np.array_equal(wf[0], orc.wemva_fwd(s, v, dv, sig, sp, rp, d))
+    wa = orc.wemva_adj(s, v, ext, sig, sp, rp, d, wavefields=True)
+    assert np.array_equal(wa[0], orc.wemva_adj(s, v, ext, sig, sp, rp, d))
+    np.testing.assert_array_equal(wf[2], wa[2])
+    np.testing.assert_array_equal(a[2], wa[2])
+    for x in (f[2], f[3], a[3], wf[3], wa[3]):
+        assert np.abs(x).max() > 0
