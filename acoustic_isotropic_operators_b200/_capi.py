@@ -62,7 +62,7 @@ EXPORTED = [
     "aio_BornTimeShotsAdjFsGpuWavefield", "aio_BornOffsetShotsAdjFsGpuWavefield",
     "aio_dot_f64", "aio_context_graph_replays", "aio_context_set_budget",
     "aio_tomo_ext_forward_wavefield", "aio_tomo_ext_adjoint_wavefield", "aio_wemva_ext_forward_wavefield",
-    "aio_wemva_ext_adjoint_wavefield",
+    "aio_wemva_ext_adjoint_wavefield", "aio_context_device_bytes", "aio_context_release_buffers",
 ]
 
 
@@ -109,6 +109,9 @@ def lib():
         L.aio_context_set_budget.argtypes = [C.c_void_p, C.c_longlong]
         L.aio_context_graph_replays.restype = C.c_longlong
         L.aio_context_graph_replays.argtypes = [C.c_void_p]
+        L.aio_context_device_bytes.restype = C.c_longlong
+        L.aio_context_device_bytes.argtypes = [C.c_void_p]
+        L.aio_context_release_buffers.argtypes = [C.c_void_p]
         L.aio_dot_f64.argtypes = [C.c_int, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p,
                                   C.POINTER(C.c_double)]
         _lib = L

@@ -82,6 +82,15 @@ class Context:
         """Device-memory budget for shot buffers from now on (<= 0: 93 % of free memory)."""
         A.check(A.lib().aio_context_set_budget(self._h, int(nbytes)))
 
+    @property
+    def device_bytes(self) -> int:
+        """Device bytes the context holds (velocity constants and its per-call buffers)."""
+        return int(A.lib().aio_context_device_bytes(self._h))
+
+    def release_buffers(self) -> None:
+        """Free the per-call buffers (and captured graphs); the next call allocates them again."""
+        A.check(A.lib().aio_context_release_buffers(self._h))
+
     def capacity(self, family: int) -> int:
         return int(A.lib().aio_context_wave_capacity(self._h, family))
 

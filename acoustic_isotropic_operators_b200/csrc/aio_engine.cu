@@ -900,6 +900,29 @@ struct Context {
     DevMem tbR;                         // extended adjoint: coarse receiver samples [shot][LAG_K][isz]
     DevMem tbSS;                        // extended forward: secondary sources [shot][2 LAG_K][isz]
     DevMem tbF2;                        // tomo / WEMVA: second full coarse field [shot][nts][isz]
+
+    // Per-call buffers: every device allocation of the context but the velocity constants. They
+    // grow to the largest wave seen and are kept between calls; a request server that plans the
+    // device memory of several contexts counts them (device_bytes) and frees those of an idle
+    // context when another needs the room (release_buffers).
+    std::vector<DevMem*> call_buffers() {
+        return {&pbuf,  &ringb,    &ssb,    &wf1,      &wf2,     &wf3,     &img,     &lists,   &desc,
+                &sig,   &dat,      &aux,    &model,    &ext,     &outv,    &offBuf,  &tbState, &tbPart,
+                &tbImg, &tbW,      &tbEnt,  &tbStart,  &tbDesc,  &shotImg, &tbWscale, &tbWmax, &tbWstage,
+                &tbWover, &tbR,    &tbSS,   &tbF2};
+    }
+    long long device_bytes() {
+        long long b = (long long)(v2.bytes + rs.bytes + taper.bytes);
+        for (DevMem* m : call_buffers()) b += (long long)m->bytes;
+        return b;
+    }
+    // Frees the per-call buffers (and the captured graphs, whose launches hold their addresses).
+    void release_buffers() {
+        AIO_CK(cudaSetDevice(dev));
+        AIO_CK(cudaStreamSynchronize(st));
+        drop_graphs();
+        for (DevMem* m : call_buffers()) m->release();
+    }
     // k_tile plan: strips of HZ (multiple of 4) output rows, NQ = HZ/4 + 10 row quads,
     // 8 column pairs per quad, x-chunks of LX columns marched in blocks of 16.
     struct TBPlan {
@@ -2768,6 +2791,13 @@ AIO_API int aio_context_stats(aio_context* ctx, long long* kernels, double* step
     return AIO_OK;
 }
 AIO_API long long aio_context_graph_replays(aio_context* ctx) { return ctx ? ctx->c.graphReplays : 0; }
+AIO_API long long aio_context_device_bytes(aio_context* ctx) { return ctx ? ctx->c.device_bytes() : 0; }
+AIO_API int aio_context_release_buffers(aio_context* ctx) {
+    return guard([&] {
+        require(ctx != nullptr, "context is NULL");
+        ctx->c.release_buffers();
+    });
+}
 AIO_API int aio_context_set_budget(aio_context* ctx, long long bytes) {
     return guard([&] {
         require(ctx != nullptr, "context is NULL");

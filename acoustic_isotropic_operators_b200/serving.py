@@ -106,14 +106,24 @@ def batch_shared_bytes(g: Grid) -> int:
     return 4 * isz * 4 + (64 << 20)
 
 
+def _ctx_key(req: Request) -> Tuple:
+    """Requests with equal keys run on the same engine context (grid and velocity)."""
+    return (req.grid, req.velocity_id)
+
+
 def _engine_batch(ctx_cache: Dict, worker: int, reqs: List[Request], device: int, wavefield: str,
                   reserved: int = 0):
-    """Run one batch on this worker's context for the batch's grid (created on first use), with
-    the context's device-memory budget set to the bytes the server reserved for the batch."""
+    """Run one batch on this worker's context for the batch's grid and velocity (created on first
+    use), with the context's device-memory budget set to the bytes the server reserved for the
+    batch. The worker's other contexts free their buffers first, so that a worker holds the
+    buffers of one context at a time. Returns (results, device bytes the worker holds after)."""
     from .batch import Context
     r0 = reqs[0]
     g = r0.grid
-    key = (worker, g, r0.velocity_id)
+    key = (worker,) + _ctx_key(r0)
+    for k, c in ctx_cache.items():
+        if k[0] == worker and k != key:
+            c.release_buffers()
     ctx = ctx_cache.get(key)
     if ctx is None:
         ctx = Context(g.nz, g.nx, g.nts, g.dts, g.sub, g.dz, g.dx, g.minPad, r0.vel2dtw2, r0.refl_scale,
@@ -123,21 +133,25 @@ def _engine_batch(ctx_cache: Dict, worker: int, reqs: List[Request], device: int
         ctx.set_budget(reserved)
     shots = [r.shot for r in reqs]
     if r0.op == "nonlinear_forward":
-        return ctx.nonlinear_forward(shots)
-    if r0.op == "born_forward":
-        return ctx.born_forward(r0.model, shots)
-    return ctx.born_adjoint_shots(shots)
+        out = ctx.nonlinear_forward(shots)
+    elif r0.op == "born_forward":
+        out = ctx.born_forward(r0.model, shots)
+    else:
+        out = ctx.born_adjoint_shots(shots)
+    return out, ctx.device_bytes
 
 
 class Server:
     """Continuous-batching request server over the engine (see module docstring).
 
     run_batch(worker, requests) -> list of results may replace the engine (tests of the
-    scheduling logic on CPU)."""
+    scheduling logic on CPU); with reports_held it returns (results, bytes the worker holds after
+    the batch), as the engine does, and release(worker) frees what a worker holds."""
 
     def __init__(self, *, device: int = 0, workers: int = 2, max_batch: int = 16,
                  mem_budget_bytes: Optional[int] = None, wavefield: str = "fp32",
-                 run_batch: Optional[Callable] = None):
+                 run_batch: Optional[Callable] = None, release: Optional[Callable] = None,
+                 reports_held: bool = False):
         self.workers = workers
         self.max_batch = max_batch
         self.wavefield = wavefield
@@ -150,8 +164,14 @@ class Server:
         self.in_use = 0
         self._ctx: Dict = {}
         self._engine = run_batch is None
+        self._with_held = self._engine or reports_held
         self._run = run_batch or (lambda w, reqs, reserved=0: _engine_batch(self._ctx, w, reqs, device, wavefield,
                                                                                reserved))
+        # memory an idle worker's context keeps between batches (its buffers are reused by the next
+        # batch of the same grid and velocity): counted in in_use, freed when the room is needed
+        self._release = release or self._release_engine
+        self._held = [0] * workers
+        self._held_key: List[Optional[Tuple]] = [None] * workers
         self._queue: deque = deque()
         self._idle = list(range(workers))
         self._lock = threading.Condition()
@@ -189,12 +209,41 @@ class Server:
         self._ctx.clear()
 
     # ------------------------------------------------------------------ scheduling
-    def _take_batch(self) -> Optional[List[Request]]:
-        """Oldest waiting request plus compatible waiting ones that fit in free memory."""
+    def _release_engine(self, w: int) -> None:
+        for k, c in self._ctx.items():
+            if k[0] == w:
+                c.release_buffers()
+
+    def _release_idle(self, keep: int) -> None:
+        """Free the buffers idle workers (other than `keep`) hold, returning their bytes."""
+        for w in list(self._idle):
+            if w != keep and self._held[w] > 0:
+                self._release(w)
+                self.in_use -= self._held[w]
+                self._held[w] = 0
+                self._held_key[w] = None
+
+    def _pick_worker(self, head: Request) -> int:
+        """An idle worker whose context already holds buffers for the head's grid and velocity,
+        else the idle worker holding the least memory."""
+        key = _ctx_key(head)
+        for w in self._idle:
+            if self._held_key[w] == key:
+                return w
+        return min(self._idle, key=lambda w: self._held[w])
+
+    def _take_batch(self, w: int) -> Optional[List[Request]]:
+        """Oldest waiting request plus compatible waiting ones that fit in free memory, for
+        worker w. The memory w holds counts as free for it (reused for the same context, freed
+        otherwise); idle workers' held memory is freed when the head would not fit."""
         head = self._queue[0]
         need = batch_shared_bytes(head.grid) + shot_bytes(head, self.wbytes)
-        if self.in_use + need > self.budget:
-            return None                                   # wait for memory; no overtaking of the head
+        reuse = self._held_key[w] == _ctx_key(head)
+        if self.in_use - self._held[w] + need > self.budget:
+            self._release_idle(keep=w)
+            if self.in_use - self._held[w] + need > self.budget:
+                return None                               # wait for memory; no overtaking of the head
+        free = self.budget - (self.in_use - self._held[w])
         batch, used = [head], need
         key = head.key()
         for r in list(self._queue)[1:]:
@@ -202,13 +251,16 @@ class Server:
                 break
             if r.key() == key:
                 b = shot_bytes(r, self.wbytes)
-                if self.in_use + used + b <= self.budget:
+                if used + b <= free:
                     batch.append(r)
                     used += b
         for r in batch:
             self._queue.remove(r)
-        self.in_use += used
-        self._reserved[id(batch[0])] = used
+        reserved = max(used, self._held[w]) if reuse else used
+        self.in_use += reserved - self._held[w]
+        self._held[w] = 0
+        self._held_key[w] = None
+        self._reserved[id(batch[0])] = reserved
         return batch
 
     def _schedule(self):
@@ -216,13 +268,14 @@ class Server:
             with self._lock:
                 while True:
                     if self._queue and self._idle:
-                        batch = self._take_batch()
+                        w = self._pick_worker(self._queue[0])
+                        batch = self._take_batch(w)
                         if batch is not None:
                             break
                     if self._closing and not self._queue:
                         return
                     self._lock.wait(timeout=0.05)
-                w = self._idle.pop(0)
+                self._idle.remove(w)
             t = threading.Thread(target=self._work, args=(w, batch), daemon=True)
             self._threads.append(t)
             t.start()
@@ -233,13 +286,23 @@ class Server:
             r.start = t0
         err = None
         reserved = self._reserved[id(batch[0])]
+        held = 0
         try:
-            results = self._run(w, batch, reserved) if self._engine else self._run(w, batch)
+            if self._engine:
+                results, held = self._run(w, batch, reserved)
+            elif self._with_held:
+                results, held = self._run(w, batch)
+            else:
+                results = self._run(w, batch)
         except Exception as e:  # reported through every future of the batch
             err, results = e, [None] * len(batch)
         t1 = time.perf_counter()
         with self._lock:
             self.in_use -= self._reserved.pop(id(batch[0]))
+            if err is None and held > 0:
+                self._held[w] = held
+                self._held_key[w] = _ctx_key(batch[0])
+                self.in_use += held
             self._idle.append(w)
             self.batches.append((w, len(batch)))
             for r, res in zip(batch, results):
@@ -294,37 +357,34 @@ def _stream(n_requests: int, n_models: int, scale: float, seed: int):
     return models, reqs
 
 
-def main(argv=None):
-    import argparse
+def run_stream(requests: int = 48, models: int = 4, scale: float = 1.0, plain: int = 4, workers: int = 2,
+               max_batch: int = 16, load: float = 0.85, seed: int = 3, wavefield: str = "fp32") -> dict:
+    """Served stream against the one-shot-per-call plain path on `requests` seeded one-shot
+    requests over `models` velocity models (grids uniform in [200x400, 1000x3000] x scale, nts in
+    [1000, 4000] x scale; nonlinear forward, Born forward, Born adjoint a third each).
+
+    1. plain: the first `plain` requests, each alone through a fresh context on the per-fine-step
+       stepper (the reference's schedule), FP32;
+    2. capacity: every request submitted at once to a Server;
+    3. served: Poisson arrivals at `load` x capacity; p50 / p99 latency and shots/s."""
     import ctypes as C
-    import json
     from . import _capi
     from .batch import Context, Shot
-    ap = argparse.ArgumentParser(description="served request stream vs one-shot-per-call plain path")
-    ap.add_argument("--requests", type=int, default=48)
-    ap.add_argument("--models", type=int, default=4)
-    ap.add_argument("--scale", type=float, default=0.3, help="grid and nts scale of the served stream")
-    ap.add_argument("--plain", type=int, default=6, help="requests timed on the plain path")
-    ap.add_argument("--workers", type=int, default=2)
-    ap.add_argument("--max-batch", type=int, default=16)
-    ap.add_argument("--load", type=float, default=0.85, help="arrival rate as a fraction of measured capacity")
-    ap.add_argument("--seed", type=int, default=3)
-    a = ap.parse_args(argv)
     lib = _capi.lib()
-    models, stream = _stream(a.requests, a.models, a.scale, a.seed)
+    mods, stream = _stream(requests, models, scale, seed)
     prepared = []
-    for g, vel, shots in models:
+    for g, vel, _ in mods:
         v2 = np.zeros(g.nz * g.nx, np.float32)
         rs = np.zeros_like(v2)
         velf = np.ascontiguousarray(vel.reshape(-1), np.float32)
-        lib.aio_fd_precompute(g.nz, g.nx, C.c_float(g.dts), g.sub, velf.ctypes.data_as(C.c_void_p),
-                              v2.ctypes.data_as(C.c_void_p), rs.ctypes.data_as(C.c_void_p))
+        _capi.check(lib.aio_fd_precompute(g.nz, g.nx, C.c_float(g.dts), g.sub, velf.ctypes.data_as(C.c_void_p),
+                                          v2.ctypes.data_as(C.c_void_p), rs.ctypes.data_as(C.c_void_p)))
         prepared.append((v2, rs))
 
-    def make(k, op, seed):
-        g, _, shots = models[k]
+    def make(k, op, rseed):
+        g, _, shots = mods[k]
         v2, rs = prepared[k]
-        rng = np.random.default_rng(seed)
+        rng = np.random.default_rng(rseed)
         a_ = shots[int(rng.integers(len(shots)))]
         sig = (np.sin(np.arange(g.ntw) * 0.01 * (1 + rng.random()))[None, :] * 1e-2).astype(np.float32)
         sig = np.repeat(sig, len(a_.src_pos), axis=0)
@@ -334,52 +394,73 @@ def main(argv=None):
         return Request(op=op, grid=g, velocity_id=f"m{k}", vel2dtw2=v2, refl_scale=rs,
                        shot=Shot(a_.src_pos, a_.rec_pos, sig, data), model_id=f"m{k}", model=m)
 
-    def run_alone(r, stepper):
+    def run_alone(r):
         ctx = Context(r.grid.nz, r.grid.nx, r.grid.nts, r.grid.dts, r.grid.sub, r.grid.dz, r.grid.dx, r.grid.minPad,
-                      r.vel2dtw2, r.refl_scale, image_fp64=True, stepper=stepper)
-        t0 = time.perf_counter()
-        if r.op == "nonlinear_forward":
-            ctx.nonlinear_forward([r.shot])
-        elif r.op == "born_forward":
-            ctx.born_forward(r.model, [r.shot])
-        else:
-            ctx.born_adjoint([r.shot])
-        dt = time.perf_counter() - t0
-        ctx.close()
-        return dt
+                      r.vel2dtw2, r.refl_scale, image_fp64=True, stepper="fine")
+        try:
+            t0 = time.perf_counter()
+            if r.op == "nonlinear_forward":
+                ctx.nonlinear_forward([r.shot])
+            elif r.op == "born_forward":
+                ctx.born_forward(r.model, [r.shot])
+            else:
+                ctx.born_adjoint([r.shot])
+            return time.perf_counter() - t0
+        finally:
+            ctx.close()
 
-    # plain path: one shot per call, the reference's per-fine-step schedule, FP32
-    plain = [run_alone(make(*stream[i]), "fine") for i in range(min(a.plain, len(stream)))]
-    plain_rate = len(plain) / sum(plain)
-    # capacity probe: everything submitted at once
-    srv = Server(workers=a.workers, max_batch=a.max_batch)
-    for f in [srv.submit(make(*s)) for s in stream]:
-        f.result()
-    cap = srv.report()["shots_per_s"]
-    srv.close()
-    # served stream: Poisson arrivals at `load` x capacity
-    rate = a.load * cap
-    gaps = np.random.default_rng(a.seed + 1).exponential(1.0 / rate, len(stream))
-    srv = Server(workers=a.workers, max_batch=a.max_batch)
-    futs = []
-    t0 = time.perf_counter()
-    for gap, s in zip(gaps, stream):
-        t0 += gap
-        time.sleep(max(0.0, t0 - time.perf_counter()))
-        r = make(*s)
-        r.arrival = time.perf_counter()
-        futs.append(srv.submit(r))
-    for f in futs:
-        f.result()
-    rep = srv.report()
-    srv.close()
+    plain_t = [run_alone(make(*stream[i])) for i in range(min(plain, len(stream)))]
+    plain_rate = len(plain_t) / sum(plain_t)
+    srv = Server(workers=workers, max_batch=max_batch, wavefield=wavefield)
+    try:
+        for f in [srv.submit(make(*x)) for x in stream]:
+            f.result()
+        cap = srv.report()["shots_per_s"]
+    finally:
+        srv.close()
+    rate = load * cap
+    gaps = np.random.default_rng(seed + 1).exponential(1.0 / rate, len(stream))
+    srv = Server(workers=workers, max_batch=max_batch, wavefield=wavefield)
+    try:
+        futs = []
+        t0 = time.perf_counter()
+        for gap, x in zip(gaps, stream):
+            t0 += gap
+            time.sleep(max(0.0, t0 - time.perf_counter()))
+            r = make(*x)
+            r.arrival = time.perf_counter()
+            futs.append(srv.submit(r))
+        for f in futs:
+            f.result()
+        rep = srv.report()
+    finally:
+        srv.close()
+    return {"shots_per_s": rep["shots_per_s"], "p50_s": rep["p50_s"], "p99_s": rep["p99_s"],
+            "mean_batch": rep["mean_batch"], "gpts_per_s": rep["gpts_per_s"], "capacity_shots_per_s": cap,
+            "arrival_rate": rate, "load": load, "plain_shots_per_s": plain_rate, "plain_requests": len(plain_t),
+            "vs_plain": rep["shots_per_s"] / plain_rate, "capacity_vs_plain": cap / plain_rate,
+            "requests": len(stream), "models": models, "scale": scale, "workers": workers,
+            "max_batch": max_batch, "wavefield": wavefield,
+            "grids": [[g.nz, g.nx, g.nts, g.sub] for g, _, _ in mods]}
+
+
+def main(argv=None):
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="served request stream vs one-shot-per-call plain path")
+    ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--models", type=int, default=4)
+    ap.add_argument("--scale", type=float, default=1.0, help="grid and nts scale of the served stream")
+    ap.add_argument("--plain", type=int, default=4, help="requests timed on the plain path")
+    ap.add_argument("--workers", type=int, default=2)
+    ap.add_argument("--max-batch", type=int, default=16)
+    ap.add_argument("--load", type=float, default=0.85, help="arrival rate as a fraction of measured capacity")
+    ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--wavefield", default="fp32", choices=("fp32", "bf16", "fp16"))
+    a = ap.parse_args(argv)
+    out = run_stream(a.requests, a.models, a.scale, a.plain, a.workers, a.max_batch, a.load, a.seed, a.wavefield)
     print(json.dumps({"metric": "served shots/s (one-shot requests, mixed grids and operators)",
-                      "value": rep["shots_per_s"], "unit": "shots/s", "p50_s": rep["p50_s"], "p99_s": rep["p99_s"],
-                      "mean_batch": rep["mean_batch"], "capacity_shots_per_s": cap, "arrival_rate": rate,
-                      "plain_shots_per_s": plain_rate, "vs_plain": rep["shots_per_s"] / plain_rate,
-                      "capacity_vs_plain": cap / plain_rate, "requests": len(stream), "models": a.models,
-                      "scale": a.scale, "workers": a.workers,
-                      "grids": [[g.nz, g.nx, g.nts, g.sub] for g, _, _ in models]}))
+                      "value": out["shots_per_s"], "unit": "shots/s", **out}))
 
 
 if __name__ == "__main__":

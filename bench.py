@@ -78,6 +78,11 @@ def parse():
     ap.add_argument("--plain", type=int, default=0,
                     help="instead of the batched step: time N shots one per call on the per-fine-step "
                          "stepper (the reference's schedule), FP32, and print that line")
+    ap.add_argument("--serve", type=int, default=0,
+                    help="instead of the Born step: N > 0 one-shot requests (nonlinear forward, Born forward, "
+                         "Born adjoint) on 4 models with grids in 200x400..1000x3000 and nts in 1000..4000, "
+                         "served with Poisson arrivals at 85%% of measured capacity; prints that line")
+    ap.add_argument("--serve-models", type=int, default=4)
     ap.add_argument("--no-configs", action="store_true",
                     help="leave out the other configurations' sub-objects of the default line")
     return ap.parse_args()
@@ -473,7 +478,25 @@ def other_configs(args, batched_value):
     a = copy.copy(args)
     a.tomo, a.tomo_nts, a.stepper = 2, 3000, "auto"
     out["tomo_wemva_2_shots"] = run_tomo(a, emit=False)
+    a = copy.copy(args)
+    a.serve = 32
+    out["served_stream"] = run_serve(a, emit=False)
     return out
+
+
+def run_serve(args, emit=True):
+    """Served request stream (continuous batching over the engine) against the plain
+    one-shot-per-call path: seeded one-shot requests on `serve_models` velocity models with grids
+    uniform in 200x400..1000x3000 and nts uniform in 1000..4000, Poisson arrivals at 85 % of the
+    capacity measured on the same stream; p50 / p99 latency and shots/s."""
+    from acoustic_isotropic_operators_b200.serving import run_stream
+    out = run_stream(requests=args.serve, models=args.serve_models, scale=1.0, plain=4, workers=2,
+                     max_batch=16, load=0.85, seed=3, wavefield="fp32")
+    line = {"metric": "served shots/s (one-shot requests, mixed grids and operators)", "value": out["shots_per_s"],
+            "unit": "shots/s", "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded)", **out}
+    if emit:
+        print(json.dumps(line))
+    return line
 
 
 def main():
@@ -490,6 +513,8 @@ def main():
         return run_variants(args)
     if args.nl:
         return run_nl(args)
+    if args.serve:
+        return run_serve(args)
 
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -127,6 +127,13 @@ int aio_context_reset_stats(aio_context* ctx);
  * environment (read at context creation) and live stepper timing (aio_context_profile) keep the
  * direct launches. */
 long long aio_context_graph_replays(aio_context* ctx);
+/* Device bytes the context holds: velocity constants plus its per-call buffers, which grow to the
+ * largest wave the context has run and stay allocated between calls. */
+long long aio_context_device_bytes(aio_context* ctx);
+/* Frees the context's per-call buffers (the next call allocates them again) and its captured
+ * CUDA graphs; waits for the context's stream first. For servers that plan the memory of many
+ * contexts on one device. */
+int aio_context_release_buffers(aio_context* ctx);
 
 /* Nonlinear: model = source traces (sourcesSignals), data per shot. */
 int aio_nonlinear_forward(aio_context* ctx, int nShots, const aio_shot* shots, int memSpace);

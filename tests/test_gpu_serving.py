@@ -1,8 +1,10 @@
 """Serving loop on the GPU: a mix of nonlinear-forward, Born-forward and
-Born-adjoint requests on two grids, arriving while earlier batches run, gives
-for every request the same result as that request run alone (relative L2
-<= 1e-6; shots of a launch are computed independently, so the results agree
-to round-off of identical arithmetic)."""
+Born-adjoint requests on two grids and three velocity models (two of them on the
+same grid), arriving while earlier batches run, gives for every request the same
+result as that request run alone (relative L2 <= 1e-6; shots of a launch are
+computed independently, so the results agree to round-off of identical
+arithmetic). A context's per-call buffers are counted and can be released
+between calls without changing its results."""
 import time
 
 import numpy as np
@@ -40,7 +42,8 @@ def make_shot(g, rng, with_data):
 def test_results_alone_equal_results_in_the_mix():
     from acoustic_isotropic_operators_b200.batch import Context
     from acoustic_isotropic_operators_b200.serving import Request, Server
-    cases = [grid_case(1, 64, 96, 36), grid_case(2, 96, 128, 28)]
+    # velocity models v0 and v2 share a grid: they run on separate contexts, overlapping on the device
+    cases = [grid_case(1, 64, 96, 36), grid_case(2, 96, 128, 28), grid_case(3, 64, 96, 36)]
     reqs = []
     for gi, (g, v2, rs, m, rng) in enumerate(cases):
         for op in ("nonlinear_forward", "born_forward", "born_adjoint"):
@@ -75,3 +78,22 @@ def test_results_alone_equal_results_in_the_mix():
         assert rel_l2(got[i], alone) <= 1e-6, (r.op, rel_l2(got[i], alone))
     rep = srv.report()
     assert rep["requests"] == len(reqs) and rep["p99_s"] >= rep["p50_s"]
+
+
+def test_context_buffers_counted_and_released():
+    from acoustic_isotropic_operators_b200.batch import Context
+    g, v2, rs, m, rng = grid_case(4, 64, 96, 36)
+    shots = [make_shot(g, rng, False) for _ in range(3)]
+    ctx = Context(g.nz, g.nx, g.nts, g.dts, g.sub, g.dz, g.dx, g.minPad, v2, rs, image_fp64=True)
+    try:
+        base = ctx.device_bytes
+        first = [d.copy() for d in ctx.born_forward(m, shots)]
+        held = ctx.device_bytes
+        assert held > base + g.nts * (g.nz - 10) * (g.nx - 10) * 4 * len(shots)  # stored wavefields
+        ctx.release_buffers()
+        assert ctx.device_bytes == base
+        again = ctx.born_forward(m, shots)
+        for a, b in zip(first, again):
+            assert rel_l2(a, b) <= 1e-6
+    finally:
+        ctx.close()

@@ -20,6 +20,7 @@ def req(op, grid, tag, vid="v0"):
 
 G1 = Grid(42, 58, 20, 0.004, 2, 10.0, 10.0, 8)
 G2 = Grid(74, 90, 30, 0.004, 2, 10.0, 10.0, 8)
+G3 = Grid(522, 1322, 30, 0.004, 2, 10.0, 10.0, 8)
 
 
 class FakeEngine:
@@ -99,3 +100,36 @@ def test_engine_error_reaches_every_future_of_its_batch():
         fb.result(timeout=10)
     assert fc.result(timeout=10) == ("result", "other")
     srv.close()
+
+
+def test_held_buffers_are_counted_reused_and_released():
+    """Memory a worker's context keeps after a batch counts against the budget while the worker
+    is idle: a batch of the same grid and velocity goes to that worker and reuses it, and when the
+    head of the queue would not fit otherwise, idle workers free what they hold."""
+    one = batch_shared_bytes(G2) + shot_bytes(req("born_adjoint", G2, 0))
+    budget = 3 * one
+    released, peaks = [], []
+    srv = None
+
+    def run(worker, reqs):
+        peaks.append(srv.in_use)
+        time.sleep(0.02)
+        return [("result", r.shot.tag) for r in reqs], one     # each worker keeps one batch's bytes
+
+    srv = Server(workers=3, max_batch=1, mem_budget_bytes=budget, run_batch=run, reports_held=True,
+                 release=lambda w: released.append(w))
+    # three velocities one after the other: every worker ends up holding buffers
+    for i, vid in enumerate(("v0", "v1", "v2")):
+        srv.submit(req("born_adjoint", G2, i, vid=vid)).result(timeout=10)
+    with srv._lock:
+        assert sum(srv._held) == srv.in_use
+    # same velocity as a holder: its worker reuses the buffers, nobody releases
+    srv.submit(req("born_adjoint", G2, "again", vid="v1")).result(timeout=10)
+    assert released == []
+    # a larger request on another grid needs more than one holder's room: idle holders free theirs
+    big = req("born_adjoint", G3, "big", vid="v3")
+    assert one < batch_shared_bytes(G3) + shot_bytes(big) <= budget
+    srv.submit(big).result(timeout=10)
+    assert released
+    srv.close()
+    assert max(peaks) <= budget
