@@ -312,8 +312,9 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
     const int xs = x0 - 5 * T;
 
     // ---- shared set-up: zero rings, column damping table, sparse entries
-    const int nRing = kt_ringcols(MODE) * RS;
-    for (int i = tid; i < nRing; i += blockDim.x) ring[i] = 0.f;
+    static_assert(RS % 4 == 0, "ring columns are whole float4s");
+    const int nRing4 = kt_ringcols(MODE) * (RS / 4);
+    for (int i = tid; i < nRing4; i += blockDim.x) kt_smem4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int i = tid; i < nDx; i += blockDim.x) {
         injFirst[i] = -1;
         recFirst[i] = -1;

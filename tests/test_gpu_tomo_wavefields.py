@@ -69,7 +69,7 @@ def test_tomo_wavefields(base, name, kw):
     ref_a = refgpu.tomo_adj_wavefields(s, base.vel, d, ext, sig, sp, rp)
     orc_a = orc.tomo_adj(s, base.vel, d, ext, sig, sp, rp, dtype=np.float32, wavefields=True)
     _check(got_a, ref_a, orc_a, "tomo adjoint")
-    assert all(np.abs(x).max() > 0 for x in got_f[1:] + got_a[1:])
+    assert all(np.abs(x).max() > 0 for x in list(got_f[1:]) + list(got_a[1:]))
 
 
 @pytest.mark.parametrize("name,kw", SCHEMES[:2], ids=[x[0] for x in SCHEMES[:2]])
