@@ -998,6 +998,39 @@ struct Context {
     std::map<int, TBPlan> tbTuned;
     TBPlan tbLast;  // plan of the most recent blocked launch
 
+    // Plans measured by any context of the process, shared by the contexts of the same device,
+    // interior size, free-surface setting and stored precision: a new context (a request server
+    // opens one per grid and velocity model) takes them instead of timing the candidates again.
+    // The velocity model does not enter a launch's duration.
+    static std::map<std::vector<int>, TBPlan>& shared_plans() {
+        static std::map<std::vector<int>, TBPlan> m;
+        return m;
+    }
+    static std::mutex& shared_plans_mu() {
+        static std::mutex mu;
+        return mu;
+    }
+    std::vector<int> shared_plan_key(int k) const {
+        return {dev, g.nzi, g.nxi, k, P.freeSurface, P.wavefieldPrecision};
+    }
+    // The shared plans of waves of nb shots, when every class has one that fits these shots.
+    bool tb_take_shared(int nb, const aio_shot* shots, bool nonlinear) {
+        const std::vector<int> classes = nonlinear ? std::vector<int>{TB_NLC} : std::vector<int>{TB_LIGHT, TB_HEAVY, TB_RECV};
+        std::vector<TBPlan> got;
+        {
+            std::lock_guard<std::mutex> lk(shared_plans_mu());
+            for (int c : classes) {
+                auto it = shared_plans().find(shared_plan_key(4 * nb + c));
+                if (it == shared_plans().end()) return false;
+                got.push_back(it->second);
+            }
+        }
+        for (const TBPlan& pl : got)
+            if (!tb_plan_fits(pl, tb_max_entries(pl, nb, shots))) return false;
+        for (size_t i = 0; i < classes.size(); i++) tbTuned[4 * nb + classes[i]] = got[i];
+        return true;
+    }
+
     // Largest sparse-entry counts one CTA of plan pl holds, per kind of pass: sources injected
     // over the halo region plus receivers recorded in the output region (SRC, NL), receivers
     // recorded (SCAT, SCATX), receivers injected over the halo region plus sources recorded
@@ -1062,6 +1095,7 @@ struct Context {
     // columns. nonlinear: the NL class alone is timed (its launch with recording off).
     void tb_autotune(int nb, const aio_shot* shots, bool nonlinear = false) {
         if (P.chunkColumns != 0 || tbTuned.count(4 * nb + (nonlinear ? TB_NLC : TB_LIGHT))) return;
+        if (tb_take_shared(nb, shots, nonlinear)) return;
         const bool small = (long long)tb_model_plan(nb, 128, 0, 0, 1).nStrips * std::max(1, g.nxi / 48) * nb <
                            2LL * smCount;
         std::vector<int> heights = {128, 112, 96, 80, 64};
@@ -1200,6 +1234,9 @@ struct Context {
             tbTuned[4 * nb + TB_HEAVY] = bestHeavy;
             tbTuned[4 * nb + TB_RECV] = bestRecv;
         }
+        std::lock_guard<std::mutex> lk(shared_plans_mu());
+        for (int c : nonlinear ? std::vector<int>{TB_NLC} : std::vector<int>{TB_LIGHT, TB_HEAVY, TB_RECV})
+            shared_plans()[shared_plan_key(4 * nb + c)] = tbTuned[4 * nb + c];
     }
 
     // Per-CTA sparse lists of every shot of a wave. inj: 0 none, 1 sources, 2 receivers

@@ -121,7 +121,7 @@ def _engine_batch(ctx_cache: Dict, worker: int, reqs: List[Request], device: int
     r0 = reqs[0]
     g = r0.grid
     key = (worker,) + _ctx_key(r0)
-    for k, c in ctx_cache.items():
+    for k, c in list(ctx_cache.items()):
         if k[0] == worker and k != key:
             c.release_buffers()
     ctx = ctx_cache.get(key)
@@ -210,7 +210,7 @@ class Server:
 
     # ------------------------------------------------------------------ scheduling
     def _release_engine(self, w: int) -> None:
-        for k, c in self._ctx.items():
+        for k, c in list(self._ctx.items()):
             if k[0] == w:
                 c.release_buffers()
 
@@ -357,7 +357,7 @@ def _stream(n_requests: int, n_models: int, scale: float, seed: int):
     return models, reqs
 
 
-def run_stream(requests: int = 48, models: int = 4, scale: float = 1.0, plain: int = 4, workers: int = 2,
+def run_stream(requests: int = 48, models: int = 4, scale: float = 1.0, plain: int = 4, workers: int = 3,
                max_batch: int = 16, load: float = 0.85, seed: int = 3, wavefield: str = "fp32") -> dict:
     """Served stream against the one-shot-per-call plain path on `requests` seeded one-shot
     requests over `models` velocity models (grids uniform in [200x400, 1000x3000] x scale, nts in
@@ -452,7 +452,7 @@ def main(argv=None):
     ap.add_argument("--models", type=int, default=4)
     ap.add_argument("--scale", type=float, default=1.0, help="grid and nts scale of the served stream")
     ap.add_argument("--plain", type=int, default=4, help="requests timed on the plain path")
-    ap.add_argument("--workers", type=int, default=2)
+    ap.add_argument("--workers", type=int, default=3)
     ap.add_argument("--max-batch", type=int, default=16)
     ap.add_argument("--load", type=float, default=0.85, help="arrival rate as a fraction of measured capacity")
     ap.add_argument("--seed", type=int, default=3)

@@ -490,7 +490,7 @@ def run_serve(args, emit=True):
     uniform in 200x400..1000x3000 and nts uniform in 1000..4000, Poisson arrivals at 85 % of the
     capacity measured on the same stream; p50 / p99 latency and shots/s."""
     from acoustic_isotropic_operators_b200.serving import run_stream
-    out = run_stream(requests=args.serve, models=args.serve_models, scale=1.0, plain=4, workers=2,
+    out = run_stream(requests=args.serve, models=args.serve_models, scale=1.0, plain=4, workers=3,
                      max_batch=16, load=0.85, seed=3, wavefield="fp32")
     line = {"metric": "served shots/s (one-shot requests, mixed grids and operators)", "value": out["shots_per_s"],
             "unit": "shots/s", "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded)", **out}
