@@ -396,20 +396,63 @@ __device__ __forceinline__ float lag_wsample(const void* __restrict__ W, long lo
 // column holds consecutive samples in pairs (one float2 per pair): every lag offset 2h - 2(e-h)
 // is even, so sample pairs (k, k+1) of any lag are one aligned float2 and the inner products
 // run on paired FP32 instructions. W is stored in FP32, BF16 or FP16 with per-slice scales sc.
+//
+// 16-bit samples: the two lanes of a point pair (p even, p + 1; slices are a whole number of
+// warps, isz % 32 == 0, so both lanes always run) share 32-bit loads. For each sample pair
+// (k, k+1) the even lane loads the pair's word of slice k, the odd lane the word of slice k+1,
+// and one shuffle hands each lane the other word: every lane then holds its own point's two
+// samples. Half the load instructions of one 16-bit load per sample, four bytes per lane.
+template <int WP>
+__device__ __forceinline__ float lag_half(unsigned word, bool high) {
+    const unsigned short u = (unsigned short)(high ? (word >> 16) : (word & 0xffffu));
+    if (WP == TBW_BF16) return __bfloat162float(__ushort_as_bfloat16(u));
+    return __half2float(__ushort_as_half(u));
+}
 template <int WP = TBW_F32>
 __device__ __forceinline__ void lag_window(float2* W2, const void* __restrict__ W, const float* __restrict__ sc,
                                            long long isz, long long p, int tlo, int hExt, int nts) {
     const int n = lag_window_len(hExt), t0 = tlo - 2 * hExt;
-    for (int k0 = 0; k0 < n; k0 += 2 * LAG_B) {
-        float v[2 * LAG_B];
+    if constexpr (WP == TBW_F32) {
+        for (int k0 = 0; k0 < n; k0 += 2 * LAG_B) {
+            float v[2 * LAG_B];
 #pragma unroll
-        for (int j = 0; j < 2 * LAG_B; j++) {
-            const int tau = t0 + k0 + j;
-            v[j] = (k0 + j < n && tau >= 0 && tau < nts) ? lag_wsample<WP>(W, (long long)tau * isz + p, sc, tau) : 0.f;
+            for (int j = 0; j < 2 * LAG_B; j++) {
+                const int tau = t0 + k0 + j;
+                v[j] = (k0 + j < n && tau >= 0 && tau < nts) ? lag_wsample<WP>(W, (long long)tau * isz + p, sc, tau)
+                                                             : 0.f;
+            }
+#pragma unroll
+            for (int j = 0; j < 2 * LAG_B; j += 2)
+                if (k0 + j < n) W2[((k0 + j) >> 1) * LAG_NP] = make_float2(v[j], v[j + 1]);
         }
+    } else {
+        const bool odd = (p & 1) != 0;
+        const unsigned* __restrict__ W32 = reinterpret_cast<const unsigned*>(W);
+        const long long iszw = isz >> 1, pw = p >> 1;
+        for (int k0 = 0; k0 < n; k0 += 2 * LAG_B) {
+            unsigned wv[LAG_B];
 #pragma unroll
-        for (int j = 0; j < 2 * LAG_B; j += 2)
-            if (k0 + j < n) W2[((k0 + j) >> 1) * LAG_NP] = make_float2(v[j], v[j + 1]);
+            for (int j = 0; j < LAG_B; j++) {
+                const int k = k0 + 2 * j + (odd ? 1 : 0);  // the sample this lane loads
+                const int tau = t0 + k;
+                wv[j] = (k < n && tau >= 0 && tau < nts) ? __ldg(W32 + (long long)tau * iszw + pw) : 0u;
+            }
+#pragma unroll
+            for (int j = 0; j < LAG_B; j++) {
+                const unsigned other = __shfl_xor_sync(0xffffffffu, wv[j], 1);
+                const int k = k0 + 2 * j;
+                if (k < n) {
+                    float va = lag_half<WP>(odd ? other : wv[j], odd);  // sample k of this point
+                    float vb = lag_half<WP>(odd ? wv[j] : other, odd);  // sample k + 1
+                    if (WP == TBW_F16) {
+                        const int ta = t0 + k;
+                        va *= (ta >= 0 && ta < nts) ? __ldg(sc + ta) : 0.f;
+                        vb *= (ta + 1 >= 0 && ta + 1 < nts) ? __ldg(sc + ta + 1) : 0.f;
+                    }
+                    W2[(k >> 1) * LAG_NP] = make_float2(va, vb);
+                }
+            }
+        }
     }
 }
 // W: stored wavefield of WSt elements per shot (FP32, or BF16 / FP16 with nts scales per shot
