@@ -1479,11 +1479,12 @@ struct Context {
 
     // Scattered pass with data recording (F/src/BornShotsGpuFunctions.cu:323-376); W: the stored
     // field the secondary sources dm * W come from (default: the source wavefield tbW).
+    // A caller's W (the tomo forward's scattered field) is FP32 whatever the stored precision.
     void tb_scat_pass(int nb, const aio_shot* shots, const float* dm, const float* W = nullptr) {
         const TBPlan pl = tb_plan(nb, true);
         const int maxEnt = tb_lists(pl, nb, shots, 0, true);
         tb_zero(nb, false);
-        tb_desc(pl, nb, false, false, true, W ? (void*)W : tbW.p, false);
+        tb_desc(pl, nb, false, false, true, W ? (void*)W : tbW.p, false, W ? g.nts : 0);
         KTArgs a = tb_args(pl, maxEnt, dm);
         tbLast = pl;
         graph_loop({2, nb, pl.HZ, pl.nStrips, pl.LX, pl.nChunks, maxEnt, (long long)tbDesc.p, (long long)dm,
@@ -1491,7 +1492,8 @@ struct Context {
                    [&] {
                        for (int its = 0; its < g.nts - 1; its++) {
                            a.its = its;
-                           tb_launch<TB_SCAT>(pl, nb, a, its & 1);
+                           if (W) tb_launch_t<TB_SCAT, TBW_F32>(pl, nb, a, its & 1);
+                           else tb_launch<TB_SCAT>(pl, nb, a, its & 1);
                        }
                    });
     }
@@ -1710,24 +1712,38 @@ struct Context {
     static constexpr int TB_RING = 2 * LAG_K;  // source and sample rings: two blocks of LAG_K
 
     struct TBSrc {                // dense secondary sources of a pass
-        const float* F = nullptr;   // full coarse field [shot][nts][isz]
+        const void* F = nullptr;    // full coarse field [shot][nts][isz], precision wp
         const float* ext = nullptr; // lag sources ss(t) = sum_e ext[e] F[t - sign 2(e-h)]; null: F (times dm)
         const float* dm = nullptr;  // zero-lag sources: dm * F(t) (null: F(t))
         int sign = 1;
+        int wp = TBW_F32;           // F's precision: FP32, or the 16-bit source field (tbW, scales tbWscale)
     };
     struct TBOut {                // what a pass does with its coarse samples
         float* full = nullptr;      // store all of them [shot][nts][isz]
-        const float* imgF = nullptr;// else image them against this full field (ring of TB_RING samples)
+        const void* imgF = nullptr; // else image them against this full field (ring of TB_RING samples)
         bool lag = false;           // time-lag image (nExt slices) or zero-lag (one slice)
         int sign = 1;
+        int wp = TBW_F32;           // imgF's precision (as TBSrc::wp)
     };
+    // precision of the tomo / WEMVA source field d2/dt2 (tbW) on the blocked stepper: the stored
+    // precision (16-bit with per-slice scales for FP16)
+    int src_wp() const {
+        return P.wavefieldPrecision == AIO_WFLD_BF16 ? TBW_BF16 : (P.wavefieldPrecision == AIO_WFLD_FP16 ? TBW_F16 : TBW_F32);
+    }
 
     void tb_lag_attr() {
         static int lagDev = -1;
         if (lagDev == dev) return;
-        AIO_CK(cudaFuncSetAttribute(k_img_lag_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        AIO_CK(cudaFuncSetAttribute(k_img_lag_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        AIO_CK(cudaFuncSetAttribute(k_ss_lag_block<TBW_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        const int b = 200 * 1024;
+        AIO_CK(cudaFuncSetAttribute(k_img_lag_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+        AIO_CK(cudaFuncSetAttribute(k_img_lag_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+        AIO_CK(cudaFuncSetAttribute(k_img_lag_block<double, TBW_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+        AIO_CK(cudaFuncSetAttribute(k_img_lag_block<float, TBW_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+        AIO_CK(cudaFuncSetAttribute(k_img_lag_block<double, TBW_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+        AIO_CK(cudaFuncSetAttribute(k_img_lag_block<float, TBW_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+        AIO_CK(cudaFuncSetAttribute(k_ss_lag_block<TBW_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+        AIO_CK(cudaFuncSetAttribute(k_ss_lag_block<TBW_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
+        AIO_CK(cudaFuncSetAttribute(k_ss_lag_block<TBW_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, b));
         lagDev = dev;
     }
     size_t tb_lag_smem(int hExt) const {
@@ -1740,9 +1756,18 @@ struct Context {
         tb_lag_attr();
         const int nP = LAG_NP;
         const dim3 grid((unsigned)((g.isz + nP - 1) / nP), nb);
-        k_ss_lag_block<TBW_F32><<<grid, nP, tb_lag_smem(g.hExt), st>>>(tbSS.as<float>(), (long long)TB_RING * g.isz, TB_RING,
-                                                                src.ext, src.F, wfSt(), g.isz, tlo, thi, g.nts, g.hExt,
-                                                                g.nExt, src.sign);
+        const size_t sm = tb_lag_smem(g.hExt);
+        const long long rSt = (long long)TB_RING * g.isz;
+        float* ss = tbSS.as<float>();
+        if (src.wp == TBW_BF16)
+            k_ss_lag_block<TBW_BF16><<<grid, nP, sm, st>>>(ss, rSt, TB_RING, src.ext, src.F, wfSt(), g.isz, tlo, thi,
+                                                           g.nts, g.hExt, g.nExt, src.sign);
+        else if (src.wp == TBW_F16)
+            k_ss_lag_block<TBW_F16><<<grid, nP, sm, st>>>(ss, rSt, TB_RING, src.ext, src.F, wfSt(), g.isz, tlo, thi,
+                                                          g.nts, g.hExt, g.nExt, src.sign, tbWscale.as<float>());
+        else
+            k_ss_lag_block<TBW_F32><<<grid, nP, sm, st>>>(ss, rSt, TB_RING, src.ext, src.F, wfSt(), g.isz, tlo, thi,
+                                                          g.nts, g.hExt, g.nExt, src.sign);
         kcheck();
     }
     // image the samples [tlo, thi] of the ring tbR against out.imgF
@@ -1752,12 +1777,21 @@ struct Context {
         const dim3 grid((unsigned)((g.isz + nP - 1) / nP), nb);
         const long long mSt = (long long)nE * g.isz, rSt = (long long)TB_RING * g.isz;
         const size_t sm = tb_lag_smem(hE);
-        if (P.imageFp64)
-            k_img_lag_block<double><<<grid, nP, sm, st>>>(img.as<double>(), mSt, tbR.as<float>(), rSt, TB_RING,
-                                                          out.imgF, wfSt(), g.isz, tlo, thi, g.nts, hE, nE, out.sign);
-        else
-            k_img_lag_block<float><<<grid, nP, sm, st>>>(img.as<float>(), mSt, tbR.as<float>(), rSt, TB_RING,
-                                                         out.imgF, wfSt(), g.isz, tlo, thi, g.nts, hE, nE, out.sign);
+        const float* R = tbR.as<float>();
+        const float* sc = out.wp == TBW_F16 ? tbWscale.as<float>() : nullptr;
+#define AIO_TB_IMG(ACC, WP)                                                                                         \
+    k_img_lag_block<ACC, WP><<<grid, nP, sm, st>>>(img.as<ACC>(), mSt, R, rSt, TB_RING, out.imgF, wfSt(), g.isz, tlo, \
+                                                   thi, g.nts, hE, nE, out.sign, sc)
+        if (P.imageFp64) {
+            if (out.wp == TBW_BF16) AIO_TB_IMG(double, TBW_BF16);
+            else if (out.wp == TBW_F16) AIO_TB_IMG(double, TBW_F16);
+            else AIO_TB_IMG(double, TBW_F32);
+        } else {
+            if (out.wp == TBW_BF16) AIO_TB_IMG(float, TBW_BF16);
+            else if (out.wp == TBW_F16) AIO_TB_IMG(float, TBW_F16);
+            else AIO_TB_IMG(float, TBW_F32);
+        }
+#undef AIO_TB_IMG
         kcheck();
     }
 
@@ -1769,8 +1803,12 @@ struct Context {
         const int maxEnt = tb_lists(pl, nb, shots, 0, false);
         tb_zero(nb, false);
         const bool lagSrc = src.ext != nullptr;
-        tb_desc(pl, nb, false, false, false, lagSrc ? tbSS.p : (void*)src.F, false, lagSrc ? TB_RING : g.nts,
-                out.full ? out.full : tbR.as<float>(), out.full ? g.nts : TB_RING);
+        // zero-lag sources straight from a 16-bit source field: W is that field (wSlices 0: the
+        // stored precision's element size), read with its per-slice scales
+        const int wp = lagSrc ? TBW_F32 : src.wp;
+        tb_desc(pl, nb, false, false, false, lagSrc ? tbSS.p : const_cast<void*>(src.F), false,
+                lagSrc ? TB_RING : (wp == TBW_F32 ? g.nts : 0), out.full ? out.full : tbR.as<float>(),
+                out.full ? g.nts : TB_RING);
         KTArgs a = tb_args(pl, maxEnt, lagSrc ? nullptr : src.dm);
         int lo = 0;  // lowest sample not yet imaged
         for (int its = 0; its < g.nts - 1; its++) {
@@ -1786,7 +1824,9 @@ struct Context {
             a.oA = out.full ? its : its % TB_RING;
             a.oB = out.full ? its + 1 : (its + 1) % TB_RING;
             a.its = its;
-            tb_launch_t<TB_SCATW, TBW_F32>(pl, nb, a, its & 1);
+            if (wp == TBW_BF16) tb_launch_t<TB_SCATW, TBW_BF16>(pl, nb, a, its & 1);
+            else if (wp == TBW_F16) tb_launch_t<TB_SCATW, TBW_F16>(pl, nb, a, its & 1);
+            else tb_launch_t<TB_SCATW, TBW_F32>(pl, nb, a, its & 1);
             if (!out.full) {
                 if ((its + 1) % LAG_K == 0) {
                     tb_img_block(nb, out, lo, its);
@@ -1804,8 +1844,9 @@ struct Context {
         const int maxEnt = tb_lists(pl, nb, shots, 0, false);
         tb_zero(nb, false);
         const bool lagSrc = src.ext != nullptr;
-        tb_desc(pl, nb, false, false, false, lagSrc ? tbSS.p : (void*)src.F, false, lagSrc ? TB_RING : g.nts,
-                out.full ? out.full : tbR.as<float>(), out.full ? g.nts : TB_RING);
+        require(lagSrc || src.wp == TBW_F32, "adjoint dense pass: zero-lag sources come from an FP32 field");
+        tb_desc(pl, nb, false, false, false, lagSrc ? tbSS.p : const_cast<void*>(src.F), false,
+                lagSrc ? TB_RING : g.nts, out.full ? out.full : tbR.as<float>(), out.full ? g.nts : TB_RING);
         KTArgs a = tb_args(pl, maxEnt, lagSrc ? nullptr : src.dm);
         int srcLo = g.nts;   // lowest source sample in the ring
         int hi = g.nts - 1;  // highest sample not yet imaged
@@ -1855,11 +1896,65 @@ struct Context {
     }
 
     // Source wavefield and its second time derivative (computeTomoSrcWfldDt2,
-    // F/src/tomoExtShotsGpuFunctions.cu:1251-1361) into tbW.
+    // F/src/tomoExtShotsGpuFunctions.cu:1251-1361) into tbW, in the stored precision.
     void tb_src_dt2(int nb, const aio_shot* shots) {
+        if (src_wp() != TBW_F32) return tb_src_dt2_16(nb, shots);
         tb_src_pass(nb, shots, false);
         k_dt2<<<ew_grid(nb, g.isz), 256, 0, st>>>(tbW.as<float>(), wfSt(), g.isz, g.nts, k.cSide, k.cCenter);
         kcheck();
+    }
+    // 16-bit source field: the source pass stores W in an FP32 ring of TB_RING slices (tbSS, which
+    // the legs use only later), and once a block of KT_DT2_B slices of d2/dt2 can be formed
+    // (W one slice past it is final) k_dt2_block forms it with k_dt2's expression: BF16 stored
+    // directly; FP16 staged in FP32 (tbR, also free until the legs) and quantized with each
+    // slice's exact unit (max / 2^15). The FP32 field of nts slices is never held.
+    void tb_src_dt2_16(int nb, const aio_shot* shots) {
+        static_assert(TB_RING >= 2 * KT_DT2_B, "the block reads the slice before it and the slice after it");
+        tb_autotune(nb, shots, false);
+        const TBPlan pl = tb_plan(nb);
+        const int maxEnt = tb_lists(pl, nb, shots, 1, false);
+        tb_zero(nb, false);
+        tb_desc(pl, nb, true, false, false, tbSS.p, false, TB_RING);
+        KTArgs a = tb_args(pl, maxEnt, nullptr);
+        a.wRing = TB_RING;
+        const int wp = src_wp();
+        if (wp == TBW_F16) AIO_CK(cudaMemsetAsync(tbWmax.p, 0, (size_t)nb * g.nts * 4, st));
+        const long long rSt = (long long)TB_RING * g.isz;
+        const dim3 grid((unsigned)std::max(1, 2 * smCount), nb);
+        auto block = [&](int t0, int t1) {
+            if (wp == TBW_BF16) {
+                k_dt2_block<TBW_BF16><<<grid, 256, 0, st>>>(tbSS.as<float>(), rSt, TB_RING, tbW.p, wfSt(), nullptr, 0,
+                                                            nullptr, g.nts, g.isz, t0, t1, k.cSide, k.cCenter);
+                kcheck();
+                return;
+            }
+            k_dt2_block<TBW_F16><<<grid, 256, 0, st>>>(tbSS.as<float>(), rSt, TB_RING, tbW.p, wfSt(), tbR.as<float>(),
+                                                       rSt, tbWmax.as<unsigned>(), g.nts, g.isz, t0, t1, k.cSide,
+                                                       k.cCenter);
+            kcheck();
+            k_dt2_f16_pack<<<grid, 256, 0, st>>>(tbR.as<float>(), rSt, tbW.p, wfSt(), tbWmax.as<unsigned>(),
+                                                 tbWscale.as<float>(), g.nts, g.isz, t0, t1);
+            kcheck();
+        };
+        tbLast = pl;
+        graph_loop({11, nb, pl.HZ, pl.nStrips, pl.LX, pl.nChunks, maxEnt, (long long)tbDesc.p, (long long)tbSS.p,
+                    (long long)tbW.p, (long long)tbR.p, wp},
+                   [&] {
+                       int lo = 0;  // first slice of d2/dt2 not yet formed
+                       for (int its = 0; its < g.nts - 1; its++) {
+                           a.its = its;
+                           tb_launch_t<TB_SRC, TBW_F32>(pl, nb, a, its & 1);
+                           // W[its] is final (and W[nts-1] after the last launch): d2/dt2 of the
+                           // slices up to `ready` can be formed
+                           const bool last = its == g.nts - 2;
+                           const int ready = last ? g.nts - 1 : its - 1;
+                           while (ready - lo + 1 >= KT_DT2_B || (last && lo <= ready)) {
+                               const int t1 = std::min(lo + KT_DT2_B - 1, ready);
+                               block(lo, t1);
+                               lo = t1 + 1;
+                           }
+                       }
+                   });
     }
 
     // Shots per wave with two full coarse fields, the rings and imgSlices image slices per shot.
@@ -1869,7 +1964,10 @@ struct Context {
             maxSrc = std::max(maxSrc, shots[s].nSourcesReg);
             maxRec = std::max(maxRec, shots[s].nReceiversReg);
         }
-        const long long per = 6LL * g.isz * 4 + 2LL * g.nts * g.isz * 4 + 2LL * TB_RING * g.isz * 4 +
+        // the source field in the stored precision (16-bit with nts FP32 scales and maxima), the
+        // second field in FP32
+        const long long wsrc = (long long)g.nts * g.isz * (src_wp() == TBW_F32 ? 4 : 2) + 8LL * g.nts;
+        const long long per = 6LL * g.isz * 4 + wsrc + (long long)g.nts * g.isz * 4 + 2LL * TB_RING * g.isz * 4 +
                               (long long)imgSlices * g.isz * (P.imageFp64 ? 8 : 4) + (long long)maxSrc * g.ntw * 4 +
                               2LL * maxRec * g.nts * 4 + 2 * g.hsz * 4 + 2 * g.isz * 4 + (1 << 16);
         const long long shared = (4LL + 2 * g.nExt) * g.isz * 4 + (64LL << 20);
@@ -1879,7 +1977,7 @@ struct Context {
     }
     void tb_fields_alloc(int nb) {
         tb_alloc(nb, false);
-        tbW.ensure((size_t)nb * g.nts * g.isz * 4);
+        tbW.ensure((size_t)nb * g.nts * g.isz * (src_wp() == TBW_F32 ? 4 : 2));
         tbF2.ensure((size_t)nb * g.nts * g.isz * 4);
         tbSS.ensure((size_t)nb * TB_RING * g.isz * 4);
         tbR.ensure((size_t)nb * TB_RING * g.isz * 4);
@@ -1893,14 +1991,15 @@ struct Context {
             setup_wave(n, nb, shots + s0, mem, false, false);
             tb_fields_alloc(nb);
             tb_src_dt2(nb, shots + s0);
-            const float* W2 = tbW.as<float>();
+            const void* W2 = tbW.p;  // d2/dt2 of the source wavefield, stored precision wp
+            const int wp = src_wp();
             float* W1 = tbF2.as<float>();
             if (P.leg1) {
-                tb_dense_fwd(nb, shots + s0, TBSrc{W2, ex, nullptr, 1}, TBOut{W1});
+                tb_dense_fwd(nb, shots + s0, TBSrc{W2, ex, nullptr, 1, wp}, TBOut{W1});
                 tb_scat_pass(nb, shots + s0, dm, W1);
             }
             if (P.leg2) {
-                tb_dense_fwd(nb, shots + s0, TBSrc{W2, nullptr, dm, 1}, TBOut{W1});
+                tb_dense_fwd(nb, shots + s0, TBSrc{W2, nullptr, dm, 1, wp}, TBOut{W1});
                 tb_scatx_pass(nb, shots + s0, ex, W1);
             }
             download_data(nb, shots + s0, mem);
@@ -1918,13 +2017,14 @@ struct Context {
             setup_wave(n, nb, shots + s0, mem, true, false);
             tb_fields_alloc(nb);
             tb_src_dt2(nb, shots + s0);
-            const float* W2 = tbW.as<float>();
+            const void* W2 = tbW.p;
+            const int wp = src_wp();
             float* R = tbF2.as<float>();
             std::vector<const float*> din(dataPtr.begin(), dataPtr.end());
             tb_rec_full(nb, shots + s0, din.data(), R);
             zero_images(nb, 1);
-            if (P.leg1) tb_dense_fwd(nb, shots + s0, TBSrc{W2, ex, nullptr, 1}, TBOut{nullptr, R, false, 1});
-            if (P.leg2) tb_dense_adj(nb, shots + s0, TBSrc{R, ex, nullptr, -1}, TBOut{nullptr, W2, false, 1});
+            if (P.leg1) tb_dense_fwd(nb, shots + s0, TBSrc{W2, ex, nullptr, 1, wp}, TBOut{nullptr, R, false, 1});
+            if (P.leg2) tb_dense_adj(nb, shots + s0, TBSrc{R, ex, nullptr, -1}, TBOut{nullptr, W2, false, 1, wp});
             reduce_images(nb, 1, 5, out, true);
             sync();
             s0 += nb;
@@ -1940,12 +2040,13 @@ struct Context {
             setup_wave(n, nb, shots + s0, mem, false, true);
             tb_fields_alloc(nb);
             tb_src_dt2(nb, shots + s0);
-            const float* W2 = tbW.as<float>();
+            const void* W2 = tbW.p;
+            const int wp = src_wp();
             float* R = tbF2.as<float>();
             tb_rec_full(nb, shots + s0, wdataPtr.data(), R);
             zero_images(nb, g.nExt);
-            if (P.leg1) tb_dense_fwd(nb, shots + s0, TBSrc{W2, nullptr, dm, 1}, TBOut{nullptr, R, true, -1});
-            if (P.leg2) tb_dense_adj(nb, shots + s0, TBSrc{R, nullptr, dm, 1}, TBOut{nullptr, W2, true, 1});
+            if (P.leg1) tb_dense_fwd(nb, shots + s0, TBSrc{W2, nullptr, dm, 1, wp}, TBOut{nullptr, R, true, -1});
+            if (P.leg2) tb_dense_adj(nb, shots + s0, TBSrc{R, nullptr, dm, 1}, TBOut{nullptr, W2, true, 1, wp});
             reduce_images(nb, g.nExt, 5, out, true);
             sync();
             s0 += nb;
@@ -1961,12 +2062,13 @@ struct Context {
             setup_wave(n, nb, shots + s0, mem, false, true);
             tb_fields_alloc(nb);
             tb_src_dt2(nb, shots + s0);
-            const float* W2 = tbW.as<float>();
+            const void* W2 = tbW.p;
+            const int wp = src_wp();
             float* R = tbF2.as<float>();
             tb_rec_full(nb, shots + s0, wdataPtr.data(), R);
             zero_images(nb, 1);
-            if (P.leg1) tb_dense_adj(nb, shots + s0, TBSrc{R, im, nullptr, -1}, TBOut{nullptr, W2, false, 1});
-            if (P.leg2) tb_dense_fwd(nb, shots + s0, TBSrc{W2, im, nullptr, 1}, TBOut{nullptr, R, false, 1});
+            if (P.leg1) tb_dense_adj(nb, shots + s0, TBSrc{R, im, nullptr, -1}, TBOut{nullptr, W2, false, 1, wp});
+            if (P.leg2) tb_dense_fwd(nb, shots + s0, TBSrc{W2, im, nullptr, 1, wp}, TBOut{nullptr, R, false, 1});
             reduce_images(nb, 1, 5, out, true);
             sync();
             s0 += nb;
@@ -2469,7 +2571,7 @@ struct Context {
     // Extended tomo forward (F/src/tomoExtShotsGpuFunctions.cu:355-465, legs :1554-1881).
     void tomo_forward(const float* model, const float* extRefl, int nShots, const aio_shot* shots, int mem) {
         begin_call();
-        require_fp32_fields("tomo and WEMVA");
+        if (!(tb_enabled() && !offsets() && !save)) require_fp32_fields("tomo and WEMVA off the blocked stepper");
         one_shot_saving(nShots);
         Needs n;
         n.nWavefields = fields_needed();
@@ -2520,7 +2622,7 @@ struct Context {
     // Extended tomo adjoint (F/src/tomoExtShotsGpuFunctions.cu:797-910, legs :2442-2701).
     void tomo_adjoint(float* modelOut, int add, const float* extRefl, int nShots, const aio_shot* shots, int mem) {
         begin_call();
-        require_fp32_fields("tomo and WEMVA");
+        if (!(tb_enabled() && !offsets() && !save)) require_fp32_fields("tomo and WEMVA off the blocked stepper");
         one_shot_saving(nShots);
         Needs n;
         n.nWavefields = fields_needed();
@@ -2579,7 +2681,7 @@ struct Context {
     // Extended WEMVA forward (F/src/wemvaExtShotsGpuFunctions.cu:344-456, legs :961-1122).
     void wemva_forward(const float* model, float* imageOut, int add, int nShots, const aio_shot* shots, int mem) {
         begin_call();
-        require_fp32_fields("tomo and WEMVA");
+        if (!(tb_enabled() && !offsets() && !save)) require_fp32_fields("tomo and WEMVA off the blocked stepper");
         one_shot_saving(nShots);
         Needs n;
         n.nWavefields = fields_needed();
@@ -2631,7 +2733,7 @@ struct Context {
     // Extended WEMVA adjoint (F/src/wemvaExtShotsGpuFunctions.cu:575-688, legs :1270-1426).
     void wemva_adjoint(float* modelOut, int add, const float* image, int nShots, const aio_shot* shots, int mem) {
         begin_call();
-        require_fp32_fields("tomo and WEMVA");
+        if (!(tb_enabled() && !offsets() && !save)) require_fp32_fields("tomo and WEMVA off the blocked stepper");
         one_shot_saving(nShots);
         Needs n;
         n.nWavefields = fields_needed();

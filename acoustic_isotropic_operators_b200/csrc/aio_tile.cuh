@@ -74,6 +74,7 @@ struct KTArgs {
                            // SCATX / SCATW / ADJX: slices of W holding the sources at its, its+1
     int oA, oB;            // SCATW / ADJX: slices of rcoarse receiving the samples its, its+1
     int f16spec;           // FP16 source pass: store slices with the speculative scale where allowed
+    int wRing;             // SRC: W is a ring of wRing FP32 slices (slice t in slot t % wRing); 0: all nts
 };
 
 // Per-thread staging slots (16 bytes each) filled by asynchronous copies: level-1 operands
@@ -259,6 +260,72 @@ __device__ __forceinline__ void kt_fs_window(float4 (&Z)[5], int zq) {
 #pragma unroll
     for (int i = 0; i < 5; i++) Z[i] = make_float4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
 }
+// 16-bit source field of tomo / WEMVA: coarse d2/dt2 (srcWfldSecondTimeDerivative,
+// F/src/kernelsGpu.cu:188-197, k_dt2's expression) of the slices [t0, t1] (at most KT_DT2_B) of a
+// source wavefield held in an FP32 ring of `ring` slices (slice t in slot t % ring; zero outside
+// [0, nts)). BF16 stores the result; FP16 stages it in FP32 (slot t - t0 of `stage`) and folds
+// each slice's max |d| into wmax[t] (one atomic per warp and slice) for k_dt2_f16_pack. Four
+// points per thread (interior slices are whole float4s: isz % 32 == 0).
+constexpr int KT_DT2_B = 32;
+template <int WP>
+__global__ void k_dt2_block(const float* __restrict__ ring, long long ringSt, int ringLen, void* out, long long outSt,
+                            float* stage, long long stageSt, unsigned* wmax, int nts, long long isz, int t0, int t1,
+                            float cSide, float cCenter) {
+    const int b = blockIdx.y;
+    ring += b * ringSt;
+    float mx[KT_DT2_B];
+#pragma unroll
+    for (int k = 0; k < KT_DT2_B; k++) mx[k] = 0.f;
+    const long long n4 = isz / 4;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += (long long)gridDim.x * blockDim.x) {
+        const long long i = 4 * q;
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 prev = t0 > 0 ? *reinterpret_cast<const float4*>(ring + (long long)((t0 - 1) % ringLen) * isz + i) : z4;
+        float4 c = *reinterpret_cast<const float4*>(ring + (long long)(t0 % ringLen) * isz + i);
+#pragma unroll
+        for (int k = 0; k < KT_DT2_B; k++) {
+            const int t = t0 + k;
+            if (t > t1) break;
+            const float4 nx =
+                t + 1 < nts ? *reinterpret_cast<const float4*>(ring + (long long)((t + 1) % ringLen) * isz + i) : z4;
+            float d[4] = {cSide * (prev.x + nx.x) + cCenter * c.x, cSide * (prev.y + nx.y) + cCenter * c.y,
+                          cSide * (prev.z + nx.z) + cCenter * c.z, cSide * (prev.w + nx.w) + cCenter * c.w};
+            if (WP == TBW_BF16) {
+                kt_wstore4<TBW_BF16>((unsigned short*)out + b * outSt + (long long)t * isz, i, d);
+            } else {
+                kt_st4(stage + b * stageSt + (long long)k * isz + i, d);
+                mx[k] = fmaxf(mx[k], fmaxf(fmaxf(fabsf(d[0]), fabsf(d[1])), fmaxf(fabsf(d[2]), fabsf(d[3]))));
+            }
+            prev = c;
+            c = nx;
+        }
+    }
+    if (WP == TBW_F16) {
+        // non-negative floats order like their bit patterns: one warp max, one atomic per warp
+#pragma unroll
+        for (int k = 0; k < KT_DT2_B; k++) {
+            const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(mx[k]));
+            if ((threadIdx.x & 31) == 0 && m && t0 + k <= t1) atomicMax(wmax + (long long)b * nts + t0 + k, m);
+        }
+    }
+}
+// FP16: slices [t0, t1] staged by k_dt2_block, quantized with each slice's exact unit (max / 2^15,
+// kt_f16_scale), and the units recorded in wscale.
+__global__ void k_dt2_f16_pack(const float* __restrict__ stage, long long stageSt, void* out, long long outSt,
+                               const unsigned* __restrict__ wmax, float* wscale, int nts, long long isz, int t0,
+                               int t1) {
+    const int b = blockIdx.y;
+    const long long n4 = isz / 4, tot = (long long)(t1 - t0 + 1) * n4;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(q / n4);
+        const long long i = 4 * (q - k * n4);
+        const float sc = kt_f16_scale(wmax[(long long)b * nts + t0 + k]);
+        const float4 v = *reinterpret_cast<const float4*>(stage + b * stageSt + (long long)k * isz + i);
+        *reinterpret_cast<uint2*>((unsigned short*)out + b * outSt + (long long)(t0 + k) * isz + i) = kt_f16_pack(v, sc);
+        if (i == 0) wscale[(long long)b * nts + t0 + k] = sc;
+    }
+}
+
 __host__ __device__ constexpr bool kt_adj(int mode) { return mode == TB_ADJ || mode == TB_ADJR || mode == TB_ADJX; }
 
 // FS: free surface at the top interior row (runs on the large-strip variant only)
@@ -298,8 +365,13 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
     const int ip = g.ip, nxi = g.nxi, nzi = g.nzi, H = g.H, sub = g.sub, its = a.its;
 
     // FP16 slice scales read by this launch (SCAT: its, its+1; ADJ: 0, its+1)
-    const float scA = (WPREC == TBW_F16 && MODE == TB_SCAT) ? sh.wscale[its] : 1.f;
-    const float scB = (WPREC == TBW_F16 && (MODE == TB_SCAT || MODE == TB_ADJ)) ? sh.wscale[its + 1] : 1.f;
+    // (SCATW reading a 16-bit stored field: its slices rSlot, rSlot0)
+    const float scA = (WPREC == TBW_F16 && MODE == TB_SCAT)    ? sh.wscale[its]
+                      : (WPREC == TBW_F16 && MODE == TB_SCATW) ? sh.wscale[a.rSlot]
+                                                               : 1.f;
+    const float scB = (WPREC == TBW_F16 && (MODE == TB_SCAT || MODE == TB_ADJ)) ? sh.wscale[its + 1]
+                      : (WPREC == TBW_F16 && MODE == TB_SCATW)                 ? sh.wscale[a.rSlot0]
+                                                                               : 1.f;
     const float sc0 = (WPREC == TBW_F16 && MODE == TB_ADJ) ? sh.wscale[0] : 1.f;
     const int tid = threadIdx.x;
     const int cp = tid / NQ;              // column pair 0..7 (>= 8: idle thread)
@@ -705,8 +777,9 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
                             wmaxB = fmaxf(wmaxB, m);
                         }
                     } else {
-                        kt_wstore4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, its), idx, wa);
-                        if (its == g.nts - 2) kt_wstore4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, its + 1), idx, wb);
+                        const int sA = a.wRing ? its % a.wRing : its, sB = a.wRing ? (its + 1) % a.wRing : its + 1;
+                        kt_wstore4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, sA), idx, wa);
+                        if (its == g.nts - 2) kt_wstore4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, sB), idx, wb);
                     }
                 } else if (MODE == TB_ADJ) {
                     float ra[4], rb[4];

@@ -327,7 +327,7 @@ def run_tomo(args, emit=True):
     ext = np.ascontiguousarray(w.extra["ext"], np.float32)
     m = np.ascontiguousarray(w.model, np.float32)
     ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs, nExt=w.nExt, image_fp64=True,
-                  stepper=args.stepper)
+                  stepper=args.stepper, wavefield=args.wavefield)
     # (name, propagation passes, full coarse-field sweeps per shot: the source wavefield written,
     # its d2/dt2 read and written, and every later write or read of a stored field; FP32)
     ops = [("tomo_forward", 5, 9, lambda: ctx.tomo_forward(m, ext, shots)),
@@ -350,7 +350,9 @@ def run_tomo(args, emit=True):
         tot_bytes += nbytes
     stepper = {"auto": "blocked stepper", "blocked": "blocked stepper", "fine": "per-fine-step stepper"}[args.stepper]
     peak, src = hbm_peak()
-    out = {"impl": f"this engine, extended tomo + WEMVA ({stepper}, FP32 wavefields)",
+    src = {"fp32": "FP32", "fp16": "FP16 + per-slice scale", "bf16": "BF16"}[args.wavefield]
+    out = {"impl": f"this engine, extended tomo + WEMVA ({stepper}, source field d2/dt2 in {src}, second field FP32)",
+           "wavefield": args.wavefield,
            "metric": "Gpts/s, extended tomo + WEMVA forward and adjoint", "value": tot_pts / tot_t / 1e9,
            "unit": UNIT, "seconds": tot_t, "ops": res, "shots": len(shots), "nExt": w.nExt,
            "interior": [w.nz - 10, w.nx - 10], "nts": w.nts,

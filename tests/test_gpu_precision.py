@@ -102,20 +102,3 @@ def test_born_ext_error_vs_fp64(medium, wavefield, tol):
     ea = rel_l2(img, ref)
     print(f"\n[{wavefield}] extended Born (nExt={n_ext}) forward rel err vs FP64 {ef:.2e}, adjoint {ea:.2e}")
     assert ef < tol and ea < tol
-
-
-def test_tomo_refuses_compressed_fields(medium):
-    """Tomo and WEMVA keep their stored fields in FP32: a context with a compressed stored
-    wavefield refuses them with an argument error rather than running FP32 fields under it."""
-    from acoustic_isotropic_operators_b200 import _capi as A
-    from acoustic_isotropic_operators_b200.batch import Context, Shot
-    w, sigs, s, k = medium
-    ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, k["v2"], k["rs"], nExt=3,
-                  wavefield="fp16")
-    try:
-        ext = np.zeros((3, w.nx, w.nz), np.float32)
-        with pytest.raises(A.AioError) as e:
-            ctx.tomo_forward(w.model, ext, [Shot(a.src_pos, a.rec_pos, g) for a, g in zip(w.shots, sigs)])
-        assert e.value.code == A.AIO_ERR_ARGUMENT
-    finally:
-        ctx.close()
