@@ -47,8 +47,12 @@ extern "C" {
 #define AIO_WEMVA_EXT 4
 
 #define AIO_WFLD_FP32 0  /* stored source wavefield in FP32 (reference behaviour) */
-#define AIO_WFLD_BF16 1  /* BF16 with a per-time-slice FP32 scale */
+#define AIO_WFLD_BF16 1  /* BF16 (no scale: BF16 keeps FP32's exponent range) */
 #define AIO_WFLD_FP16 2  /* FP16 with a per-time-slice FP32 scale */
+/* Compressed settings apply on the interval-blocked stepper to the Born source wavefield, the
+ * extended Born (time lags) source wavefield, and the tomo / WEMVA source field d2/dt2 (their
+ * second stored field stays FP32); the subsurface-offset extension and the per-fine-step paths
+ * refuse them with AIO_ERR_ARGUMENT. */
 
 typedef struct aio_context aio_context;
 
