@@ -383,58 +383,6 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
     const int x1 = min(x0 + a.LX, nxi);
     const int xs = x0 - 5 * T;
 
-    // ---- shared set-up: zero rings, column damping table, sparse entries
-    static_assert(RS % 4 == 0, "ring columns are whole float4s");
-    const int nRing4 = kt_ringcols(MODE) * (RS / 4);
-    for (int i = tid; i < nRing4; i += blockDim.x) kt_smem4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int i = tid; i < nDx; i += blockDim.x) {
-        injFirst[i] = -1;
-        recFirst[i] = -1;
-        const int c = xs - 32 + i;
-        float d = 0.f;
-        if (c >= 0 && c < nxi) {
-            const int dd = min(c, nxi - 1 - c);
-            d = dd < g.minPad ? __ldg(a.taper + dd) : 1.f;
-        }
-        dxt[i] = d;
-    }
-    int nInj = 0, nRec = 0, recOff = 0;
-    if (sh.entStart) {
-        const int4 se = sh.entStart[strip * a.nChunks + chunk];
-        const int n = min(se.w - se.x, a.maxEnt);
-        for (int i = tid; i < n; i += blockDim.x) sEnt[i] = sh.ent[se.x + i];
-        nInj = se.y - se.x;
-        recOff = se.z - se.x;
-        nRec = se.w - se.z;
-    }
-    __syncthreads();
-    // Injected values of this interval, one per entry and fine step, read once here
-    // instead of inside the level loop (adjoint: the v2 factor is applied at use).
-    if (!tb_scatlike(MODE)) {
-        for (int i = tid; i < nInj * T; i += blockDim.x) {
-            const int e = i / T, t = i - e * T + 1;
-            const float* tr = pInj + (long long)sEnt[e].dev * injLd;
-            float v;
-            if (MODE == TB_ADJ || MODE == TB_ADJR) {
-                const int it2 = sub - t;
-                v = tr[its] * a.h[it2 + 1] + tr[its + 1] * a.h[H + it2 + 1];
-            } else {
-                v = tr[its * sub + t - 1];
-            }
-            sInjV[i] = v;
-        }
-    }
-    // column -> first entry (entries are sorted by column; inside [xs - 32, xs - 32 + nDx))
-    for (int e = tid; e < nInj; e += blockDim.x)
-        if (e == 0 || sEnt[e - 1].col != sEnt[e].col) injFirst[sEnt[e].col - xs + 32] = e;
-    for (int e = tid; e < nRec; e += blockDim.x)
-        if (e == 0 || sEnt[recOff + e - 1].col != sEnt[recOff + e].col) recFirst[sEnt[recOff + e].col - xs + 32] = e;
-    __syncthreads();
-    // does any injection / recording point fall in this thread's row quad?
-    bool qInj = false, qRec = false;
-    for (int e = 0; e < nInj; e++) qInj |= (unsigned)(sEnt[e].row - zq) < 4u;
-    for (int e = 0; e < nRec; e++) qRec |= (unsigned)(sEnt[recOff + e].row - zq) < 4u;
-
     // ---- per-thread constants
     float Dz[4];
 #pragma unroll
@@ -495,6 +443,62 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
             }
         }
     };
+    // ---- shared set-up: zero rings, column damping table, sparse entries
+    static_assert(RS % 4 == 0, "ring columns are whole float4s");
+    const int nRing4 = kt_ringcols(MODE) * (RS / 4);
+    for (int i = tid; i < nRing4; i += blockDim.x) kt_smem4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = tid; i < nDx; i += blockDim.x) {
+        injFirst[i] = -1;
+        recFirst[i] = -1;
+        const int c = xs - 32 + i;
+        float d = 0.f;
+        if (c >= 0 && c < nxi) {
+            const int dd = min(c, nxi - 1 - c);
+            d = dd < g.minPad ? __ldg(a.taper + dd) : 1.f;
+        }
+        dxt[i] = d;
+    }
+    int nInj = 0, nRec = 0, recOff = 0;
+    if (sh.entStart) {
+        const int4 se = sh.entStart[strip * a.nChunks + chunk];
+        const int n = min(se.w - se.x, a.maxEnt);
+        for (int i = tid; i < n; i += blockDim.x) sEnt[i] = sh.ent[se.x + i];
+        nInj = se.y - se.x;
+        recOff = se.z - se.x;
+        nRec = se.w - se.z;
+    }
+    __syncthreads();
+    // the rings are zeroed: the first input block's copies go out now, and land while the
+    // per-launch tables below are built
+    issue_input(0);
+    kt_commit();
+    // Injected values of this interval, one per entry and fine step, read once here
+    // instead of inside the level loop (adjoint: the v2 factor is applied at use).
+    if (!tb_scatlike(MODE)) {
+        for (int i = tid; i < nInj * T; i += blockDim.x) {
+            const int e = i / T, t = i - e * T + 1;
+            const float* tr = pInj + (long long)sEnt[e].dev * injLd;
+            float v;
+            if (MODE == TB_ADJ || MODE == TB_ADJR) {
+                const int it2 = sub - t;
+                v = tr[its] * a.h[it2 + 1] + tr[its + 1] * a.h[H + it2 + 1];
+            } else {
+                v = tr[its * sub + t - 1];
+            }
+            sInjV[i] = v;
+        }
+    }
+    // column -> first entry (entries are sorted by column; inside [xs - 32, xs - 32 + nDx))
+    for (int e = tid; e < nInj; e += blockDim.x)
+        if (e == 0 || sEnt[e - 1].col != sEnt[e].col) injFirst[sEnt[e].col - xs + 32] = e;
+    for (int e = tid; e < nRec; e += blockDim.x)
+        if (e == 0 || sEnt[recOff + e - 1].col != sEnt[recOff + e].col) recFirst[sEnt[recOff + e].col - xs + 32] = e;
+    __syncthreads();
+    // does any injection / recording point fall in this thread's row quad?
+    bool qInj = false, qRec = false;
+    for (int e = 0; e < nInj; e++) qInj |= (unsigned)(sEnt[e].row - zq) < 4u;
+    for (int e = 0; e < nRec; e++) qRec |= (unsigned)(sEnt[recOff + e].row - zq) < 4u;
+
     // FP16 source pass: slice its is stored directly with the speculative scale of slice its-1's
     // max when that max allows it (the same decision in every CTA), else staged in FP32
     const bool f16Spec = WPREC == TBW_F16 && MODE == TB_SRC && kt_f16_spec_slice(sh.wmax, its, g.nts, a.f16spec);
@@ -505,8 +509,6 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
         kt_f16_quantize(sh, a.wStride, ip, its - 1, z0, min(z0 + a.HZ, nzi), x0, x1, tid, blockDim.x);
         __syncthreads();  // the region's staging slots are rewritten below (slice its+1 at the end)
     }
-    issue_input(0);
-    kt_commit();
     kt_wait<0>();
     __syncthreads();
     // FP16 source pass: max |W| of this thread's points of slice its (and its+1 at the end),
