@@ -8,6 +8,7 @@
 // launch per coarse step for imaging. The pass sequences follow the reference
 // drivers (F/src/*ShotsGpuFunctions.cu), cited at each pass.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -224,6 +225,27 @@ struct Context {
         budget = p.memBudgetBytes > 0 ? p.memBudgetBytes : (long long)(0.93 * (double)fr);
         const char* gEnv = std::getenv("AIO_GRAPHS");  // AIO_GRAPHS=0: launch every interval directly
         graphsOn = !(gEnv && gEnv[0] == '0');
+        // AIO_PDL=0: no programmatic dependent launches; 1: the next launch may start as soon as
+        // every CTA has passed its dependency wait; 2: once every CTA has begun its last iteration
+        const char* pEnv = std::getenv("AIO_PDL");
+        if (pEnv && pEnv[0] >= '0' && pEnv[0] <= '2') pdlMode = pEnv[0] - '0';
+        live_contexts()[dev & 63]++;
+        counted = true;
+    }
+    // contexts alive per device (process-wide): the launch overlap policy depends on it
+    static std::atomic<int>* live_contexts() {
+        static std::atomic<int> n[64];
+        return n;
+    }
+    bool counted = false;
+    // Effective overlap mode of this context's stepper launches. Alone on its device, a launch
+    // lets the next one start right after its dependency wait (the next launch's CTAs fill the SMs
+    // its own leave free and finish their prologue early). Beside other contexts, whose streams
+    // run kernels at the same time, CTAs waiting that long would hold SM resources those kernels
+    // could use, so the release moves to the last iteration.
+    int pdl_mode() const {
+        if (pdlMode != 3) return pdlMode;
+        return live_contexts()[dev & 63].load() > 1 ? 2 : 1;
     }
 
     void set_velocity(const float* vel2Dtw2, const float* reflScale) {
@@ -236,6 +258,8 @@ struct Context {
     }
 
     void destroy() {
+        if (counted) live_contexts()[dev & 63]--;
+        counted = false;
         drop_graphs();
         for (auto& e : evFree) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
         for (auto& e : evBusy) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
@@ -263,6 +287,9 @@ struct Context {
     std::map<std::vector<long long>, GraphEntry> graphs;
     std::map<std::vector<long long>, int> graphRuns;
     bool graphsOn = true;
+    // blocked-stepper launches may start their prologue (ring zeroing, tables, entries) while the
+    // previous launch of the stream still runs; the kernel waits for it before reading its output
+    int pdlMode = 3;  // 0 off, 1 early release, 2 release at the last iteration, 3 by live contexts
     long long graphReplays = 0;
 
     void drop_graphs() {
@@ -279,7 +306,7 @@ struct Context {
             body();
             return;
         }
-        key.insert(key.end(), {P.freeSurface, P.wavefieldPrecision, P.extension, P.sloth, P.stepper});
+        key.insert(key.end(), {P.freeSurface, P.wavefieldPrecision, P.extension, P.sloth, P.stepper, pdl_mode()});
         auto it = graphs.find(key);
         if (it != graphs.end()) {
             AIO_CK(cudaGraphLaunch(it->second.exec, st));
@@ -1134,6 +1161,30 @@ struct Context {
         const char* logEnv = std::getenv("AIO_AUTOTUNE_LOG");  // print every candidate's timings
         const bool logTune = logEnv && *logEnv && *logEnv != '0';
         profEvery = 0;
+        // Per-launch time: the fastest of three timings of n back-to-back launches (after a timed
+        // warm-up launch: smem carve-out, caches), so that a disturbed timing does not decide the
+        // plan; n makes a timing span >= 0.2 ms, which for single-shot launches of ~20 us keeps
+        // event and clock jitter from deciding it.
+        auto timeMin = [&](auto launch) {
+            AIO_CK(cudaEventRecord(e0, st));
+            launch();
+            AIO_CK(cudaEventRecord(e1, st));
+            AIO_CK(cudaEventSynchronize(e1));
+            float t1 = 0.f;
+            AIO_CK(cudaEventElapsedTime(&t1, e0, e1));
+            const int n = std::min(12, std::max(2, (int)std::ceil(0.2f / std::max(t1, 1e-3f))));
+            float best2 = 1e30f;
+            for (int rep = 0; rep < 3; rep++) {
+                AIO_CK(cudaEventRecord(e0, st));
+                for (int i = 0; i < n; i++) launch();
+                AIO_CK(cudaEventRecord(e1, st));
+                AIO_CK(cudaEventSynchronize(e1));
+                float t = 0.f;
+                AIO_CK(cudaEventElapsedTime(&t, e0, e1));
+                best2 = std::min(best2, t / n);
+            }
+            return best2;
+        };
         for (const TBPlan& pl : cand) {
             const int maxEnt = tb_lists(pl, nb, shots, 1, false);
             tb_zero(nb, false);
@@ -1141,21 +1192,7 @@ struct Context {
             KTArgs a = tb_args(pl, maxEnt, nullptr);
             a.its = 0;
             if (nonlinear) {  // NL class: the launch without recording (the data stay untouched)
-                const float ms = [&] {
-                    tb_launch<TB_NL>(pl, nb, a, 0);
-                    float best2 = 1e30f;
-                    for (int rep = 0; rep < 3; rep++) {
-                        AIO_CK(cudaEventRecord(e0, st));
-                        tb_launch<TB_NL>(pl, nb, a, 0);
-                        tb_launch<TB_NL>(pl, nb, a, 0);
-                        AIO_CK(cudaEventRecord(e1, st));
-                        AIO_CK(cudaEventSynchronize(e1));
-                        float t = 0.f;
-                        AIO_CK(cudaEventElapsedTime(&t, e0, e1));
-                        best2 = std::min(best2, t);
-                    }
-                    return best2;
-                }();
+                const float ms = timeMin([&] { tb_launch<TB_NL>(pl, nb, a, 0); });
                 if (ms < bestMs) {
                     bestMs = ms;
                     best = pl;
@@ -1166,23 +1203,6 @@ struct Context {
                 continue;
             }
             if (f16()) AIO_CK(cudaMemsetAsync(tbWmax.p, 0, (size_t)nb * g.nts * 4, st));
-            // fastest of three timings of two launches each (after a warm-up launch: smem
-            // carve-out, caches), so that a disturbed timing does not decide the plan
-            auto timeMin = [&](auto launch) {
-                launch();
-                float best2 = 1e30f;
-                for (int rep = 0; rep < 3; rep++) {
-                    AIO_CK(cudaEventRecord(e0, st));
-                    launch();
-                    launch();
-                    AIO_CK(cudaEventRecord(e1, st));
-                    AIO_CK(cudaEventSynchronize(e1));
-                    float t = 0.f;
-                    AIO_CK(cudaEventElapsedTime(&t, e0, e1));
-                    best2 = std::min(best2, t);
-                }
-                return best2;
-            };
             float ms = timeMin([&] { tb_launch<TB_SRC>(pl, nb, a, 0); });
             if (ms < bestMs) {
                 bestMs = ms;
@@ -1401,8 +1421,19 @@ struct Context {
             ev = take_events();
             AIO_CK(cudaEventRecord(ev.first, st));
         }
-        k_tile<MODE, WP, MAXQ, FS><<<dim3(pl.nStrips, pl.nChunks, nb), pl.threads, smem, st>>>(a);
-        AIO_CK(cudaGetLastError());
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(pl.nStrips, pl.nChunks, nb);
+        cfg.blockDim = dim3(pl.threads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        const int pm = pdl_mode();
+        cfg.numAttrs = pm ? 1 : 0;
+        a.relIter = pm == 1 ? 0 : pl.iters - 1;
+        AIO_CK(cudaLaunchKernelEx(&cfg, k_tile<MODE, WP, MAXQ, FS>, a));
         if (timed) {
             AIO_CK(cudaEventRecord(ev.second, st));
             evBusy.push_back(ev);

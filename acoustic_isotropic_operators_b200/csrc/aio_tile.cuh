@@ -75,6 +75,8 @@ struct KTArgs {
     int oA, oB;            // SCATW / ADJX: slices of rcoarse receiving the samples its, its+1
     int f16spec;           // FP16 source pass: store slices with the speculative scale where allowed
     int wRing;             // SRC: W is a ring of wRing FP32 slices (slice t in slot t % wRing); 0: all nts
+    int relIter;           // iteration at whose start the stream's next launch may begin its prologue
+                           // (0: right after the dependency wait; >= iters: when the CTA exits)
 };
 
 // Per-thread staging slots (16 bytes each) filled by asynchronous copies: level-1 operands
@@ -111,6 +113,13 @@ __device__ __forceinline__ void kt_cp8(void* s, const void* g, bool ok) {
 __device__ __forceinline__ void kt_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void kt_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+// Programmatic dependent launch: a launch made with programmatic stream serialization may start
+// while the previous kernel of its stream still runs. kt_grid_wait returns once that kernel has
+// finished and its writes are visible (at once when there is no such dependency); before it a
+// kernel reads only what the host uploaded ahead of the pass and writes only shared memory.
+// kt_grid_release lets the next launch of the stream start its own prologue.
+__device__ __forceinline__ void kt_grid_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void kt_grid_release() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
 // four stored-wavefield samples from a staging slot (FP32: 16 bytes, BF16 / FP16: the first 8)
 template <int WPREC>
 __device__ __forceinline__ float4 kt_wfrom(const float4& slot, float sc) {
@@ -364,15 +373,6 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
     const int strip = blockIdx.x, chunk = blockIdx.y;
     const int ip = g.ip, nxi = g.nxi, nzi = g.nzi, H = g.H, sub = g.sub, its = a.its;
 
-    // FP16 slice scales read by this launch (SCAT: its, its+1; ADJ: 0, its+1)
-    // (SCATW reading a 16-bit stored field: its slices rSlot, rSlot0)
-    const float scA = (WPREC == TBW_F16 && MODE == TB_SCAT)    ? sh.wscale[its]
-                      : (WPREC == TBW_F16 && MODE == TB_SCATW) ? sh.wscale[a.rSlot]
-                                                               : 1.f;
-    const float scB = (WPREC == TBW_F16 && (MODE == TB_SCAT || MODE == TB_ADJ)) ? sh.wscale[its + 1]
-                      : (WPREC == TBW_F16 && MODE == TB_SCATW)                 ? sh.wscale[a.rSlot0]
-                                                                               : 1.f;
-    const float sc0 = (WPREC == TBW_F16 && MODE == TB_ADJ) ? sh.wscale[0] : 1.f;
     const int tid = threadIdx.x;
     const int cp = tid / NQ;              // column pair 0..7 (>= 8: idle thread)
     const int q = tid - cp * NQ;          // row quad
@@ -443,7 +443,8 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
             }
         }
     };
-    // ---- shared set-up: zero rings, column damping table, sparse entries
+    // ---- shared set-up: zero rings, column damping table, sparse entries (descriptors, entries
+    // and the taper are uploaded before the pass: read before the grid dependency wait)
     static_assert(RS % 4 == 0, "ring columns are whole float4s");
     const int nRing4 = kt_ringcols(MODE) * (RS / 4);
     for (int i = tid; i < nRing4; i += blockDim.x) kt_smem4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -467,11 +468,24 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
         recOff = se.z - se.x;
         nRec = se.w - se.z;
     }
+    // everything below reads what the previous launch of the stream wrote (state, partial sums,
+    // stored slices and their scales, recordings)
+    kt_grid_wait();
+    if (a.relIter == 0) kt_grid_release();
     __syncthreads();
     // the rings are zeroed: the first input block's copies go out now, and land while the
     // per-launch tables below are built
     issue_input(0);
     kt_commit();
+    // FP16 slice scales read by this launch (SCAT: its, its+1; ADJ: 0, its+1)
+    // (SCATW reading a 16-bit stored field: its slices rSlot, rSlot0)
+    const float scA = (WPREC == TBW_F16 && MODE == TB_SCAT)    ? sh.wscale[its]
+                      : (WPREC == TBW_F16 && MODE == TB_SCATW) ? sh.wscale[a.rSlot]
+                                                               : 1.f;
+    const float scB = (WPREC == TBW_F16 && (MODE == TB_SCAT || MODE == TB_ADJ)) ? sh.wscale[its + 1]
+                      : (WPREC == TBW_F16 && MODE == TB_SCATW)                 ? sh.wscale[a.rSlot0]
+                                                                               : 1.f;
+    const float sc0 = (WPREC == TBW_F16 && MODE == TB_ADJ) ? sh.wscale[0] : 1.f;
     // Injected values of this interval, one per entry and fine step, read once here
     // instead of inside the level loop (adjoint: the v2 factor is applied at use).
     if (!tb_scatlike(MODE)) {
@@ -517,6 +531,7 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
 
     for (int k = 0; k < a.iters; k++) {
         const int B = xs + KT_BX * k;
+        if (k > 0 && k == a.relIter) kt_grid_release();
         // Output operands of this iteration's level-T columns, copied asynchronously into
         // this thread's staging slots (read at the output stage).
         if (MODE == TB_SRC || MODE == TB_ADJ || MODE == TB_ADJR) {

@@ -434,13 +434,18 @@ def run_nl(args, emit=True):
         for _ in range(3):
             ctx.nonlinear_forward([shot])
         torch.cuda.synchronize()
-        reps = 10
-        t0 = time.perf_counter()
-        for _ in range(reps):
-            ctx.nonlinear_forward([shot])
-        t = (time.perf_counter() - t0) / reps
+        reps, batches = 10, 5
+        ts = []
+        for _ in range(batches):
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                ctx.nonlinear_forward([shot])
+            ts.append((time.perf_counter() - t0) / reps)
+        t = sorted(ts)[batches // 2]  # median batch
         out["blocked" if stepper == "auto" else "per_fine_step"] = {
             "seconds_per_call": t, "Gpts_s": w.n_interior * w.fine_steps / t / 1e9}
+        if stepper == "auto":
+            out["blocked"]["plan"] = ctx.blocked_plan(0)
         ctx.close()
     peak, src = hbm_peak()
     t = out["blocked"]["seconds_per_call"]
@@ -516,7 +521,8 @@ def main():
     if args.nl:
         return run_nl(args)
     if args.serve:
-        return run_serve(args)
+        run_serve(args)
+        return 0
 
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
