@@ -1369,6 +1369,7 @@ struct Context {
                 t.ent = tbEnt.as<TBEnt>();
                 t.W = W ? (void*)((char*)W + (size_t)s * wSlices * g.isz * wElem) : nullptr;
                 t.img = tbImg.p ? tbImg.as<double>() + (size_t)s * g.isz : nullptr;
+                t.imgF = tbImg.p ? tbImg.as<float>() + (size_t)s * g.isz : nullptr;
                 t.rcoarse = out ? out + (size_t)s * outSlices * g.isz : nullptr;
                 if (f16()) {
                     t.wscale = tbWscale.as<float>() + (size_t)s * g.nts;
@@ -1397,6 +1398,7 @@ struct Context {
         a.iters = pl.iters;
         a.maxEnt = maxEnt;
         a.wStride = g.isz;
+        a.imgF32 = P.imageFp64 ? 0 : 1;
         return a;
     }
 
@@ -2218,20 +2220,27 @@ struct Context {
             tb_src_pass(nb, shots + s0, false);
             tb_adj_pass(nb, shots + s0);
             // images of U = v2*p: the reference's v2*(2/v^3) scaling reduces to 2/v^3
+            // (FP32 images when imageFp64 = 0: accumulated in the receiver pass as the reference does)
             const long long nI = g.isz;
-            k_scale_d<<<ew_grid(nb, nI), 256, 0, st>>>(tbImg.as<double>(), nI, 1, v2.as<float>(), rs.as<float>(),
-                                                       g.isz, 3);
+            if (P.imageFp64)
+                k_scale_d<<<ew_grid(nb, nI), 256, 0, st>>>(tbImg.as<double>(), nI, 1, v2.as<float>(), rs.as<float>(),
+                                                           g.isz, 3);
+            else
+                k_scale<<<ew_grid(nb, nI), 256, 0, st>>>(tbImg.as<float>(), nI, 1, v2.as<float>(), rs.as<float>(),
+                                                         g.isz, 3);
             kcheck();
-            if (out) {
-                k_sum_shots<double><<<ew_grid(1, nI), 256, 0, st>>>(out, tbImg.as<double>(), nI, nb, nI, 1);
+            auto sum = [&](float* dst, int s, int n, int add) {
+                if (P.imageFp64)
+                    k_sum_shots<double><<<ew_grid(1, nI), 256, 0, st>>>(dst, tbImg.as<double>() + s * nI, nI, n, nI, add);
+                else
+                    k_sum_shots<float><<<ew_grid(1, nI), 256, 0, st>>>(dst, tbImg.as<float>() + s * nI, nI, n, nI, add);
                 kcheck();
-            }
+            };
+            if (out) sum(out, 0, nb, 1);
             if (perShot) {
                 shotImg.ensure((size_t)g.isz * 4);
                 for (int s = 0; s < nb; s++) {
-                    k_sum_shots<double><<<ew_grid(1, nI), 256, 0, st>>>(shotImg.as<float>(), tbImg.as<double>() + s * nI,
-                                                                        nI, 1, nI, 0);
-                    kcheck();
+                    sum(shotImg.as<float>(), s, 1, 0);
                     write_model(perShot[s0 + s], 1, 0, mem, shotImg.as<float>());
                 }
             }

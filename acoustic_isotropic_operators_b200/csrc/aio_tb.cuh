@@ -48,7 +48,8 @@ struct TBShot {
     void* W;              // stored coarse wavefield [nts] (SRC: out, SCAT/ADJ: in)
     const float* part;    // coarse partial sum carried in (SRC: W[its], ADJ: R(its+1))
     float* partOut;       // coarse partial sum carried out (SRC: W[its+1], ADJ: R(its))
-    double* img;          // ADJ: image accumulator
+    double* img;          // ADJ: image accumulator (FP64 imaging)
+    float* imgF;          // ADJ: image accumulator (FP32 imaging, the reference's precision)
     int injLd, recLd;
     // FP16 stored wavefield only
     float* wscale;        // [nts] value of one FP16 unit of slice t

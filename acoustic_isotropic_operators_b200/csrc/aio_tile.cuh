@@ -75,6 +75,7 @@ struct KTArgs {
     int oA, oB;            // SCATW / ADJX: slices of rcoarse receiving the samples its, its+1
     int f16spec;           // FP16 source pass: store slices with the speculative scale where allowed
     int wRing;             // SRC: W is a ring of wRing FP32 slices (slice t in slot t % wRing); 0: all nts
+    int imgF32;            // ADJ: accumulate the image in FP32 (imgF) instead of FP64 (img)
     int relIter;           // iteration at whose start the stream's next launch may begin its prologue
                            // (0: right after the dependency wait; >= iters: when the CTA exits)
 };
@@ -363,6 +364,7 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
     const float* __restrict__ pPart = sh.part;
     float* __restrict__ pPartOut = sh.partOut;
     double* __restrict__ pImg = sh.img;
+    float* __restrict__ pImgF = sh.imgF;
     float* __restrict__ pRec = sh.recSig;
     const float* __restrict__ pInj = sh.injSig;
     const float* __restrict__ cur = sh.cur;
@@ -545,8 +547,12 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
                         const void* w = tb_wslice<WPREC>(sh.W, a.wStride, its + 1);
                         if (WPREC == TBW_F32) kt_cp16(mySlot + (SO + 2 + j) * bd, (const float*)w + idx, true);
                         else kt_cp8(mySlot + (SO + 2 + j) * bd, (const __nv_bfloat16*)w + idx, true);
-                        kt_cp16(mySlot + (SO + 4 + 2 * j) * bd, pImg + idx, true);
-                        kt_cp16(mySlot + (SO + 5 + 2 * j) * bd, pImg + idx + 2, true);
+                        if (a.imgF32) {
+                            kt_cp16(mySlot + (SO + 4 + 2 * j) * bd, pImgF + idx, true);
+                        } else {
+                            kt_cp16(mySlot + (SO + 4 + 2 * j) * bd, pImg + idx, true);
+                            kt_cp16(mySlot + (SO + 5 + 2 * j) * bd, pImg + idx + 2, true);
+                        }
                     }
                 }
             }
@@ -800,12 +806,8 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
                     }
                 } else if (MODE == TB_ADJ) {
                     float ra[4], rb[4];
-                    double acc[4];
                     const float4 oP = mySlot[(SO + j) * bd];
                     const float4 oW = kt_wfrom<WPREC>(mySlot[(SO + 2 + j) * bd], scB);
-                    const double2* oI = reinterpret_cast<const double2*>(&mySlot[(SO + 4 + 2 * j) * bd]);
-                    const double2* oI2 = reinterpret_cast<const double2*>(&mySlot[(SO + 5 + 2 * j) * bd]);
-                    const double oImg[4] = {oI->x, oI->y, oI2->x, oI2->y};
                     float4 w0 = make_float4(0.f, 0.f, 0.f, 0.f);
                     if (its == 0) w0 = kt_wload4<WPREC>(tb_wslice<WPREC>(sh.W, a.wStride, 0), idx, sc0);
 #pragma unroll
@@ -817,12 +819,32 @@ __global__ void __launch_bounds__((8 * MAXQ + 31) / 32 * 32, kt_v2s(MAXQ) ? 1 : 
                             ra[i] += lvT[j][l][i] * a.h[sub - l];
                             rb[i] += lvT[j][l][i] * a.h[H + sub - l];
                         }
-                        acc[i] = oImg[i] + (double)(kt_el(oW, i) * rb[i]);
-                        if (its == 0) acc[i] += (double)(kt_el(w0, i) * ra[i]);
                     }
                     kt_st4(pPartOut + idx, ra);
-                    *reinterpret_cast<double2*>(pImg + idx) = make_double2(acc[0], acc[1]);
-                    *reinterpret_cast<double2*>(pImg + idx + 2) = make_double2(acc[2], acc[3]);
+                    if (a.imgF32) {
+                        // imagingAdjGpu (F/src/kernelsGpu.cu:318-325): model += W * R in FP32,
+                        // R(its+1) here and R(0) after it at its == 0, as the reference's loop
+                        const float4 oI = mySlot[(SO + 4 + 2 * j) * bd];
+                        float acc[4];
+#pragma unroll
+                        for (int i = 0; i < 4; i++) {
+                            acc[i] = fmaf(kt_el(oW, i), rb[i], kt_el(oI, i));
+                            if (its == 0) acc[i] = fmaf(kt_el(w0, i), ra[i], acc[i]);
+                        }
+                        kt_st4(pImgF + idx, acc);
+                    } else {
+                        const double2* oI = reinterpret_cast<const double2*>(&mySlot[(SO + 4 + 2 * j) * bd]);
+                        const double2* oI2 = reinterpret_cast<const double2*>(&mySlot[(SO + 5 + 2 * j) * bd]);
+                        const double oImg[4] = {oI->x, oI->y, oI2->x, oI2->y};
+                        double acc[4];
+#pragma unroll
+                        for (int i = 0; i < 4; i++) {
+                            acc[i] = oImg[i] + (double)(kt_el(oW, i) * rb[i]);
+                            if (its == 0) acc[i] += (double)(kt_el(w0, i) * ra[i]);
+                        }
+                        *reinterpret_cast<double2*>(pImg + idx) = make_double2(acc[0], acc[1]);
+                        *reinterpret_cast<double2*>(pImg + idx + 2) = make_double2(acc[2], acc[3]);
+                    }
                 } else if (MODE == TB_SCATW) {
                     // interpFineToCoarseSlice on the scattered field (F/src/kernelsGpu.cu:166-182); the
                     // partial sum is read directly (staging slots 4-7 hold the sources)

@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--shots", type=int, default=32, help="shots per GPU")
     ap.add_argument("--nts", type=int, default=2000)
     ap.add_argument("--wavefield", default="fp32", choices=["fp32", "bf16", "fp16"])
+    ap.add_argument("--image", default="fp32", choices=["fp64", "fp32"],
+                    help="Born image accumulation: FP32 as the reference accumulates it, or FP64")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-nts", type=int, default=0, help="coarse samples of the CPU sample (0 = auto)")
@@ -208,7 +210,7 @@ def config_dict(args, w):
     return {"workload": "batched Born forward+adjoint, 400x1200 at 10 m, nts=2000, 15 Hz Ricker",
             "shots_per_gpu": args.shots, "grid_padded": [w.nz, w.nx],
             "interior": [w.nz - 10, w.nx - 10], "nts": w.nts, "sub": w.sub, "fine_steps": w.fine_steps,
-            "passes_per_shot": PASSES, "wavefield": args.wavefield, "receivers_per_shot": 1200,
+            "passes_per_shot": PASSES, "wavefield": args.wavefield, "image": args.image, "receivers_per_shot": 1200,
             "stepper": args.stepper, "chunk": args.chunk,
             "parallelism": f"dp{args.gpus} (shots)", "l2": "inputs larger than L2 (5.4 GB wavefield per shot)"}
 
@@ -246,8 +248,8 @@ def run_plain(args, emit=True):
     model = np.ascontiguousarray(w.model, np.float32)
     times = []
     for i, (a, sg) in enumerate(zip(w.shots, sigs)):
-        ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs, image_fp64=True,
-                      stepper="fine")
+        ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs,
+                      image_fp64=getattr(args, "image", "fp32") == "fp64", stepper="fine")
         shot = Shot(a.src_pos, a.rec_pos, sg)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -553,7 +555,7 @@ def main():
     sigs = prepare_signals(w_mine, lib)
 
     ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs, wavefield=args.wavefield,
-                  image_fp64=True, device=local, stepper=args.stepper, chunk_columns=args.chunk)
+                  image_fp64=args.image == "fp64", device=local, stepper=args.stepper, chunk_columns=args.chunk)
     dev = torch.device("cuda", local)
     model_d = torch.from_numpy(np.ascontiguousarray(w.model, np.float32)).to(dev)
     image_d = torch.zeros((w.nx, w.nz), dtype=torch.float32, device=dev)

@@ -97,9 +97,9 @@ def born32():
     return w, v2, rs, sigs
 
 
-def _ctx(w, v2, rs):
+def _ctx(w, v2, rs, image_fp64=True):
     from acoustic_isotropic_operators_b200.batch import Context
-    return Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs, image_fp64=True)
+    return Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs, image_fp64=image_fp64)
 
 
 def test_born_benchmark_plan(born32):
@@ -144,11 +144,14 @@ def test_born_benchmark_plan(born32):
         ctx.close()
 
 
-def test_born_benchmark_dot(born32):
+@pytest.mark.parametrize("image_fp64", [True, False])
+def test_born_benchmark_dot(born32, image_fp64):
+    """Dot-product test of the benchmark's Born pair, with the image accumulated in FP64 and in
+    FP32 (the reference's accumulation)."""
     from acoustic_isotropic_operators_b200 import _capi as A
     from acoustic_isotropic_operators_b200.batch import Shot
     w, v2, rs, sigs = born32
-    ctx = _ctx(w, v2, rs)
+    ctx = _ctx(w, v2, rs, image_fp64)
     try:
         rng = np.random.default_rng(22)
         m = np.zeros((w.nx, w.nz), np.float32)
@@ -160,7 +163,8 @@ def test_born_benchmark_dot(born32):
         lhs = A.dot_f64(fm, np.concatenate([x.reshape(-1) for x in d]))
         rhs = A.dot_f64(m, ad)
         err = abs(lhs - rhs) / abs(rhs)
-        print(f"Born dot test 522x1322 nts=60, 32 shots: <Fm,d>={lhs:.10e} <m,F*d>={rhs:.10e} rel {err:.2e}")
+        print(f"Born dot test 522x1322 nts=60, 32 shots, FP{64 if image_fp64 else 32} image: "
+              f"<Fm,d>={lhs:.10e} <m,F*d>={rhs:.10e} rel {err:.2e}")
         assert err < 1e-5
     finally:
         ctx.close()

@@ -24,12 +24,15 @@ def medium():
     return w, sigs, s, k
 
 
-@pytest.mark.parametrize("wavefield,tol", [("fp32", 1e-4), ("fp16", 1e-4), ("bf16", 1e-2)])
-def test_born_error_vs_fp64(medium, wavefield, tol):
+@pytest.mark.parametrize("wavefield,tol,image_fp64", [("fp32", 1e-4, True), ("fp32", 1e-4, False),
+                                                      ("fp16", 1e-4, True), ("bf16", 1e-2, True)])
+def test_born_error_vs_fp64(medium, wavefield, tol, image_fp64):
+    """image_fp64 = False: the image accumulated in FP32 over the coarse samples, as the reference
+    accumulates it."""
     from acoustic_isotropic_operators_b200.batch import Context, Shot
     w, sigs, s, k = medium
     assert w.sub == 4
-    ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, k["v2"], k["rs"], image_fp64=True,
+    ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, k["v2"], k["rs"], image_fp64=image_fp64,
                   wavefield=wavefield)
     shots = [Shot(a.src_pos, a.rec_pos, sg) for a, sg in zip(w.shots, sigs)]
     d = ctx.born_forward(w.model, shots)
@@ -40,7 +43,8 @@ def test_born_error_vs_fp64(medium, wavefield, tol):
              for i, a in enumerate(w.shots))
     ref_img = sum(orc.born_adj(s, v64, d[i], sigs[i], a.src_pos, a.rec_pos) for i, a in enumerate(w.shots))
     ea = rel_l2(img, ref_img)
-    print(f"\n[{wavefield}] Born forward rel err vs FP64 {ef:.2e}, adjoint {ea:.2e}")
+    print(f"\n[{wavefield}, FP{64 if image_fp64 else 32} image] Born forward rel err vs FP64 {ef:.2e}, "
+          f"adjoint {ea:.2e}")
     assert ef < tol and ea < tol
 
 
