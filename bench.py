@@ -615,8 +615,9 @@ def main():
     tr = os.path.join(ROOT, "profiles", "stepper_traffic.json")
     if os.path.exists(tr):
         try:
-            bpp = json.load(open(tr))["bytes_per_point_update"][args.wavefield]
-            traffic = bpp * launch_pts
+            byp = json.load(open(tr))["bytes_per_point_update"]
+            key = args.wavefield if args.image == "fp32" else args.wavefield + "_fp64_image"
+            traffic = byp[key] * launch_pts if key in byp else None
         except Exception:
             traffic = None
 
