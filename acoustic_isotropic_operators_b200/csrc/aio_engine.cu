@@ -1163,8 +1163,9 @@ struct Context {
         profEvery = 0;
         // Per-launch time: the fastest of three timings of n back-to-back launches (after a timed
         // warm-up launch: smem carve-out, caches), so that a disturbed timing does not decide the
-        // plan; n makes a timing span >= 0.2 ms, which for single-shot launches of ~20 us keeps
-        // event and clock jitter from deciding it.
+        // plan; n makes a timing span >= 0.1 ms (at most 8 launches), which for single-shot
+        // launches of ~20 us keeps event and clock jitter from deciding it while keeping the
+        // tuning of a new wave size short (serving tunes one per grid and wave size).
         auto timeMin = [&](auto launch) {
             AIO_CK(cudaEventRecord(e0, st));
             launch();
@@ -1172,7 +1173,7 @@ struct Context {
             AIO_CK(cudaEventSynchronize(e1));
             float t1 = 0.f;
             AIO_CK(cudaEventElapsedTime(&t1, e0, e1));
-            const int n = std::min(12, std::max(2, (int)std::ceil(0.2f / std::max(t1, 1e-3f))));
+            const int n = std::min(8, std::max(2, (int)std::ceil(0.1f / std::max(t1, 1e-3f))));
             float best2 = 1e30f;
             for (int rep = 0; rep < 3; rep++) {
                 AIO_CK(cudaEventRecord(e0, st));

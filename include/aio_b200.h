@@ -66,7 +66,8 @@ typedef struct {
     int leg1, leg2;      /* tomo / WEMVA legs (reference par leg1, leg2) */
     int sloth;           /* extended Born / tomo: slowness-squared perturbation */
     int wavefieldPrecision;  /* AIO_WFLD_* for the stored source wavefield */
-    int imageFp64;       /* 1: accumulate imaging conditions in FP64 on the GPU */
+    int imageFp64;       /* 1: accumulate imaging conditions in FP64 on the GPU; 0: in FP32, as the
+                            reference's imaging kernels do */
     int device;          /* CUDA device ordinal */
     long long memBudgetBytes; /* cap on device memory for shot buffers; 0 = 93% of free */
     int stepper;         /* AIO_STEPPER_*: how Born / nonlinear passes advance time */
