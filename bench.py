@@ -283,8 +283,8 @@ def run_ext(args, emit=True):
     rng = np.random.default_rng(4)
     shots = [Shot(a.src_pos, a.rec_pos, sg, (rng.standard_normal((len(a.rec_pos), w.nts)) * 1e-3).astype(np.float32))
              for a, sg in zip(w.shots, sigs)]
-    ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs, nExt=n_ext, image_fp64=True,
-                  wavefield=args.wavefield)
+    ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs, nExt=n_ext,
+                  image_fp64=getattr(args, "image", "fp32") == "fp64", wavefield=args.wavefield)
     ctx.born_ext_adjoint(shots)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -297,6 +297,7 @@ def run_ext(args, emit=True):
     peak, src = hbm_peak()
     out = {"impl": f"this engine, extended Born adjoint (blocked stepper, blocked lag imaging, "
                    f"{args.wavefield.upper()} stored W)", "wavefield": args.wavefield,
+           "image": getattr(args, "image", "fp32"),
            "metric": "Gpts/s, extended (time-lag) Born adjoint", "value": pts / t / 1e9, "unit": UNIT,
            "seconds": t, "shots": len(shots), "shots_per_s": len(shots) / t, "nExt": n_ext,
            "interior": [w.nz - 10, w.nx - 10], "nts": w.nts,
@@ -328,8 +329,8 @@ def run_tomo(args, emit=True):
     shots = [Shot(a.src_pos, a.rec_pos, sg, noise(a), noise(a)) for a, sg in zip(w.shots, sigs)]
     ext = np.ascontiguousarray(w.extra["ext"], np.float32)
     m = np.ascontiguousarray(w.model, np.float32)
-    ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs, nExt=w.nExt, image_fp64=True,
-                  stepper=args.stepper, wavefield=args.wavefield)
+    ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, v2, rs, nExt=w.nExt,
+                  image_fp64=getattr(args, "image", "fp32") == "fp64", stepper=args.stepper, wavefield=args.wavefield)
     # (name, propagation passes, full coarse-field sweeps per shot: the source wavefield written,
     # its d2/dt2 read and written, and every later write or read of a stored field; FP32)
     ops = [("tomo_forward", 5, 9, lambda: ctx.tomo_forward(m, ext, shots)),
@@ -352,9 +353,9 @@ def run_tomo(args, emit=True):
         tot_bytes += nbytes
     stepper = {"auto": "blocked stepper", "blocked": "blocked stepper", "fine": "per-fine-step stepper"}[args.stepper]
     peak, src = hbm_peak()
-    src = {"fp32": "FP32", "fp16": "FP16 + per-slice scale", "bf16": "BF16"}[args.wavefield]
-    out = {"impl": f"this engine, extended tomo + WEMVA ({stepper}, source field d2/dt2 in {src}, second field FP32)",
-           "wavefield": args.wavefield,
+    wsrc = {"fp32": "FP32", "fp16": "FP16 + per-slice scale", "bf16": "BF16"}[args.wavefield]
+    out = {"impl": f"this engine, extended tomo + WEMVA ({stepper}, source field d2/dt2 in {wsrc}, second field FP32)",
+           "wavefield": args.wavefield, "image": getattr(args, "image", "fp32"),
            "metric": "Gpts/s, extended tomo + WEMVA forward and adjoint", "value": tot_pts / tot_t / 1e9,
            "unit": UNIT, "seconds": tot_t, "ops": res, "shots": len(shots), "nExt": w.nExt,
            "interior": [w.nz - 10, w.nx - 10], "nts": w.nts,

@@ -80,19 +80,21 @@ def test_fp16_speculative_scale_overflow_falls_back(medium):
     assert ef < 1e-3 and ea < 1e-3
 
 
-@pytest.mark.parametrize("wavefield,tol", [("fp32", 1e-4), ("fp16", 5e-4), ("bf16", 1e-2)])
-def test_born_ext_error_vs_fp64(medium, wavefield, tol):
+@pytest.mark.parametrize("wavefield,tol,image_fp64", [("fp32", 1e-4, True), ("fp32", 1e-4, False),
+                                                      ("fp16", 5e-4, True), ("bf16", 1e-2, True)])
+def test_born_ext_error_vs_fp64(medium, wavefield, tol, image_fp64):
     """Extended (time-lag) Born forward and adjoint with the stored source wavefield in each
     precision (the lag imaging and the lag sources read it as stored), against the FP64 oracle:
     FP32 within 1e-4, FP16 with per-slice scales within 5e-4 (the extended image is spread over
     lags whose energy is small next to lag 0, so its relative error sits above the Born image's),
-    BF16 reported and bounded by 1e-2."""
+    BF16 reported and bounded by 1e-2. image_fp64 = False: the extended image accumulated in FP32,
+    as the reference accumulates it."""
     from acoustic_isotropic_operators_b200.batch import Context, Shot
     w, sigs, s, k = medium
     n_ext = 9
     s9 = orc.Scheme(nz=s.nz, nx=s.nx, nts=s.nts, dts=s.dts, sub=s.sub, dz=s.dz, dx=s.dx, minPad=s.minPad, nExt=n_ext)
     ctx = Context(w.nz, w.nx, w.nts, w.dts, w.sub, w.dz, w.dx, w.minPad, k["v2"], k["rs"], nExt=n_ext,
-                  image_fp64=True, wavefield=wavefield)
+                  image_fp64=image_fp64, wavefield=wavefield)
     try:
         prof = np.exp(-(np.arange(n_ext) - n_ext // 2) ** 2 / 8.0).astype(np.float32)
         m = np.ascontiguousarray(prof[:, None, None] * w.model[None], np.float32)
@@ -104,5 +106,6 @@ def test_born_ext_error_vs_fp64(medium, wavefield, tol):
     ef = max(rel_l2(d[i], orc.bornext_fwd(s9, v64, m, sigs[i], a.src_pos, a.rec_pos)) for i, a in enumerate(w.shots))
     ref = sum(orc.bornext_adj(s9, v64, d[i], sigs[i], a.src_pos, a.rec_pos) for i, a in enumerate(w.shots))
     ea = rel_l2(img, ref)
-    print(f"\n[{wavefield}] extended Born (nExt={n_ext}) forward rel err vs FP64 {ef:.2e}, adjoint {ea:.2e}")
+    print(f"\n[{wavefield}, FP{64 if image_fp64 else 32} image] extended Born (nExt={n_ext}) forward rel err vs "
+          f"FP64 {ef:.2e}, adjoint {ea:.2e}")
     assert ef < tol and ea < tol
