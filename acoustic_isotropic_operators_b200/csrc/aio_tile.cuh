@@ -83,7 +83,7 @@ struct KTArgs {
 // Per-thread staging slots (16 bytes each) filled by asynchronous copies: level-1 operands
 // of the next iteration (old level: slots 0-1; v^2: 2-3 when v2s) and the output operands of
 // the current iteration from slot kt_so(v2s) on (partial sum: +0..1, stored wavefield: +2..3,
-// FP64 image: +4..7; the scattered passes' sources: +0..3).
+// image: +4..7 in FP64, +4 and +6 in FP32; the scattered passes' sources: +0..3).
 __host__ __device__ constexpr int kt_so(bool v2s) { return v2s ? 4 : 2; }
 __host__ __device__ constexpr int kt_slots(int mode, bool v2s = true) {
     return kt_so(v2s) +
