@@ -662,7 +662,7 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, BASELINE shapes)",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, the workload's shapes)",
                 "config": dict(config_dict(args, w), plan=plan),
                 "roofline": {"bound": "hbm", "kernel": kernel_name(args, w),
                              "achieved": achieved, "peak": hbm_peak, "peak_source": peak_src, "unit": "GB/s",
